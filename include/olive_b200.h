@@ -1,0 +1,107 @@
+/*
+ * olive_b200 -- C ABI of the B200 frontier engine (libolive_b200.so).
+ *
+ * The reference (ACSAlab/olive) has no FFI: its boundary is the header-only
+ * C++ template class Oliver<VertexValue,EdgeValue,AccumValue> (oliver.h:46-249)
+ * driven by the apps BFS.cu, SSSP.cu and PageRank.cu.  This header is the flat
+ * C boundary a non-C++ caller binds (ctypes, cgo, JNI); each entry point names
+ * the reference code whose result it reproduces.  The source-compatible C++
+ * layer (include/olive/oliver.h) sits beside it for the reference apps.
+ *
+ * Conventions
+ *   - Every function returns 0 (OLV_OK) or a negative OLV_ERR_* code and never
+ *     aborts or throws.  olv_last_error() returns the message of the last
+ *     failure on the calling thread.
+ *   - Vertex ids and CSR offsets are uint32 (VertexId/EdgeId, common.h:55-59).
+ *   - Pointers the caller passes may be host or device memory; the library
+ *     inspects each with cudaPointerGetAttributes.  The caller owns them.  The
+ *     library owns everything reachable from an olv_graph until
+ *     olv_graph_destroy.
+ *   - A graph handle is bound to one CUDA stream (olv_set_stream) and must be
+ *     used by one host thread at a time.  Calls are stream-ordered; a call that
+ *     writes a host buffer returns after the data has landed.
+ */
+#ifndef OLIVE_B200_H
+#define OLIVE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OLV_OK            0
+#define OLV_ERR_ARG      -1   /* invalid argument (null pointer, id out of range, ...) */
+#define OLV_ERR_CUDA     -2   /* a CUDA runtime call failed                             */
+#define OLV_ERR_NOMEM    -3   /* device or host allocation failed                       */
+#define OLV_ERR_TIMEOUT  -4   /* a bounded device-side wait ran out                     */
+#define OLV_ERR_STATE    -5   /* call not valid in the handle's current state           */
+#define OLV_ERR_LIMIT    -6   /* size beyond a documented limit                          */
+
+/* weight_type for olv_graph_create */
+#define OLV_W_NONE 0
+#define OLV_W_U32  1
+#define OLV_W_F32  2
+
+/* dangling_mode for olv_pagerank */
+#define OLV_DANGLING_UNIFORM 0   /* redistribute dangling mass uniformly          */
+#define OLV_DANGLING_LEAK    1   /* drop it, as PageRank.cu:63-75 / testPageRank */
+
+typedef struct olv_graph olv_graph;
+
+typedef struct olv_stats {
+    uint32_t iterations;        /* BFS/SSSP supersteps, PageRank iterations            */
+    uint32_t pull_steps;        /* BFS levels run bottom-up                             */
+    uint64_t vertices_reached;  /* BFS/SSSP: vertices with a finite result              */
+    uint64_t edges_traversed;   /* sum of out-degrees of reached vertices (GTEPS basis)  */
+    uint64_t edges_relaxed;     /* SSSP: edges actually relaxed (>= edges_traversed)     */
+    double   residual;          /* PageRank: last L1 residual (FP64)                     */
+    double   device_ms;         /* device time of the call (CUDA events)                */
+} olv_stats;
+
+const char *olv_last_error(void);
+const char *olv_version(void);
+
+/* ---- graph ----------------------------------------------------------------
+ * Replaces Oliver::readGraph (oliver.h:190-202) + CsrGraph (csrGraph.h:55-84):
+ * uploads a CSR (rowptr[V+1], col[E], optional weights[E]) to the device and
+ * builds the reverse (CSC) graph on the device.  Rows need not be sorted.      */
+int olv_graph_create(const uint32_t *rowptr, const uint32_t *col, const void *weights,
+                     int weight_type, uint32_t V, uint64_t E, olv_graph **out);
+/* Device-side RMAT generator (no reference counterpart): ef*2^scale draws with
+ * (a,b,c,d) = (0.57,0.19,0.19,0.05), ids permuted by a seeded bijection,
+ * self-loops and duplicates removed, CSR sorted by (src,dst).  weight_type
+ * OLV_W_U32 adds weights uniform in [1,255] drawn from a stream indexed by
+ * CSR position (seed wseed).                                                   */
+int olv_graph_create_rmat(int scale, int edge_factor, uint64_t seed, int weight_type,
+                          uint64_t wseed, olv_graph **out);
+int olv_graph_destroy(olv_graph *g);
+int olv_graph_info(const olv_graph *g, uint32_t *V, uint64_t *E, int *weight_type);
+/* Copy the CSR back (any of the pointers may be NULL). */
+int olv_graph_copy_csr(const olv_graph *g, uint32_t *rowptr, uint32_t *col, void *weights);
+/* Replace the FP32 edge weights (CSR order) without rebuilding the graph.   */
+int olv_graph_set_weights_f32(olv_graph *g, const float *w);
+/* Bind the handle to a CUDA stream (a cudaStream_t; NULL = the handle's own). */
+int olv_set_stream(olv_graph *g, void *stream);
+/* Maximum out-degree vertex, ties to the smallest id. */
+int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
+
+/* ---- traversal --------------------------------------------------------------
+ * BFS levels: reproduces testBFS.cu:42-87 and BFS.cu:82-160 run to completion
+ * (int32 level, 0x7fffffff unreached).  Direction-optimising (push/pull).      */
+int olv_bfs(olv_graph *g, uint32_t src, int32_t *level_out, olv_stats *st);
+/* SSSP distances with non-negative uint32 weights: the frontier Bellman-Ford of
+ * SSSP.cu:106-174 (atomicMin relaxation) with near/far bucketing.  uint32
+ * distance, 0x7fffffff unreached.  Needs an OLV_W_U32 graph.                   */
+int olv_sssp(olv_graph *g, uint32_t src, uint32_t *dist_out, olv_stats *st);
+/* PageRank (PageRank.cu:89-147 / testPageRank.cu:41-115), FP32 ranks from a
+ * deterministic pull over the reverse graph, FP64 residual.  Runs max_it
+ * iterations or until the L1 residual < tol.                                  */
+int olv_pagerank(olv_graph *g, double alpha, int max_it, double tol, int dangling_mode,
+                 float *rank_out, olv_stats *st);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OLIVE_B200_H */

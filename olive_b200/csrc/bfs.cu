@@ -1,0 +1,283 @@
+// Direction-optimising BFS.
+//
+// Result contract: testBFS.cu:42-87 and BFS.cu:82-160 run to completion --
+// int32 level per vertex, 0x7fffffff when unreached, level[src] = 0.
+//
+// Reference path, per level (BFS.cu:124-148): edgeFilter over the queue
+// (oliver.h:56-83: host refill of V accumulators + H2D, edgeFilterKernel with
+// a plain-store "benign race", BFS.cu:52-55), then vertexFilter over all V
+// flags (oliver.h:92-113) and a blocking D2H of the queue size.
+//
+// Here each superstep is a fixed chain of kernels that decide on the device
+// what to do, so the whole traversal is one CUDA graph launch:
+//   k_bfs_begin      choose push or pull from the frontier's edge count
+//                    (Beamer's alpha/beta rule), reset the output queue
+//   k_advance_chunks push: claim unvisited neighbours with atomicCAS on the
+//   k_advance_pieces level array and append them to the next queue (the
+//                    claim fuses edgeFilter's reduce and vertexFilter's
+//                    cond/update into one step)
+//   k_bfs_pull       pull: every unvisited vertex scans its in-edges for a
+//                    parent at the current level and stops at the first one
+//   k_bfs_end        account edges, swap queues, stop when the queue is empty
+#include <stdio.h>
+
+#include "olv_advance.cuh"
+#include "olv_graphexec.cuh"
+#include "olv_internal.cuh"
+
+namespace olv {
+
+struct BfsPushOp {
+    static constexpr bool kHasFar = false;
+    const uint32_t *rowptr;
+    int32_t *level;
+    int next;
+    unsigned long long acc;
+    unsigned long long *m_next;
+
+    __device__ __forceinline__ void begin(TravCtl *c) {
+        level = static_cast<int32_t *>(c->vdata);
+        next = (int)c->level + 1;
+        acc = 0;
+        m_next = &c->m_next;
+    }
+    __device__ __forceinline__ uint32_t src_value(uint32_t) const { return 0; }
+    __device__ __forceinline__ int edge(uint32_t, uint32_t, uint32_t v) {
+        if (__ldcg(&level[v]) != kInf) return 0;
+        return atomicCAS(&level[v], kInf, next) == kInf ? 1 : 0;
+    }
+    __device__ __forceinline__ void on_push(bool p, uint32_t v) {
+        if (p) acc += __ldg(&rowptr[v + 1]) - __ldg(&rowptr[v]);
+    }
+    __device__ __forceinline__ void flush(unsigned long long) { warp_add64(acc, m_next); }
+};
+
+__global__ void k_fill_i32(int32_t *__restrict__ a, uint32_t n, int32_t x) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (reinterpret_cast<uintptr_t>(a) & 15) {   // caller buffer not 16-byte aligned
+        for (uint64_t i = tid; i < n; i += stride) a[i] = x;
+        return;
+    }
+    const uint64_t n4 = n / 4;
+    int4 *a4 = reinterpret_cast<int4 *>(a);
+    for (uint64_t i = tid; i < n4; i += stride) a4[i] = make_int4(x, x, x, x);
+    for (uint64_t i = n4 * 4 + tid; i < n; i += stride) a[i] = x;
+}
+
+__global__ void k_bfs_init(TravCtl *c, int32_t *level, uint32_t *q0, const uint32_t *rowptr,
+                           uint32_t src, unsigned long long E) {
+    TravCtl t = {};
+    t.qsize[0] = 1;
+    t.vdata = level;
+    const uint32_t d = rowptr[src + 1] - rowptr[src];
+    t.m_f = d;
+    t.m_unvisited = E - d;
+    *c = t;
+    level[src] = 0;
+    q0[0] = src;
+}
+
+__global__ void k_bfs_begin(TravCtl *c, uint32_t V, float alpha, float beta) {
+    if (c->done) return;
+    const uint32_t n = c->qsize[c->cur];
+    if (n == 0) {
+        c->done = 1;
+        return;
+    }
+    if (c->mode == 0) {
+        if ((double)c->m_f * alpha > (double)c->m_unvisited) c->mode = 1;
+    } else if ((double)n * beta < (double)V) {
+        c->mode = 0;
+    }
+    c->qsize[c->cur ^ 1] = 0;
+    c->npieces = 0;
+    c->m_next = 0;
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_bfs_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowidx,
+           const uint32_t *__restrict__ rowptr, uint32_t V, TravCtl *c, uint32_t *q0,
+           uint32_t *q1) {
+    if (c->done || c->mode != 1) return;
+    int32_t *level = static_cast<int32_t *>(c->vdata);
+    const int L = (int)c->level;
+    const uint32_t cur = c->cur;
+    uint32_t *qout = cur ? q0 : q1;
+    uint32_t *qsz = &c->qsize[cur ^ 1];
+    unsigned long long acc = 0;
+    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V;
+         base += (uint64_t)gridDim.x * kBlock) {
+        const uint32_t v = (uint32_t)base + threadIdx.x;
+        bool found = false;
+        if (v < V && level[v] == kInf) {
+            const uint32_t b = __ldg(&colptr[v]), e = __ldg(&colptr[v + 1]);
+            for (uint32_t i = b; i < e; i++)
+                if (level[__ldg(&rowidx[i])] == L) {
+                    found = true;
+                    break;
+                }
+            if (found) {
+                level[v] = L + 1;
+                acc += __ldg(&rowptr[v + 1]) - __ldg(&rowptr[v]);
+            }
+        }
+        warp_push(found, v, qout, qsz);
+    }
+    warp_add64(acc, &c->m_next);
+}
+
+__global__ void k_bfs_end(TravCtl *c, cudaGraphConditionalHandle h, int use_cond, uint32_t V) {
+    if (!c->done) {
+        c->edges_traversed += c->m_f;
+        c->reached += c->qsize[c->cur];
+        if (c->mode) c->pull_steps++;
+        c->m_unvisited -= (c->m_next < c->m_unvisited ? c->m_next : c->m_unvisited);
+        c->m_f = c->m_next;
+        c->cur ^= 1;
+        c->level++;
+        c->steps++;
+        if (c->qsize[c->cur] == 0) c->done = 1;
+        if (c->steps > V + 1) {   // cannot happen for a correct run; stop rather than spin
+            c->err = 1;
+            c->done = 1;
+        }
+    }
+    if (use_cond) cudaGraphSetConditional(h, c->done ? 0u : 1u);
+}
+
+// ------------------------------------------------------------------ host --
+int traversal_workspace(olv_graph *g, bool pieces) {
+    Workspace &w = g->ws;
+    const size_t V = g->V;
+    OLV_TRY(w.q0.ensure(V * 4 + 16));
+    OLV_TRY(w.q1.ensure(V * 4 + 16));
+    OLV_TRY(w.ctl.ensure(sizeof(TravCtl)));
+    if (pieces) {
+        const uint64_t np = g->E / g->tune.piece + g->E / g->tune.hub_degree + 16;
+        OLV_TRY(w.pieces.ensure(np * sizeof(uint2)));
+    }
+    if (g->persist_blocks == 0) {
+        int per_sm = 0;
+        OLV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, k_advance_chunks<BfsPushOp>, kBlock, 0));
+        if (per_sm < 1) per_sm = 1;
+        g->persist_blocks = per_sm * g->num_sms;
+    }
+    return OLV_OK;
+}
+
+static AdvanceArgs bfs_adv_args(olv_graph *g) {
+    AdvanceArgs a;
+    a.rowptr = g->rowptr.as<uint32_t>();
+    a.col = g->col.as<uint32_t>();
+    a.ctl = g->ws.ctl.as<TravCtl>();
+    a.q0 = g->ws.q0.as<uint32_t>();
+    a.q1 = g->ws.q1.as<uint32_t>();
+    a.far0 = a.far1 = nullptr;
+    a.pieces = g->ws.pieces.as<uint2>();
+    a.hub_degree = g->tune.hub_degree;
+    a.piece = g->tune.piece;
+    a.want_mode = 0;
+    return a;
+}
+
+// One superstep's kernel chain, either launched on a stream or added to a graph.
+template <class Sink>
+static int bfs_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle h, int use_cond) {
+    TravCtl *ctl = g->ws.ctl.as<TravCtl>();
+    uint32_t V = g->V;
+    float alpha = g->tune.alpha, beta = g->tune.beta;
+    AdvanceArgs a = bfs_adv_args(g);
+    BfsPushOp op = {};
+    op.rowptr = a.rowptr;
+    const uint32_t *colptr = g->colptr.as<uint32_t>();
+    const uint32_t *rowidx = g->rowidx.as<uint32_t>();
+    const uint32_t *rowptr = a.rowptr;
+    uint32_t *q0 = a.q0, *q1 = a.q1;
+    const int nb = g->persist_blocks;
+    void *a_begin[] = {&ctl, &V, &alpha, &beta};
+    OLV_TRY(sink((const void *)k_bfs_begin, dim3(1), dim3(1), a_begin));
+    void *a_adv[] = {&a, &op};
+    OLV_TRY(sink((const void *)k_advance_chunks<BfsPushOp>, dim3(nb), dim3(kBlock), a_adv));
+    OLV_TRY(sink((const void *)k_advance_pieces<BfsPushOp>, dim3(nb), dim3(kBlock), a_adv));
+    void *a_pull[] = {&colptr, &rowidx, &rowptr, &V, &ctl, &q0, &q1};
+    OLV_TRY(sink((const void *)k_bfs_pull, dim3(nb), dim3(kBlock), a_pull));
+    void *a_end[] = {&ctl, &h, &use_cond, &V};
+    OLV_TRY(sink((const void *)k_bfs_end, dim3(1), dim3(1), a_end));
+    return OLV_OK;
+}
+
+static int bfs_graph(olv_graph *g) {
+    if (g->bfs_graph && g->bfs_graph->ready) return OLV_OK;
+    if (!g->bfs_graph) g->bfs_graph = new WhileGraph();
+    WhileGraph &wg = *g->bfs_graph;
+    OLV_TRY(wg.begin());
+    auto sink = [&](const void *f, dim3 gr, dim3 bl, void **args) { return wg.add(f, gr, bl, args); };
+    OLV_TRY(bfs_superstep(g, sink, wg.handle, 1));
+    return wg.finish();
+}
+
+int run_bfs_device(olv_graph *g, uint32_t src, int32_t *level_dev) {
+    cudaStream_t s = g->stream;
+    TravCtl *ctl = g->ws.ctl.as<TravCtl>();
+    const int fill_blocks = g->num_sms * 8;
+    k_fill_i32<<<fill_blocks, kBlock, 0, s>>>(level_dev, g->V, kInf);
+    k_bfs_init<<<1, 1, 0, s>>>(ctl, level_dev, g->ws.q0.as<uint32_t>(), g->rowptr.as<uint32_t>(),
+                               src, (unsigned long long)g->E);
+    OLV_CUDA(cudaGetLastError());
+    if (g->tune.use_graphs) {
+        int r = bfs_graph(g);
+        if (r == OLV_OK) return g->bfs_graph->launch(s);
+        g->tune.use_graphs = 0;   // conditional graphs unavailable: host loop below
+    }
+    auto launch = [&](const void *f, dim3 gr, dim3 bl, void **args) {
+        OLV_CUDA(cudaLaunchKernel(f, gr, bl, args, 0, s));
+        return OLV_OK;
+    };
+    for (;;) {
+        for (int i = 0; i < g->tune.levels_per_sync; i++) OLV_TRY(bfs_superstep(g, launch, 0, 0));
+        OLV_CUDA(cudaMemcpyAsync(g->host_ctl, ctl, sizeof(TravCtl), cudaMemcpyDeviceToHost, s));
+        OLV_CUDA(cudaStreamSynchronize(s));
+        if (g->host_ctl->done) break;
+    }
+    return OLV_OK;
+}
+
+}  // namespace olv
+
+using namespace olv;
+
+extern "C" int olv_bfs(olv_graph *g, uint32_t src, int32_t *level_out, olv_stats *st) {
+    OLV_CHECK_ARG(g && level_out, "olv_bfs: null pointer");
+    OLV_CHECK_ARG(src < g->V, "olv_bfs: source %u out of range (V=%u)", src, g->V);
+    OLV_TRY(traversal_workspace(g, true));
+    const bool dev_out = is_device_ptr(level_out);
+    if (!dev_out) OLV_TRY(g->ws.level.ensure((size_t)g->V * 4 + 16));
+    int32_t *level = dev_out ? level_out : g->ws.level.as<int32_t>();
+    cudaStream_t s = g->stream;
+    OLV_CUDA(cudaEventRecord(g->ev0, s));
+    OLV_TRY(run_bfs_device(g, src, level));
+    OLV_CUDA(cudaEventRecord(g->ev1, s));
+    OLV_CUDA(cudaMemcpyAsync(g->host_ctl, g->ws.ctl.p, sizeof(TravCtl), cudaMemcpyDeviceToHost, s));
+    if (!dev_out)
+        OLV_CUDA(cudaMemcpyAsync(level_out, level, (size_t)g->V * 4, cudaMemcpyDeviceToHost, s));
+    OLV_CUDA(cudaStreamSynchronize(s));
+    const TravCtl &h = *g->host_ctl;
+    if (h.err) {
+        set_error("olv_bfs: device-side check failed (code %u)", h.err);
+        return OLV_ERR_STATE;
+    }
+    if (st) {
+        float ms = 0;
+        OLV_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+        st->iterations = h.steps;
+        st->pull_steps = h.pull_steps;
+        st->vertices_reached = h.reached;
+        st->edges_traversed = h.edges_traversed;
+        st->edges_relaxed = h.edges_traversed;
+        st->residual = 0;
+        st->device_ms = ms;
+    }
+    return OLV_OK;
+}

@@ -1,0 +1,195 @@
+// Load-balanced frontier advance for sm_100a.
+//
+// Replaces edgeFilterKernel (oliverKernel.h:45-83), which gave every queued
+// source a fixed group of 1..32 threads (hubs serialised, lanes idle on short
+// rows).  Here a CTA takes a chunk of kBlock queued sources, scans their
+// out-degrees in shared memory and lets all kBlock threads walk the chunk's
+// edges in order, so column indices are read as contiguous runs.  Rows longer
+// than Tuning::hub_degree are cut into pieces of Tuning::piece edges that a
+// second kernel spreads over all warps of the GPU.  Destinations are appended
+// to the output queue with one atomic per warp.
+//
+// An Op supplies the per-edge work:
+//   void begin(TravCtl *c)                          load per-superstep values
+//   uint32_t src_value(uint32_t u)                  value carried from the source
+//   int edge(uint32_t sv, uint32_t e, uint32_t v)   0: nothing, 1: push v to the
+//                                                   output queue, 2: push to the
+//                                                   secondary (far) queue
+//   void on_push(bool pushed, uint32_t v)           after each warp-wide push
+//   void flush(unsigned long long relaxed)          once per thread at the end
+#pragma once
+#include "olv_internal.cuh"
+
+namespace olv {
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
+
+// Append v (where p) to q with one atomic per warp.  All 32 lanes must call.
+__device__ __forceinline__ void warp_push(bool p, uint32_t v, uint32_t *__restrict__ q,
+                                          uint32_t *__restrict__ qsize) {
+    const unsigned m = __ballot_sync(0xffffffffu, p);
+    if (!m) return;
+    const uint32_t lane = lane_id();
+    const uint32_t leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(qsize, (uint32_t)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (p) q[base + __popc(m & ((1u << lane) - 1u))] = v;
+}
+
+// Warp sum of a 64-bit value added to *dst by lane 0.  All lanes must call.
+__device__ __forceinline__ void warp_add64(unsigned long long x, unsigned long long *dst) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane_id() == 0 && x) atomicAdd(dst, x);
+}
+
+// Exclusive scan over the CTA (blockDim.x == kBlock).  s_warp holds 33 words.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *total,
+                                                         uint32_t *s_warp) {
+    const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
+    uint32_t incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += t;
+    }
+    if (lane == 31) s_warp[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        constexpr int NW = kBlock / 32;
+        uint32_t t = lane < NW ? s_warp[lane] : 0;
+        uint32_t ti = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, ti, o);
+            if (lane >= (uint32_t)o) ti += y;
+        }
+        if (lane < NW) s_warp[lane] = ti - t;
+        if (lane == NW - 1) s_warp[32] = ti;
+    }
+    __syncthreads();
+    const uint32_t r = s_warp[wid] + incl - x;
+    *total = s_warp[32];
+    __syncthreads();
+    return r;
+}
+
+struct AdvanceArgs {
+    const uint32_t *rowptr;
+    const uint32_t *col;
+    TravCtl *ctl;
+    uint32_t *q0, *q1;          // queue buffers; ctl->cur selects the input
+    uint32_t *far0, *far1;      // secondary queue buffers; ctl->far_cur selects
+    uint2 *pieces;              // (row, piece index) of split hub rows
+    uint32_t hub_degree;
+    uint32_t piece;
+    uint32_t want_mode;         // kernel runs only when ctl->mode == want_mode
+};
+
+// Per-superstep chunk expansion over the input queue.
+template <class Op>
+__global__ void __launch_bounds__(kBlock) k_advance_chunks(AdvanceArgs a, Op op) {
+    TravCtl *c = a.ctl;
+    if (c->done || c->mode != a.want_mode) return;
+    op.begin(c);
+    const uint32_t cur = c->cur;
+    const uint32_t n = c->qsize[cur];
+    const uint32_t *__restrict__ qin = cur ? a.q1 : a.q0;
+    uint32_t *__restrict__ qout = cur ? a.q0 : a.q1;
+    uint32_t *qout_size = &c->qsize[cur ^ 1];
+    uint32_t *__restrict__ far = c->far_cur ? a.far1 : a.far0;
+    uint32_t *far_size = &c->far_size[c->far_cur];
+
+    __shared__ uint32_t s_beg[kBlock];
+    __shared__ uint32_t s_off[kBlock];
+    __shared__ uint32_t s_val[kBlock];
+    __shared__ uint32_t s_warp[33];
+
+    unsigned long long relaxed = 0;
+    for (uint32_t chunk = blockIdx.x; (uint64_t)chunk * kBlock < n; chunk += gridDim.x) {
+        const uint32_t i = chunk * kBlock + threadIdx.x;
+        uint32_t beg = 0, deg = 0, sv = 0;
+        if (i < n) {
+            const uint32_t u = qin[i];
+            beg = __ldg(&a.rowptr[u]);
+            deg = __ldg(&a.rowptr[u + 1]) - beg;
+            if (deg > a.hub_degree) {
+                const uint32_t np = (deg + a.piece - 1) / a.piece;
+                const uint32_t b = atomicAdd(&c->npieces, np);
+                for (uint32_t p = 0; p < np; p++) a.pieces[b + p] = make_uint2(u, p);
+                relaxed += deg;
+                deg = 0;
+            } else {
+                sv = op.src_value(u);
+            }
+        }
+        relaxed += deg;
+        uint32_t total;
+        const uint32_t off = block_exclusive_scan(deg, &total, s_warp);
+        s_beg[threadIdx.x] = beg;
+        s_off[threadIdx.x] = off;
+        s_val[threadIdx.x] = sv;
+        __syncthreads();
+        for (uint32_t base = 0; base < total; base += kBlock) {
+            const uint32_t k = base + threadIdx.x;
+            int act = 0;
+            uint32_t v = 0;
+            if (k < total) {
+                uint32_t lo = 0;
+#pragma unroll
+                for (uint32_t step = kBlock / 2; step > 0; step >>= 1)
+                    if (s_off[lo + step] <= k) lo += step;
+                const uint32_t e = s_beg[lo] + (k - s_off[lo]);
+                v = __ldg(&a.col[e]);
+                act = op.edge(s_val[lo], e, v);
+            }
+            warp_push(act == 1, v, qout, qout_size);
+            if (Op::kHasFar) warp_push(act == 2, v, far, far_size);
+            op.on_push(act == 1, v);
+        }
+        __syncthreads();
+    }
+    op.flush(relaxed);
+}
+
+// Hub pieces: one warp per piece of up to a.piece edges.
+template <class Op>
+__global__ void __launch_bounds__(kBlock) k_advance_pieces(AdvanceArgs a, Op op) {
+    TravCtl *c = a.ctl;
+    if (c->done || c->mode != a.want_mode) return;
+    const uint32_t np = c->npieces;
+    if (np == 0) return;
+    op.begin(c);
+    const uint32_t cur = c->cur;
+    uint32_t *__restrict__ qout = cur ? a.q0 : a.q1;
+    uint32_t *qout_size = &c->qsize[cur ^ 1];
+    uint32_t *__restrict__ far = c->far_cur ? a.far1 : a.far0;
+    uint32_t *far_size = &c->far_size[c->far_cur];
+    const uint32_t lane = lane_id();
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t p = warp; p < np; p += nwarps) {
+        const uint2 pc = a.pieces[p];
+        const uint32_t u = pc.x;
+        const uint32_t rb = __ldg(&a.rowptr[u]), re = __ldg(&a.rowptr[u + 1]);
+        const uint32_t b = rb + pc.y * a.piece;
+        const uint32_t e_end = min(re, b + a.piece);
+        const uint32_t sv = op.src_value(u);
+        for (uint32_t base = b; base < e_end; base += 32) {
+            const uint32_t e = base + lane;
+            int act = 0;
+            uint32_t v = 0;
+            if (e < e_end) {
+                v = __ldg(&a.col[e]);
+                act = op.edge(sv, e, v);
+            }
+            warp_push(act == 1, v, qout, qout_size);
+            if (Op::kHasFar) warp_push(act == 2, v, far, far_size);
+            op.on_push(act == 1, v);
+        }
+    }
+    op.flush(0);
+}
+
+}  // namespace olv

@@ -1,0 +1,126 @@
+// Internal declarations shared by the translation units of libolive_b200.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "olive_b200.h"
+
+namespace olv {
+
+constexpr int32_t kInf = 0x7fffffff;     // unreached level / distance (BFS.cu:101, SSSP.cu:123)
+constexpr int kBlock = 256;              // threads per CTA for the streaming kernels
+
+// ---------------------------------------------------------------- errors --
+void set_error(const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *what, const char *file, int line);
+
+#define OLV_CUDA(call)                                                          \
+    do {                                                                        \
+        cudaError_t _e = (call);                                                \
+        if (_e != cudaSuccess) return ::olv::cuda_fail(_e, #call, __FILE__, __LINE__); \
+    } while (0)
+
+#define OLV_CHECK_ARG(cond, ...)                                                \
+    do {                                                                        \
+        if (!(cond)) { ::olv::set_error(__VA_ARGS__); return OLV_ERR_ARG; }     \
+    } while (0)
+
+#define OLV_TRY(call)                                                           \
+    do { int _r = (call); if (_r != OLV_OK) return _r; } while (0)
+
+// -------------------------------------------------------- device buffer --
+// A plain owned device allocation (no host mirror: the reference's GRD<T>,
+// grd.h:43-170, kept a host copy and synchronised it every superstep).
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t n);     // grow to at least n bytes (contents not kept)
+    void release();
+    template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+// Where a caller's pointer lives.
+bool is_device_ptr(const void *p);
+
+// ------------------------------------------------------------ control --
+// Device-resident control block of one BFS / SSSP run.  Kernels read and
+// update it, so a run needs no host round trip per superstep.
+struct TravCtl {
+    uint32_t qsize[2];          // entries in the two queue buffers
+    uint32_t cur;               // input queue buffer of this superstep
+    uint32_t level;             // BFS level of the input frontier
+    uint32_t mode;              // 0 = push (top-down), 1 = pull (bottom-up)
+    uint32_t done;
+    uint32_t npieces;           // hub row pieces queued this superstep
+    uint32_t steps;             // supersteps executed
+    uint32_t pull_steps;
+    uint32_t far_size[2];       // SSSP far pile buffers
+    uint32_t far_cur;
+    uint32_t threshold;         // SSSP near/far split distance
+    uint32_t delta;
+    uint32_t err;               // nonzero: a device-side check failed
+    uint32_t err_info;
+    uint32_t epoch;             // SSSP far-pile generation
+    uint32_t far_min;           // SSSP smallest distance kept in the far pile
+    uint32_t split_lo;          // SSSP: lower edge of the bucket being split
+    void *vdata;                // per-vertex result array of the run (level / dist)
+    unsigned long long m_f;         // out-edges of the input frontier
+    unsigned long long m_next;      // out-edges of vertices discovered this superstep
+    unsigned long long m_unvisited; // out-edges of vertices not yet reached
+    unsigned long long edges_traversed;
+    unsigned long long edges_relaxed;
+    unsigned long long reached;
+};
+
+// Tunables (olv_autotune writes them; defaults are set at graph creation).
+struct Tuning {
+    uint32_t hub_degree = 1024;   // rows longer than this are split into pieces
+    uint32_t piece = 1024;        // edges per piece
+    float alpha = 14.0f;          // push -> pull when m_f > m_unvisited / alpha
+    float beta = 24.0f;           // pull -> push when n_f < V / beta
+    uint32_t sssp_delta = 0;      // 0 = derived from the weights
+    int levels_per_sync = 4;      // host loop: supersteps enqueued per check
+    int use_graphs = 1;           // run supersteps inside a CUDA graph
+};
+
+struct Workspace {
+    DevBuf level, q0, q1, pieces, ctl, mark, far0, far1, tmp, partials;
+    void release() {
+        level.release(); q0.release(); q1.release(); pieces.release(); ctl.release();
+        mark.release(); far0.release(); far1.release(); tmp.release(); partials.release();
+    }
+};
+
+}  // namespace olv
+
+namespace olv { struct WhileGraph; }
+
+struct olv_graph {
+    int device = 0;
+    int num_sms = 148;
+    uint32_t V = 0;
+    uint64_t E = 0;
+    int weight_type = OLV_W_NONE;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    // CSR (out-edges) and CSC (in-edges), device resident
+    olv::DevBuf rowptr, col, w, colptr, rowidx, csc_w, csc_eid;
+    // per-vertex derived data
+    olv::DevBuf outdeg_f;        // FP32 out-degree (PageRank)
+    olv::Workspace ws;
+    olv::Tuning tune;
+    olv::TravCtl *host_ctl = nullptr;   // pinned mirror of the control block
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    uint32_t max_out_degree = 0;
+    uint32_t max_in_degree = 0;
+    int persist_blocks = 0;              // resident CTAs of kBlock threads (all SMs)
+    olv::WhileGraph *bfs_graph = nullptr;
+    olv::WhileGraph *sssp_graph = nullptr;
+    void *pr_state = nullptr;            // PageRank plan + graph (pagerank.cu)
+};
+
+namespace olv {
+void release_pr_state(olv_graph *g);
+}

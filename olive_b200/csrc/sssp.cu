@@ -1,0 +1,310 @@
+// Single-source shortest paths with non-negative uint32 weights.
+//
+// Result contract: the frontier Bellman-Ford of SSSP.cu:106-174 run to
+// convergence -- gather = dist[u] + w (SSSP.cu:54-57), reduce = atomicMin
+// (SSSP.cu:60-63), a vertex re-enters the frontier when its distance drops
+// (cond/update, SSSP.cu:66-76).  Distances are unique, so the result equals
+// serial Dijkstra bit for bit; 0x7fffffff marks unreached vertices.
+//
+// B200 formulation: the same atomicMin relaxation, ordered by a near/far split
+// (a two-bucket delta-stepping) so that most vertices are relaxed once.  The
+// near queue holds vertices whose tentative distance is below `threshold`; an
+// improvement at or above it goes to the far pile (deduplicated per pile
+// generation).  When the near queue drains, one split pass raises the
+// threshold by delta and moves the far vertices under it to the near queue.
+// Supersteps (relax or split) run as one CUDA graph, as for BFS.
+#include "olv_advance.cuh"
+#include "olv_graphexec.cuh"
+#include "olv_internal.cuh"
+
+namespace olv {
+
+int traversal_workspace(olv_graph *g, bool pieces);
+__global__ void k_fill_i32(int32_t *__restrict__ a, uint32_t n, int32_t x);
+
+constexpr uint32_t kModeRelax = 0;
+constexpr uint32_t kModeSplit = 2;
+
+struct SsspOp {
+    static constexpr bool kHasFar = true;
+    const uint32_t *w;
+    uint32_t *mark;       // stamp of the superstep that last queued v as near
+    uint32_t *farmark;    // far-pile generation that holds v
+    uint32_t *dist;
+    uint32_t stamp, epoch, threshold, fmin;
+    unsigned long long *relaxed_ctr;
+    uint32_t *far_min;
+
+    __device__ __forceinline__ void begin(TravCtl *c) {
+        dist = static_cast<uint32_t *>(c->vdata);
+        stamp = c->steps + 1;
+        epoch = c->epoch;
+        threshold = c->threshold;
+        relaxed_ctr = &c->edges_relaxed;
+        far_min = &c->far_min;
+        fmin = 0xffffffffu;
+    }
+    __device__ __forceinline__ uint32_t src_value(uint32_t u) const { return __ldcg(&dist[u]); }
+    __device__ __forceinline__ int edge(uint32_t du, uint32_t e, uint32_t v) {
+        uint32_t nd = du + __ldg(&w[e]);
+        if (nd < du || nd > (uint32_t)kInf) nd = (uint32_t)kInf;   // saturate
+        if (nd >= __ldcg(&dist[v])) return 0;
+        const uint32_t old = atomicMin(&dist[v], nd);
+        if (nd >= old) return 0;
+        if (nd < threshold) return atomicExch(&mark[v], stamp) != stamp ? 1 : 0;
+        fmin = nd < fmin ? nd : fmin;
+        return atomicExch(&farmark[v], epoch) != epoch ? 2 : 0;
+    }
+    __device__ __forceinline__ void on_push(bool, uint32_t) {}
+    __device__ __forceinline__ void flush(unsigned long long relaxed) {
+        warp_add64(relaxed, relaxed_ctr);
+        const uint32_t m = __reduce_min_sync(0xffffffffu, fmin);
+        if (lane_id() == 0 && m != 0xffffffffu) atomicMin(far_min, m);
+    }
+};
+
+__global__ void k_sssp_init(TravCtl *c, uint32_t *dist, uint32_t *q0, uint32_t src,
+                            uint32_t delta) {
+    TravCtl t = {};
+    t.qsize[0] = 1;
+    t.vdata = dist;
+    t.threshold = delta;
+    t.delta = delta;
+    t.epoch = 1;
+    t.far_min = 0xffffffffu;
+    *c = t;
+    dist[src] = 0;
+    q0[0] = src;
+}
+
+__global__ void k_sssp_begin(TravCtl *c) {
+    if (c->done) return;
+    if (c->qsize[c->cur] > 0) {
+        c->mode = kModeRelax;
+        c->qsize[c->cur ^ 1] = 0;
+        c->npieces = 0;
+        return;
+    }
+    if (c->far_size[c->far_cur] == 0) {
+        c->done = 1;
+        return;
+    }
+    // near queue drained: next bucket starts at max(threshold, smallest far distance)
+    c->mode = kModeSplit;
+    c->split_lo = c->threshold;   // far entries below it were settled already
+    uint32_t lo = c->threshold > c->far_min ? c->threshold : c->far_min;
+    uint64_t t = (uint64_t)lo + c->delta;
+    c->threshold = t > (uint64_t)kInf ? (uint32_t)kInf : (uint32_t)t;
+    c->far_size[c->far_cur ^ 1] = 0;
+    c->far_min = 0xffffffffu;
+}
+
+// Split the far pile: stale entries (distance below the old threshold) are
+// dropped, entries under the new threshold become the near queue, the rest
+// move to the other far buffer under the next generation.
+__global__ void __launch_bounds__(kBlock)
+k_sssp_split(TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0, uint32_t *far1,
+             uint32_t *farmark) {
+    if (c->done || c->mode != kModeSplit) return;
+    const uint32_t *dist = static_cast<const uint32_t *>(c->vdata);
+    const uint32_t fc = c->far_cur;
+    const uint32_t n = c->far_size[fc];
+    const uint32_t *fin = fc ? far1 : far0;
+    uint32_t *fout = fc ? far0 : far1;
+    uint32_t *fout_size = &c->far_size[fc ^ 1];
+    uint32_t *qn = c->cur ? q1 : q0;
+    uint32_t *qn_size = &c->qsize[c->cur];
+    const uint32_t lo = c->split_lo, hi = c->threshold, next_epoch = c->epoch + 1;
+    uint32_t fmin = 0xffffffffu;
+    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < n;
+         base += (uint64_t)gridDim.x * kBlock) {
+        const uint64_t i = base + threadIdx.x;
+        bool to_near = false, keep = false;
+        uint32_t v = 0;
+        if (i < n) {
+            v = fin[i];
+            const uint32_t d = __ldcg(&dist[v]);
+            if (d >= lo) {
+                if (d < hi) {
+                    to_near = true;
+                } else {
+                    keep = true;
+                    farmark[v] = next_epoch;
+                    fmin = d < fmin ? d : fmin;
+                }
+            }
+        }
+        warp_push(to_near, v, qn, qn_size);
+        warp_push(keep, v, fout, fout_size);
+    }
+    const uint32_t m = __reduce_min_sync(0xffffffffu, fmin);
+    if (lane_id() == 0 && m != 0xffffffffu) atomicMin(&c->far_min, m);
+}
+
+__global__ void k_sssp_end(TravCtl *c, cudaGraphConditionalHandle h, int use_cond,
+                           uint32_t max_steps) {
+    if (!c->done) {
+        if (c->mode == kModeRelax) {
+            c->cur ^= 1;
+        } else {
+            c->far_cur ^= 1;
+            c->epoch++;
+        }
+        c->steps++;
+        if (c->qsize[c->cur] == 0 && c->far_size[c->far_cur] == 0) c->done = 1;
+        if (c->steps > max_steps) {
+            c->err = 2;
+            c->done = 1;
+        }
+    }
+    if (use_cond) cudaGraphSetConditional(h, c->done ? 0u : 1u);
+}
+
+// Sum of out-degrees and count of reached vertices (the GTEPS basis).
+__global__ void k_reached_edges(const uint32_t *__restrict__ rowptr,
+                                const uint32_t *__restrict__ dist, uint32_t V,
+                                unsigned long long *out /*[2]*/) {
+    unsigned long long e = 0, n = 0;
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+         v += (uint64_t)gridDim.x * blockDim.x)
+        if (dist[v] != (uint32_t)kInf) {
+            e += rowptr[v + 1] - rowptr[v];
+            n++;
+        }
+    warp_add64(e, &out[0]);
+    warp_add64(n, &out[1]);
+}
+
+// ------------------------------------------------------------------ host --
+static uint32_t sssp_delta(olv_graph *g) {
+    if (g->tune.sssp_delta) return g->tune.sssp_delta;
+    return 256;
+}
+
+template <class Sink>
+static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle h,
+                          int use_cond) {
+    Workspace &ws = g->ws;
+    TravCtl *ctl = ws.ctl.as<TravCtl>();
+    AdvanceArgs a;
+    a.rowptr = g->rowptr.as<uint32_t>();
+    a.col = g->col.as<uint32_t>();
+    a.ctl = ctl;
+    a.q0 = ws.q0.as<uint32_t>();
+    a.q1 = ws.q1.as<uint32_t>();
+    a.far0 = ws.far0.as<uint32_t>();
+    a.far1 = ws.far1.as<uint32_t>();
+    a.pieces = ws.pieces.as<uint2>();
+    a.hub_degree = g->tune.hub_degree;
+    a.piece = g->tune.piece;
+    a.want_mode = kModeRelax;
+    SsspOp op = {};
+    op.w = g->w.as<uint32_t>();
+    op.mark = ws.mark.as<uint32_t>();
+    op.farmark = ws.mark.as<uint32_t>() + g->V;
+    uint32_t *q0 = a.q0, *q1 = a.q1, *far0 = a.far0, *far1 = a.far1, *farmark = op.farmark;
+    // a correct run needs far fewer supersteps; the bound only stops a runaway loop
+    uint32_t max_steps = (uint32_t)(3ULL * g->V + 1000 > 0xfffffff0ULL ? 0xfffffff0ULL
+                                                                    : 3ULL * g->V + 1000);
+    const int nb = g->persist_blocks;
+    void *a_begin[] = {&ctl};
+    OLV_TRY(sink((const void *)k_sssp_begin, dim3(1), dim3(1), a_begin));
+    void *a_adv[] = {&a, &op};
+    OLV_TRY(sink((const void *)k_advance_chunks<SsspOp>, dim3(nb), dim3(kBlock), a_adv));
+    OLV_TRY(sink((const void *)k_advance_pieces<SsspOp>, dim3(nb), dim3(kBlock), a_adv));
+    void *a_split[] = {&ctl, &q0, &q1, &far0, &far1, &farmark};
+    OLV_TRY(sink((const void *)k_sssp_split, dim3(nb), dim3(kBlock), a_split));
+    void *a_end[] = {&ctl, &h, &use_cond, &max_steps};
+    OLV_TRY(sink((const void *)k_sssp_end, dim3(1), dim3(1), a_end));
+    return OLV_OK;
+}
+
+static int sssp_graph(olv_graph *g) {
+    if (g->sssp_graph && g->sssp_graph->ready) return OLV_OK;
+    if (!g->sssp_graph) g->sssp_graph = new WhileGraph();
+    WhileGraph &wg = *g->sssp_graph;
+    OLV_TRY(wg.begin());
+    auto sink = [&](const void *f, dim3 gr, dim3 bl, void **args) { return wg.add(f, gr, bl, args); };
+    OLV_TRY(sssp_superstep(g, sink, wg.handle, 1));
+    return wg.finish();
+}
+
+int sssp_workspace(olv_graph *g) {
+    OLV_TRY(traversal_workspace(g, true));
+    const size_t V = g->V;
+    OLV_TRY(g->ws.far0.ensure(V * 4 + 16));
+    OLV_TRY(g->ws.far1.ensure(V * 4 + 16));
+    OLV_TRY(g->ws.mark.ensure(V * 8 + 16));
+    return OLV_OK;
+}
+
+int run_sssp_device(olv_graph *g, uint32_t src, uint32_t *dist_dev) {
+    cudaStream_t s = g->stream;
+    TravCtl *ctl = g->ws.ctl.as<TravCtl>();
+    OLV_CUDA(cudaMemsetAsync(g->ws.mark.p, 0, (size_t)g->V * 8, s));
+    k_fill_i32<<<g->num_sms * 8, kBlock, 0, s>>>((int32_t *)dist_dev, g->V, kInf);
+    k_sssp_init<<<1, 1, 0, s>>>(ctl, dist_dev, g->ws.q0.as<uint32_t>(), src, sssp_delta(g));
+    OLV_CUDA(cudaGetLastError());
+    if (g->tune.use_graphs) {
+        if (sssp_graph(g) == OLV_OK) return g->sssp_graph->launch(s);
+        g->tune.use_graphs = 0;
+    }
+    auto launch = [&](const void *f, dim3 gr, dim3 bl, void **args) {
+        OLV_CUDA(cudaLaunchKernel(f, gr, bl, args, 0, s));
+        return OLV_OK;
+    };
+    for (;;) {
+        for (int i = 0; i < g->tune.levels_per_sync; i++) OLV_TRY(sssp_superstep(g, launch, 0, 0));
+        OLV_CUDA(cudaMemcpyAsync(g->host_ctl, ctl, sizeof(TravCtl), cudaMemcpyDeviceToHost, s));
+        OLV_CUDA(cudaStreamSynchronize(s));
+        if (g->host_ctl->done) break;
+    }
+    return OLV_OK;
+}
+
+}  // namespace olv
+
+using namespace olv;
+
+extern "C" int olv_sssp(olv_graph *g, uint32_t src, uint32_t *dist_out, olv_stats *st) {
+    OLV_CHECK_ARG(g && dist_out, "olv_sssp: null pointer");
+    OLV_CHECK_ARG(src < g->V, "olv_sssp: source %u out of range (V=%u)", src, g->V);
+    OLV_CHECK_ARG(g->weight_type == OLV_W_U32, "olv_sssp: graph has no uint32 weights");
+    OLV_TRY(sssp_workspace(g));
+    const bool dev_out = is_device_ptr(dist_out);
+    if (!dev_out) OLV_TRY(g->ws.level.ensure((size_t)g->V * 4 + 16));
+    uint32_t *dist = dev_out ? dist_out : g->ws.level.as<uint32_t>();
+    cudaStream_t s = g->stream;
+    OLV_CUDA(cudaEventRecord(g->ev0, s));
+    OLV_TRY(run_sssp_device(g, src, dist));
+    OLV_CUDA(cudaEventRecord(g->ev1, s));
+    OLV_CUDA(cudaMemcpyAsync(g->host_ctl, g->ws.ctl.p, sizeof(TravCtl), cudaMemcpyDeviceToHost, s));
+    unsigned long long red[2] = {0, 0};
+    if (st) {
+        OLV_TRY(g->ws.tmp.ensure(16));
+        OLV_CUDA(cudaMemsetAsync(g->ws.tmp.p, 0, 16, s));
+        k_reached_edges<<<g->num_sms * 4, kBlock, 0, s>>>(g->rowptr.as<uint32_t>(), dist, g->V,
+                                                         g->ws.tmp.as<unsigned long long>());
+        OLV_CUDA(cudaMemcpyAsync(red, g->ws.tmp.p, 16, cudaMemcpyDeviceToHost, s));
+    }
+    if (!dev_out)
+        OLV_CUDA(cudaMemcpyAsync(dist_out, dist, (size_t)g->V * 4, cudaMemcpyDeviceToHost, s));
+    OLV_CUDA(cudaStreamSynchronize(s));
+    const TravCtl &h = *g->host_ctl;
+    if (h.err) {
+        set_error("olv_sssp: device-side check failed (code %u)", h.err);
+        return OLV_ERR_STATE;
+    }
+    if (st) {
+        float ms = 0;
+        OLV_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+        st->iterations = h.steps;
+        st->pull_steps = 0;
+        st->vertices_reached = red[1];
+        st->edges_traversed = red[0];
+        st->edges_relaxed = h.edges_relaxed;
+        st->residual = 0;
+        st->device_ms = ms;
+    }
+    return OLV_OK;
+}

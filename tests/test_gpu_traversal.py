@@ -1,0 +1,215 @@
+"""GPU parity tests: BFS, SSSP and PageRank through the C ABI against the
+reference checkers' golden outputs and the CPU oracle."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+FIXTURES = sorted(glob.glob(os.path.join(GOLDEN, "fixture_*.npz")))
+INF = oracle.INF
+
+
+@pytest.fixture(scope="module")
+def ob():
+    import torch
+    assert torch.cuda.is_available()
+    import olive_b200
+    return olive_b200
+
+
+def _fid(p):
+    return os.path.basename(p)[8:-4]
+
+
+# ------------------------------------------------------------------ BFS --
+@pytest.mark.parametrize("path", FIXTURES, ids=_fid)
+def test_bfs_reference_fixtures_every_source(ob, path):
+    """Bit-exact against testBFS on the CSR the reference loader builds."""
+    z = np.load(path)
+    with ob.Graph.from_csr(z["rowptr"], z["col"]) as g:
+        for i, s in enumerate(z["bfs_sources"]):
+            lv = g.bfs(int(s))
+            np.testing.assert_array_equal(lv, z["bfs_levels"][i], err_msg=f"source {s}")
+
+
+def test_bfs_grid_128(ob):
+    z = np.load(os.path.join(GOLDEN, "gen_grid_128x128.npz"))
+    rp, cl = oracle.grid_csr(128, 128)
+    with ob.Graph.from_csr(rp, cl) as g:
+        for i, s in enumerate(z["bfs_sources"]):
+            np.testing.assert_array_equal(g.bfs(int(s)), z["bfs_levels"][i])
+        g.bfs(0)
+        # 254 levels beyond the source (the reference app stops at -round 100)
+        assert g.last_stats.iterations == int(z["bfs_levels"][0].max()) + 1
+        assert g.last_stats.vertices_reached == 16384
+        assert g.last_stats.edges_traversed == 65024
+
+
+@pytest.mark.parametrize("scale", [10, 12])
+def test_bfs_rmat_golden_and_generator(ob, scale):
+    z = np.load(os.path.join(GOLDEN, f"gen_rmat{scale}_ef16_s1.npz"))
+    rp, cl = oracle.rmat_csr(scale, 16, 1)
+    with ob.Graph.rmat(scale, 16, 1) as g:
+        grp, gcl, _ = g.csr()
+        np.testing.assert_array_equal(grp, rp)   # device generator == CPU restatement
+        np.testing.assert_array_equal(gcl, cl)
+        for i, s in enumerate(z["bfs_sources"]):
+            np.testing.assert_array_equal(g.bfs(int(s)), z["bfs_levels"][i])
+
+
+@pytest.mark.parametrize("scale,seed", [(14, 1), (16, 7)])
+def test_bfs_rmat_vs_oracle(ob, scale, seed):
+    with ob.Graph.rmat(scale, 16, seed) as g:
+        rp, cl, _ = g.csr()
+        hub, _ = g.max_degree_vertex()
+        deg = np.diff(rp.astype(np.int64))
+        rng = np.random.default_rng(scale)
+        for s in [hub] + rng.choice(np.flatnonzero(deg > 0), 4, replace=False).tolist():
+            ref, e_ref = oracle.bfs(rp, cl, int(s))
+            np.testing.assert_array_equal(g.bfs(int(s)), ref)
+            st = g.last_stats
+            assert st.edges_traversed == e_ref
+            assert st.vertices_reached == int((ref != INF).sum())
+
+
+def test_bfs_device_output_and_repeat(ob):
+    import torch
+    with ob.Graph.rmat(15, 16, 3) as g:
+        rp, cl, _ = g.csr()
+        hub, _ = g.max_degree_vertex()
+        ref, _ = oracle.bfs(rp, cl, hub)
+        out = torch.empty(g.V, dtype=torch.int32, device="cuda")
+        for _ in range(3):
+            g.bfs(hub, out=out)
+            np.testing.assert_array_equal(out.cpu().numpy(), ref)
+        # unaligned device output (offset by one element)
+        big = torch.empty(g.V + 1, dtype=torch.int32, device="cuda")
+        g.bfs(hub, out=big[1:])
+        np.testing.assert_array_equal(big[1:].cpu().numpy(), ref)
+
+
+def test_bfs_source_out_of_range(ob):
+    rp, cl = oracle.grid_csr(4, 4)
+    with ob.Graph.from_csr(rp, cl) as g:
+        with pytest.raises(ob.OliveError):
+            g.bfs(16)
+
+
+def test_bfs_unsorted_rows_and_duplicates(ob):
+    """Rows in any order, duplicate edges and self-loops give the same levels."""
+    rng = np.random.default_rng(5)
+    V = 3000
+    src = rng.integers(0, V, 40000)
+    dst = rng.integers(0, V, 40000)
+    dst[:500] = src[:500]                      # self-loops
+    src = np.concatenate([src, src[:1000]])    # duplicates
+    dst = np.concatenate([dst, dst[:1000]])
+    order = np.argsort(src, kind="stable")
+    rp = np.zeros(V + 1, np.int64)
+    np.add.at(rp, src + 1, 1)
+    rp = np.cumsum(rp).astype(np.uint32)
+    cl = dst[order].astype(np.uint32)
+    with ob.Graph.from_csr(rp, cl) as g:
+        for s in (0, 17, 2999):
+            np.testing.assert_array_equal(g.bfs(s), oracle.bfs(rp, cl, s)[0])
+
+
+# ----------------------------------------------------------------- SSSP --
+@pytest.mark.parametrize("path", [p for p in FIXTURES if "weights" in np.load(p)], ids=_fid)
+def test_sssp_weighted_fixtures(ob, path):
+    z = np.load(path)
+    rp, cl, w = z["sorted_rowptr"], z["sorted_col"], z["sorted_weights"]
+    with ob.Graph.from_csr(rp, cl, w) as g:
+        for s in range(0, len(rp) - 1, 7):
+            ref, *_ = oracle.dijkstra(rp, cl, w, s)
+            np.testing.assert_array_equal(g.sssp(s), ref)
+
+
+@pytest.mark.parametrize("path", FIXTURES, ids=_fid)
+def test_sssp_unit_weights_equal_reference_bfs(ob, path):
+    """SSSP.cu forces every weight to 1 (SSSP.cu:131): distances are BFS levels."""
+    z = np.load(path)
+    w = np.ones(len(z["col"]), np.uint32)
+    with ob.Graph.from_csr(z["rowptr"], z["col"], w) as g:
+        for i, s in enumerate(z["bfs_sources"][:20]):
+            d = g.sssp(int(s))
+            np.testing.assert_array_equal(d.astype(np.int64),
+                                          z["bfs_levels"][i].astype(np.int64))
+
+
+@pytest.mark.parametrize("scale,seed", [(12, 1), (16, 2)])
+def test_sssp_rmat_vs_dijkstra(ob, scale, seed):
+    with ob.Graph.rmat(scale, 16, seed, weights=True, wseed=seed + 10) as g:
+        rp, cl, w = g.csr()
+        np.testing.assert_array_equal(w, oracle.uint_weights(len(cl), seed + 10))
+        hub, _ = g.max_degree_vertex()
+        deg = np.diff(rp.astype(np.int64))
+        for s in (hub, int(np.flatnonzero(deg > 0)[3])):
+            ref, e_ref, _, nset = oracle.dijkstra(rp, cl, w, s)
+            np.testing.assert_array_equal(g.sssp(s), ref)
+            st = g.last_stats
+            assert st.edges_traversed == e_ref and st.vertices_reached == nset
+            assert st.edges_relaxed >= st.edges_traversed
+
+
+def test_sssp_needs_weights(ob):
+    rp, cl = oracle.grid_csr(3, 3)
+    with ob.Graph.from_csr(rp, cl) as g:
+        with pytest.raises(ob.OliveError):
+            g.sssp(0)
+
+
+# ------------------------------------------------------------- PageRank --
+@pytest.mark.parametrize("path", FIXTURES, ids=_fid)
+def test_pagerank_leak_matches_reference_checker(ob, path):
+    """dangling='leak' reproduces testPageRank (printed with %f)."""
+    z = np.load(path)
+    # testPageRank converged on every fixture: it ran pr_iterations + 1 sweeps
+    # (it breaks before counting the last one, testPageRank.cu:102-103)
+    sweeps = int(z["pr_iterations"]) + 1
+    with ob.Graph.from_csr(z["rowptr"], z["col"]) as g:
+        r = g.pagerank(0.85, sweeps, 0.0, dangling="leak")
+        assert g.last_stats.iterations == sweeps
+        np.testing.assert_allclose(r, z["pr_ranks"], rtol=0, atol=6e-7)
+        r50 = g.pagerank(0.85, 50, 0.0, dangling="leak")
+        if int(z["pr50_iterations"]) == 50:
+            np.testing.assert_allclose(r50, z["pr50_ranks"], rtol=0, atol=6e-7)
+
+
+@pytest.mark.parametrize("scale,seed", [(12, 1), (16, 3), (18, 4)])
+def test_pagerank_fp32_vs_fp64_oracle(ob, scale, seed):
+    """FP32 ranks within 1e-6 max relative error of the FP64 oracle after the
+    same number of iterations (dangling mass redistributed)."""
+    with ob.Graph.rmat(scale, 16, seed) as g:
+        rp, cl, _ = g.csr()
+        r = g.pagerank(0.85, 50, 1e-7)
+        it = g.last_stats.iterations
+        ref, it_ref, res = oracle.pagerank(rp, cl, 0.85, it, 0.0)
+        assert it_ref == it
+        rel = np.abs(r.astype(np.float64) - ref) / ref
+        assert rel.max() < 1e-6, rel.max()
+        # the GPU residual is summed from FP32 ranks: ~1e-7 absolute noise
+        assert abs(g.last_stats.residual - res[-1]) <= 1e-3 * res[-1] + 2e-7
+
+
+def test_pagerank_deterministic(ob):
+    with ob.Graph.rmat(17, 16, 9) as g:
+        a = g.pagerank(0.85, 30, 0.0)
+        b = g.pagerank(0.85, 30, 0.0)
+        assert a.tobytes() == b.tobytes()
+
+
+def test_pagerank_tolerance_stop(ob):
+    rp, cl = oracle.grid_csr(20, 20)
+    with ob.Graph.from_csr(rp, cl) as g:
+        g.pagerank(0.85, 1000, 1e-5)
+        it = g.last_stats.iterations
+        _, it_ref, res = oracle.pagerank(rp, cl, 0.85, 1000, 1e-5)
+        assert abs(it - it_ref) <= 1
+        assert g.last_stats.residual < 1e-5
