@@ -86,6 +86,17 @@ int olv_graph_set_weights_f32(olv_graph *g, const float *w);
 int olv_set_stream(olv_graph *g, void *stream);
 /* Maximum out-degree vertex, ties to the smallest id. */
 int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
+/* Engine tunables by name (no reference counterpart; the reference fixed its
+ * launch shape in util::kernelConfig, utils.h:56-72, and the app's -g flag):
+ *   "hub_degree"  rows longer than this are split into pieces       (1024)
+ *   "piece"       edges per piece                                   (1024)
+ *   "alpha"       BFS push->pull when m_f * alpha > m_unvisited     (14)
+ *   "beta"        BFS pull->push when n_f * beta < V                (24)
+ *   "sssp_delta"  SSSP bucket width, 0 = default                    (0)
+ *   "use_graphs"  run supersteps inside CUDA graphs (1) or a host loop (0)
+ *   "levels_per_sync" host loop: supersteps enqueued per check      (4)  */
+int olv_tune_set(olv_graph *g, const char *key, double value);
+int olv_tune_get(const olv_graph *g, const char *key, double *value);
 
 /* ---- traversal --------------------------------------------------------------
  * BFS levels: reproduces testBFS.cu:42-87 and BFS.cu:82-160 run to completion

@@ -51,6 +51,8 @@ _SIGS = [
     ("olv_graph_set_weights_f32", _I, [_VP, _VP]),
     ("olv_set_stream", _I, [_VP, _VP]),
     ("olv_graph_max_degree_vertex", _I, [_VP, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
+    ("olv_tune_set", _I, [_VP, ctypes.c_char_p, _D]),
+    ("olv_tune_get", _I, [_VP, ctypes.c_char_p, ctypes.POINTER(_D)]),
     ("olv_bfs", _I, [_VP, _U32, _VP, ctypes.POINTER(Stats)]),
     ("olv_sssp", _I, [_VP, _U32, _VP, ctypes.POINTER(Stats)]),
     ("olv_pagerank", _I, [_VP, _D, _I, _D, _I, _VP, ctypes.POINTER(Stats)]),
@@ -175,6 +177,18 @@ class Graph:
         _check(lib().olv_graph_max_degree_vertex(self._h, ctypes.byref(v), ctypes.byref(d)),
                "olv_graph_max_degree_vertex")
         return v.value, d.value
+
+    def tune(self, **kw):
+        """Set engine tunables (see olv_tune_set); returns the current values."""
+        for k, v in kw.items():
+            _check(lib().olv_tune_set(self._h, k.encode(), float(v)), f"olv_tune_set({k})")
+        out = {}
+        for k in ("hub_degree", "piece", "alpha", "beta", "sssp_delta", "use_graphs",
+                  "levels_per_sync"):
+            d = _D()
+            _check(lib().olv_tune_get(self._h, k.encode(), ctypes.byref(d)), "olv_tune_get")
+            out[k] = d.value
+        return out
 
     def set_weights_f32(self, w):
         w = np.ascontiguousarray(w, np.float32) if not hasattr(w, "data_ptr") else w.contiguous()

@@ -41,9 +41,15 @@ struct BfsPushOp {
         acc = 0;
         m_next = &c->m_next;
     }
+    struct Pre {
+        int lvl;
+    };
     __device__ __forceinline__ uint32_t src_value(uint32_t) const { return 0; }
-    __device__ __forceinline__ int edge(uint32_t, uint32_t, uint32_t v) {
-        if (__ldcg(&level[v]) != kInf) return 0;
+    __device__ __forceinline__ Pre prepare(uint32_t, uint32_t, uint32_t v) const {
+        return Pre{__ldcg(&level[v])};
+    }
+    __device__ __forceinline__ int apply(const Pre &p, uint32_t v) {
+        if (p.lvl != kInf) return 0;
         return atomicCAS(&level[v], kInf, next) == kInf ? 1 : 0;
     }
     __device__ __forceinline__ void on_push(bool p, uint32_t v) {
@@ -95,16 +101,38 @@ __global__ void k_bfs_begin(TravCtl *c, uint32_t V, float alpha, float beta) {
     c->m_next = 0;
 }
 
+// Bitmap of the current frontier (level == L), one ballot per warp; used when
+// a pull level follows a push level.  Words of vertices >= V are zero.
+__global__ void __launch_bounds__(kBlock)
+k_bfs_bitmap(uint32_t V, TravCtl *c, uint32_t *fb0, uint32_t *fb1) {
+    if (c->done || c->mode != 1 || c->fb_valid) return;
+    const int32_t *level = static_cast<const int32_t *>(c->vdata);
+    const int L = (int)c->level;
+    uint32_t *fb = c->fb_cur ? fb1 : fb0;
+    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V;
+         base += (uint64_t)gridDim.x * kBlock) {
+        const uint64_t v = base + threadIdx.x;
+        const unsigned word = __ballot_sync(0xffffffffu, v < V && __ldcg(&level[v]) == L);
+        if (lane_id() == 0) fb[v >> 5] = word;
+    }
+}
+
+// Pull: every unvisited vertex looks for an in-neighbour in the frontier
+// bitmap, kParents in-edges per probe, and stops at the first hit.
+constexpr int kParents = 4;
+
 __global__ void __launch_bounds__(kBlock)
 k_bfs_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowidx,
            const uint32_t *__restrict__ rowptr, uint32_t V, TravCtl *c, uint32_t *q0,
-           uint32_t *q1) {
+           uint32_t *q1, uint32_t *fb0, uint32_t *fb1) {
     if (c->done || c->mode != 1) return;
     int32_t *level = static_cast<int32_t *>(c->vdata);
     const int L = (int)c->level;
     const uint32_t cur = c->cur;
     uint32_t *qout = cur ? q0 : q1;
     uint32_t *qsz = &c->qsize[cur ^ 1];
+    const uint32_t *__restrict__ fin = c->fb_cur ? fb1 : fb0;
+    uint32_t *__restrict__ fout = c->fb_cur ? fb0 : fb1;
     unsigned long long acc = 0;
     for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V;
          base += (uint64_t)gridDim.x * kBlock) {
@@ -112,16 +140,21 @@ k_bfs_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ row
         bool found = false;
         if (v < V && level[v] == kInf) {
             const uint32_t b = __ldg(&colptr[v]), e = __ldg(&colptr[v + 1]);
-            for (uint32_t i = b; i < e; i++)
-                if (level[__ldg(&rowidx[i])] == L) {
-                    found = true;
-                    break;
-                }
+            for (uint32_t i = b; i < e && !found; i += kParents) {
+                uint32_t u[kParents];
+#pragma unroll
+                for (int j = 0; j < kParents; j++) u[j] = i + j < e ? __ldg(&rowidx[i + j]) : 0xffffffffu;
+#pragma unroll
+                for (int j = 0; j < kParents; j++)
+                    if (u[j] != 0xffffffffu && ((fin[u[j] >> 5] >> (u[j] & 31)) & 1u)) found = true;
+            }
             if (found) {
                 level[v] = L + 1;
                 acc += __ldg(&rowptr[v + 1]) - __ldg(&rowptr[v]);
             }
         }
+        const unsigned word = __ballot_sync(0xffffffffu, found);
+        if (lane_id() == 0) fout[v >> 5] = word;
         warp_push(found, v, qout, qsz);
     }
     warp_add64(acc, &c->m_next);
@@ -134,6 +167,12 @@ __global__ void k_bfs_end(TravCtl *c, cudaGraphConditionalHandle h, int use_cond
         if (c->mode) c->pull_steps++;
         c->m_unvisited -= (c->m_next < c->m_unvisited ? c->m_next : c->m_unvisited);
         c->m_f = c->m_next;
+        if (c->mode) {          // the pull kernel wrote the next frontier's bitmap
+            c->fb_cur ^= 1;
+            c->fb_valid = 1;
+        } else {
+            c->fb_valid = 0;
+        }
         c->cur ^= 1;
         c->level++;
         c->steps++;
@@ -153,6 +192,7 @@ int traversal_workspace(olv_graph *g, bool pieces) {
     OLV_TRY(w.q0.ensure(V * 4 + 16));
     OLV_TRY(w.q1.ensure(V * 4 + 16));
     OLV_TRY(w.ctl.ensure(sizeof(TravCtl)));
+    OLV_TRY(w.fbits.ensure(2 * (((size_t)V + 31) / 32 + 8) * 4));
     if (pieces) {
         const uint64_t np = g->E / g->tune.piece + g->E / g->tune.hub_degree + 16;
         OLV_TRY(w.pieces.ensure(np * sizeof(uint2)));
@@ -201,7 +241,11 @@ static int bfs_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle h
     void *a_adv[] = {&a, &op};
     OLV_TRY(sink((const void *)k_advance_chunks<BfsPushOp>, dim3(nb), dim3(kBlock), a_adv));
     OLV_TRY(sink((const void *)k_advance_pieces<BfsPushOp>, dim3(nb), dim3(kBlock), a_adv));
-    void *a_pull[] = {&colptr, &rowidx, &rowptr, &V, &ctl, &q0, &q1};
+    uint32_t *fb0 = g->ws.fbits.as<uint32_t>();
+    uint32_t *fb1 = fb0 + ((size_t)V + 31) / 32 + 8;
+    void *a_bm[] = {&V, &ctl, &fb0, &fb1};
+    OLV_TRY(sink((const void *)k_bfs_bitmap, dim3(nb), dim3(kBlock), a_bm));
+    void *a_pull[] = {&colptr, &rowidx, &rowptr, &V, &ctl, &q0, &q1, &fb0, &fb1};
     OLV_TRY(sink((const void *)k_bfs_pull, dim3(nb), dim3(kBlock), a_pull));
     void *a_end[] = {&ctl, &h, &use_cond, &V};
     OLV_TRY(sink((const void *)k_bfs_end, dim3(1), dim3(1), a_end));

@@ -479,6 +479,58 @@ int olv_graph_set_weights_f32(olv_graph *g, const float *w) {
     return OLV_OK;
 }
 
+int olv_tune_set(olv_graph *g, const char *key, double value) {
+    OLV_CHECK_ARG(g && key, "olv_tune_set: null pointer");
+    Tuning &t = g->tune;
+    if (!strcmp(key, "hub_degree")) {
+        OLV_CHECK_ARG(value >= 32 && value <= 1e9, "olv_tune_set: hub_degree out of range");
+        t.hub_degree = (uint32_t)value;
+        g->ws.pieces.release();
+    } else if (!strcmp(key, "piece")) {
+        OLV_CHECK_ARG(value >= 32 && value <= 1e9, "olv_tune_set: piece out of range");
+        t.piece = (uint32_t)value;
+        g->ws.pieces.release();
+    } else if (!strcmp(key, "alpha")) {
+        OLV_CHECK_ARG(value > 0, "olv_tune_set: alpha must be > 0");
+        t.alpha = (float)value;
+    } else if (!strcmp(key, "beta")) {
+        OLV_CHECK_ARG(value > 0, "olv_tune_set: beta must be > 0");
+        t.beta = (float)value;
+    } else if (!strcmp(key, "sssp_delta")) {
+        OLV_CHECK_ARG(value >= 0 && value < 2147483647.0, "olv_tune_set: bad sssp_delta");
+        t.sssp_delta = (uint32_t)value;
+    } else if (!strcmp(key, "use_graphs")) {
+        t.use_graphs = value != 0;
+    } else if (!strcmp(key, "levels_per_sync")) {
+        OLV_CHECK_ARG(value >= 1 && value <= 1024, "olv_tune_set: levels_per_sync out of range");
+        t.levels_per_sync = (int)value;
+    } else {
+        set_error("olv_tune_set: unknown key '%s'", key);
+        return OLV_ERR_ARG;
+    }
+    // launch parameters are baked into the cached superstep graphs
+    for (WhileGraph *wg : {g->bfs_graph, g->sssp_graph})
+        if (wg) wg->destroy();
+    return OLV_OK;
+}
+
+int olv_tune_get(const olv_graph *g, const char *key, double *value) {
+    OLV_CHECK_ARG(g && key && value, "olv_tune_get: null pointer");
+    const Tuning &t = g->tune;
+    if (!strcmp(key, "hub_degree")) *value = t.hub_degree;
+    else if (!strcmp(key, "piece")) *value = t.piece;
+    else if (!strcmp(key, "alpha")) *value = t.alpha;
+    else if (!strcmp(key, "beta")) *value = t.beta;
+    else if (!strcmp(key, "sssp_delta")) *value = t.sssp_delta;
+    else if (!strcmp(key, "use_graphs")) *value = t.use_graphs;
+    else if (!strcmp(key, "levels_per_sync")) *value = t.levels_per_sync;
+    else {
+        set_error("olv_tune_get: unknown key '%s'", key);
+        return OLV_ERR_ARG;
+    }
+    return OLV_OK;
+}
+
 int olv_set_stream(olv_graph *g, void *stream) {
     OLV_CHECK_ARG(g, "olv_set_stream: null graph");
     g->stream = stream ? (cudaStream_t)stream : g->own_stream;

@@ -9,10 +9,12 @@
 // second kernel spreads over all warps of the GPU.  Destinations are appended
 // to the output queue with one atomic per warp.
 //
-// An Op supplies the per-edge work:
+// An Op supplies the per-edge work, split so that a thread can keep several
+// edges' loads in flight before it issues their atomics:
 //   void begin(TravCtl *c)                          load per-superstep values
 //   uint32_t src_value(uint32_t u)                  value carried from the source
-//   int edge(uint32_t sv, uint32_t e, uint32_t v)   0: nothing, 1: push v to the
+//   Pre prepare(uint32_t sv, uint32_t e, uint32_t v)   plain loads for one edge
+//   int apply(const Pre &p, uint32_t v)             0: nothing, 1: push v to the
 //                                                   output queue, 2: push to the
 //                                                   secondary (far) queue
 //   void on_push(bool pushed, uint32_t v)           after each warp-wide push
@@ -35,6 +37,30 @@ __device__ __forceinline__ void warp_push(bool p, uint32_t v, uint32_t *__restri
     if (lane == leader) base = atomicAdd(qsize, (uint32_t)__popc(m));
     base = __shfl_sync(0xffffffffu, base, leader);
     if (p) q[base + __popc(m & ((1u << lane) - 1u))] = v;
+}
+
+// Append the v[j] with act[j] == want (j < N) to q with one atomic per warp.
+template <int N>
+__device__ __forceinline__ void warp_push_n(const int (&act)[N], const uint32_t (&v)[N], int want,
+                                            uint32_t *__restrict__ q, uint32_t *__restrict__ qsize) {
+    unsigned m[N];
+    uint32_t tot = 0;
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+        m[j] = __ballot_sync(0xffffffffu, act[j] == want);
+        tot += __popc(m[j]);
+    }
+    if (!tot) return;
+    const uint32_t lane = lane_id();
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(qsize, tot);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+        if (act[j] == want) q[base + __popc(m[j] & lt)] = v[j];
+        base += __popc(m[j]);
+    }
 }
 
 // Warp sum of a 64-bit value added to *dst by lane 0.  All lanes must call.
@@ -74,6 +100,8 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *t
     __syncthreads();
     return r;
 }
+
+constexpr int kItems = 4;   // edges per thread kept in flight
 
 struct AdvanceArgs {
     const uint32_t *rowptr;
@@ -131,22 +159,38 @@ __global__ void __launch_bounds__(kBlock) k_advance_chunks(AdvanceArgs a, Op op)
         s_off[threadIdx.x] = off;
         s_val[threadIdx.x] = sv;
         __syncthreads();
-        for (uint32_t base = 0; base < total; base += kBlock) {
-            const uint32_t k = base + threadIdx.x;
-            int act = 0;
-            uint32_t v = 0;
-            if (k < total) {
-                uint32_t lo = 0;
+        for (uint32_t base = 0; base < total; base += kBlock * kItems) {
+            uint32_t e[kItems], v[kItems], sv[kItems];
+            int act[kItems];
 #pragma unroll
-                for (uint32_t step = kBlock / 2; step > 0; step >>= 1)
-                    if (s_off[lo + step] <= k) lo += step;
-                const uint32_t e = s_beg[lo] + (k - s_off[lo]);
-                v = __ldg(&a.col[e]);
-                act = op.edge(s_val[lo], e, v);
+            for (int j = 0; j < kItems; j++) {
+                const uint32_t k = base + j * kBlock + threadIdx.x;
+                act[j] = k < total;
+                e[j] = 0;
+                sv[j] = 0;
+                v[j] = 0;
+                if (act[j]) {
+                    uint32_t lo = 0;
+#pragma unroll
+                    for (uint32_t step = kBlock / 2; step > 0; step >>= 1)
+                        if (s_off[lo + step] <= k) lo += step;
+                    e[j] = s_beg[lo] + (k - s_off[lo]);
+                    sv[j] = s_val[lo];
+                }
             }
-            warp_push(act == 1, v, qout, qout_size);
-            if (Op::kHasFar) warp_push(act == 2, v, far, far_size);
-            op.on_push(act == 1, v);
+#pragma unroll
+            for (int j = 0; j < kItems; j++)
+                if (act[j]) v[j] = __ldg(&a.col[e[j]]);
+            typename Op::Pre pre[kItems];
+#pragma unroll
+            for (int j = 0; j < kItems; j++)
+                if (act[j]) pre[j] = op.prepare(sv[j], e[j], v[j]);
+#pragma unroll
+            for (int j = 0; j < kItems; j++) act[j] = act[j] ? op.apply(pre[j], v[j]) : 0;
+            warp_push_n<kItems>(act, v, 1, qout, qout_size);
+            if (Op::kHasFar) warp_push_n<kItems>(act, v, 2, far, far_size);
+#pragma unroll
+            for (int j = 0; j < kItems; j++) op.on_push(act[j] == 1, v[j]);
         }
         __syncthreads();
     }
@@ -176,17 +220,25 @@ __global__ void __launch_bounds__(kBlock) k_advance_pieces(AdvanceArgs a, Op op)
         const uint32_t b = rb + pc.y * a.piece;
         const uint32_t e_end = min(re, b + a.piece);
         const uint32_t sv = op.src_value(u);
-        for (uint32_t base = b; base < e_end; base += 32) {
-            const uint32_t e = base + lane;
-            int act = 0;
-            uint32_t v = 0;
-            if (e < e_end) {
-                v = __ldg(&a.col[e]);
-                act = op.edge(sv, e, v);
+        for (uint32_t base = b; base < e_end; base += 32 * kItems) {
+            uint32_t e[kItems], v[kItems];
+            int act[kItems];
+#pragma unroll
+            for (int j = 0; j < kItems; j++) {
+                e[j] = base + j * 32 + lane;
+                act[j] = e[j] < e_end;
+                v[j] = act[j] ? __ldg(&a.col[e[j]]) : 0;
             }
-            warp_push(act == 1, v, qout, qout_size);
-            if (Op::kHasFar) warp_push(act == 2, v, far, far_size);
-            op.on_push(act == 1, v);
+            typename Op::Pre pre[kItems];
+#pragma unroll
+            for (int j = 0; j < kItems; j++)
+                if (act[j]) pre[j] = op.prepare(sv, e[j], v[j]);
+#pragma unroll
+            for (int j = 0; j < kItems; j++) act[j] = act[j] ? op.apply(pre[j], v[j]) : 0;
+            warp_push_n<kItems>(act, v, 1, qout, qout_size);
+            if (Op::kHasFar) warp_push_n<kItems>(act, v, 2, far, far_size);
+#pragma unroll
+            for (int j = 0; j < kItems; j++) op.on_push(act[j] == 1, v[j]);
         }
     }
     op.flush(0);

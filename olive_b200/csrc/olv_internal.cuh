@@ -65,6 +65,8 @@ struct TravCtl {
     uint32_t epoch;             // SSSP far-pile generation
     uint32_t far_min;           // SSSP smallest distance kept in the far pile
     uint32_t split_lo;          // SSSP: lower edge of the bucket being split
+    uint32_t fb_cur;            // BFS: which frontier bitmap holds the current level
+    uint32_t fb_valid;          // BFS: that bitmap is up to date
     void *vdata;                // per-vertex result array of the run (level / dist)
     unsigned long long m_f;         // out-edges of the input frontier
     unsigned long long m_next;      // out-edges of vertices discovered this superstep
@@ -86,9 +88,10 @@ struct Tuning {
 };
 
 struct Workspace {
-    DevBuf level, q0, q1, pieces, ctl, mark, far0, far1, tmp, partials;
+    DevBuf level, q0, q1, pieces, ctl, mark, far0, far1, tmp, partials, fbits;
     void release() {
         level.release(); q0.release(); q1.release(); pieces.release(); ctl.release();
+        fbits.release();
         mark.release(); far0.release(); far1.release(); tmp.release(); partials.release();
     }
 };

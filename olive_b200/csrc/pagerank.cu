@@ -31,7 +31,9 @@ namespace olv {
 
 constexpr uint32_t kNnz = 2048;      // in-edges staged per row block
 constexpr uint32_t kRows = 2048;     // rows per row block at most
+constexpr uint32_t kSeg = 4096;      // in-edges per segment of a long row
 constexpr int kRedThreads = 1024;
+constexpr int kGather = kNnz / kBlock;
 
 struct PrCtl {
     double base;        // (1-alpha)/N + alpha*d/N for the running iteration
@@ -69,7 +71,8 @@ __global__ void __launch_bounds__(kBlock)
 k_pr_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowidx,
           const uint32_t *__restrict__ blocks, const uint32_t *__restrict__ outdeg,
           const float *c0, const float *c1, float *__restrict__ rank, PrCtl *ctl,
-          double *__restrict__ partials, float a_hi, float a_lo) {
+          double *__restrict__ partials, float a_hi, float a_lo,
+          const uint32_t *__restrict__ segbase, const float2 *__restrict__ segs) {
     if (ctl->done) return;
     const float *__restrict__ cin = (ctl->iter & 1) ? c1 : c0;
     float *__restrict__ cout = (float *)((ctl->iter & 1) ? c0 : c1);
@@ -77,7 +80,6 @@ k_pr_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowi
     const uint32_t r0 = blocks[blockIdx.x], r1 = blocks[blockIdx.x + 1];
     const uint32_t e0 = colptr[r0], e1 = colptr[r1];
     __shared__ float s_val[kNnz];
-    __shared__ float s_red[2][kBlock];
     __shared__ double s_dred[2][kBlock / 32];
     double res = 0.0, dang = 0.0;
 
@@ -96,8 +98,18 @@ k_pr_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowi
     };
 
     if (e1 - e0 <= kNnz) {
-        for (uint32_t i = threadIdx.x; i < e1 - e0; i += kBlock)
-            s_val[i] = __ldg(&cin[__ldg(&rowidx[e0 + i])]);
+        const uint32_t n = e1 - e0;
+        uint32_t idx[kGather];
+#pragma unroll
+        for (int j = 0; j < kGather; j++) {
+            const uint32_t i = threadIdx.x + j * kBlock;
+            idx[j] = i < n ? __ldg(&rowidx[e0 + i]) : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < kGather; j++) {
+            const uint32_t i = threadIdx.x + j * kBlock;
+            if (i < n) s_val[i] = __ldg(&cin[idx[j]]);
+        }
         __syncthreads();
         for (uint32_t v = r0 + threadIdx.x; v < r1; v += kBlock) {
             const uint32_t b = colptr[v] - e0, e = colptr[v + 1] - e0;
@@ -105,24 +117,16 @@ k_pr_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowi
             for (uint32_t i = b; i < e; i++) two_sum_acc(s, c, s_val[i]);
             finish_row(v, s, c);
         }
-    } else {
-        // one long row: strided compensated sums, then a fixed tree
+    } else if (threadIdx.x == 0) {
+        // one long row: its segments were summed by k_pr_segments; fold in order
+        const uint32_t first = segbase[blockIdx.x];
+        const uint32_t nseg = (e1 - e0 + kSeg - 1) / kSeg;
         float s = 0.0f, c = 0.0f;
-        for (uint32_t i = e0 + threadIdx.x; i < e1; i += kBlock)
-            two_sum_acc(s, c, __ldg(&cin[__ldg(&rowidx[i])]));
-        s_red[0][threadIdx.x] = s;
-        s_red[1][threadIdx.x] = c;
-        __syncthreads();
-        for (int w = kBlock / 2; w > 0; w >>= 1) {
-            if (threadIdx.x < (uint32_t)w) {
-                float a = s_red[0][threadIdx.x], ac = s_red[1][threadIdx.x];
-                pair_add(a, ac, s_red[0][threadIdx.x + w], s_red[1][threadIdx.x + w]);
-                s_red[0][threadIdx.x] = a;
-                s_red[1][threadIdx.x] = ac;
-            }
-            __syncthreads();
+        for (uint32_t k = 0; k < nseg; k++) {
+            const float2 p = segs[first + k];
+            pair_add(s, c, p.x, p.y);
         }
-        if (threadIdx.x == 0) finish_row(r0, s_red[0][0], s_red[1][0]);
+        finish_row(r0, s, c);
     }
     // fixed-order CTA reduction of the FP64 partials
 #pragma unroll
@@ -144,6 +148,43 @@ k_pr_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowi
         partials[2 * blockIdx.x] = a;
         partials[2 * blockIdx.x + 1] = b;
     }
+}
+
+// Compensated sums of the kSeg-edge segments of long rows: thread t sums
+// elements t, t+kBlock, ... of its segment, then a fixed-shape tree.
+__global__ void __launch_bounds__(kBlock)
+k_pr_segments(const uint32_t *__restrict__ rowidx, const uint2 *__restrict__ seg_range,
+              const float *c0, const float *c1, const PrCtl *ctl, float2 *__restrict__ segs) {
+    if (ctl->done) return;
+    const float *__restrict__ cin = (ctl->iter & 1) ? c1 : c0;
+    const uint2 r = seg_range[blockIdx.x];
+    __shared__ float s_red[2][kBlock];
+    float s = 0.0f, c = 0.0f;
+    constexpr int U = kSeg / kBlock;
+    uint32_t idx[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) {
+        const uint32_t i = r.x + threadIdx.x + j * kBlock;
+        idx[j] = i < r.y ? __ldg(&rowidx[i]) : 0xffffffffu;
+    }
+    float x[U];
+#pragma unroll
+    for (int j = 0; j < U; j++) x[j] = idx[j] != 0xffffffffu ? __ldg(&cin[idx[j]]) : 0.0f;
+#pragma unroll
+    for (int j = 0; j < U; j++) two_sum_acc(s, c, x[j]);
+    s_red[0][threadIdx.x] = s;
+    s_red[1][threadIdx.x] = c;
+    __syncthreads();
+    for (int w = kBlock / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < (uint32_t)w) {
+            float a = s_red[0][threadIdx.x], ac = s_red[1][threadIdx.x];
+            pair_add(a, ac, s_red[0][threadIdx.x + w], s_red[1][threadIdx.x + w]);
+            s_red[0][threadIdx.x] = a;
+            s_red[1][threadIdx.x] = ac;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) segs[blockIdx.x] = make_float2(s_red[0][0], s_red[1][0]);
 }
 
 // Fold the per-CTA partials (fixed order), publish residual and the next
@@ -223,13 +264,14 @@ __global__ void k_outdeg(const uint32_t *__restrict__ rowptr, uint32_t V, uint32
 
 // ------------------------------------------------------------------ host --
 struct PrPlan {
-    DevBuf blocks, outdeg, contrib, partials, ctl, dang;
+    DevBuf blocks, outdeg, contrib, partials, ctl, dang, segbase, seg_range, segs;
     uint32_t nblocks = 0;
+    uint32_t nsegs = 0;
     float a_hi = 0, a_lo = 0;
     double alpha = -1;
     ~PrPlan() {
         blocks.release(); outdeg.release(); contrib.release(); partials.release();
-        ctl.release(); dang.release();
+        ctl.release(); dang.release(); segbase.release(); seg_range.release(); segs.release();
     }
 };
 
@@ -255,6 +297,24 @@ static int build_pr_plan(olv_graph *g, PrPlan &p) {
         b.push_back(v);
     }
     p.nblocks = (uint32_t)b.size() - 1;
+    // long rows (one per block) are cut into kSeg-edge segments
+    std::vector<uint32_t> segbase(p.nblocks, 0xffffffffu);
+    std::vector<uint2> ranges;
+    for (uint32_t k = 0; k < p.nblocks; k++) {
+        const uint32_t e0 = cp[b[k]], e1 = cp[b[k + 1]];
+        if (e1 - e0 <= kNnz) continue;
+        segbase[k] = (uint32_t)ranges.size();
+        for (uint32_t x = e0; x < e1; x += kSeg) ranges.push_back(make_uint2(x, std::min(e1, x + kSeg)));
+    }
+    p.nsegs = (uint32_t)ranges.size();
+    OLV_TRY(p.segbase.ensure(segbase.size() * 4 + 16));
+    OLV_TRY(p.seg_range.ensure(ranges.size() * 8 + 16));
+    OLV_TRY(p.segs.ensure(ranges.size() * 8 + 16));
+    OLV_CUDA(cudaMemcpyAsync(p.segbase.p, segbase.data(), segbase.size() * 4,
+                             cudaMemcpyHostToDevice, g->stream));
+    if (!ranges.empty())
+        OLV_CUDA(cudaMemcpyAsync(p.seg_range.p, ranges.data(), ranges.size() * 8,
+                                 cudaMemcpyHostToDevice, g->stream));
     OLV_TRY(p.blocks.ensure(b.size() * 4));
     OLV_CUDA(cudaMemcpyAsync(p.blocks.p, b.data(), b.size() * 4, cudaMemcpyHostToDevice,
                              g->stream));
@@ -283,8 +343,17 @@ static int pr_iteration(olv_graph *g, PrPlan &p, float *rank, Sink &&sink,
     double *partials = p.partials.as<double>();
     float a_hi = p.a_hi, a_lo = p.a_lo;
     uint32_t nparts = p.nblocks;
+    const uint32_t *segbase = p.segbase.as<uint32_t>();
+    const uint2 *seg_range = p.seg_range.as<uint2>();
+    float2 *segs = p.segs.as<float2>();
+    const float2 *csegs = segs;
+    const PrCtl *cctl = ctl;
+    if (p.nsegs) {
+        void *a_seg[] = {&rowidx, &seg_range, &c0, &c1, &cctl, &segs};
+        OLV_TRY(sink((const void *)k_pr_segments, dim3(p.nsegs), dim3(kBlock), a_seg));
+    }
     void *a_pull[] = {&colptr, &rowidx, &blocks, &outdeg, &c0, &c1, &rank, &ctl, &partials,
-                      &a_hi, &a_lo};
+                      &a_hi, &a_lo, &segbase, &csegs};
     OLV_TRY(sink((const void *)k_pr_pull, dim3(p.nblocks), dim3(kBlock), a_pull));
     const double *cpart = partials;
     void *a_red[] = {&ctl, &cpart, &nparts, &h, &use_cond};

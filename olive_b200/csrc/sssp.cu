@@ -44,11 +44,18 @@ struct SsspOp {
         far_min = &c->far_min;
         fmin = 0xffffffffu;
     }
+    struct Pre {
+        uint32_t nd, cur;
+    };
     __device__ __forceinline__ uint32_t src_value(uint32_t u) const { return __ldcg(&dist[u]); }
-    __device__ __forceinline__ int edge(uint32_t du, uint32_t e, uint32_t v) {
+    __device__ __forceinline__ Pre prepare(uint32_t du, uint32_t e, uint32_t v) const {
         uint32_t nd = du + __ldg(&w[e]);
         if (nd < du || nd > (uint32_t)kInf) nd = (uint32_t)kInf;   // saturate
-        if (nd >= __ldcg(&dist[v])) return 0;
+        return Pre{nd, __ldcg(&dist[v])};
+    }
+    __device__ __forceinline__ int apply(const Pre &p, uint32_t v) {
+        const uint32_t nd = p.nd;
+        if (nd >= p.cur) return 0;
         const uint32_t old = atomicMin(&dist[v], nd);
         if (nd >= old) return 0;
         if (nd < threshold) return atomicExch(&mark[v], stamp) != stamp ? 1 : 0;

@@ -547,3 +547,100 @@ void orc_wpr_backward(uint32_t V, const uint32_t *rowptr, const uint32_t *col,
     }
     free(W); free(t);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Parallel host version of orc_rmat_csr (same graph, bit for bit): OpenMP */
+/* key generation and an LSD radix sort over the 2*scale significant bits.  */
+/* Used to build the benchmark graph on the host for the CPU reference arm. */
+/* ------------------------------------------------------------------------ */
+static void radix_sort_u64(uint64_t *a, uint64_t *tmp, uint64_t n, int bits, int nthreads) {
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#else
+    nthreads = 1;
+#endif
+    const int R = 256;
+    size_t *hist = (size_t *)calloc((size_t)nthreads * R, sizeof(size_t));
+    for (int shift = 0; shift < bits; shift += 8) {
+        memset(hist, 0, (size_t)nthreads * R * sizeof(size_t));
+        #pragma omp parallel num_threads(nthreads)
+        {
+#ifdef _OPENMP
+            int t = omp_get_thread_num();
+#else
+            int t = 0;
+#endif
+            uint64_t lo = n * t / nthreads, hi = n * (t + 1) / nthreads;
+            size_t *h = hist + (size_t)t * R;
+            for (uint64_t i = lo; i < hi; i++) h[(a[i] >> shift) & 255]++;
+            #pragma omp barrier
+            #pragma omp single
+            {
+                size_t sum = 0;
+                for (int d = 0; d < R; d++)
+                    for (int tt = 0; tt < nthreads; tt++) {
+                        size_t c = hist[(size_t)tt * R + d];
+                        hist[(size_t)tt * R + d] = sum;
+                        sum += c;
+                    }
+            }
+            for (uint64_t i = lo; i < hi; i++) tmp[h[(a[i] >> shift) & 255]++] = a[i];
+        }
+        memcpy(a, tmp, n * sizeof(uint64_t));
+    }
+    free(hist);
+}
+
+uint64_t orc_rmat_csr_par(int scale, int ef, uint64_t seed, int nthreads, uint32_t *rowptr,
+                          uint32_t *col) {
+    uint64_t V = 1ULL << scale;
+    uint64_t M = (uint64_t)ef * V;
+    uint64_t *keys = (uint64_t *)malloc(M * sizeof(uint64_t));
+    uint64_t *tmp = (uint64_t *)malloc(M * sizeof(uint64_t));
+    uint64_t pseed = seed ^ 0x5bd1e9955bd1e995ULL;
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#endif
+    #pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t i = 0; i < (int64_t)M; i++) {
+        uint32_t s, d;
+        orc_rmat_edge(scale, seed, (uint64_t)i, &s, &d);
+        s = orc_permute(s, scale, pseed);
+        d = orc_permute(d, scale, pseed);
+        /* compact key (s << scale | d); a self-loop becomes all ones (sorted last) */
+        keys[i] = (s == d) ? ~0ULL : (((uint64_t)s << scale) | d);
+    }
+    radix_sort_u64(keys, tmp, M, 2 * scale, nthreads);
+    free(tmp);
+    uint64_t m = 0;
+    const uint64_t dmask = V - 1;
+    memset(rowptr, 0, (V + 1) * sizeof(uint32_t));
+    for (uint64_t i = 0; i < M; i++) {
+        if (keys[i] == ~0ULL) break;
+        if (i && keys[i] == keys[i - 1]) continue;
+        rowptr[(keys[i] >> scale) + 1]++;
+        col[m++] = (uint32_t)(keys[i] & dmask);
+    }
+    for (uint64_t v = 0; v < V; v++) rowptr[v + 1] += rowptr[v];
+    free(keys);
+    return m;
+}
+
+void orc_uint_weights_par(uint64_t E, uint64_t seed, uint32_t lo, uint32_t hi, uint32_t *w,
+                          int nthreads) {
+    uint32_t span = hi - lo + 1;
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#endif
+    #pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t e = 0; e < (int64_t)E; e++)
+        w[e] = lo + (uint32_t)((orc_hash(seed, (uint64_t)e) >> 32) % span);
+}
+
+int orc_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

@@ -41,6 +41,13 @@ def lib():
         L.orc_permute.argtypes = [c.c_uint32, c.c_int, c.c_uint64]
         L.orc_rmat_csr.restype = c.c_uint64
         L.orc_rmat_csr.argtypes = [c.c_int, c.c_int, c.c_uint64, u32p, u32p]
+        L.orc_rmat_csr_par.restype = c.c_uint64
+        L.orc_rmat_csr_par.argtypes = [c.c_int, c.c_int, c.c_uint64, c.c_int, u32p, u32p]
+        L.orc_uint_weights_par.restype = None
+        L.orc_uint_weights_par.argtypes = [c.c_uint64, c.c_uint64, c.c_uint32, c.c_uint32, u32p,
+                                           c.c_int]
+        L.orc_max_threads.restype = c.c_int
+        L.orc_max_threads.argtypes = []
         L.orc_uint_weights.restype = None
         L.orc_uint_weights.argtypes = [c.c_uint64, c.c_uint64, c.c_uint32, c.c_uint32, u32p]
         L.orc_grid_csr.restype = c.c_uint64
@@ -91,6 +98,26 @@ def rmat_csr(scale, ef=16, seed=1):
     col = np.zeros(ef * V, np.uint32)
     E = lib().orc_rmat_csr(scale, ef, seed, _p(rowptr, ctypes.c_uint32), _p(col, ctypes.c_uint32))
     return rowptr, col[:E].copy()
+
+
+def rmat_csr_par(scale, ef=16, seed=1, threads=0):
+    """orc_rmat_csr on all host threads (identical output)."""
+    V = 1 << scale
+    rowptr = np.zeros(V + 1, np.uint32)
+    col = np.zeros(ef * V, np.uint32)
+    E = lib().orc_rmat_csr_par(scale, ef, seed, threads, _p(rowptr, ctypes.c_uint32),
+                               _p(col, ctypes.c_uint32))
+    return rowptr, col[:E]
+
+
+def uint_weights_par(E, seed, lo=1, hi=255, threads=0):
+    w = np.zeros(max(E, 1), np.uint32)
+    lib().orc_uint_weights_par(E, seed, lo, hi, _p(w, ctypes.c_uint32), threads)
+    return w[:E]
+
+
+def max_threads():
+    return lib().orc_max_threads()
 
 
 def uint_weights(E, seed, lo=1, hi=255):

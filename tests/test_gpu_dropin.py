@@ -1,0 +1,109 @@
+"""The reference's own applications (BFS.cu, SSSP.cu, PageRank.cu), compiled
+unmodified against include/olive/ (olive_b200/dropin.py), run on the GPU and
+compared with the reference checkers' golden outputs."""
+import glob
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+APPS = os.path.join(ROOT, "olive_b200", "_apps")
+FIXTURES = sorted(glob.glob(os.path.join(GOLDEN, "fixture_*.npz")))
+INF = oracle.INF
+
+
+def app(name):
+    p = os.path.join(APPS, name)
+    if not os.path.exists(p):
+        pytest.fail(f"{p} missing: build with python -m olive_b200.dropin (needs the "
+                    f"reference sources at build time)")
+    return p
+
+
+def run(name, args, cwd):
+    p = subprocess.run([app(name)] + [str(a) for a in args], cwd=cwd, capture_output=True,
+                       text=True, timeout=300)
+    assert p.returncode == 0, p.stderr[-2000:]
+    return p
+
+
+def _fid(p):
+    return os.path.basename(p)[8:-4]
+
+
+def edge_file(tmp_path, rowptr, col, w=None, name="g.txt"):
+    path = os.path.join(str(tmp_path), name)
+    oracle.write_edge_list(path, rowptr, col, w)
+    return path
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", FIXTURES, ids=_fid)
+def test_bfs_app(tmp_path, path):
+    z = np.load(path)
+    f = edge_file(tmp_path, z["sorted_rowptr"], z["sorted_col"])
+    sorted_input = np.array_equal(z["rowptr"], z["sorted_rowptr"])
+    for i, s in enumerate(z["bfs_sources"][:12]):
+        run("BFS", [f, "-s", s, "-round", 1000000], tmp_path)
+        got = np.loadtxt(os.path.join(str(tmp_path), "BFS.txt"), dtype=np.int64, ndmin=1)
+        if sorted_input:
+            want = z["bfs_levels"][i]
+        else:   # the reference mis-builds unsorted input; compare with the sorted CSR
+            want, _ = oracle.bfs(z["sorted_rowptr"], z["sorted_col"], int(s))
+        np.testing.assert_array_equal(got, want.astype(np.int64))
+
+
+@pytest.mark.gpu
+def test_bfs_app_grid_and_round_limit(tmp_path):
+    g = np.load(os.path.join(GOLDEN, "gen_grid_128x128.npz"))
+    rp, cl = oracle.grid_csr(128, 128)
+    f = edge_file(tmp_path, rp, cl)
+    run("BFS", [f, "-s", 0, "-round", 1000000, "-g", 4, "-scan"], tmp_path)
+    got = np.loadtxt(os.path.join(str(tmp_path), "BFS.txt"), dtype=np.int64)
+    np.testing.assert_array_equal(got, g["bfs_levels"][0].astype(np.int64))
+    # BFS.cu's default -round 100 stops after 101 supersteps (BFS.cu:86,142)
+    run("BFS", [f, "-s", 0], tmp_path)
+    got = np.loadtxt(os.path.join(str(tmp_path), "BFS.txt"), dtype=np.int64)
+    want = g["bfs_levels"][0].astype(np.int64)
+    want[want > 101] = INF
+    np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", FIXTURES, ids=_fid)
+def test_sssp_app_unit_weights(tmp_path, path):
+    """SSSP.cu sets every weight to 1 (SSSP.cu:131): distances are BFS levels."""
+    z = np.load(path)
+    f = edge_file(tmp_path, z["sorted_rowptr"], z["sorted_col"])
+    for s in z["bfs_sources"][:6]:
+        run("SSSP", [f, "-s", s, "-round", 1000000], tmp_path)
+        got = np.loadtxt(os.path.join(str(tmp_path), "SSSP.txt"), dtype=np.int64, ndmin=1)
+        want, _ = oracle.bfs(z["sorted_rowptr"], z["sorted_col"], int(s))
+        np.testing.assert_array_equal(got, want.astype(np.int64))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", FIXTURES, ids=_fid)
+def test_pagerank_app(tmp_path, path):
+    z = np.load(path)
+    if not np.array_equal(z["rowptr"], z["sorted_rowptr"]):
+        pytest.skip("testPageRank ran on the mis-built CSR of unsorted input")
+    f = edge_file(tmp_path, z["sorted_rowptr"], z["sorted_col"])
+    run("PageRank", [f, "-round", 1000], tmp_path)
+    got = np.loadtxt(os.path.join(str(tmp_path), "PageRank.txt"), dtype=np.float64, ndmin=1)
+    # both sides print "%f"; FP64 atomics may move the last printed digit
+    np.testing.assert_allclose(got, z["pr_ranks"], rtol=0, atol=1.01e-6)
+
+
+def test_csr_app_matches_reference_counts(tmp_path):
+    """testCsrGraph built on the header layer reports what the reference's does."""
+    for path in FIXTURES[:4]:
+        z = np.load(path)
+        f = edge_file(tmp_path, z["sorted_rowptr"], z["sorted_col"])
+        p = run("testCsrGraph", [f], tmp_path)
+        assert f"Nodes:{len(z['rowptr']) - 1} Edges:{len(z['col'])}" in p.stdout
