@@ -44,7 +44,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["sssp", "bfs", "pagerank"], default="sssp")
+    ap.add_argument("--workload", choices=["sssp", "bfs", "pagerank", "msbfs", "wpr", "batch"],
+                    default="sssp")
     ap.add_argument("--scale", type=int, default=None)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
@@ -52,7 +53,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     a = ap.parse_args()
     if a.scale is None:
-        a.scale = 22 if a.workload == "pagerank" else 24
+        a.scale = {"pagerank": 22, "wpr": 20, "batch": 0}.get(a.workload, 24)
     a.warmup = max(a.warmup, 3) if a.impl == "ours" else a.warmup
     return a
 
@@ -62,6 +63,15 @@ def metric_name(w, scale):
         return f"SSSP GTEPS, RMAT-{scale} ef16, uint32 weights U[1,255], src = max out-degree"
     if w == "bfs":
         return f"BFS GTEPS, RMAT-{scale} ef16, src = max out-degree"
+    if w == "msbfs":
+        return (f"64-source BFS aggregate GTEPS, RMAT-{scale} ef16, sources uniform over "
+                f"out-degree >= 1")
+    if w == "wpr":
+        return (f"weighted PageRank forward GE/s/iter, RMAT-{scale} ef16, lognormal FP32 weights; "
+                f"forward+adjoint time reported against forward time")
+    if w == "batch":
+        return ("512 ER graphs (V in [1K,64K], 8 edges/vertex) block-diagonal: BFS + K=32 PPR "
+                "per graph in one persistent launch, edge visits per second")
     return f"PageRank GE/s/iter, RMAT-{scale} ef16, alpha 0.85, FP32, dangling redistributed"
 
 
@@ -73,6 +83,9 @@ def workload_config(a, V=None, E=None, src=None, extra=None):
         c.update(weights="uint32 U[1,255], wseed 2", source=src)
     elif a.workload == "bfs":
         c.update(source=src)
+    elif a.workload == "msbfs":
+        c.update(sources="64 distinct, uniform over out-degree >= 1 (numpy seed 4)",
+                 output="int32 levels [64][V]")
     else:
         c.update(alpha=0.85, max_it=50, tol=1e-7, dangling="uniform")
     c["l2"] = "inputs larger than L2 (CSR/CSC arrays >= 1 GB per pass), no flush needed"
@@ -158,14 +171,25 @@ def run_ours(a, rank, world, local_rank):
     g.set_stream(stream)
     src, _ = g.max_degree_vertex()
     V, E = g.V, g.E
-    out = torch.empty(V, dtype=torch.float32 if a.workload == "pagerank" else torch.int32,
-                      device="cuda")
+    if a.workload == "msbfs":
+        rp, _, _ = g.csr()
+        deg = np.diff(rp.astype(np.int64))
+        srcs_np = np.random.default_rng(4).choice(np.flatnonzero(deg > 0), 64,
+                                                 replace=False).astype(np.uint32)
+        srcs = torch.from_numpy(srcs_np.astype(np.int32)).cuda()
+        src = srcs_np.tolist()
+        out = torch.empty((64, V), dtype=torch.int32, device="cuda")
+    else:
+        out = torch.empty(V, dtype=torch.float32 if a.workload == "pagerank" else torch.int32,
+                          device="cuda")
 
     def step(dst):
         if a.workload == "sssp":
             return g.sssp(src, out=dst)
         if a.workload == "bfs":
             return g.bfs(src, out=dst)
+        if a.workload == "msbfs":
+            return g.msbfs(srcs, out=dst)
         return g.pagerank(0.85, 50, 1e-7, out=dst)
 
     for _ in range(a.warmup):
@@ -205,6 +229,13 @@ def run_ours(a, rank, world, local_rank):
         unit = "GE/s/iter"
         alg_bytes = (8 * E + 20 * V) * st.iterations
         bytes_formula = "(8 B/edge + 20 B/vertex) per iteration"
+    elif a.workload == "msbfs":
+        units = st.edges_traversed
+        value = world * units / (ms_max * 1e-3) / 1e9
+        unit = "GTEPS"
+        alg_bytes = 4 * 64 * V + 12 * E + 24 * V * st.iterations
+        bytes_formula = ("4 B per output level (64 x V) + 12 B/edge (one pass: index + "
+                         "64-bit mask) + 24 B/vertex/level (visit, cur, next masks)")
     else:
         units = st.edges_traversed
         value = world * units / (ms_max * 1e-3) / 1e9
@@ -226,12 +257,14 @@ def run_ours(a, rank, world, local_rank):
         per_step = 2 + 5 * st.iterations + 1
     elif a.workload == "bfs":
         per_step = 2 + 6 * st.iterations
+    elif a.workload == "msbfs":
+        per_step = 2 + 6 * st.iterations
     else:
         per_step = 2 + 2 * st.iterations
     launches = per_step * a.steps
 
     # end to end through the public API: host (pinned) output buffer, D2H inside
-    host_out = torch.empty(V, dtype=out.dtype, pin_memory=True)
+    host_out = torch.empty(out.shape, dtype=out.dtype, pin_memory=True)
     step(host_out)
     x0 = torch.cuda.Event(enable_timing=True)
     x1 = torch.cuda.Event(enable_timing=True)
@@ -249,12 +282,33 @@ def run_ours(a, rank, world, local_rank):
         dist.all_reduce(t_e, op=dist.ReduceOp.MAX)
     e2e_ms = float(t_e.item())
     e2e = {"value": round(world * units / (e2e_ms * 1e-3) / 1e9, 3), "unit": unit,
-           "h2d_bytes_per_step": 0, "d2h_bytes_per_step": int(V * 4),
+           "h2d_bytes_per_step": 256 if a.workload == "msbfs" else 0,
+           "d2h_bytes_per_step": int(out.numel() * 4),
            "ms_per_step": round(e2e_ms, 4),
            "note": "olv_* call with a pinned host output buffer; the per-call input is the "
                    "source id passed by value; graph resident as after Oliver::readGraph"}
 
     extra = {}
+    if a.workload == "msbfs":
+        # the same 64 sources as 64 sequential plain BFS runs
+        lv = torch.empty(V, dtype=torch.int32, device="cuda")
+        for s0 in src[:3]:
+            g.bfs(s0, out=lv)
+        q0 = torch.cuda.Event(enable_timing=True)
+        q1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        q0.record(stream)
+        seq_edges = 0
+        for s0 in src:
+            g.bfs(s0, out=lv)
+            seq_edges += g.last_stats.edges_traversed
+        q1.record(stream)
+        torch.cuda.synchronize()
+        seq_ms = q0.elapsed_time(q1)
+        seq_gteps = seq_edges / (seq_ms * 1e-3) / 1e9
+        extra["sequential_plain"] = {"value": round(seq_gteps, 3), "unit": "GTEPS",
+                                     "ms_for_64": round(seq_ms, 3),
+                                     "speedup_of_batched": round(value / world / seq_gteps, 2)}
     # BFS on the same graph, reported beside the SSSP headline
     if a.workload == "sssp":
         lv = torch.empty(V, dtype=torch.int32, device="cuda")
@@ -309,6 +363,19 @@ def cpu_baseline(a, g, src, st):
                           f"({'complete' if done else 'stopped after %.0f s' % a.cpu_seconds}, "
                           f"{settled} vertices settled, {edges} edges scanned, {secs:.2f} s); "
                           f"the reference has no CPU SSSP"}
+    if a.workload == "msbfs":
+        edges, secs, runs = 0, 0.0, 0
+        for s0 in src:
+            e, t, _ = oracle.bfs_timed(rp, cl, s0, a.cpu_seconds)
+            edges += e
+            secs += t
+            runs += 1
+            if secs > a.cpu_seconds:
+                break
+        return {"value": round(edges / secs / 1e9, 5), "unit": "GTEPS", "cores": 1,
+                "kind": "port",
+                "sample": f"restatement of testBFS.cu:64-79 run sequentially for the first "
+                          f"{runs} of the 64 sources ({secs:.2f} s)"}
     if a.workload == "bfs":
         edges, secs, reached = oracle.bfs_timed(rp, cl, src, a.cpu_seconds)
         return {"value": round(edges / secs / 1e9, 5), "unit": "GTEPS", "cores": 1,
@@ -323,6 +390,233 @@ def cpu_baseline(a, g, src, st):
             "kind": "port",
             "sample": f"FP64 PageRank restating testPageRank.cu:74-104 (plus dangling "
                       f"redistribution), {it} iterations on the same graph, {secs:.2f} s"}
+
+
+def common_line(a, world, metric_unit, value, ms, dtype, data, config, roofline, cpu, e2e,
+                launches, clk, extra):
+    line = {"metric": metric_name(a.workload, a.scale), "value": round(value, 3),
+            "unit": metric_unit, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": dtype, "data": data, "config": config,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clk}
+    line.update(extra)
+    return line
+
+
+def timed(stream, fn, steps):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def max_over_ranks(x, world):
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_wpr(a, rank, world, local_rank):
+    """Weighted PageRank forward + adjoint on RMAT-20 (lognormal FP32 weights,
+    Dirichlet(1) personalisation, g ~ N(0,1)); a step is one forward and one
+    backward solve of 100 sweeps each."""
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    import olive_b200 as ob
+    stream = torch.cuda.current_stream()
+    g = ob.Graph.rmat(a.scale, 16, a.seed)
+    g.set_stream(stream)
+    V, E = g.V, g.E
+    rng = np.random.default_rng(7)
+    w = torch.from_numpy(rng.lognormal(0.0, 1.0, E).astype(np.float32)).cuda()
+    pn = rng.exponential(1.0, V)
+    p = torch.from_numpy((pn / pn.sum()).astype(np.float32)).cuda()
+    gv = torch.from_numpy(rng.standard_normal(V).astype(np.float32)).cuda()
+    r = torch.empty(V, dtype=torch.float32, device="cuda")
+    dw = torch.empty(E, dtype=torch.float32, device="cuda")
+    dp = torch.empty(V, dtype=torch.float32, device="cuda")
+    it = 100
+    g.wpr_forward(p, w=w, max_it=it, out=r)
+
+    def fwd():
+        g.wpr_forward(p, max_it=it, out=r)
+
+    def bwd():
+        g.wpr_backward(gv, max_it=it, dw_out=dw, dp_out=dp)
+
+    for _ in range(a.warmup):
+        fwd()
+        bwd()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    ms_f = max_over_ranks(timed(stream, fwd, a.steps), world)
+    ms_b = max_over_ranks(timed(stream, bwd, a.steps), world)
+    clk = clocks.stop()
+    fs = g.last_stats
+    units = E * it
+    value = world * units / (ms_f * 1e-3) / 1e9
+    peak, peak_src = peaks()
+    alg = (12 * E + 20 * V) * it
+    roofline = {"bound": "hbm", "achieved": round(alg / (ms_f * 1e-3) / 1e9, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(alg / (ms_f * 1e-3) / 1e9 / peak, 4),
+                "traffic": None, "kernel": "forward solve (100 pull sweeps, CUDA graph)",
+                "algorithmic_bytes": int(alg),
+                "bytes_formula": "(12 B/edge: CSC index, weight, r/W gather + 20 B/vertex) per sweep",
+                "peak_source": peak_src}
+    host_dw = torch.empty(E, dtype=torch.float32, pin_memory=True)
+    host_dp = torch.empty(V, dtype=torch.float32, pin_memory=True)
+    host_r = torch.empty(V, dtype=torch.float32, pin_memory=True)
+    host_p = p.cpu().pin_memory()
+    host_g = gv.cpu().pin_memory()
+
+    def e2e_step():
+        g.wpr_forward(host_p, max_it=it, out=host_r)
+        g.wpr_backward(host_g, max_it=it, dw_out=host_dw, dp_out=host_dp)
+
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        e2e_step()
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / a.steps, world)
+    e2e = {"value": round(world * units / (e2e_ms * 1e-3) / 1e9, 3), "unit": "GE/s/iter",
+           "h2d_bytes_per_step": 8 * V, "d2h_bytes_per_step": 4 * (E + 2 * V),
+           "ms_per_step": round(e2e_ms, 3),
+           "note": "forward + backward through olv_wpr_* with pinned host p, g, r, dw, dp"}
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        from oracle import oracle
+        rp, cl, _ = g.csr()
+        w64 = w.double().cpu().numpy()
+        t = time.perf_counter()
+        rr = oracle.wpr_forward(rp, cl, w64, p.double().cpu().numpy(), 0.85, 3)
+        secs = time.perf_counter() - t
+        cpu = {"value": round(E * 3 / secs / 1e9, 5), "unit": "GE/s/iter", "cores": 1,
+               "kind": "port", "sample": f"FP64 weighted PageRank forward (oracle), 3 sweeps, "
+                                         f"{secs:.2f} s"}
+    launches = (2 + 3 * it) + (5 + 3 * it)
+    config = workload_config(a, V, E, None, {
+        "weights": "lognormal(0,1) FP32, numpy seed 7", "p": "Dirichlet(1)", "g": "N(0,1)",
+        "alpha": 0.85, "sweeps": it, "forward_ms": round(ms_f, 3), "backward_ms": round(ms_b, 3)})
+    extra = {"fwd_bwd_over_fwd": round((ms_f + ms_b) / ms_f, 3),
+             "target": "forward+adjoint <= 3x forward"}
+    line = common_line(a, world, "GE/s/iter", value, ms_f + ms_b, "f32",
+                       "synthetic (seeded RMAT on the device, numpy weights)", config, roofline,
+                       cpu, e2e, launches * a.steps, clk, extra)
+    g.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_batch(a, rank, world, local_rank):
+    """512 ER digraphs packed block-diagonally; a step is one persistent launch
+    running BFS from local vertex 0 and K=32 PPR vectors (max 50 iterations,
+    tol 1e-7) for every graph."""
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    import olive_b200 as ob
+    stream = torch.cuda.current_stream()
+    count, K = 512, 32
+    g, off = ob.Graph.er_batch(count, 1024, 65536, 8, seed=a.seed)
+    g.set_stream(stream)
+    V, E = g.V, g.E
+    n = np.diff(off.astype(np.int64))
+    rng = np.random.default_rng(11)
+    seeds = np.stack([rng.integers(0, ni, K) for ni in n]).astype(np.uint32)
+    lv = torch.empty(V, dtype=torch.int32, device="cuda")
+    pr = torch.empty((V, K), dtype=torch.float32, device="cuda")
+
+    def step():
+        g.batch(off, seeds, K=K, alpha=0.85, max_it=50, tol=1e-7, levels_out=lv, ppr_out=pr)
+
+    for _ in range(a.warmup):
+        step()
+    st = g.last_stats
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    ms = max_over_ranks(timed(stream, step, a.steps), world)
+    clk = clocks.stop()
+    st = g.last_stats
+    visits = st.edges_traversed + st.edges_relaxed      # BFS edges + PPR edge-vectors
+    value = world * visits / (ms * 1e-3) / 1e9
+    peak, peak_src = peaks()
+    _, _, iters = g.batch(off, seeds, K=K, max_it=50, tol=1e-7, levels_out=lv, ppr_out=pr)
+    alg = 8 * st.edges_traversed + 4 * st.edges_relaxed + (4 + 8 * K) * V * 1
+    roofline = {"bound": "hbm", "achieved": round(alg / (ms * 1e-3) / 1e9, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(alg / (ms * 1e-3) / 1e9 / peak, 4), "traffic": None,
+                "kernel": "k_batch (one persistent launch)", "algorithmic_bytes": int(alg),
+                "bytes_formula": "8 B/BFS edge + 4 B per PPR edge-vector visit (128 B row per "
+                                 "in-edge for K=32) + (4 + 8K) B/vertex"}
+    host_lv = torch.empty(V, dtype=torch.int32, pin_memory=True)
+    host_pr = torch.empty((V, K), dtype=torch.float32, pin_memory=True)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        g.batch(off, seeds, K=K, max_it=50, tol=1e-7, levels_out=host_lv, ppr_out=host_pr)
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / a.steps, world)
+    e2e = {"value": round(world * visits / (e2e_ms * 1e-3) / 1e9, 3), "unit": "G visits/s",
+           "h2d_bytes_per_step": int(4 * (count + 1) + seeds.nbytes),
+           "d2h_bytes_per_step": int(4 * V * (1 + K)), "ms_per_step": round(e2e_ms, 3)}
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        from oracle import oracle
+        rp, cl, _ = g.csr()
+        t = time.perf_counter()
+        done, cvis = 0, 0
+        for i in range(count):
+            b0, b1 = int(off[i]), int(off[i + 1])
+            lrp = (rp[b0:b1 + 1] - rp[b0]).astype(np.uint32)
+            lcl = (cl[rp[b0]:rp[b1]] - b0).astype(np.uint32)
+            _, e = oracle.bfs(lrp, lcl, 0)
+            _, itn = oracle.ppr(lrp, lcl, seeds[i], 0.85, 50, 1e-7)
+            cvis += e + itn * len(lcl) * K
+            done += 1
+            if time.perf_counter() - t > a.cpu_seconds:
+                break
+        secs = time.perf_counter() - t
+        cpu = {"value": round(cvis / secs / 1e9, 5), "unit": "G visits/s", "cores": 1,
+               "kind": "port", "sample": f"oracle BFS + FP64 PPR-32 per instance, first {done} "
+                                         f"of {count} instances, {secs:.1f} s"}
+    config = {"workload": "batch-er512", "instances": count, "V_range": [1024, 65536],
+              "avg_degree": 8, "K": K, "alpha": 0.85, "max_it": 50, "tol": 1e-7,
+              "seed": a.seed, "V": V, "E": E, "ppr_iterations_mean": float(np.mean(iters)),
+              "parallelism": f"replicas x{world}",
+              "l2": "inputs larger than L2 (PPR state 2 x V x 128 B = 4.3 GB)"}
+    line = common_line(a, world, "G visits/s", value, ms, "f32+i32",
+                       "synthetic (seeded ER batch generated on the host)", config, roofline,
+                       cpu, e2e, a.steps, clk, {})
+    g.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 # ------------------------------------------------------------ reference --
@@ -347,6 +641,23 @@ def run_reference(a, rank, world):
                 vals.append(edges / secs / 1e9)
                 ms.append(secs * 1e3)
         unit, cores = "GTEPS", threads
+    elif a.workload == "msbfs":
+        deg = np.diff(rp.astype(np.int64))
+        srcs = np.random.default_rng(4).choice(np.flatnonzero(deg > 0), 64, replace=False)
+        desc = ("restatement of testBFS.cu:64-79 (serial queue BFS, 1 core) run once per source; "
+                f"each step the 64 sources in turn, stopped after {bound:.0f} s")
+        for i in range(a.warmup + a.steps):
+            edges, secs = 0, 0.0
+            for s0 in srcs:
+                e, t, _ = oracle.bfs_timed(rp, cl, int(s0), bound)
+                edges += e
+                secs += t
+                if secs > bound:
+                    break
+            if i >= a.warmup:
+                vals.append(edges / secs / 1e9)
+                ms.append(secs * 1e3)
+        unit, cores = "GTEPS", 1
     elif a.workload == "bfs":
         desc = ("restatement of testBFS.cu:64-79 (the reference's serial queue BFS; 1 core); "
                 f"each step a full traversal or stopped after {bound:.0f} s")
@@ -389,6 +700,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if a.impl == "reference":
         run_reference(a, rank, world)
+    elif a.workload == "wpr":
+        run_wpr(a, rank, world, local_rank)
+    elif a.workload == "batch":
+        run_batch(a, rank, world, local_rank)
     else:
         run_ours(a, rank, world, local_rank)
 

@@ -49,6 +49,7 @@ extern "C" {
 #define OLV_DANGLING_LEAK    1   /* drop it, as PageRank.cu:63-75 / testPageRank */
 
 typedef struct olv_graph olv_graph;
+typedef struct olv_wpr_ctx olv_wpr_ctx;
 
 typedef struct olv_stats {
     uint32_t iterations;        /* BFS/SSSP supersteps, PageRank iterations            */
@@ -93,6 +94,7 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
  *   "alpha"       BFS push->pull when m_f * alpha > m_unvisited     (14)
  *   "beta"        BFS pull->push when n_f * beta < V                (24)
  *   "sssp_delta"  SSSP bucket width, 0 = default                    (0)
+ *   "ms_alpha"    msBFS pull when active out-edges * ms_alpha > E   (4)
  *   "use_graphs"  run supersteps inside CUDA graphs (1) or a host loop (0)
  *   "levels_per_sync" host loop: supersteps enqueued per check      (4)  */
 int olv_tune_set(olv_graph *g, const char *key, double value);
@@ -106,6 +108,45 @@ int olv_bfs(olv_graph *g, uint32_t src, int32_t *level_out, olv_stats *st);
  * SSSP.cu:106-174 (atomicMin relaxation) with near/far bucketing.  uint32
  * distance, 0x7fffffff unreached.  Needs an OLV_W_U32 graph.                   */
 int olv_sssp(olv_graph *g, uint32_t src, uint32_t *dist_out, olv_stats *st);
+/* Multi-source BFS (no reference counterpart): n <= 64 sources advanced
+ * together with one 64-bit mask per vertex.  levels_out is [n][V] int32
+ * (row s = BFS levels from srcs[s], 0x7fffffff unreached), each row equal to
+ * olv_bfs from that source.  st->edges_traversed sums E_reached over sources. */
+int olv_msbfs(olv_graph *g, const uint32_t *srcs, int n, int32_t *levels_out, olv_stats *st);
+/* Batch of graphs packed block-diagonally (no reference counterpart).
+ * olv_graph_create_er_batch builds `count` Erdos-Renyi digraphs, instance i
+ * with V_i uniform in [vmin, vmax] and exactly avg_degree*V_i edges (no
+ * self-loops or duplicates), packed in one CSR; inst_offsets[count+1]
+ * receives the first global id of each instance.
+ * olv_batch_run runs, in ONE persistent kernel with a device work queue, a
+ * BFS from local vertex 0 of every instance (levels_out[V], levels relative
+ * to the instance) and/or K <= 32 personalised PageRank vectors per instance
+ * (seeds[count][K] local ids; ppr_out[V][K] FP32, vertex-major; dangling mass
+ * returns to the seed; stop after max_it or when every vector's L1 change
+ * < tol; ppr_iters_out[count] gets the iterations run).  Each instance's
+ * result equals a run of that instance alone.  Instances hold <= 65,536
+ * vertices.  Either output may be NULL.                                        */
+int olv_graph_create_er_batch(int count, uint32_t vmin, uint32_t vmax, uint32_t avg_degree,
+                              uint64_t seed, uint32_t *inst_offsets, olv_graph **out);
+int olv_batch_run(olv_graph *g, const uint32_t *inst_offsets, int count, int K,
+                  const uint32_t *seeds, double alpha, int max_it, double tol,
+                  int32_t *levels_out, float *ppr_out, uint32_t *ppr_iters_out, olv_stats *st);
+/* Differentiable weighted PageRank (no reference counterpart).  With
+ * W_u = sum_v w_uv and P_uv = w_uv / W_u (rows without out-edges are zero):
+ *   forward   r = (1-alpha) p + alpha P^T r           (pull over in-edges)
+ *   backward  lambda = g + alpha P lambda             (pull over out-edges)
+ *             dw_uv = alpha r_u (lambda_v - sum_x P_ux lambda_x) / W_u
+ *             dp    = (1-alpha) lambda                for L = sum_v g_v r_v.
+ * w (FP32, CSR order) replaces the graph's weights unless NULL (then the
+ * graph must hold FP32 weights).  Each solve runs max_it Jacobi sweeps or
+ * stops when the L1 change < tol.  *ctx is created on first use (pass a
+ * pointer to NULL) and keeps r and W for the backward pass: O(V+E) memory, no
+ * per-iteration tape.  dw_out is [E] in CSR order; dp_out may be NULL.       */
+int olv_wpr_forward(olv_graph *g, const float *w, const float *p, double alpha, int max_it,
+                    double tol, float *r_out, olv_wpr_ctx **ctx, olv_stats *st);
+int olv_wpr_backward(olv_wpr_ctx *ctx, const float *g, int max_it, double tol, float *dw_out,
+                     float *dp_out, olv_stats *st);
+int olv_wpr_ctx_destroy(olv_wpr_ctx *ctx);
 /* PageRank (PageRank.cu:89-147 / testPageRank.cu:41-115), FP32 ranks from a
  * deterministic pull over the reverse graph, FP64 residual.  Runs max_it
  * iterations or until the L1 residual < tol.                                  */

@@ -55,7 +55,15 @@ _SIGS = [
     ("olv_tune_get", _I, [_VP, ctypes.c_char_p, ctypes.POINTER(_D)]),
     ("olv_bfs", _I, [_VP, _U32, _VP, ctypes.POINTER(Stats)]),
     ("olv_sssp", _I, [_VP, _U32, _VP, ctypes.POINTER(Stats)]),
+    ("olv_msbfs", _I, [_VP, _VP, _I, _VP, ctypes.POINTER(Stats)]),
+    ("olv_graph_create_er_batch", _I, [_I, _U32, _U32, _U32, _U64, _VP, ctypes.POINTER(_VP)]),
+    ("olv_batch_run", _I, [_VP, _VP, _I, _I, _VP, _D, _I, _D, _VP, _VP, _VP,
+                           ctypes.POINTER(Stats)]),
     ("olv_pagerank", _I, [_VP, _D, _I, _D, _I, _VP, ctypes.POINTER(Stats)]),
+    ("olv_wpr_forward", _I, [_VP, _VP, _VP, _D, _I, _D, _VP, ctypes.POINTER(_VP),
+                             ctypes.POINTER(Stats)]),
+    ("olv_wpr_backward", _I, [_VP, _VP, _I, _D, _VP, _VP, ctypes.POINTER(Stats)]),
+    ("olv_wpr_ctx_destroy", _I, [_VP]),
 ]
 
 
@@ -135,6 +143,15 @@ class Graph:
         return cls(h)
 
     @classmethod
+    def er_batch(cls, count, vmin=1024, vmax=65536, avg_degree=8, seed=1):
+        """Block-diagonal batch of ER digraphs; returns (graph, inst_offsets)."""
+        off = np.zeros(count + 1, np.uint32)
+        h = _VP()
+        _check(lib().olv_graph_create_er_batch(count, vmin, vmax, avg_degree, seed, _ptr(off),
+                                               ctypes.byref(h)), "olv_graph_create_er_batch")
+        return cls(h), off
+
+    @classmethod
     def rmat(cls, scale, edge_factor=16, seed=1, weights=False, wseed=2):
         h = _VP()
         _check(lib().olv_graph_create_rmat(scale, edge_factor, seed, W_U32 if weights else W_NONE,
@@ -142,6 +159,9 @@ class Graph:
         return cls(h)
 
     def close(self):
+        if getattr(self, "_wctx", None):
+            lib().olv_wpr_ctx_destroy(self._wctx)
+            self._wctx = None
         if self._h:
             lib().olv_graph_destroy(self._h)
             self._h = None
@@ -183,8 +203,8 @@ class Graph:
         for k, v in kw.items():
             _check(lib().olv_tune_set(self._h, k.encode(), float(v)), f"olv_tune_set({k})")
         out = {}
-        for k in ("hub_degree", "piece", "alpha", "beta", "sssp_delta", "use_graphs",
-                  "levels_per_sync"):
+        for k in ("hub_degree", "piece", "alpha", "beta", "sssp_delta", "ms_alpha",
+                  "use_graphs", "levels_per_sync"):
             d = _D()
             _check(lib().olv_tune_get(self._h, k.encode(), ctypes.byref(d)), "olv_tune_get")
             out[k] = d.value
@@ -205,12 +225,81 @@ class Graph:
         self.last_stats = st
         return out
 
+    def msbfs(self, srcs, out=None):
+        """Levels from up to 64 sources at once: array [len(srcs), V] int32."""
+        if not hasattr(srcs, "data_ptr"):
+            srcs = np.ascontiguousarray(srcs, np.uint32)
+        n = len(srcs)
+        if out is None:
+            out = np.empty((n, self.V), np.int32)
+        st = Stats()
+        _check(lib().olv_msbfs(self._h, _ptr(srcs), n, _ptr(out), ctypes.byref(st)), "olv_msbfs")
+        self.last_stats = st
+        return out
+
+    def batch(self, inst_offsets, seeds=None, K=32, alpha=0.85, max_it=50, tol=1e-7,
+              bfs=True, levels_out=None, ppr_out=None):
+        """BFS from local vertex 0 and/or K-vector PPR of every instance, in one
+        persistent launch.  Returns (levels [V] or None, ppr [V, K] or None,
+        iterations per instance)."""
+        off = np.ascontiguousarray(inst_offsets, np.uint32)
+        count = len(off) - 1
+        V = int(off[-1])
+        lv = None
+        if bfs:
+            lv = np.empty(V, np.int32) if levels_out is None else levels_out
+        pr = None
+        if seeds is not None:
+            if not hasattr(seeds, "data_ptr"):
+                seeds = np.ascontiguousarray(seeds, np.uint32)
+            K = seeds.shape[1]
+            pr = np.empty((V, K), np.float32) if ppr_out is None else ppr_out
+        iters = np.zeros(count, np.uint32)
+        st = Stats()
+        _check(lib().olv_batch_run(self._h, _ptr(off), count, K, _ptr(seeds), alpha, max_it, tol,
+                                   _ptr(lv), _ptr(pr), _ptr(iters), ctypes.byref(st)),
+               "olv_batch_run")
+        self.last_stats = st
+        return lv, pr, iters
+
     def sssp(self, src, out=None):
         out = self._out(out, np.uint32)
         st = Stats()
         _check(lib().olv_sssp(self._h, src, _ptr(out), ctypes.byref(st)), "olv_sssp")
         self.last_stats = st
         return out
+
+    def wpr_forward(self, p, w=None, alpha=0.85, max_it=100, tol=0.0, out=None):
+        """Weighted PageRank r = (1-alpha) p + alpha P^T r; keeps a context for
+        wpr_backward.  w (FP32, CSR order) replaces the graph weights if given."""
+        def f32(a):
+            if a is None or hasattr(a, "data_ptr"):
+                return a
+            return np.ascontiguousarray(a, np.float32)
+        p, w = f32(p), f32(w)
+        out = np.empty(self.V, np.float32) if out is None else out
+        if not hasattr(self, "_wctx") or self._wctx is None:
+            self._wctx = _VP()
+        st = Stats()
+        _check(lib().olv_wpr_forward(self._h, _ptr(w), _ptr(p), alpha, max_it, tol, _ptr(out),
+                                     ctypes.byref(self._wctx), ctypes.byref(st)),
+               "olv_wpr_forward")
+        if w is not None:
+            self.weight_type = W_F32
+        self.last_stats = st
+        return out
+
+    def wpr_backward(self, g, max_it=100, tol=0.0, dw_out=None, dp_out=None):
+        """dL/dw [E] (CSR order) and dL/dp [V] for L = g . r of the last forward."""
+        if not hasattr(g, "data_ptr"):
+            g = np.ascontiguousarray(g, np.float32)
+        dw = np.empty(self.E, np.float32) if dw_out is None else dw_out
+        dp = np.empty(self.V, np.float32) if dp_out is None else dp_out
+        st = Stats()
+        _check(lib().olv_wpr_backward(self._wctx, _ptr(g), max_it, tol, _ptr(dw), _ptr(dp),
+                                      ctypes.byref(st)), "olv_wpr_backward")
+        self.last_stats = st
+        return dw, dp
 
     def pagerank(self, alpha=0.85, max_it=50, tol=1e-7, dangling="uniform", out=None):
         out = self._out(out, np.float32)

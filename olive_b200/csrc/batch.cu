@@ -1,0 +1,335 @@
+// Batched traversal of many small graphs packed block-diagonally in one CSR,
+// run by ONE persistent kernel with a device-side work queue (no reference
+// counterpart; each instance's result equals its solo run, bit for bit).
+//
+// Work items are (instance, task) pairs handed out by an atomic counter,
+// largest instances first.  A CTA runs its item to completion:
+//   BFS from the instance's local vertex 0 (testBFS.cu semantics, levels
+//     relative to the instance, 0x7fffffff unreached).  The visited, current
+//     and next frontier bitmaps of the instance live in shared memory
+//     (3 x 8 KB for up to 65,536 vertices); a thread per vertex expands the
+//     frontier with shared-memory atomicOr claims.
+//   PPR: K <= 32 personalised PageRank vectors with one-hot seeds (the
+//     oracle's orc_ppr definition: dangling mass returns to the seed), pulled
+//     over the in-edges with one warp per vertex and lane k = vector k, so
+//     each in-edge reads one 128-byte row.  Sums run in CSC order per lane
+//     and cross-warp reductions in a fixed order, so results do not depend on
+//     which CTA runs the item or when.  Stops after max_it iterations or when
+//     every vector's L1 change (FP64) is below tol.
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "olv_advance.cuh"
+#include "olv_internal.cuh"
+
+namespace olv {
+
+constexpr int kBatchThreads = 512;
+constexpr uint32_t kBatchMaxV = 65536;
+constexpr int kBatchWarps = kBatchThreads / 32;
+
+struct BatchArgs {
+    const uint32_t *rowptr, *col, *colptr, *rowidx;
+    const uint32_t *inst_off;
+    const uint32_t *order;       // instances, largest first
+    const uint32_t *seeds;       // [count][K] local ids
+    int count, K, max_it, tasks; // tasks: 1 = BFS only / PPR only, 2 = both
+    int do_bfs, do_ppr;
+    float alpha;
+    double tol;
+    int32_t *levels;             // [V]
+    float *ppr, *ppr_tmp;        // [V][K]
+    uint32_t *counter;           // work queue head
+    uint32_t *ppr_iters;         // [count]
+    unsigned long long *stats;   // [0] BFS edges traversed, [1] PPR edge visits, [2] error bits
+};
+
+__device__ void cta_bfs(const BatchArgs &a, uint32_t inst, uint32_t *bm) {
+    const uint32_t base = a.inst_off[inst], n = a.inst_off[inst + 1] - base;
+    const uint32_t words = (n + 31) / 32;
+    uint32_t *vis = bm, *cur = bm + kBatchMaxV / 32, *nxt = bm + 2 * (kBatchMaxV / 32);
+    __shared__ int s_any;
+    __shared__ unsigned long long s_edges;
+    for (uint32_t w = threadIdx.x; w < words; w += blockDim.x) {
+        vis[w] = 0;
+        cur[w] = 0;
+    }
+    for (uint32_t v = threadIdx.x; v < n; v += blockDim.x) a.levels[base + v] = kInf;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        vis[0] = 1u;
+        cur[0] = 1u;
+        a.levels[base] = 0;
+        s_edges = 0;
+    }
+    unsigned long long edges = 0;
+    for (int L = 0;; L++) {
+        for (uint32_t w = threadIdx.x; w < words; w += blockDim.x) nxt[w] = 0;
+        if (threadIdx.x == 0) s_any = 0;
+        __syncthreads();
+        int any = 0;
+        for (uint32_t u = threadIdx.x; u < n; u += blockDim.x) {
+            if (!((cur[u >> 5] >> (u & 31)) & 1u)) continue;
+            const uint32_t b = a.rowptr[base + u], e = a.rowptr[base + u + 1];
+            edges += e - b;
+            for (uint32_t i = b; i < e; i++) {
+                const uint32_t v = a.col[i] - base;
+                if (v >= n) {   // edge leaves the instance: not block-diagonal
+                    atomicOr((unsigned int *)&a.stats[2], 1u);
+                    continue;
+                }
+                const uint32_t bit = 1u << (v & 31);
+                if (vis[v >> 5] & bit) continue;
+                if (!(atomicOr(&vis[v >> 5], bit) & bit)) {
+                    atomicOr(&nxt[v >> 5], bit);
+                    a.levels[base + v] = L + 1;
+                    any = 1;
+                }
+            }
+        }
+        if (any) s_any = 1;
+        __syncthreads();
+        uint32_t *t = cur;
+        cur = nxt;
+        nxt = t;
+        const int go = s_any;
+        __syncthreads();
+        if (!go) break;
+    }
+    atomicAdd(&s_edges, edges);
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(&a.stats[0], s_edges);
+    __syncthreads();
+}
+
+__device__ void cta_ppr(const BatchArgs &a, uint32_t inst) {
+    const uint32_t base = a.inst_off[inst], n = a.inst_off[inst + 1] - base;
+    const int K = a.K;
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const bool lk = (int)lane < K;
+    const uint32_t seed = lk ? a.seeds[(size_t)inst * K + lane] : 0xffffffffu;
+    const float alpha = a.alpha;
+    __shared__ float s_d[kBatchWarps][32];
+    __shared__ double s_res[kBatchWarps][32];
+    __shared__ float s_dang[32];
+    __shared__ int s_stop;
+    float *r0 = a.ppr + (size_t)base * K, *r1 = a.ppr_tmp + (size_t)base * K;
+    for (uint32_t v = wid; v < n; v += kBatchWarps)
+        if (lk) r0[(size_t)v * K + lane] = (v == seed) ? 1.0f : 0.0f;
+    __syncthreads();
+    int it = 0;
+    unsigned long long visits = 0;
+    while (it < a.max_it) {
+        const float *src = (it & 1) ? r1 : r0;
+        float *dst = (it & 1) ? r0 : r1;
+        // dangling mass of each vector, fixed order: per warp, then warp 0..W-1
+        float d = 0.0f;
+        for (uint32_t u = wid; u < n; u += kBatchWarps)
+            if (a.rowptr[base + u + 1] == a.rowptr[base + u] && lk) d += src[(size_t)u * K + lane];
+        s_d[wid][lane] = d;
+        __syncthreads();
+        if (wid == 0) {
+            float t = 0.0f;
+            for (int w = 0; w < kBatchWarps; w++) t += s_d[w][lane];
+            s_dang[lane] = t;
+        }
+        __syncthreads();
+        const float dk = s_dang[lane];
+        double res = 0.0;
+        for (uint32_t v = wid; v < n; v += kBatchWarps) {
+            const uint32_t b = a.colptr[base + v], e = a.colptr[base + v + 1];
+            float acc = 0.0f;
+            for (uint32_t i = b; i < e; i++) {
+                const uint32_t u = a.rowidx[i];
+                if (u - base >= n) {   // edge enters from outside the instance
+                    if (lane == 0) atomicOr((unsigned int *)&a.stats[2], 2u);
+                    continue;
+                }
+                const float deg = (float)(a.rowptr[u + 1] - a.rowptr[u]);
+                if (lk) acc += __fdiv_rn(src[(size_t)(u - base) * K + lane], deg);
+            }
+            visits += e - b;
+            if (lk) {
+                const float tele = (v == seed) ? fmaf(alpha, dk, 1.0f - alpha) : 0.0f;
+                const float nv = fmaf(alpha, acc, tele);
+                res += fabs((double)nv - (double)src[(size_t)v * K + lane]);
+                dst[(size_t)v * K + lane] = nv;
+            }
+        }
+        s_res[wid][lane] = res;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double mx = 0.0;
+            for (int k = 0; k < K; k++) {
+                double t = 0.0;
+                for (int w = 0; w < kBatchWarps; w++) t += s_res[w][k];
+                mx = t > mx ? t : mx;
+            }
+            s_stop = mx < a.tol;
+        }
+        __syncthreads();
+        it++;
+        if (s_stop) break;
+    }
+    if (it & 1) {   // result is in the scratch copy
+        for (uint32_t v = wid; v < n; v += kBatchWarps)
+            if (lk) r0[(size_t)v * K + lane] = r1[(size_t)v * K + lane];
+    }
+    if (threadIdx.x == 0) a.ppr_iters[inst] = it;
+    if (lane == 0 && visits) atomicAdd(&a.stats[1], visits * (unsigned long long)K);
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kBatchThreads) k_batch(BatchArgs a) {
+    __shared__ uint32_t bm[3 * (kBatchMaxV / 32)];
+    __shared__ uint32_t s_item;
+    const uint32_t n_items = (uint32_t)a.count * a.tasks;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(a.counter, 1u);
+        __syncthreads();
+        const uint32_t item = s_item;
+        __syncthreads();
+        if (item >= n_items) break;
+        const uint32_t inst = a.order[item / a.tasks];
+        const bool bfs = a.tasks == 2 ? (item % 2 == 0) : (a.do_bfs != 0);
+        if (bfs)
+            cta_bfs(a, inst, bm);
+        else
+            cta_ppr(a, inst);
+    }
+}
+
+struct BatchState {
+    DevBuf off, order, seeds, tmp, counter, iters, stats, levels, ppr;
+    ~BatchState() {
+        off.release(); order.release(); seeds.release(); tmp.release(); counter.release();
+        iters.release(); stats.release(); levels.release(); ppr.release();
+    }
+};
+
+}  // namespace olv
+
+using namespace olv;
+
+extern "C" int olv_batch_run(olv_graph *g, const uint32_t *inst_offsets, int count, int K,
+                             const uint32_t *seeds, double alpha, int max_it, double tol,
+                             int32_t *levels_out, float *ppr_out, uint32_t *ppr_iters_out,
+                             olv_stats *st) {
+    OLV_CHECK_ARG(g && inst_offsets, "olv_batch_run: null pointer");
+    OLV_CHECK_ARG(count >= 1, "olv_batch_run: count must be >= 1");
+    OLV_CHECK_ARG(levels_out || ppr_out, "olv_batch_run: nothing to compute");
+    OLV_CHECK_ARG(!ppr_out || (seeds && K >= 1 && K <= 32),
+                  "olv_batch_run: PPR needs seeds and 1 <= K <= 32");
+    OLV_CHECK_ARG(alpha >= 0 && alpha < 1 && max_it >= 0, "olv_batch_run: bad alpha / max_it");
+    std::vector<uint32_t> off(count + 1);
+    if (is_device_ptr(inst_offsets))
+        OLV_CUDA(cudaMemcpy(off.data(), inst_offsets, (count + 1) * 4, cudaMemcpyDeviceToHost));
+    else
+        memcpy(off.data(), inst_offsets, (count + 1) * 4);
+    OLV_CHECK_ARG(off[count] <= g->V, "olv_batch_run: offsets exceed the graph");
+    for (int i = 0; i < count; i++) {
+        OLV_CHECK_ARG(off[i + 1] > off[i], "olv_batch_run: empty or decreasing instance %d", i);
+        if (off[i + 1] - off[i] > kBatchMaxV) {
+            set_error("olv_batch_run: instance %d has %u vertices (limit %u)", i,
+                      off[i + 1] - off[i], kBatchMaxV);
+            return OLV_ERR_LIMIT;
+        }
+    }
+    const int K_ = ppr_out ? K : 0;
+    std::vector<uint32_t> hseeds;
+    if (ppr_out) {
+        hseeds.resize((size_t)count * K);
+        if (is_device_ptr(seeds))
+            OLV_CUDA(cudaMemcpy(hseeds.data(), seeds, hseeds.size() * 4, cudaMemcpyDeviceToHost));
+        else
+            memcpy(hseeds.data(), seeds, hseeds.size() * 4);
+        for (int i = 0; i < count; i++)
+            for (int k = 0; k < K; k++)
+                OLV_CHECK_ARG(hseeds[(size_t)i * K + k] < off[i + 1] - off[i],
+                              "olv_batch_run: seed %d of instance %d out of range", k, i);
+    }
+    // largest instances first
+    std::vector<uint32_t> order(count);
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+        return off[x + 1] - off[x] > off[y + 1] - off[y];
+    });
+    BatchState bs;
+    cudaStream_t s = g->stream;
+    const size_t V = off[count];
+    OLV_TRY(bs.off.ensure((count + 1) * 4));
+    OLV_TRY(bs.order.ensure(count * 4));
+    OLV_TRY(bs.counter.ensure(16));
+    OLV_TRY(bs.iters.ensure(count * 4 + 16));
+    OLV_TRY(bs.stats.ensure(32));
+    OLV_CUDA(cudaMemcpyAsync(bs.off.p, off.data(), (count + 1) * 4, cudaMemcpyHostToDevice, s));
+    OLV_CUDA(cudaMemcpyAsync(bs.order.p, order.data(), count * 4, cudaMemcpyHostToDevice, s));
+    const bool dev_lv = levels_out && is_device_ptr(levels_out);
+    const bool dev_pr = ppr_out && is_device_ptr(ppr_out);
+    if (levels_out && !dev_lv) OLV_TRY(bs.levels.ensure(V * 4));
+    if (ppr_out) {
+        OLV_TRY(bs.seeds.ensure(hseeds.size() * 4));
+        OLV_CUDA(cudaMemcpyAsync(bs.seeds.p, hseeds.data(), hseeds.size() * 4,
+                                 cudaMemcpyHostToDevice, s));
+        OLV_TRY(bs.tmp.ensure(V * K * 4));
+        if (!dev_pr) OLV_TRY(bs.ppr.ensure(V * K * 4));
+    }
+    BatchArgs a;
+    a.rowptr = g->rowptr.as<uint32_t>();
+    a.col = g->col.as<uint32_t>();
+    a.colptr = g->colptr.as<uint32_t>();
+    a.rowidx = g->rowidx.as<uint32_t>();
+    a.inst_off = bs.off.as<uint32_t>();
+    a.order = bs.order.as<uint32_t>();
+    a.seeds = bs.seeds.as<uint32_t>();
+    a.count = count;
+    a.K = K_;
+    a.max_it = max_it;
+    a.do_bfs = levels_out != nullptr;
+    a.do_ppr = ppr_out != nullptr;
+    a.tasks = a.do_bfs + a.do_ppr;
+    a.alpha = (float)alpha;
+    a.tol = tol;
+    a.levels = levels_out ? (dev_lv ? levels_out : bs.levels.as<int32_t>()) : nullptr;
+    a.ppr = ppr_out ? (dev_pr ? ppr_out : bs.ppr.as<float>()) : nullptr;
+    a.ppr_tmp = bs.tmp.as<float>();
+    a.counter = bs.counter.as<uint32_t>();
+    a.ppr_iters = bs.iters.as<uint32_t>();
+    a.stats = bs.stats.as<unsigned long long>();
+    int per_sm = 0;
+    OLV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, kBatchThreads, 0));
+    const int grid = std::max(1, per_sm) * g->num_sms;
+    OLV_CUDA(cudaEventRecord(g->ev0, s));
+    OLV_CUDA(cudaMemsetAsync(bs.counter.p, 0, 16, s));
+    OLV_CUDA(cudaMemsetAsync(bs.stats.p, 0, 32, s));
+    k_batch<<<grid, kBatchThreads, 0, s>>>(a);
+    OLV_CUDA(cudaGetLastError());
+    OLV_CUDA(cudaEventRecord(g->ev1, s));
+    unsigned long long hst[3];
+    OLV_CUDA(cudaMemcpyAsync(hst, bs.stats.p, 24, cudaMemcpyDeviceToHost, s));
+    if (levels_out && !dev_lv)
+        OLV_CUDA(cudaMemcpyAsync(levels_out, a.levels, V * 4, cudaMemcpyDeviceToHost, s));
+    if (ppr_out && !dev_pr)
+        OLV_CUDA(cudaMemcpyAsync(ppr_out, a.ppr, V * K * 4, cudaMemcpyDeviceToHost, s));
+    if (ppr_iters_out)
+        OLV_CUDA(cudaMemcpyAsync(ppr_iters_out, bs.iters.p, count * 4, cudaMemcpyDefault, s));
+    OLV_CUDA(cudaStreamSynchronize(s));
+    if (hst[2]) {
+        set_error("olv_batch_run: the graph is not block-diagonal under inst_offsets "
+                  "(edges cross instances; code %llu)", hst[2]);
+        return OLV_ERR_ARG;
+    }
+    if (st) {
+        float ms = 0;
+        OLV_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+        st->iterations = (uint32_t)count;
+        st->pull_steps = 0;
+        st->vertices_reached = V;
+        st->edges_traversed = hst[0];   // BFS: out-edges of reached vertices, all instances
+        st->edges_relaxed = hst[1];     // PPR: in-edge visits x K, all iterations
+        st->residual = 0;
+        st->device_ms = ms;
+    }
+    return OLV_OK;
+}

@@ -28,6 +28,7 @@
 namespace olv {
 
 struct BfsPushOp {
+    using SV = uint32_t;
     static constexpr bool kHasFar = false;
     const uint32_t *rowptr;
     int32_t *level;

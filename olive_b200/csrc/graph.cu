@@ -431,6 +431,8 @@ int olv_graph_destroy(olv_graph *g) {
     g->outdeg_f.release();
     g->ws.release();
     release_pr_state(g);
+    release_ms_state(g);
+    release_wpr_state(g);
     for (WhileGraph **wg : {&g->bfs_graph, &g->sssp_graph}) {
         if (*wg) {
             (*wg)->destroy();
@@ -499,6 +501,9 @@ int olv_tune_set(olv_graph *g, const char *key, double value) {
     } else if (!strcmp(key, "sssp_delta")) {
         OLV_CHECK_ARG(value >= 0 && value < 2147483647.0, "olv_tune_set: bad sssp_delta");
         t.sssp_delta = (uint32_t)value;
+    } else if (!strcmp(key, "ms_alpha")) {
+        OLV_CHECK_ARG(value > 0, "olv_tune_set: ms_alpha must be > 0");
+        t.ms_alpha = (float)value;
     } else if (!strcmp(key, "use_graphs")) {
         t.use_graphs = value != 0;
     } else if (!strcmp(key, "levels_per_sync")) {
@@ -511,6 +516,7 @@ int olv_tune_set(olv_graph *g, const char *key, double value) {
     // launch parameters are baked into the cached superstep graphs
     for (WhileGraph *wg : {g->bfs_graph, g->sssp_graph})
         if (wg) wg->destroy();
+    release_ms_state(g);
     return OLV_OK;
 }
 
@@ -522,6 +528,7 @@ int olv_tune_get(const olv_graph *g, const char *key, double *value) {
     else if (!strcmp(key, "alpha")) *value = t.alpha;
     else if (!strcmp(key, "beta")) *value = t.beta;
     else if (!strcmp(key, "sssp_delta")) *value = t.sssp_delta;
+    else if (!strcmp(key, "ms_alpha")) *value = t.ms_alpha;
     else if (!strcmp(key, "use_graphs")) *value = t.use_graphs;
     else if (!strcmp(key, "levels_per_sync")) *value = t.levels_per_sync;
     else {

@@ -1,0 +1,359 @@
+// Multi-source BFS: up to 64 sources advanced together with one uint64 mask
+// per vertex (bit s = source s).  No reference counterpart; each source's
+// levels equal a plain BFS from it (testBFS.cu:42-87 semantics, int32 levels,
+// 0x7fffffff unreached).
+//
+// Per vertex: visit (sources that reached it), cur (sources whose frontier
+// holds it this level), next (sources reaching it next level).  A level is
+//   push  (few active vertices): for each active u and out-edge u->v,
+//         atomicOr(next[v], cur[u] & ~visit[v])   -- the shared chunk/piece
+//         advance of olv_advance.cuh with a 64-bit source value;
+//   pull  (large frontier): each vertex with unvisited bits ORs cur[] over its
+//         in-edges, stopping once every missing source is found;
+//   apply (dense pass): new = next & ~visit; visit |= new; cur = new; the
+//         level of each new (source, vertex) pair is written straight into
+//         the [n][V] output; vertices with new bits form the next active queue.
+// A final pass writes 0x7fffffff for pairs never reached, so every output
+// element is written exactly once.  Levels run in a CUDA graph as for BFS.
+#include <string.h>
+
+#include <vector>
+
+#include "olv_advance.cuh"
+#include "olv_graphexec.cuh"
+#include "olv_internal.cuh"
+
+namespace olv {
+
+int traversal_workspace(olv_graph *g, bool pieces);
+
+struct MsState {
+    DevBuf masks;     // visit | cur | next, V words each
+    DevBuf srcs;
+    WhileGraph graph;
+    int32_t *graph_levels = nullptr;
+    uint32_t graph_n = 0;
+    ~MsState() {
+        masks.release();
+        srcs.release();
+        graph.destroy();
+    }
+};
+
+struct MsPushOp {
+    using SV = unsigned long long;
+    static constexpr bool kHasFar = false;
+    const unsigned long long *cur;
+    const unsigned long long *visit;
+    unsigned long long *next;
+    struct Pre {
+        unsigned long long bits;
+    };
+    __device__ __forceinline__ void begin(TravCtl *) {}
+    __device__ __forceinline__ SV src_value(uint32_t u) const { return cur[u]; }
+    __device__ __forceinline__ Pre prepare(SV sv, uint32_t, uint32_t v) const {
+        return Pre{sv & ~__ldg(&visit[v])};
+    }
+    __device__ __forceinline__ int apply(const Pre &p, uint32_t v) {
+        if (p.bits) atomicOr(&next[v], p.bits);
+        return 0;
+    }
+    __device__ __forceinline__ void on_push(bool, uint32_t) {}
+    __device__ __forceinline__ void flush(unsigned long long) {}
+};
+
+__device__ __forceinline__ void write_levels(int32_t *levels, uint64_t V, uint32_t v,
+                                             unsigned long long bits, int32_t value) {
+    while (bits) {
+        const int s = __ffsll((long long)bits) - 1;
+        bits &= bits - 1;
+        levels[(uint64_t)s * V + v] = value;
+    }
+}
+
+__global__ void k_ms_init(TravCtl *c, int32_t *levels, const uint32_t *srcs, int n, uint32_t V,
+                          const uint32_t *rowptr, unsigned long long *visit,
+                          unsigned long long *cur, uint32_t *q0) {
+    __shared__ unsigned long long s_edges;
+    if (threadIdx.x == 0) {
+        TravCtl t = {};
+        t.vdata = levels;
+        *c = t;
+        s_edges = 0;
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < n) {
+        const uint32_t u = srcs[threadIdx.x];
+        const unsigned long long bit = 1ULL << threadIdx.x;
+        const unsigned long long old = atomicOr(&cur[u], bit);
+        atomicOr(&visit[u], bit);
+        levels[(uint64_t)threadIdx.x * V + u] = 0;
+        const uint32_t d = rowptr[u + 1] - rowptr[u];
+        atomicAdd(&s_edges, (unsigned long long)d);
+        if (old == 0) {
+            const uint32_t pos = atomicAdd(&c->qsize[0], 1u);
+            q0[pos] = u;
+            atomicAdd(&c->m_f, (unsigned long long)d);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) c->edges_traversed = s_edges;
+}
+
+__global__ void k_ms_begin(TravCtl *c, unsigned long long E, float alpha) {
+    if (c->done) return;
+    if (c->qsize[c->cur] == 0) {
+        c->done = 1;
+        return;
+    }
+    c->mode = ((double)c->m_f * alpha > (double)E) ? 1u : 0u;
+    c->qsize[c->cur ^ 1] = 0;
+    c->npieces = 0;
+    c->m_next = 0;
+}
+
+constexpr int kMsParents = 4;
+
+__global__ void __launch_bounds__(kBlock)
+k_ms_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowidx, uint32_t V,
+          unsigned long long srcmask, const TravCtl *c, const unsigned long long *__restrict__ visit,
+          const unsigned long long *__restrict__ cur, unsigned long long *__restrict__ next) {
+    if (c->done || c->mode != 1) return;
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+         v += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned long long todo = ~visit[v] & srcmask;
+        if (!todo) continue;
+        const uint32_t b = __ldg(&colptr[v]), e = __ldg(&colptr[v + 1]);
+        unsigned long long acc = 0;
+        for (uint32_t i = b; i < e; i += kMsParents) {
+            uint32_t u[kMsParents];
+#pragma unroll
+            for (int j = 0; j < kMsParents; j++) u[j] = i + j < e ? __ldg(&rowidx[i + j]) : 0xffffffffu;
+#pragma unroll
+            for (int j = 0; j < kMsParents; j++)
+                if (u[j] != 0xffffffffu) acc |= __ldg(&cur[u[j]]);
+            if ((acc & todo) == todo) break;
+        }
+        if (acc & todo) next[v] = acc & todo;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_ms_apply(uint32_t V, TravCtl *c, const uint32_t *__restrict__ rowptr,
+           unsigned long long *__restrict__ visit, unsigned long long *__restrict__ cur,
+           unsigned long long *__restrict__ next, uint32_t *q0, uint32_t *q1) {
+    if (c->done) return;
+    int32_t *levels = static_cast<int32_t *>(c->vdata);
+    const int32_t lv = (int32_t)c->level + 1;
+    uint32_t *qout = c->cur ? q0 : q1;
+    uint32_t *qsz = &c->qsize[c->cur ^ 1];
+    unsigned long long m_next = 0, traversed = 0;
+    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V;
+         base += (uint64_t)gridDim.x * kBlock) {
+        const uint64_t v = base + threadIdx.x;
+        bool act = false;
+        if (v < V) {
+            const unsigned long long nx = next[v], oc = cur[v];
+            unsigned long long nw = 0;
+            if (nx) {
+                const unsigned long long vis = visit[v];
+                nw = nx & ~vis;
+                next[v] = 0;
+                if (nw) {
+                    visit[v] = vis | nw;
+                    write_levels(levels, V, (uint32_t)v, nw, lv);
+                    const uint32_t d = __ldg(&rowptr[v + 1]) - __ldg(&rowptr[v]);
+                    m_next += d;
+                    traversed += (unsigned long long)d * __popcll(nw);
+                    act = true;
+                }
+            }
+            if (oc != nw) cur[v] = nw;
+        }
+        warp_push(act, (uint32_t)v, qout, qsz);
+    }
+    warp_add64(m_next, &c->m_next);
+    warp_add64(traversed, &c->edges_traversed);
+}
+
+__global__ void k_ms_end(TravCtl *c, cudaGraphConditionalHandle h, int use_cond, uint32_t V) {
+    if (!c->done) {
+        if (c->mode) c->pull_steps++;
+        c->m_f = c->m_next;
+        c->cur ^= 1;
+        c->level++;
+        c->steps++;
+        if (c->qsize[c->cur] == 0) c->done = 1;
+        if (c->steps > V + 1) {
+            c->err = 1;
+            c->done = 1;
+        }
+    }
+    if (use_cond) cudaGraphSetConditional(h, c->done ? 0u : 1u);
+}
+
+// 0x7fffffff for every (source, vertex) pair the traversal did not reach;
+// counts reached pairs.
+__global__ void __launch_bounds__(kBlock)
+k_ms_finish(uint32_t V, unsigned long long srcmask, TravCtl *c,
+            const unsigned long long *__restrict__ visit) {
+    int32_t *levels = static_cast<int32_t *>(c->vdata);
+    unsigned long long reached = 0;
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+         v += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned long long vis = visit[v] & srcmask;
+        reached += __popcll(vis);
+        write_levels(levels, V, (uint32_t)v, ~vis & srcmask, kInf);
+    }
+    warp_add64(reached, &c->reached);
+}
+
+// ------------------------------------------------------------------ host --
+template <class Sink>
+static int ms_superstep(olv_graph *g, MsState &ms, Sink &&sink, cudaGraphConditionalHandle h,
+                        int use_cond, unsigned long long srcmask) {
+    TravCtl *ctl = g->ws.ctl.as<TravCtl>();
+    uint32_t V = g->V;
+    unsigned long long E = g->E;
+    float alpha = g->tune.ms_alpha;
+    unsigned long long *visit = ms.masks.as<unsigned long long>();
+    unsigned long long *cur = visit + V;
+    unsigned long long *next = cur + V;
+    AdvanceArgs a;
+    a.rowptr = g->rowptr.as<uint32_t>();
+    a.col = g->col.as<uint32_t>();
+    a.ctl = ctl;
+    a.q0 = g->ws.q0.as<uint32_t>();
+    a.q1 = g->ws.q1.as<uint32_t>();
+    a.far0 = a.far1 = nullptr;
+    a.pieces = g->ws.pieces.as<uint2>();
+    a.hub_degree = g->tune.hub_degree;
+    a.piece = g->tune.piece;
+    a.want_mode = 0;
+    MsPushOp op;
+    op.cur = cur;
+    op.visit = visit;
+    op.next = next;
+    const uint32_t *colptr = g->colptr.as<uint32_t>();
+    const uint32_t *rowidx = g->rowidx.as<uint32_t>();
+    const uint32_t *rowptr = a.rowptr;
+    const TravCtl *cctl = ctl;
+    const unsigned long long *cvisit = visit, *ccur = cur;
+    uint32_t *q0 = a.q0, *q1 = a.q1;
+    const int nb = g->persist_blocks;
+    void *a_begin[] = {&ctl, &E, &alpha};
+    OLV_TRY(sink((const void *)k_ms_begin, dim3(1), dim3(1), a_begin));
+    void *a_adv[] = {&a, &op};
+    OLV_TRY(sink((const void *)k_advance_chunks<MsPushOp>, dim3(nb), dim3(kBlock), a_adv));
+    OLV_TRY(sink((const void *)k_advance_pieces<MsPushOp>, dim3(nb), dim3(kBlock), a_adv));
+    void *a_pull[] = {&colptr, &rowidx, &V, &srcmask, &cctl, &cvisit, &ccur, &next};
+    OLV_TRY(sink((const void *)k_ms_pull, dim3(nb), dim3(kBlock), a_pull));
+    void *a_apply[] = {&V, &ctl, &rowptr, &visit, &cur, &next, &q0, &q1};
+    OLV_TRY(sink((const void *)k_ms_apply, dim3(nb), dim3(kBlock), a_apply));
+    void *a_end[] = {&ctl, &h, &use_cond, &V};
+    OLV_TRY(sink((const void *)k_ms_end, dim3(1), dim3(1), a_end));
+    return OLV_OK;
+}
+
+static MsState *ms_state(olv_graph *g) {
+    if (!g->ms_state) g->ms_state = new MsState();
+    return static_cast<MsState *>(g->ms_state);
+}
+
+void release_ms_state(olv_graph *g) {
+    delete static_cast<MsState *>(g->ms_state);
+    g->ms_state = nullptr;
+}
+
+}  // namespace olv
+
+using namespace olv;
+
+extern "C" int olv_msbfs(olv_graph *g, const uint32_t *srcs, int n, int32_t *levels_out,
+                         olv_stats *st) {
+    OLV_CHECK_ARG(g && srcs && levels_out, "olv_msbfs: null pointer");
+    OLV_CHECK_ARG(n >= 1 && n <= 64, "olv_msbfs: n=%d sources, must be in [1,64]", n);
+    const bool dev_src = is_device_ptr(srcs);
+    std::vector<uint32_t> hs(n);
+    if (dev_src) {
+        OLV_CUDA(cudaMemcpy(hs.data(), srcs, n * 4, cudaMemcpyDeviceToHost));
+    } else {
+        memcpy(hs.data(), srcs, n * 4);
+    }
+    for (int i = 0; i < n; i++)
+        OLV_CHECK_ARG(hs[i] < g->V, "olv_msbfs: source %u out of range (V=%u)", hs[i], g->V);
+    OLV_TRY(traversal_workspace(g, true));
+    MsState &ms = *ms_state(g);
+    const size_t V = g->V;
+    OLV_TRY(ms.masks.ensure(V * 24 + 64));
+    OLV_TRY(ms.srcs.ensure(64 * 4));
+    const bool dev_out = is_device_ptr(levels_out);
+    const size_t out_bytes = (size_t)n * V * 4;
+    DevBuf tmp_out;
+    if (!dev_out) OLV_TRY(tmp_out.ensure(out_bytes));
+    int32_t *levels = dev_out ? levels_out : tmp_out.as<int32_t>();
+    cudaStream_t s = g->stream;
+    const unsigned long long srcmask = n == 64 ? ~0ULL : ((1ULL << n) - 1);
+    TravCtl *ctl = g->ws.ctl.as<TravCtl>();
+    unsigned long long *visit = ms.masks.as<unsigned long long>();
+
+    OLV_CUDA(cudaEventRecord(g->ev0, s));
+    OLV_CUDA(cudaMemcpyAsync(ms.srcs.p, hs.data(), n * 4, cudaMemcpyHostToDevice, s));
+    OLV_CUDA(cudaMemsetAsync(ms.masks.p, 0, V * 24, s));
+    k_ms_init<<<1, 64, 0, s>>>(ctl, levels, ms.srcs.as<uint32_t>(), n, g->V,
+                               g->rowptr.as<uint32_t>(), visit, visit + V, g->ws.q0.as<uint32_t>());
+    OLV_CUDA(cudaGetLastError());
+    bool launched = false;
+    if (g->tune.use_graphs) {
+        if (!ms.graph.ready || ms.graph_n != (uint32_t)n) {
+            int r = ms.graph.begin();
+            auto sink = [&](const void *f, dim3 gr, dim3 bl, void **args) {
+                return ms.graph.add(f, gr, bl, args);
+            };
+            if (r == OLV_OK) r = ms_superstep(g, ms, sink, ms.graph.handle, 1, srcmask);
+            if (r == OLV_OK) r = ms.graph.finish();
+            if (r != OLV_OK) ms.graph.destroy();
+            ms.graph_n = n;
+        }
+        if (ms.graph.ready) {
+            OLV_TRY(ms.graph.launch(s));
+            launched = true;
+        }
+    }
+    if (!launched) {
+        auto launch = [&](const void *f, dim3 gr, dim3 bl, void **args) {
+            OLV_CUDA(cudaLaunchKernel(f, gr, bl, args, 0, s));
+            return OLV_OK;
+        };
+        for (;;) {
+            for (int i = 0; i < g->tune.levels_per_sync; i++)
+                OLV_TRY(ms_superstep(g, ms, launch, 0, 0, srcmask));
+            OLV_CUDA(cudaMemcpyAsync(g->host_ctl, ctl, sizeof(TravCtl), cudaMemcpyDeviceToHost, s));
+            OLV_CUDA(cudaStreamSynchronize(s));
+            if (g->host_ctl->done) break;
+        }
+    }
+    k_ms_finish<<<g->persist_blocks, kBlock, 0, s>>>(g->V, srcmask, ctl, visit);
+    OLV_CUDA(cudaGetLastError());
+    OLV_CUDA(cudaEventRecord(g->ev1, s));
+    OLV_CUDA(cudaMemcpyAsync(g->host_ctl, ctl, sizeof(TravCtl), cudaMemcpyDeviceToHost, s));
+    if (!dev_out) OLV_CUDA(cudaMemcpyAsync(levels_out, levels, out_bytes, cudaMemcpyDeviceToHost, s));
+    OLV_CUDA(cudaStreamSynchronize(s));
+    const TravCtl &h = *g->host_ctl;
+    if (h.err) {
+        set_error("olv_msbfs: device-side check failed (code %u)", h.err);
+        return OLV_ERR_STATE;
+    }
+    if (st) {
+        float ms_ = 0;
+        OLV_CUDA(cudaEventElapsedTime(&ms_, g->ev0, g->ev1));
+        st->iterations = h.steps;
+        st->pull_steps = h.pull_steps;
+        st->vertices_reached = h.reached;          // reached (source, vertex) pairs
+        st->edges_traversed = h.edges_traversed;   // sum over sources of E_reached
+        st->edges_relaxed = h.edges_traversed;
+        st->residual = 0;
+        st->device_ms = ms_;
+    }
+    return OLV_OK;
+}

@@ -12,8 +12,8 @@
 // An Op supplies the per-edge work, split so that a thread can keep several
 // edges' loads in flight before it issues their atomics:
 //   void begin(TravCtl *c)                          load per-superstep values
-//   uint32_t src_value(uint32_t u)                  value carried from the source
-//   Pre prepare(uint32_t sv, uint32_t e, uint32_t v)   plain loads for one edge
+//   SV src_value(uint32_t u)                        value carried from the source
+//   Pre prepare(SV sv, uint32_t e, uint32_t v)      plain loads for one edge
 //   int apply(const Pre &p, uint32_t v)             0: nothing, 1: push v to the
 //                                                   output queue, 2: push to the
 //                                                   secondary (far) queue
@@ -129,15 +129,17 @@ __global__ void __launch_bounds__(kBlock) k_advance_chunks(AdvanceArgs a, Op op)
     uint32_t *__restrict__ far = c->far_cur ? a.far1 : a.far0;
     uint32_t *far_size = &c->far_size[c->far_cur];
 
+    using SV = typename Op::SV;
     __shared__ uint32_t s_beg[kBlock];
     __shared__ uint32_t s_off[kBlock];
-    __shared__ uint32_t s_val[kBlock];
+    __shared__ SV s_val[kBlock];
     __shared__ uint32_t s_warp[33];
 
     unsigned long long relaxed = 0;
     for (uint32_t chunk = blockIdx.x; (uint64_t)chunk * kBlock < n; chunk += gridDim.x) {
         const uint32_t i = chunk * kBlock + threadIdx.x;
-        uint32_t beg = 0, deg = 0, sv = 0;
+        uint32_t beg = 0, deg = 0;
+        SV sv = 0;
         if (i < n) {
             const uint32_t u = qin[i];
             beg = __ldg(&a.rowptr[u]);
@@ -160,7 +162,8 @@ __global__ void __launch_bounds__(kBlock) k_advance_chunks(AdvanceArgs a, Op op)
         s_val[threadIdx.x] = sv;
         __syncthreads();
         for (uint32_t base = 0; base < total; base += kBlock * kItems) {
-            uint32_t e[kItems], v[kItems], sv[kItems];
+            uint32_t e[kItems], v[kItems];
+            SV sv[kItems];
             int act[kItems];
 #pragma unroll
             for (int j = 0; j < kItems; j++) {
@@ -219,7 +222,7 @@ __global__ void __launch_bounds__(kBlock) k_advance_pieces(AdvanceArgs a, Op op)
         const uint32_t rb = __ldg(&a.rowptr[u]), re = __ldg(&a.rowptr[u + 1]);
         const uint32_t b = rb + pc.y * a.piece;
         const uint32_t e_end = min(re, b + a.piece);
-        const uint32_t sv = op.src_value(u);
+        const typename Op::SV sv = op.src_value(u);
         for (uint32_t base = b; base < e_end; base += 32 * kItems) {
             uint32_t e[kItems], v[kItems];
             int act[kItems];

@@ -83,6 +83,7 @@ struct Tuning {
     float alpha = 14.0f;          // push -> pull when m_f > m_unvisited / alpha
     float beta = 24.0f;           // pull -> push when n_f < V / beta
     uint32_t sssp_delta = 0;      // 0 = derived from the weights
+    float ms_alpha = 4.0f;        // msBFS: pull when active out-edges * ms_alpha > E
     int levels_per_sync = 4;      // host loop: supersteps enqueued per check
     int use_graphs = 1;           // run supersteps inside a CUDA graph
 };
@@ -122,8 +123,12 @@ struct olv_graph {
     olv::WhileGraph *bfs_graph = nullptr;
     olv::WhileGraph *sssp_graph = nullptr;
     void *pr_state = nullptr;            // PageRank plan + graph (pagerank.cu)
+    void *ms_state = nullptr;            // multi-source BFS masks + graph (msbfs.cu)
+    void *wpr_state = nullptr;           // weighted PageRank row plans (wpr.cu)
 };
 
 namespace olv {
 void release_pr_state(olv_graph *g);
+void release_ms_state(olv_graph *g);
+void release_wpr_state(olv_graph *g);
 }

@@ -26,14 +26,11 @@
 #include "olv_advance.cuh"
 #include "olv_graphexec.cuh"
 #include "olv_internal.cuh"
+#include "olv_rowsum.cuh"
 
 namespace olv {
 
-constexpr uint32_t kNnz = 2048;      // in-edges staged per row block
-constexpr uint32_t kRows = 2048;     // rows per row block at most
-constexpr uint32_t kSeg = 4096;      // in-edges per segment of a long row
 constexpr int kRedThreads = 1024;
-constexpr int kGather = kNnz / kBlock;
 
 struct PrCtl {
     double base;        // (1-alpha)/N + alpha*d/N for the running iteration
@@ -48,42 +45,34 @@ struct PrCtl {
     double inv_n;
 };
 
-// (s, c) <- s + x with the rounding error of the addition accumulated in c.
-__device__ __forceinline__ void two_sum_acc(float &s, float &c, float x) {
-    const float t = s + x;
-    const float bp = t - s;
-    c += (s - (t - bp)) + (x - bp);
-    s = t;
-}
-
-__device__ __forceinline__ void pair_add(float &s, float &c, float s2, float c2) {
-    two_sum_acc(s, c, s2);
-    c += c2;
-}
-
 // r' = alpha * (s + c) + base, with alpha split into hi + lo FP32 parts.
 __device__ __forceinline__ float pr_update(float s, float c, float a_hi, float a_lo, float base) {
     const float t = fmaf(a_lo, s, fmaf(a_hi, c, base));
     return fmaf(a_hi, s, t);
 }
 
-__global__ void __launch_bounds__(kBlock)
-k_pr_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowidx,
-          const uint32_t *__restrict__ blocks, const uint32_t *__restrict__ outdeg,
-          const float *c0, const float *c1, float *__restrict__ rank, PrCtl *ctl,
-          double *__restrict__ partials, float a_hi, float a_lo,
-          const uint32_t *__restrict__ segbase, const float2 *__restrict__ segs) {
-    if (ctl->done) return;
-    const float *__restrict__ cin = (ctl->iter & 1) ? c1 : c0;
-    float *__restrict__ cout = (float *)((ctl->iter & 1) ? c0 : c1);
-    const float base = (float)ctl->base;
-    const uint32_t r0 = blocks[blockIdx.x], r1 = blocks[blockIdx.x + 1];
-    const uint32_t e0 = colptr[r0], e1 = colptr[r1];
-    __shared__ float s_val[kNnz];
-    __shared__ double s_dred[2][kBlock / 32];
-    double res = 0.0, dang = 0.0;
+// Row sums over in-edges of the contributions r[u]/outdeg(u); the row update
+// writes the rank, the next contribution and FP64 |r'-r| / dangling partials.
+struct PrOp {
+    const uint32_t *done;
+    const PrCtl *ctl;
+    const float *c0, *c1;
+    float *rank;
+    const uint32_t *outdeg;
+    float a_hi, a_lo;
+    const float *cin;
+    float *cout;
+    float base;
 
-    auto finish_row = [&](uint32_t v, float s, float c) {
+    __device__ __forceinline__ void begin() {
+        const bool odd = ctl->iter & 1;
+        cin = odd ? c1 : c0;
+        cout = const_cast<float *>(odd ? c0 : c1);
+        base = (float)ctl->base;
+    }
+    __device__ __forceinline__ float term(uint32_t, uint32_t j) const { return __ldg(&cin[j]); }
+    __device__ __forceinline__ void finish(uint32_t v, float s, float c, double &res,
+                                           double &dang) const {
         const float nr = pr_update(s, c, a_hi, a_lo, base);
         const float old = rank[v];
         rank[v] = nr;
@@ -95,97 +84,8 @@ k_pr_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowi
             cout[v] = 0.0f;
             dang += (double)nr;
         }
-    };
-
-    if (e1 - e0 <= kNnz) {
-        const uint32_t n = e1 - e0;
-        uint32_t idx[kGather];
-#pragma unroll
-        for (int j = 0; j < kGather; j++) {
-            const uint32_t i = threadIdx.x + j * kBlock;
-            idx[j] = i < n ? __ldg(&rowidx[e0 + i]) : 0u;
-        }
-#pragma unroll
-        for (int j = 0; j < kGather; j++) {
-            const uint32_t i = threadIdx.x + j * kBlock;
-            if (i < n) s_val[i] = __ldg(&cin[idx[j]]);
-        }
-        __syncthreads();
-        for (uint32_t v = r0 + threadIdx.x; v < r1; v += kBlock) {
-            const uint32_t b = colptr[v] - e0, e = colptr[v + 1] - e0;
-            float s = 0.0f, c = 0.0f;
-            for (uint32_t i = b; i < e; i++) two_sum_acc(s, c, s_val[i]);
-            finish_row(v, s, c);
-        }
-    } else if (threadIdx.x == 0) {
-        // one long row: its segments were summed by k_pr_segments; fold in order
-        const uint32_t first = segbase[blockIdx.x];
-        const uint32_t nseg = (e1 - e0 + kSeg - 1) / kSeg;
-        float s = 0.0f, c = 0.0f;
-        for (uint32_t k = 0; k < nseg; k++) {
-            const float2 p = segs[first + k];
-            pair_add(s, c, p.x, p.y);
-        }
-        finish_row(r0, s, c);
     }
-    // fixed-order CTA reduction of the FP64 partials
-#pragma unroll
-    for (int o = 16; o; o >>= 1) {
-        res += __shfl_down_sync(0xffffffffu, res, o);
-        dang += __shfl_down_sync(0xffffffffu, dang, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        s_dred[0][threadIdx.x >> 5] = res;
-        s_dred[1][threadIdx.x >> 5] = dang;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double a = 0, b = 0;
-        for (int i = 0; i < kBlock / 32; i++) {
-            a += s_dred[0][i];
-            b += s_dred[1][i];
-        }
-        partials[2 * blockIdx.x] = a;
-        partials[2 * blockIdx.x + 1] = b;
-    }
-}
-
-// Compensated sums of the kSeg-edge segments of long rows: thread t sums
-// elements t, t+kBlock, ... of its segment, then a fixed-shape tree.
-__global__ void __launch_bounds__(kBlock)
-k_pr_segments(const uint32_t *__restrict__ rowidx, const uint2 *__restrict__ seg_range,
-              const float *c0, const float *c1, const PrCtl *ctl, float2 *__restrict__ segs) {
-    if (ctl->done) return;
-    const float *__restrict__ cin = (ctl->iter & 1) ? c1 : c0;
-    const uint2 r = seg_range[blockIdx.x];
-    __shared__ float s_red[2][kBlock];
-    float s = 0.0f, c = 0.0f;
-    constexpr int U = kSeg / kBlock;
-    uint32_t idx[U];
-#pragma unroll
-    for (int j = 0; j < U; j++) {
-        const uint32_t i = r.x + threadIdx.x + j * kBlock;
-        idx[j] = i < r.y ? __ldg(&rowidx[i]) : 0xffffffffu;
-    }
-    float x[U];
-#pragma unroll
-    for (int j = 0; j < U; j++) x[j] = idx[j] != 0xffffffffu ? __ldg(&cin[idx[j]]) : 0.0f;
-#pragma unroll
-    for (int j = 0; j < U; j++) two_sum_acc(s, c, x[j]);
-    s_red[0][threadIdx.x] = s;
-    s_red[1][threadIdx.x] = c;
-    __syncthreads();
-    for (int w = kBlock / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < (uint32_t)w) {
-            float a = s_red[0][threadIdx.x], ac = s_red[1][threadIdx.x];
-            pair_add(a, ac, s_red[0][threadIdx.x + w], s_red[1][threadIdx.x + w]);
-            s_red[0][threadIdx.x] = a;
-            s_red[1][threadIdx.x] = ac;
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) segs[blockIdx.x] = make_float2(s_red[0][0], s_red[1][0]);
-}
+};
 
 // Fold the per-CTA partials (fixed order), publish residual and the next
 // iteration's constant term, decide convergence.
@@ -264,65 +164,21 @@ __global__ void k_outdeg(const uint32_t *__restrict__ rowptr, uint32_t V, uint32
 
 // ------------------------------------------------------------------ host --
 struct PrPlan {
-    DevBuf blocks, outdeg, contrib, partials, ctl, dang, segbase, seg_range, segs;
-    uint32_t nblocks = 0;
-    uint32_t nsegs = 0;
+    RowPlan rows;
+    DevBuf outdeg, contrib, ctl, dang;
     float a_hi = 0, a_lo = 0;
-    double alpha = -1;
     ~PrPlan() {
-        blocks.release(); outdeg.release(); contrib.release(); partials.release();
-        ctl.release(); dang.release(); segbase.release(); seg_range.release(); segs.release();
+        rows.release(); outdeg.release(); contrib.release(); ctl.release(); dang.release();
     }
 };
 
-// Row blocks over the CSC offsets: consecutive rows while the block holds at
-// most kNnz in-edges and kRows rows; a longer row forms a block of its own.
 static int build_pr_plan(olv_graph *g, PrPlan &p) {
     const uint32_t V = g->V;
-    std::vector<uint32_t> cp(V + 1);
-    OLV_CUDA(cudaMemcpyAsync(cp.data(), g->colptr.p, ((size_t)V + 1) * 4, cudaMemcpyDeviceToHost,
-                             g->stream));
-    OLV_CUDA(cudaStreamSynchronize(g->stream));
-    std::vector<uint32_t> b;
-    b.reserve(g->E / kNnz + V / kRows + 16);
-    uint32_t v = 0;
-    b.push_back(0);
-    while (v < V) {
-        const uint32_t start = v;
-        if (cp[v + 1] - cp[v] > kNnz) {
-            v++;
-        } else {
-            while (v < V && v - start < kRows && cp[v + 1] - cp[start] <= kNnz) v++;
-        }
-        b.push_back(v);
-    }
-    p.nblocks = (uint32_t)b.size() - 1;
-    // long rows (one per block) are cut into kSeg-edge segments
-    std::vector<uint32_t> segbase(p.nblocks, 0xffffffffu);
-    std::vector<uint2> ranges;
-    for (uint32_t k = 0; k < p.nblocks; k++) {
-        const uint32_t e0 = cp[b[k]], e1 = cp[b[k + 1]];
-        if (e1 - e0 <= kNnz) continue;
-        segbase[k] = (uint32_t)ranges.size();
-        for (uint32_t x = e0; x < e1; x += kSeg) ranges.push_back(make_uint2(x, std::min(e1, x + kSeg)));
-    }
-    p.nsegs = (uint32_t)ranges.size();
-    OLV_TRY(p.segbase.ensure(segbase.size() * 4 + 16));
-    OLV_TRY(p.seg_range.ensure(ranges.size() * 8 + 16));
-    OLV_TRY(p.segs.ensure(ranges.size() * 8 + 16));
-    OLV_CUDA(cudaMemcpyAsync(p.segbase.p, segbase.data(), segbase.size() * 4,
-                             cudaMemcpyHostToDevice, g->stream));
-    if (!ranges.empty())
-        OLV_CUDA(cudaMemcpyAsync(p.seg_range.p, ranges.data(), ranges.size() * 8,
-                                 cudaMemcpyHostToDevice, g->stream));
-    OLV_TRY(p.blocks.ensure(b.size() * 4));
-    OLV_CUDA(cudaMemcpyAsync(p.blocks.p, b.data(), b.size() * 4, cudaMemcpyHostToDevice,
-                             g->stream));
+    OLV_TRY(build_row_plan(g->colptr.as<uint32_t>(), V, g->stream, p.rows));
     OLV_TRY(p.outdeg.ensure((size_t)V * 4 + 16));
     k_outdeg<<<g->num_sms * 8, kBlock, 0, g->stream>>>(g->rowptr.as<uint32_t>(), V,
                                                       p.outdeg.as<uint32_t>());
     OLV_TRY(p.contrib.ensure((size_t)V * 8 + 32));
-    OLV_TRY(p.partials.ensure((size_t)p.nblocks * 16 + 16));
     OLV_TRY(p.ctl.ensure(sizeof(PrCtl)));
     OLV_TRY(p.dang.ensure(16));
     OLV_CUDA(cudaGetLastError());
@@ -333,29 +189,22 @@ static int build_pr_plan(olv_graph *g, PrPlan &p) {
 template <class Sink>
 static int pr_iteration(olv_graph *g, PrPlan &p, float *rank, Sink &&sink,
                         cudaGraphConditionalHandle h, int use_cond) {
-    const uint32_t *colptr = g->colptr.as<uint32_t>();
-    const uint32_t *rowidx = g->rowidx.as<uint32_t>();
-    const uint32_t *blocks = p.blocks.as<uint32_t>();
-    const uint32_t *outdeg = p.outdeg.as<uint32_t>();
-    const float *c0 = p.contrib.as<float>();
-    const float *c1 = p.contrib.as<float>() + g->V;
     PrCtl *ctl = p.ctl.as<PrCtl>();
-    double *partials = p.partials.as<double>();
-    float a_hi = p.a_hi, a_lo = p.a_lo;
-    uint32_t nparts = p.nblocks;
-    const uint32_t *segbase = p.segbase.as<uint32_t>();
-    const uint2 *seg_range = p.seg_range.as<uint2>();
-    float2 *segs = p.segs.as<float2>();
-    const float2 *csegs = segs;
-    const PrCtl *cctl = ctl;
-    if (p.nsegs) {
-        void *a_seg[] = {&rowidx, &seg_range, &c0, &c1, &cctl, &segs};
-        OLV_TRY(sink((const void *)k_pr_segments, dim3(p.nsegs), dim3(kBlock), a_seg));
-    }
-    void *a_pull[] = {&colptr, &rowidx, &blocks, &outdeg, &c0, &c1, &rank, &ctl, &partials,
-                      &a_hi, &a_lo, &segbase, &csegs};
-    OLV_TRY(sink((const void *)k_pr_pull, dim3(p.nblocks), dim3(kBlock), a_pull));
-    const double *cpart = partials;
+    PrOp op;
+    op.done = &ctl->done;
+    op.ctl = ctl;
+    op.c0 = p.contrib.as<float>();
+    op.c1 = p.contrib.as<float>() + g->V;
+    op.rank = rank;
+    op.outdeg = p.outdeg.as<uint32_t>();
+    op.a_hi = p.a_hi;
+    op.a_lo = p.a_lo;
+    op.cin = nullptr;
+    op.cout = nullptr;
+    op.base = 0;
+    OLV_TRY(row_pass(p.rows, g->colptr.as<uint32_t>(), g->rowidx.as<uint32_t>(), op, sink));
+    const double *cpart = p.rows.partials.as<double>();
+    uint32_t nparts = p.rows.nblocks;
     void *a_red[] = {&ctl, &cpart, &nparts, &h, &use_cond};
     OLV_TRY(sink((const void *)k_pr_reduce, dim3(1), dim3(kRedThreads), a_red));
     return OLV_OK;

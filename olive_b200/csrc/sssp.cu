@@ -26,6 +26,7 @@ constexpr uint32_t kModeRelax = 0;
 constexpr uint32_t kModeSplit = 2;
 
 struct SsspOp {
+    using SV = uint32_t;
     static constexpr bool kHasFar = true;
     const uint32_t *w;
     uint32_t *mark;       // stamp of the superstep that last queued v as near

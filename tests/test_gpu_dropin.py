@@ -48,7 +48,7 @@ def test_bfs_app(tmp_path, path):
     z = np.load(path)
     f = edge_file(tmp_path, z["sorted_rowptr"], z["sorted_col"])
     sorted_input = np.array_equal(z["rowptr"], z["sorted_rowptr"])
-    for i, s in enumerate(z["bfs_sources"][:12]):
+    for i, s in enumerate(z["bfs_sources"][:4]):
         run("BFS", [f, "-s", s, "-round", 1000000], tmp_path)
         got = np.loadtxt(os.path.join(str(tmp_path), "BFS.txt"), dtype=np.int64, ndmin=1)
         if sorted_input:
@@ -80,7 +80,7 @@ def test_sssp_app_unit_weights(tmp_path, path):
     """SSSP.cu sets every weight to 1 (SSSP.cu:131): distances are BFS levels."""
     z = np.load(path)
     f = edge_file(tmp_path, z["sorted_rowptr"], z["sorted_col"])
-    for s in z["bfs_sources"][:6]:
+    for s in z["bfs_sources"][:2]:
         run("SSSP", [f, "-s", s, "-round", 1000000], tmp_path)
         got = np.loadtxt(os.path.join(str(tmp_path), "SSSP.txt"), dtype=np.int64, ndmin=1)
         want, _ = oracle.bfs(z["sorted_rowptr"], z["sorted_col"], int(s))

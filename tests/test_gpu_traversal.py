@@ -213,3 +213,47 @@ def test_pagerank_tolerance_stop(ob):
         _, it_ref, res = oracle.pagerank(rp, cl, 0.85, 1000, 1e-5)
         assert abs(it - it_ref) <= 1
         assert g.last_stats.residual < 1e-5
+
+
+# ------------------------------------------------------------------ msBFS --
+@pytest.mark.parametrize("scale,seed,n", [(12, 1, 64), (16, 5, 64), (14, 2, 5), (10, 3, 1)])
+def test_msbfs_rows_equal_solo_bfs(ob, scale, seed, n):
+    with ob.Graph.rmat(scale, 16, seed) as g:
+        rp, cl, _ = g.csr()
+        deg = np.diff(rp.astype(np.int64))
+        rng = np.random.default_rng(seed)
+        srcs = rng.choice(np.flatnonzero(deg > 0), n, replace=False).astype(np.uint32)
+        lv = g.msbfs(srcs)
+        st = g.last_stats
+        e_tot = 0
+        for s in range(n):
+            ref, e = oracle.bfs(rp, cl, int(srcs[s]))
+            np.testing.assert_array_equal(lv[s], ref, err_msg=f"row {s}")
+            e_tot += e
+            np.testing.assert_array_equal(lv[s], g.bfs(int(srcs[s])))
+        assert st.edges_traversed == e_tot
+
+
+def test_msbfs_fixtures_duplicates_and_device_output(ob):
+    import torch
+    for path in FIXTURES:
+        z = np.load(path)
+        srcs = z["bfs_sources"][:64].astype(np.uint32)
+        with ob.Graph.from_csr(z["rowptr"], z["col"]) as g:
+            lv = g.msbfs(srcs)
+            np.testing.assert_array_equal(lv, z["bfs_levels"][:64])
+            dup = np.array([srcs[0], srcs[0], srcs[-1]], np.uint32)
+            out = torch.empty((3, g.V), dtype=torch.int32, device="cuda")
+            g.msbfs(dup, out=out)
+            o = out.cpu().numpy()
+            np.testing.assert_array_equal(o[0], z["bfs_levels"][0])
+            np.testing.assert_array_equal(o[1], z["bfs_levels"][0])
+
+
+def test_msbfs_bad_arguments(ob):
+    rp, cl = oracle.grid_csr(4, 4)
+    with ob.Graph.from_csr(rp, cl) as g:
+        with pytest.raises(ob.OliveError):
+            g.msbfs(np.arange(65, dtype=np.uint32) % 16)
+        with pytest.raises(ob.OliveError):
+            g.msbfs(np.array([16], np.uint32))
