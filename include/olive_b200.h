@@ -104,6 +104,18 @@ int olv_tune_get(const olv_graph *g, const char *key, double *value);
  * BFS levels: reproduces testBFS.cu:42-87 and BFS.cu:82-160 run to completion
  * (int32 level, 0x7fffffff unreached).  Direction-optimising (push/pull).      */
 int olv_bfs(olv_graph *g, uint32_t src, int32_t *level_out, olv_stats *st);
+/* BFS for callers that cannot allocate device memory (no reference
+ * counterpart: the reference allocated in every VertexSubset and GRD).  The
+ * caller passes the CSR (rowptr[V+1], col[E]) and level_out[V], all device
+ * memory; nothing is allocated inside the call.  The engine's scratch is a
+ * fixed file-scope device array (about 8.6 MB per GPU that loads the
+ * library), so graphs are limited to 1,048,576 vertices and 16,777,216 edges
+ * (larger ones return OLV_ERR_LIMIT).  Push-only traversal; the CSR is
+ * validated on the device first.  All calls on a device share the scratch:
+ * calls that overlap on the GPU race.  The first call on a device looks up
+ * the scratch address; make it before any stream capture.  st->device_ms is 0. */
+int olv_bfs_noalloc(const uint32_t *rowptr, const uint32_t *col, uint32_t V, uint64_t E,
+                    uint32_t src, int32_t *level_out, void *stream, olv_stats *st);
 /* SSSP distances with non-negative uint32 weights: the frontier Bellman-Ford of
  * SSSP.cu:106-174 (atomicMin relaxation) with near/far bucketing.  uint32
  * distance, 0x7fffffff unreached.  Needs an OLV_W_U32 graph.                   */

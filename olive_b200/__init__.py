@@ -54,6 +54,7 @@ _SIGS = [
     ("olv_tune_set", _I, [_VP, ctypes.c_char_p, _D]),
     ("olv_tune_get", _I, [_VP, ctypes.c_char_p, ctypes.POINTER(_D)]),
     ("olv_bfs", _I, [_VP, _U32, _VP, ctypes.POINTER(Stats)]),
+    ("olv_bfs_noalloc", _I, [_VP, _VP, _U32, _U64, _U32, _VP, _VP, ctypes.POINTER(Stats)]),
     ("olv_sssp", _I, [_VP, _U32, _VP, ctypes.POINTER(Stats)]),
     ("olv_msbfs", _I, [_VP, _VP, _I, _VP, ctypes.POINTER(Stats)]),
     ("olv_graph_create_er_batch", _I, [_I, _U32, _U32, _U32, _U64, _VP, ctypes.POINTER(_VP)]),
