@@ -252,15 +252,16 @@ def run_ours(a, rank, world, local_rank):
                 "algorithmic_bytes": int(alg_bytes), "bytes_formula": bytes_formula,
                 "peak_source": peak_src, "kernel_ms": round(kern_ms, 4)}
 
-    # launches of our kernels per step (kernel nodes executed by the graph)
+    # launches of our kernels per step (kernel nodes executed by the graph):
+    # sssp: fill, init, 4 per superstep, reached count; bfs: fill, init, 8 per level
     if a.workload == "sssp":
-        per_step = 2 + 5 * st.iterations + 1
+        per_step = 2 + 4 * st.iterations + 1
     elif a.workload == "bfs":
-        per_step = 2 + 6 * st.iterations
+        per_step = 2 + 8 * st.iterations
     elif a.workload == "msbfs":
-        per_step = 2 + 6 * st.iterations
-    else:
-        per_step = 2 + 2 * st.iterations
+        per_step = 2 + 7 * st.iterations + 1
+    else:   # pagerank: segments (when the graph has long rows), blocks, fold per iteration
+        per_step = 2 + 3 * st.iterations
     launches = per_step * a.steps
 
     # end to end through the public API: host (pinned) output buffer, D2H inside

@@ -44,6 +44,10 @@ extern "C" {
 #define OLV_W_U32  1
 #define OLV_W_F32  2
 
+/* format for olv_graph_load */
+#define OLV_FMT_EDGE_LIST 0   /* "V E" then "src dst [weight]" lines, '#' comments  */
+#define OLV_FMT_DIMACS    1   /* METIS / DIMACS-10 adjacency lines, 1-based ids     */
+
 /* dangling_mode for olv_pagerank */
 #define OLV_DANGLING_UNIFORM 0   /* redistribute dangling mass uniformly          */
 #define OLV_DANGLING_LEAK    1   /* drop it, as PageRank.cu:63-75 / testPageRank */
@@ -77,6 +81,11 @@ int olv_graph_create(const uint32_t *rowptr, const uint32_t *col, const void *we
  * CSR position (seed wseed).                                                   */
 int olv_graph_create_rmat(int scale, int edge_factor, uint64_t seed, int weight_type,
                           uint64_t wseed, olv_graph **out);
+/* Load a graph file, parsed on the device (replaces CsrGraph::fromEdgeListFile,
+ * csrGraph.h:106-171, and fromDimacsFile, csrGraph.h:177-236).  Edge lists are
+ * stably sorted by source (the reference assumed sorted input); an optional
+ * third column becomes uint32 weights.  DIMACS stores both directions (2E). */
+int olv_graph_load(const char *path, int format, olv_graph **out);
 int olv_graph_destroy(olv_graph *g);
 int olv_graph_info(const olv_graph *g, uint32_t *V, uint64_t *E, int *weight_type);
 /* Copy the CSR back (any of the pointers may be NULL). */
@@ -99,6 +108,15 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
  *   "levels_per_sync" host loop: supersteps enqueued per check      (4)  */
 int olv_tune_set(olv_graph *g, const char *key, double value);
 int olv_tune_get(const olv_graph *g, const char *key, double *value);
+/* Autotuner: coordinate descent over hub_degree, alpha, beta (BFS) and, on
+ * uint32-weighted graphs, sssp_delta and piece (SSSP), each candidate timed
+ * `reps` times from the highest out-degree vertex; the fastest values are
+ * applied to the handle and, if json_path is not NULL, written to a JSON table
+ * keyed by GPU name and graph shape.  olv_autotune_load applies such a table
+ * when its key matches the handle (*applied = 1) and leaves the handle alone
+ * otherwise.  Results stay bit-exact; only speed changes.                     */
+int olv_autotune(olv_graph *g, const char *json_path, int reps);
+int olv_autotune_load(olv_graph *g, const char *json_path, int *applied);
 
 /* ---- traversal --------------------------------------------------------------
  * BFS levels: reproduces testBFS.cu:42-87 and BFS.cu:82-160 run to completion

@@ -45,6 +45,7 @@ _SIGS = [
     ("olv_version", ctypes.c_char_p, []),
     ("olv_graph_create", _I, [_VP, _VP, _VP, _I, _U32, _U64, ctypes.POINTER(_VP)]),
     ("olv_graph_create_rmat", _I, [_I, _I, _U64, _I, _U64, ctypes.POINTER(_VP)]),
+    ("olv_graph_load", _I, [ctypes.c_char_p, _I, ctypes.POINTER(_VP)]),
     ("olv_graph_destroy", _I, [_VP]),
     ("olv_graph_info", _I, [_VP, ctypes.POINTER(_U32), ctypes.POINTER(_U64), ctypes.POINTER(_I)]),
     ("olv_graph_copy_csr", _I, [_VP, _VP, _VP, _VP]),
@@ -53,6 +54,8 @@ _SIGS = [
     ("olv_graph_max_degree_vertex", _I, [_VP, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
     ("olv_tune_set", _I, [_VP, ctypes.c_char_p, _D]),
     ("olv_tune_get", _I, [_VP, ctypes.c_char_p, ctypes.POINTER(_D)]),
+    ("olv_autotune", _I, [_VP, ctypes.c_char_p, _I]),
+    ("olv_autotune_load", _I, [_VP, ctypes.c_char_p, ctypes.POINTER(_I)]),
     ("olv_bfs", _I, [_VP, _U32, _VP, ctypes.POINTER(Stats)]),
     ("olv_bfs_noalloc", _I, [_VP, _VP, _U32, _U64, _U32, _VP, _VP, ctypes.POINTER(Stats)]),
     ("olv_sssp", _I, [_VP, _U32, _VP, ctypes.POINTER(Stats)]),
@@ -144,6 +147,14 @@ class Graph:
         return cls(h)
 
     @classmethod
+    def load(cls, path, fmt="edgelist"):
+        """Parse an edge-list or DIMACS file on the device."""
+        h = _VP()
+        _check(lib().olv_graph_load(str(path).encode(), 1 if fmt == "dimacs" else 0,
+                                    ctypes.byref(h)), "olv_graph_load")
+        return cls(h)
+
+    @classmethod
     def er_batch(cls, count, vmin=1024, vmax=65536, avg_degree=8, seed=1):
         """Block-diagonal batch of ER digraphs; returns (graph, inst_offsets)."""
         off = np.zeros(count + 1, np.uint32)
@@ -210,6 +221,19 @@ class Graph:
             _check(lib().olv_tune_get(self._h, k.encode(), ctypes.byref(d)), "olv_tune_get")
             out[k] = d.value
         return out
+
+    def autotune(self, json_path=None, reps=3):
+        """Time the tunables on this graph, keep the fastest; returns them."""
+        _check(lib().olv_autotune(self._h, json_path.encode() if json_path else None, reps),
+               "olv_autotune")
+        return self.tune()
+
+    def autotune_load(self, json_path):
+        """Apply a table written by autotune(); True if it matched this graph."""
+        applied = _I()
+        _check(lib().olv_autotune_load(self._h, json_path.encode(), ctypes.byref(applied)),
+               "olv_autotune_load")
+        return bool(applied.value)
 
     def set_weights_f32(self, w):
         w = np.ascontiguousarray(w, np.float32) if not hasattr(w, "data_ptr") else w.contiguous()

@@ -55,7 +55,18 @@ def compile_one(src, force=False, extra=()):
 
 
 def build(jobs=None, force=False, verbose=False, extra=()):
+    # OLV_NVCC_EXTRA: extra nvcc flags (e.g. -DOLV_ITEMS=8 to change the edges each
+    # thread of the advance keeps in flight); a changed value forces a rebuild
+    env_extra = os.environ.get("OLV_NVCC_EXTRA", "").split()
+    stamp = os.path.join(BUILD, "flags.txt")
     os.makedirs(BUILD, exist_ok=True)
+    if env_extra or os.path.exists(stamp):
+        old = open(stamp).read() if os.path.exists(stamp) else ""
+        if old != " ".join(env_extra):
+            force = True
+            with open(stamp, "w") as f:
+                f.write(" ".join(env_extra))
+    extra = list(extra) + env_extra
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     jobs = jobs or min(len(srcs), os.cpu_count() or 4)
     with cf.ThreadPoolExecutor(jobs) as ex:

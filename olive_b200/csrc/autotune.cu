@@ -1,0 +1,130 @@
+// Autotuner (no reference counterpart; the reference fixed its launch shape
+// in util::kernelConfig, utils.h:56-72, and took the edge-group size from the
+// -g flag, BFS.cu:89).  Coordinate descent over the engine's tunables, each
+// candidate timed with CUDA events on the graph's own stream from its highest
+// out-degree vertex; the winners are applied to the handle and, optionally,
+// written to a JSON table keyed by GPU and graph shape, which olv_autotune_load
+// re-applies when the key matches.  Tuning changes speed only: every result
+// stays bit-exact (tests check it).
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "olv_internal.cuh"
+
+namespace olv {
+
+static int time_call(olv_graph *g, int (*fn)(olv_graph *, uint32_t, void *), uint32_t src,
+                     void *out, int reps, double *ms_out) {
+    OLV_TRY(fn(g, src, out));   // warm-up (also builds cached graphs)
+    double best = 1e30;
+    for (int r = 0; r < reps; r++) {
+        olv_stats st;
+        (void)st;
+        OLV_TRY(fn(g, src, out));
+        float ms = 0;
+        OLV_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
+        best = ms < best ? ms : best;
+    }
+    *ms_out = best;
+    return OLV_OK;
+}
+
+static int run_bfs(olv_graph *g, uint32_t src, void *out) {
+    return olv_bfs(g, src, static_cast<int32_t *>(out), nullptr);
+}
+static int run_sssp(olv_graph *g, uint32_t src, void *out) {
+    return olv_sssp(g, src, static_cast<uint32_t *>(out), nullptr);
+}
+
+static std::string tune_key(olv_graph *g) {
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, g->device);
+    char buf[512];
+    snprintf(buf, sizeof buf, "%s|V=%u|E=%llu|maxout=%u|maxin=%u|w=%d", prop.name, g->V,
+             (unsigned long long)g->E, g->max_out_degree, g->max_in_degree, g->weight_type);
+    return buf;
+}
+
+}  // namespace olv
+
+using namespace olv;
+
+extern "C" int olv_autotune(olv_graph *g, const char *json_path, int reps) {
+    OLV_CHECK_ARG(g, "olv_autotune: null graph");
+    if (reps < 1) reps = 3;
+    uint32_t src = 0, deg = 0;
+    OLV_TRY(olv_graph_max_degree_vertex(g, &src, &deg));
+    DevBuf out;
+    OLV_TRY(out.ensure((size_t)g->V * 4 + 16));
+    struct Cand {
+        const char *key;
+        std::vector<double> values;
+        int (*fn)(olv_graph *, uint32_t, void *);
+    };
+    std::vector<Cand> plan = {
+        {"hub_degree", {256, 1024, 4096}, run_bfs},
+        {"alpha", {2, 6, 14, 30, 60}, run_bfs},
+        {"beta", {6, 24, 100}, run_bfs},
+    };
+    if (g->weight_type == OLV_W_U32) {
+        plan.push_back({"sssp_delta", {16, 32, 64, 128, 256, 512, 1024}, run_sssp});
+        plan.push_back({"piece", {256, 1024, 4096}, run_sssp});
+    }
+    std::string log;
+    for (auto &c : plan) {
+        double best_ms = 1e30, best_v = 0;
+        for (double v : c.values) {
+            OLV_TRY(olv_tune_set(g, c.key, v));
+            double ms = 0;
+            OLV_TRY(time_call(g, c.fn, src, out.p, reps, &ms));
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_v = v;
+            }
+        }
+        OLV_TRY(olv_tune_set(g, c.key, best_v));
+        char line[160];
+        snprintf(line, sizeof line, "%s  \"%s\": %.6g", log.empty() ? "" : ",\n", c.key, best_v);
+        log += line;
+    }
+    if (json_path) {
+        FILE *f = fopen(json_path, "w");
+        if (!f) {
+            set_error("olv_autotune: cannot write %s", json_path);
+            return OLV_ERR_ARG;
+        }
+        fprintf(f, "{\n  \"key\": \"%s\",\n%s\n}\n", tune_key(g).c_str(), log.c_str());
+        fclose(f);
+    }
+    return OLV_OK;
+}
+
+extern "C" int olv_autotune_load(olv_graph *g, const char *json_path, int *applied) {
+    OLV_CHECK_ARG(g && json_path, "olv_autotune_load: null pointer");
+    if (applied) *applied = 0;
+    FILE *f = fopen(json_path, "r");
+    if (!f) {
+        set_error("olv_autotune_load: cannot read %s", json_path);
+        return OLV_ERR_ARG;
+    }
+    std::string text;
+    char buf[4096];
+    size_t n;
+    while ((n = fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, n);
+    fclose(f);
+    const std::string want = "\"key\": \"" + tune_key(g) + "\"";
+    if (text.find(want) == std::string::npos) return OLV_OK;   // table is for another graph/GPU
+    const char *keys[] = {"hub_degree", "piece", "alpha", "beta", "sssp_delta", "ms_alpha"};
+    for (const char *k : keys) {
+        const std::string pat = std::string("\"") + k + "\":";
+        size_t pos = text.find(pat);
+        if (pos == std::string::npos) continue;
+        double v = atof(text.c_str() + pos + pat.size());
+        OLV_TRY(olv_tune_set(g, k, v));
+    }
+    if (applied) *applied = 1;
+    return OLV_OK;
+}

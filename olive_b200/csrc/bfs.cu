@@ -21,6 +21,8 @@
 //   k_bfs_end        account edges, swap queues, stop when the queue is empty
 #include <stdio.h>
 
+#include <cub/cub.cuh>
+
 #include "olv_advance.cuh"
 #include "olv_graphexec.cuh"
 #include "olv_internal.cuh"
@@ -87,7 +89,7 @@ __global__ void k_bfs_init(TravCtl *c, int32_t *level, uint32_t *q0, const uint3
 
 __global__ void k_bfs_begin(TravCtl *c, uint32_t V, float alpha, float beta) {
     if (c->done) return;
-    const uint32_t n = c->qsize[c->cur];
+    const uint32_t n = c->qsize[c->cur];   // frontier size (queue or bitmap)
     if (n == 0) {
         c->done = 1;
         return;
@@ -100,65 +102,176 @@ __global__ void k_bfs_begin(TravCtl *c, uint32_t V, float alpha, float beta) {
     c->qsize[c->cur ^ 1] = 0;
     c->npieces = 0;
     c->m_next = 0;
+    c->reached_pull = 0;
+    c->ncand[0] = 0;   // pull overflow list
+    if (c->mode == 0 && c->queue_stale) c->qsize[c->cur] = 0;   // rebuilt from the bitmap
 }
 
-// Bitmap of the current frontier (level == L), one ballot per warp; used when
-// a pull level follows a push level.  Words of vertices >= V are zero.
+// Pull-level preparation (pull levels only), two independent index ranges:
+//   - bitmap of the current frontier (level == L), one ballot per warp, when the
+//     previous level was a push level;
+//   - zero the next frontier's bitmap.
+struct PullLists {
+    uint32_t V;
+    const uint32_t *pidx;      // in-edges, highest out-degree source first
+    const uint32_t *order;     // vertices by in-degree (heavy: in-degree > kPullHeavy)
+    uint32_t n_heavy, n_light;
+    uint32_t *cand;            // pull overflow list (V entries)
+    uint32_t *fb0, *fb1;
+    uint32_t words;            // words per bitmap
+};
+
+constexpr uint32_t kPullHeavy = 128;   // in-degree split of the sorted vertex list
+
+
 __global__ void __launch_bounds__(kBlock)
-k_bfs_bitmap(uint32_t V, TravCtl *c, uint32_t *fb0, uint32_t *fb1) {
-    if (c->done || c->mode != 1 || c->fb_valid) return;
+k_bfs_pull_prep(uint32_t V, TravCtl *c, PullLists p) {
+    if (c->done || c->mode != 1) return;
     const int32_t *level = static_cast<const int32_t *>(c->vdata);
     const int L = (int)c->level;
-    uint32_t *fb = c->fb_cur ? fb1 : fb0;
-    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V;
+    uint32_t *fcur = c->fb_cur ? p.fb1 : p.fb0;
+    uint32_t *fnext = c->fb_cur ? p.fb0 : p.fb1;
+    const uint64_t stride = (uint64_t)gridDim.x * kBlock;
+    if (!c->fb_valid)
+        for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V; base += stride) {
+            const uint64_t v = base + threadIdx.x;
+            const unsigned word = __ballot_sync(0xffffffffu, v < V && __ldcg(&level[v]) == L);
+            if (lane_id() == 0) fcur[v >> 5] = word;
+        }
+    for (uint64_t w = blockIdx.x * (uint64_t)kBlock + threadIdx.x; w < p.words; w += stride)
+        fnext[w] = 0;
+}
+
+// The current frontier as a queue, from its bitmap, when a push level follows
+// a pull level.
+__global__ void __launch_bounds__(kBlock)
+k_bfs_fb_to_queue(TravCtl *c, uint32_t *q0, uint32_t *q1, PullLists p) {
+    if (c->done || c->mode != 0 || !c->queue_stale) return;
+    const uint32_t *fb = c->fb_cur ? p.fb1 : p.fb0;
+    uint32_t *q = c->cur ? q1 : q0;
+    uint32_t *qsz = &c->qsize[c->cur];
+    const uint32_t lane = lane_id();
+    const uint64_t nw = ((uint64_t)p.V + 31) / 32;
+    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < nw;
          base += (uint64_t)gridDim.x * kBlock) {
-        const uint64_t v = base + threadIdx.x;
-        const unsigned word = __ballot_sync(0xffffffffu, v < V && __ldcg(&level[v]) == L);
-        if (lane_id() == 0) fb[v >> 5] = word;
+        const uint64_t w = base + threadIdx.x;
+        uint32_t bits = w < nw ? fb[w] : 0;
+        // one atomic per warp for all the warp's set bits
+        const uint32_t cnt = __popc(bits);
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (uint32_t)o) incl += t;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        uint32_t off = 0;
+        if (lane == 31 && total) off = atomicAdd(qsz, total);
+        off = __shfl_sync(0xffffffffu, off, 31) + incl - cnt;
+        while (bits) {
+            const uint32_t b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            q[off++] = (uint32_t)(w * 32 + b);
+        }
     }
 }
 
-// Pull: every unvisited vertex looks for an in-neighbour in the frontier
-// bitmap, kParents in-edges per probe, and stops at the first hit.
+__device__ __forceinline__ bool in_bitmap(const uint32_t *__restrict__ fb, uint32_t u) {
+    return (__ldg(&fb[u >> 5]) >> (u & 31)) & 1u;
+}
+
+// Pull, pass 1: every unvisited vertex probes its first kProbe1 in-edges (the
+// in-edge lists are ordered by source out-degree, so the likeliest parents
+// come first) against the frontier bitmap, kParents at a time.  A vertex that
+// finds a parent gets level L+1, a bit in the next bitmap and a queue slot;
+// one that has more in-edges left goes to the overflow list.  Every thread
+// does at most kProbe1 probes, so the lanes of a warp finish together.
 constexpr int kParents = 4;
+constexpr uint32_t kProbe1 = 8;
+
 
 __global__ void __launch_bounds__(kBlock)
-k_bfs_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowidx,
-           const uint32_t *__restrict__ rowptr, uint32_t V, TravCtl *c, uint32_t *q0,
-           uint32_t *q1, uint32_t *fb0, uint32_t *fb1) {
+k_bfs_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowptr,
+           TravCtl *c, uint32_t *q0, uint32_t *q1, PullLists p) {
     if (c->done || c->mode != 1) return;
     int32_t *level = static_cast<int32_t *>(c->vdata);
     const int L = (int)c->level;
-    const uint32_t cur = c->cur;
-    uint32_t *qout = cur ? q0 : q1;
-    uint32_t *qsz = &c->qsize[cur ^ 1];
-    const uint32_t *__restrict__ fin = c->fb_cur ? fb1 : fb0;
-    uint32_t *__restrict__ fout = c->fb_cur ? fb0 : fb1;
-    unsigned long long acc = 0;
-    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V;
+    const uint32_t *__restrict__ fin = c->fb_cur ? p.fb1 : p.fb0;
+    uint32_t *fout = c->fb_cur ? p.fb0 : p.fb1;
+    uint32_t *ovf = p.cand;
+    const uint32_t lane = lane_id();
+    unsigned long long acc = 0, nfound = 0;
+    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < p.V;
          base += (uint64_t)gridDim.x * kBlock) {
         const uint32_t v = (uint32_t)base + threadIdx.x;
-        bool found = false;
-        if (v < V && level[v] == kInf) {
+        bool found = false, more = false;
+        if (v < p.V && level[v] == kInf) {
             const uint32_t b = __ldg(&colptr[v]), e = __ldg(&colptr[v + 1]);
-            for (uint32_t i = b; i < e && !found; i += kParents) {
+            const uint32_t e1 = e - b > kProbe1 ? b + kProbe1 : e;
+            for (uint32_t k = b; k < e1 && !found; k += kParents) {
                 uint32_t u[kParents];
 #pragma unroll
-                for (int j = 0; j < kParents; j++) u[j] = i + j < e ? __ldg(&rowidx[i + j]) : 0xffffffffu;
+                for (int j = 0; j < kParents; j++)
+                    u[j] = k + j < e1 ? __ldg(&p.pidx[k + j]) : 0xffffffffu;
 #pragma unroll
                 for (int j = 0; j < kParents; j++)
-                    if (u[j] != 0xffffffffu && ((fin[u[j] >> 5] >> (u[j] & 31)) & 1u)) found = true;
+                    if (u[j] != 0xffffffffu && in_bitmap(fin, u[j])) found = true;
             }
             if (found) {
                 level[v] = L + 1;
                 acc += __ldg(&rowptr[v + 1]) - __ldg(&rowptr[v]);
+            } else {
+                more = e1 < e;
             }
         }
         const unsigned word = __ballot_sync(0xffffffffu, found);
-        if (lane_id() == 0) fout[v >> 5] = word;
-        warp_push(found, v, qout, qsz);
+        if (lane == 0 && word) atomicOr(&fout[v >> 5], word);
+        nfound += found;
+        warp_push(more, v, ovf, &c->ncand[0]);
     }
     warp_add64(acc, &c->m_next);
+    // the next frontier lives in the bitmap; only its size is counted here
+    // (one atomic per warp at the end, not one per iteration)
+    warp_add64(nfound, &c->reached_pull);
+}
+
+// Pull, pass 2: one warp per overflow vertex scans the rest of its in-edges,
+// 32 per probe, and stops at the first parent.
+__global__ void __launch_bounds__(kBlock)
+k_bfs_pull_overflow(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowptr,
+                    TravCtl *c, uint32_t *q0, uint32_t *q1, PullLists p) {
+    if (c->done || c->mode != 1) return;
+    const uint32_t n = c->ncand[0];
+    if (n == 0) return;
+    int32_t *level = static_cast<int32_t *>(c->vdata);
+    const int L = (int)c->level;
+    const uint32_t *__restrict__ fin = c->fb_cur ? p.fb1 : p.fb0;
+    uint32_t *fout = c->fb_cur ? p.fb0 : p.fb1;
+    const uint32_t lane = lane_id();
+    const uint32_t gwarp = (blockIdx.x * kBlock + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * kBlock) >> 5;
+    unsigned long long acc = 0, nfound = 0;
+    for (uint32_t i = gwarp; i < n; i += nwarps) {
+        const uint32_t v = p.cand[i];
+        const uint32_t b = __ldg(&colptr[v]) + kProbe1, e = __ldg(&colptr[v + 1]);
+        bool found = false;
+        for (uint32_t base = b; base < e; base += 32) {
+            const uint32_t j = base + lane;
+            const bool hit = j < e && in_bitmap(fin, __ldg(&p.pidx[j]));
+            if (__any_sync(0xffffffffu, hit)) {
+                found = true;
+                break;
+            }
+        }
+        if (lane == 0 && found) {
+            level[v] = L + 1;
+            atomicOr(&fout[v >> 5], 1u << (v & 31));
+            acc += __ldg(&rowptr[v + 1]) - __ldg(&rowptr[v]);
+            nfound++;
+        }
+    }
+    warp_add64(acc, &c->m_next);
+    warp_add64(nfound, &c->reached_pull);
 }
 
 __global__ void k_bfs_end(TravCtl *c, cudaGraphConditionalHandle h, int use_cond, uint32_t V) {
@@ -168,11 +281,14 @@ __global__ void k_bfs_end(TravCtl *c, cudaGraphConditionalHandle h, int use_cond
         if (c->mode) c->pull_steps++;
         c->m_unvisited -= (c->m_next < c->m_unvisited ? c->m_next : c->m_unvisited);
         c->m_f = c->m_next;
-        if (c->mode) {          // the pull kernel wrote the next frontier's bitmap
+        if (c->mode) {          // the pull kernels wrote the next bitmap and counted it
             c->fb_cur ^= 1;
             c->fb_valid = 1;
+            c->queue_stale = 1;
+            c->qsize[c->cur ^ 1] = (uint32_t)c->reached_pull;
         } else {
             c->fb_valid = 0;
+            c->queue_stale = 0;
         }
         c->cur ^= 1;
         c->level++;
@@ -208,9 +324,106 @@ int traversal_workspace(olv_graph *g, bool pieces) {
     return OLV_OK;
 }
 
+__global__ void k_indeg_keys(const uint32_t *__restrict__ colptr, uint32_t V,
+                             uint32_t *__restrict__ key, uint32_t *__restrict__ val,
+                             unsigned int *__restrict__ counts) {
+    unsigned heavy = 0, light = 0;
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+         v += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t d = colptr[v + 1] - colptr[v];
+        key[v] = d;
+        val[v] = (uint32_t)v;
+        heavy += d > kPullHeavy;
+        light += d > 0 && d <= kPullHeavy;
+    }
+    if (heavy) atomicAdd(&counts[0], heavy);
+    if (light) atomicAdd(&counts[1], light);
+}
+
+// key = (dst << 32) | ~outdeg(src) for every CSC entry: sorting by it orders
+// each vertex's in-edges from the highest out-degree source down.
+__global__ void k_pull_keys(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowidx,
+                            const uint32_t *__restrict__ rowptr, uint32_t V,
+                            unsigned long long *__restrict__ key) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t v = warp; v < V; v += nwarps) {
+        const uint32_t b = colptr[v], e = colptr[v + 1];
+        for (uint32_t i = b + lane; i < e; i += 32) {
+            const uint32_t u = rowidx[i];
+            const uint32_t d = rowptr[u + 1] - rowptr[u];
+            key[i] = ((unsigned long long)v << 32) | (0xffffffffu - d);
+        }
+    }
+}
+
+// Vertices with in-edges, sorted by in-degree (descending, ties by id), split
+// into heavy and light lists for the pull kernel, and the in-edge lists
+// reordered so each vertex first probes its highest out-degree in-neighbours
+// (the ones a BFS reaches first); built once per graph.
+int bfs_pull_lists(olv_graph *g) {
+    Workspace &w = g->ws;
+    if (w.order.p) return OLV_OK;
+    const uint32_t V = g->V;
+    cudaStream_t s = g->stream;
+    DevBuf key, val, key2, temp, cnt;
+    OLV_TRY(key.ensure((size_t)V * 4));
+    OLV_TRY(val.ensure((size_t)V * 4));
+    OLV_TRY(key2.ensure((size_t)V * 4));
+    OLV_TRY(cnt.ensure(16));
+    OLV_TRY(w.order.ensure((size_t)V * 4 + 16));
+    OLV_CUDA(cudaMemsetAsync(cnt.p, 0, 16, s));
+    k_indeg_keys<<<g->num_sms * 8, kBlock, 0, s>>>(g->colptr.as<uint32_t>(), V, key.as<uint32_t>(),
+                                                  val.as<uint32_t>(), cnt.as<unsigned int>());
+    size_t tb = 0;
+    OLV_CUDA(cub::DeviceRadixSort::SortPairsDescending(
+        nullptr, tb, (const uint32_t *)nullptr, (uint32_t *)nullptr, (const uint32_t *)nullptr,
+        (uint32_t *)nullptr, (int64_t)V, 0, 32, s));
+    OLV_TRY(temp.ensure(tb));
+    OLV_CUDA(cub::DeviceRadixSort::SortPairsDescending(
+        temp.p, tb, key.as<uint32_t>(), key2.as<uint32_t>(), val.as<uint32_t>(),
+        w.order.as<uint32_t>(), (int64_t)V, 0, 32, s));
+    unsigned int h[2];
+    OLV_CUDA(cudaMemcpyAsync(h, cnt.p, 8, cudaMemcpyDeviceToHost, s));
+    OLV_CUDA(cudaStreamSynchronize(s));
+    w.n_heavy = h[0];
+    w.n_light = h[1];
+    OLV_TRY(w.cand.ensure((size_t)V * 4 + 16));   // pull overflow list
+    key.release();
+    val.release();
+    key2.release();
+    temp.release();
+    // in-edges by source out-degree, stable (ties keep ascending source ids)
+    const uint64_t E = g->E;
+    OLV_TRY(w.pull_idx.ensure(E * 4 + 16));
+    if (E) {
+        DevBuf k0, k1;
+        OLV_TRY(k0.ensure(E * 8));
+        OLV_TRY(k1.ensure(E * 8));
+        k_pull_keys<<<g->num_sms * 16, kBlock, 0, s>>>(g->colptr.as<uint32_t>(),
+                                                      g->rowidx.as<uint32_t>(),
+                                                      g->rowptr.as<uint32_t>(), V,
+                                                      k0.as<unsigned long long>());
+        size_t tb2 = 0;
+        OLV_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb2, (const unsigned long long *)nullptr,
+                                                 (unsigned long long *)nullptr,
+                                                 (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                                 (int64_t)E, 0, 64, s));
+        OLV_TRY(temp.ensure(tb2));
+        OLV_CUDA(cub::DeviceRadixSort::SortPairs(temp.p, tb2, k0.as<unsigned long long>(),
+                                                 k1.as<unsigned long long>(),
+                                                 g->rowidx.as<uint32_t>(),
+                                                 w.pull_idx.as<uint32_t>(), (int64_t)E, 0, 64, s));
+        OLV_CUDA(cudaStreamSynchronize(s));
+    }
+    return OLV_OK;
+}
+
 static AdvanceArgs bfs_adv_args(olv_graph *g) {
     AdvanceArgs a;
-    a.rowptr = g->rowptr.as<uint32_t>();
+    a.rbeg = g->rowptr.as<uint32_t>();
+    a.rend = g->rowptr.as<uint32_t>() + 1;
     a.col = g->col.as<uint32_t>();
     a.ctl = g->ws.ctl.as<TravCtl>();
     a.q0 = g->ws.q0.as<uint32_t>();
@@ -220,6 +433,8 @@ static AdvanceArgs bfs_adv_args(olv_graph *g) {
     a.hub_degree = g->tune.hub_degree;
     a.piece = g->tune.piece;
     a.want_mode = 0;
+    a.rbeg2 = a.rend2 = nullptr;
+    a.want_mode2 = 0xffffffffu;
     return a;
 }
 
@@ -231,23 +446,33 @@ static int bfs_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle h
     float alpha = g->tune.alpha, beta = g->tune.beta;
     AdvanceArgs a = bfs_adv_args(g);
     BfsPushOp op = {};
-    op.rowptr = a.rowptr;
+    op.rowptr = g->rowptr.as<uint32_t>();
     const uint32_t *colptr = g->colptr.as<uint32_t>();
-    const uint32_t *rowidx = g->rowidx.as<uint32_t>();
-    const uint32_t *rowptr = a.rowptr;
+    const uint32_t *rowptr = g->rowptr.as<uint32_t>();
     uint32_t *q0 = a.q0, *q1 = a.q1;
     const int nb = g->persist_blocks;
+    PullLists pl;
+    pl.V = V;
+    pl.pidx = g->ws.pull_idx.as<uint32_t>();
+    pl.order = g->ws.order.as<uint32_t>();
+    pl.n_heavy = g->ws.n_heavy;
+    pl.n_light = g->ws.n_light;
+    pl.cand = g->ws.cand.as<uint32_t>();
+    pl.words = ((uint32_t)V + 31) / 32 + 8;
+    pl.fb0 = g->ws.fbits.as<uint32_t>();
+    pl.fb1 = pl.fb0 + pl.words;
     void *a_begin[] = {&ctl, &V, &alpha, &beta};
     OLV_TRY(sink((const void *)k_bfs_begin, dim3(1), dim3(1), a_begin));
+    void *a_fq[] = {&ctl, &q0, &q1, &pl};
+    OLV_TRY(sink((const void *)k_bfs_fb_to_queue, dim3(nb), dim3(kBlock), a_fq));
     void *a_adv[] = {&a, &op};
     OLV_TRY(sink((const void *)k_advance_chunks<BfsPushOp>, dim3(nb), dim3(kBlock), a_adv));
     OLV_TRY(sink((const void *)k_advance_pieces<BfsPushOp>, dim3(nb), dim3(kBlock), a_adv));
-    uint32_t *fb0 = g->ws.fbits.as<uint32_t>();
-    uint32_t *fb1 = fb0 + ((size_t)V + 31) / 32 + 8;
-    void *a_bm[] = {&V, &ctl, &fb0, &fb1};
-    OLV_TRY(sink((const void *)k_bfs_bitmap, dim3(nb), dim3(kBlock), a_bm));
-    void *a_pull[] = {&colptr, &rowidx, &rowptr, &V, &ctl, &q0, &q1, &fb0, &fb1};
+    void *a_prep[] = {&V, &ctl, &pl};
+    OLV_TRY(sink((const void *)k_bfs_pull_prep, dim3(nb), dim3(kBlock), a_prep));
+    void *a_pull[] = {&colptr, &rowptr, &ctl, &q0, &q1, &pl};
     OLV_TRY(sink((const void *)k_bfs_pull, dim3(nb), dim3(kBlock), a_pull));
+    OLV_TRY(sink((const void *)k_bfs_pull_overflow, dim3(nb), dim3(kBlock), a_pull));
     void *a_end[] = {&ctl, &h, &use_cond, &V};
     OLV_TRY(sink((const void *)k_bfs_end, dim3(1), dim3(1), a_end));
     return OLV_OK;
@@ -297,6 +522,7 @@ extern "C" int olv_bfs(olv_graph *g, uint32_t src, int32_t *level_out, olv_stats
     OLV_CHECK_ARG(g && level_out, "olv_bfs: null pointer");
     OLV_CHECK_ARG(src < g->V, "olv_bfs: source %u out of range (V=%u)", src, g->V);
     OLV_TRY(traversal_workspace(g, true));
+    OLV_TRY(bfs_pull_lists(g));
     const bool dev_out = is_device_ptr(level_out);
     if (!dev_out) OLV_TRY(g->ws.level.ensure((size_t)g->V * 4 + 16));
     int32_t *level = dev_out ? level_out : g->ws.level.as<int32_t>();

@@ -157,7 +157,8 @@ extern "C" int olv_bfs_noalloc(const uint32_t *rowptr, const uint32_t *col, uint
     k_fill_i32<<<sms * 8, kBlock, 0, s>>>(level_out, V, kInf);
     k_bfs_init<<<1, 1, 0, s>>>(ctl, level_out, sc->q0, rowptr, src, (unsigned long long)E);
     AdvanceArgs a;
-    a.rowptr = rowptr;
+    a.rbeg = rowptr;
+    a.rend = rowptr + 1;
     a.col = col;
     a.ctl = ctl;
     a.q0 = sc->q0;
@@ -167,6 +168,8 @@ extern "C" int olv_bfs_noalloc(const uint32_t *rowptr, const uint32_t *col, uint
     a.hub_degree = kNoAllocHub;
     a.piece = kNoAllocPiece;
     a.want_mode = 0;
+    a.rbeg2 = a.rend2 = nullptr;
+    a.want_mode2 = 0xffffffffu;
     NoAllocBfsOp op = {};
     op.rowptr = rowptr;
     op.V = V;

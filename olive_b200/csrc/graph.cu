@@ -49,6 +49,13 @@ void DevBuf::release() {
     bytes = 0;
 }
 
+int resident_blocks(const olv_graph *g, const void *kernel, int *blocks) {
+    int per_sm = 0;
+    OLV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, 0));
+    *blocks = (per_sm < 1 ? 1 : per_sm) * g->num_sms;
+    return OLV_OK;
+}
+
 bool is_device_ptr(const void *p) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {

@@ -26,16 +26,23 @@
 namespace olv {
 
 int traversal_workspace(olv_graph *g, bool pieces);
+int bfs_pull_lists(olv_graph *g);
+
+constexpr uint32_t kMsHeavy = 128;     // in-degree above which pieces are used (same split as BFS)
+constexpr uint32_t kMsPiece = 2048;    // in-edges per heavy piece
 
 struct MsState {
     DevBuf masks;     // visit | cur | next, V words each
     DevBuf srcs;
+    DevBuf pieces;    // (vertex, first in-edge, end) of heavy vertices' in-edge pieces
+    uint32_t npieces = 0;
     WhileGraph graph;
     int32_t *graph_levels = nullptr;
     uint32_t graph_n = 0;
     ~MsState() {
         masks.release();
         srcs.release();
+        pieces.release();
         graph.destroy();
     }
 };
@@ -62,12 +69,18 @@ struct MsPushOp {
     __device__ __forceinline__ void flush(unsigned long long) {}
 };
 
-__device__ __forceinline__ void write_levels(int32_t *levels, uint64_t V, uint32_t v,
-                                             unsigned long long bits, int32_t value) {
-    while (bits) {
-        const int s = __ffsll((long long)bits) - 1;
-        bits &= bits - 1;
-        levels[(uint64_t)s * V + v] = value;
+// levels[s][v] = value for every set bit s of bits.  All 32 lanes call it with
+// consecutive v: the loop runs over the bits set in any lane, so each store
+// instruction writes one row s at consecutive columns (coalesced).
+__device__ __forceinline__ void write_levels_warp(int32_t *levels, uint64_t V, uint32_t v,
+                                                  unsigned long long bits, int32_t value) {
+    unsigned long long any = bits;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) any |= __shfl_xor_sync(0xffffffffu, any, o);
+    while (any) {
+        const int s = __ffsll((long long)any) - 1;
+        any &= any - 1;
+        if ((bits >> s) & 1ULL) levels[(uint64_t)s * V + v] = value;
     }
 }
 
@@ -107,23 +120,55 @@ __global__ void k_ms_begin(TravCtl *c, unsigned long long E, float alpha) {
         return;
     }
     c->mode = ((double)c->m_f * alpha > (double)E) ? 1u : 0u;
+    if (c->mode == 0 && c->level > 0) c->qsize[c->cur] = 0;   // rebuilt by k_ms_queue
     c->qsize[c->cur ^ 1] = 0;
     c->npieces = 0;
     c->m_next = 0;
+    c->reached_pull = 0;
 }
 
 constexpr int kMsParents = 4;
 
+// Pull.  Heavy vertices' in-edges come as pieces of kMsPiece edges, one warp
+// per piece, ORed into next[v] with atomicOr (OR is order-free).  Light
+// vertices (in-degree 1..kMsHeavy) are scanned by one thread each over
+// consecutive ids.  Both stop once every missing source is found.
 __global__ void __launch_bounds__(kBlock)
 k_ms_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowidx, uint32_t V,
           unsigned long long srcmask, const TravCtl *c, const unsigned long long *__restrict__ visit,
-          const unsigned long long *__restrict__ cur, unsigned long long *__restrict__ next) {
+          const unsigned long long *__restrict__ cur, unsigned long long *__restrict__ next,
+          const uint4 *__restrict__ pieces, uint32_t npieces) {
     if (c->done || c->mode != 1) return;
-    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
-         v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t p = gwarp; p < npieces; p += nwarps) {
+        const uint4 pc = pieces[p];
+        const uint32_t v = pc.x;
         const unsigned long long todo = ~visit[v] & srcmask;
         if (!todo) continue;
+        unsigned long long acc = 0;
+        for (uint32_t base = pc.y; base < pc.z; base += 32 * kMsParents) {
+#pragma unroll
+            for (int j = 0; j < kMsParents; j++) {
+                const uint32_t i = base + j * 32 + lane;
+                if (i < pc.z) acc |= __ldg(&cur[__ldg(&rowidx[i])]);
+            }
+            unsigned long long all = acc;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) all |= __shfl_xor_sync(0xffffffffu, all, o);
+            if ((all & todo) == todo) break;
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) acc |= __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0 && (acc & todo)) atomicOr(&next[v], acc & todo);
+    }
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+         v += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t b = __ldg(&colptr[v]), e = __ldg(&colptr[v + 1]);
+        if (e - b > kMsHeavy || e == b) continue;
+        const unsigned long long todo = ~visit[v] & srcmask;
+        if (!todo) continue;
         unsigned long long acc = 0;
         for (uint32_t i = b; i < e; i += kMsParents) {
             uint32_t u[kMsParents];
@@ -134,24 +179,23 @@ k_ms_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowi
                 if (u[j] != 0xffffffffu) acc |= __ldg(&cur[u[j]]);
             if ((acc & todo) == todo) break;
         }
-        if (acc & todo) next[v] = acc & todo;
+        if (acc & todo) atomicOr(&next[v], acc & todo);
     }
 }
 
 __global__ void __launch_bounds__(kBlock)
 k_ms_apply(uint32_t V, TravCtl *c, const uint32_t *__restrict__ rowptr,
            unsigned long long *__restrict__ visit, unsigned long long *__restrict__ cur,
-           unsigned long long *__restrict__ next, uint32_t *q0, uint32_t *q1) {
+           unsigned long long *__restrict__ next) {
     if (c->done) return;
     int32_t *levels = static_cast<int32_t *>(c->vdata);
     const int32_t lv = (int32_t)c->level + 1;
-    uint32_t *qout = c->cur ? q0 : q1;
-    uint32_t *qsz = &c->qsize[c->cur ^ 1];
-    unsigned long long m_next = 0, traversed = 0;
+    unsigned long long m_next = 0, traversed = 0, nact = 0;
     for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V;
          base += (uint64_t)gridDim.x * kBlock) {
         const uint64_t v = base + threadIdx.x;
         bool act = false;
+        unsigned long long bits = 0;
         if (v < V) {
             const unsigned long long nx = next[v], oc = cur[v];
             unsigned long long nw = 0;
@@ -161,7 +205,6 @@ k_ms_apply(uint32_t V, TravCtl *c, const uint32_t *__restrict__ rowptr,
                 next[v] = 0;
                 if (nw) {
                     visit[v] = vis | nw;
-                    write_levels(levels, V, (uint32_t)v, nw, lv);
                     const uint32_t d = __ldg(&rowptr[v + 1]) - __ldg(&rowptr[v]);
                     m_next += d;
                     traversed += (unsigned long long)d * __popcll(nw);
@@ -169,17 +212,35 @@ k_ms_apply(uint32_t V, TravCtl *c, const uint32_t *__restrict__ rowptr,
                 }
             }
             if (oc != nw) cur[v] = nw;
+            bits = nw;
         }
-        warp_push(act, (uint32_t)v, qout, qsz);
+        write_levels_warp(levels, V, (uint32_t)v, bits, lv);
+        nact += act;
     }
+    // the next frontier is the dense cur[] array; only its size is counted here
     warp_add64(m_next, &c->m_next);
     warp_add64(traversed, &c->edges_traversed);
+    warp_add64(nact, &c->reached_pull);
+}
+
+// Queue of the active vertices (cur != 0) for a push level.
+__global__ void __launch_bounds__(kBlock)
+k_ms_queue(uint32_t V, TravCtl *c, const unsigned long long *__restrict__ cur, uint32_t *q0,
+           uint32_t *q1) {
+    if (c->done || c->mode != 0 || c->level == 0) return;   // level 0: init wrote the queue
+    uint32_t *q = c->cur ? q1 : q0;
+    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V;
+         base += (uint64_t)gridDim.x * kBlock) {
+        const uint64_t v = base + threadIdx.x;
+        warp_push(v < V && cur[v] != 0, (uint32_t)v, q, &c->qsize[c->cur]);
+    }
 }
 
 __global__ void k_ms_end(TravCtl *c, cudaGraphConditionalHandle h, int use_cond, uint32_t V) {
     if (!c->done) {
         if (c->mode) c->pull_steps++;
         c->m_f = c->m_next;
+        c->qsize[c->cur ^ 1] = (uint32_t)c->reached_pull;
         c->cur ^= 1;
         c->level++;
         c->steps++;
@@ -199,11 +260,16 @@ k_ms_finish(uint32_t V, unsigned long long srcmask, TravCtl *c,
             const unsigned long long *__restrict__ visit) {
     int32_t *levels = static_cast<int32_t *>(c->vdata);
     unsigned long long reached = 0;
-    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
-         v += (uint64_t)gridDim.x * blockDim.x) {
-        const unsigned long long vis = visit[v] & srcmask;
-        reached += __popcll(vis);
-        write_levels(levels, V, (uint32_t)v, ~vis & srcmask, kInf);
+    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V;
+         base += (uint64_t)gridDim.x * kBlock) {
+        const uint64_t v = base + threadIdx.x;
+        unsigned long long miss = 0;
+        if (v < V) {
+            const unsigned long long vis = visit[v] & srcmask;
+            reached += __popcll(vis);
+            miss = ~vis & srcmask;
+        }
+        write_levels_warp(levels, V, (uint32_t)v, miss, kInf);
     }
     warp_add64(reached, &c->reached);
 }
@@ -220,7 +286,8 @@ static int ms_superstep(olv_graph *g, MsState &ms, Sink &&sink, cudaGraphConditi
     unsigned long long *cur = visit + V;
     unsigned long long *next = cur + V;
     AdvanceArgs a;
-    a.rowptr = g->rowptr.as<uint32_t>();
+    a.rbeg = g->rowptr.as<uint32_t>();
+    a.rend = g->rowptr.as<uint32_t>() + 1;
     a.col = g->col.as<uint32_t>();
     a.ctl = ctl;
     a.q0 = g->ws.q0.as<uint32_t>();
@@ -230,28 +297,61 @@ static int ms_superstep(olv_graph *g, MsState &ms, Sink &&sink, cudaGraphConditi
     a.hub_degree = g->tune.hub_degree;
     a.piece = g->tune.piece;
     a.want_mode = 0;
+    a.rbeg2 = a.rend2 = nullptr;
+    a.want_mode2 = 0xffffffffu;
     MsPushOp op;
     op.cur = cur;
     op.visit = visit;
     op.next = next;
     const uint32_t *colptr = g->colptr.as<uint32_t>();
-    const uint32_t *rowidx = g->rowidx.as<uint32_t>();
-    const uint32_t *rowptr = a.rowptr;
+    // in-edges ordered by source out-degree: early exits come sooner
+    const uint32_t *rowidx = g->ws.pull_idx.p ? g->ws.pull_idx.as<uint32_t>()
+                                              : g->rowidx.as<uint32_t>();
+    const uint32_t *rowptr = g->rowptr.as<uint32_t>();
     const TravCtl *cctl = ctl;
     const unsigned long long *cvisit = visit, *ccur = cur;
     uint32_t *q0 = a.q0, *q1 = a.q1;
-    const int nb = g->persist_blocks;
+    int nb = 0;
+    OLV_TRY(resident_blocks(g, (const void *)k_advance_chunks<MsPushOp>, &nb));
     void *a_begin[] = {&ctl, &E, &alpha};
     OLV_TRY(sink((const void *)k_ms_begin, dim3(1), dim3(1), a_begin));
+    const unsigned long long *ccur2 = cur;
+    void *a_q[] = {&V, &ctl, &ccur2, &q0, &q1};
+    OLV_TRY(sink((const void *)k_ms_queue, dim3(nb), dim3(kBlock), a_q));
     void *a_adv[] = {&a, &op};
     OLV_TRY(sink((const void *)k_advance_chunks<MsPushOp>, dim3(nb), dim3(kBlock), a_adv));
     OLV_TRY(sink((const void *)k_advance_pieces<MsPushOp>, dim3(nb), dim3(kBlock), a_adv));
-    void *a_pull[] = {&colptr, &rowidx, &V, &srcmask, &cctl, &cvisit, &ccur, &next};
+    const uint4 *pcs = ms.pieces.as<uint4>();
+    uint32_t npcs = ms.npieces;
+    void *a_pull[] = {&colptr, &rowidx, &V, &srcmask, &cctl, &cvisit, &ccur, &next, &pcs, &npcs};
     OLV_TRY(sink((const void *)k_ms_pull, dim3(nb), dim3(kBlock), a_pull));
-    void *a_apply[] = {&V, &ctl, &rowptr, &visit, &cur, &next, &q0, &q1};
+    void *a_apply[] = {&V, &ctl, &rowptr, &visit, &cur, &next};
     OLV_TRY(sink((const void *)k_ms_apply, dim3(nb), dim3(kBlock), a_apply));
     void *a_end[] = {&ctl, &h, &use_cond, &V};
     OLV_TRY(sink((const void *)k_ms_end, dim3(1), dim3(1), a_end));
+    return OLV_OK;
+}
+
+// In-edge pieces of the heavy vertices (in-degree above kMsHeavy), once per graph.
+static int ms_pieces(olv_graph *g, MsState &ms) {
+    if (ms.pieces.p) return OLV_OK;
+    OLV_TRY(bfs_pull_lists(g));
+    const uint32_t nh = g->ws.n_heavy;
+    std::vector<uint32_t> order(nh), cp((size_t)g->V + 1);
+    if (nh)
+        OLV_CUDA(cudaMemcpy(order.data(), g->ws.order.p, (size_t)nh * 4, cudaMemcpyDeviceToHost));
+    OLV_CUDA(cudaMemcpy(cp.data(), g->colptr.p, ((size_t)g->V + 1) * 4, cudaMemcpyDeviceToHost));
+    std::vector<uint4> pcs;
+    for (uint32_t i = 0; i < nh; i++) {
+        const uint32_t v = order[i], b = cp[v], e = cp[v + 1];
+        for (uint32_t x = b; x < e; x += kMsPiece)
+            pcs.push_back(make_uint4(v, x, e - x > kMsPiece ? x + kMsPiece : e, 0));
+    }
+    ms.npieces = (uint32_t)pcs.size();
+    OLV_TRY(ms.pieces.ensure(pcs.size() * sizeof(uint4) + 16));
+    if (!pcs.empty())
+        OLV_CUDA(cudaMemcpy(ms.pieces.p, pcs.data(), pcs.size() * sizeof(uint4),
+                            cudaMemcpyHostToDevice));
     return OLV_OK;
 }
 
@@ -284,6 +384,7 @@ extern "C" int olv_msbfs(olv_graph *g, const uint32_t *srcs, int n, int32_t *lev
         OLV_CHECK_ARG(hs[i] < g->V, "olv_msbfs: source %u out of range (V=%u)", hs[i], g->V);
     OLV_TRY(traversal_workspace(g, true));
     MsState &ms = *ms_state(g);
+    OLV_TRY(ms_pieces(g, ms));
     const size_t V = g->V;
     OLV_TRY(ms.masks.ensure(V * 24 + 64));
     OLV_TRY(ms.srcs.ensure(64 * 4));

@@ -63,6 +63,88 @@ __device__ __forceinline__ void warp_push_n(const int (&act)[N], const uint32_t 
     }
 }
 
+// Pushes are staged in shared memory and moved to the global queue in bulk,
+// so the queue's tail counter sees one atomic per CTA chunk (or per warp
+// buffer) instead of one per warp per round: a single counter hit by every
+// warp serialises at its L2 slice.
+constexpr uint32_t kStage = 2048;   // staged entries per CTA and queue
+constexpr uint32_t kWarpStage = 512;  // staged entries per warp and queue (pieces)
+
+// Warp appends its entries with act[j] == want to a staging buffer (shared
+// atomics).  A batch that does not fit goes straight to the global queue and
+// records its reservation start in *s_lim: reservations are ordered, so every
+// batch staged before it lies below that position, and the buffer's valid
+// entries are [0, min(*s_n, *s_lim)).
+template <int N>
+__device__ __forceinline__ void stage_push_n(const int (&act)[N], const uint32_t (&v)[N], int want,
+                                             uint32_t *s_buf, uint32_t *s_n, uint32_t *s_lim,
+                                             uint32_t cap, uint32_t *__restrict__ q,
+                                             uint32_t *qsize) {
+    unsigned m[N];
+    uint32_t tot = 0;
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+        m[j] = __ballot_sync(0xffffffffu, act[j] == want);
+        tot += __popc(m[j]);
+    }
+    if (!tot) return;
+    const uint32_t lane = lane_id();
+    uint32_t pos = 0;
+    if (lane == 0) {
+        pos = atomicAdd(s_n, tot);
+        if (pos + tot > cap) {               // does not fit: global queue instead
+            atomicMin(s_lim, pos);
+            pos = 0x80000000u | atomicAdd(qsize, tot);
+        }
+    }
+    pos = __shfl_sync(0xffffffffu, pos, 0);
+    uint32_t *dst = s_buf;
+    if (pos & 0x80000000u) {
+        dst = q;
+        pos &= 0x7fffffffu;
+    }
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+        if (act[j] == want) dst[pos + __popc(m[j] & lt)] = v[j];
+        pos += __popc(m[j]);
+    }
+}
+
+// Whole CTA: move the staged entries to the global queue with one atomic.
+__device__ __forceinline__ void stage_flush(uint32_t *s_buf, uint32_t *s_n, uint32_t *s_lim,
+                                            uint32_t *s_base, uint32_t *__restrict__ q,
+                                            uint32_t *qsize) {
+    __syncthreads();
+    const uint32_t n = min(*s_n, *s_lim);
+    if (threadIdx.x == 0) *s_base = n ? atomicAdd(qsize, n) : 0;
+    __syncthreads();
+    const uint32_t base = *s_base;
+    for (uint32_t i = threadIdx.x; i < n; i += kBlock) q[base + i] = s_buf[i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *s_n = 0;
+        *s_lim = kStage;
+    }
+}
+
+// One warp: move its staged entries to the global queue with one atomic.
+__device__ __forceinline__ void warp_stage_flush(uint32_t *s_buf, uint32_t *s_n, uint32_t *s_lim,
+                                                 uint32_t *__restrict__ q, uint32_t *qsize) {
+    __syncwarp();
+    const uint32_t n = min(*s_n, *s_lim);
+    uint32_t base = 0;
+    if (lane_id() == 0 && n) base = atomicAdd(qsize, n);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (uint32_t i = lane_id(); i < n; i += 32) q[base + i] = s_buf[i];
+    __syncwarp();
+    if (lane_id() == 0) {
+        *s_n = 0;
+        *s_lim = kWarpStage;
+    }
+    __syncwarp();
+}
+
 // Warp sum of a 64-bit value added to *dst by lane 0.  All lanes must call.
 __device__ __forceinline__ void warp_add64(unsigned long long x, unsigned long long *dst) {
 #pragma unroll
@@ -101,10 +183,14 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *t
     return r;
 }
 
-constexpr int kItems = 4;   // edges per thread kept in flight
+#ifndef OLV_ITEMS
+#define OLV_ITEMS 8
+#endif
+constexpr int kItems = OLV_ITEMS;   // edges per thread kept in flight
 
 struct AdvanceArgs {
-    const uint32_t *rowptr;
+    const uint32_t *rbeg;       // row u's edges are [rbeg[u], rend[u]) (CSR: rowptr, rowptr+1)
+    const uint32_t *rend;
     const uint32_t *col;
     TravCtl *ctl;
     uint32_t *q0, *q1;          // queue buffers; ctl->cur selects the input
@@ -112,14 +198,36 @@ struct AdvanceArgs {
     uint2 *pieces;              // (row, piece index) of split hub rows
     uint32_t hub_degree;
     uint32_t piece;
-    uint32_t want_mode;         // kernel runs only when ctl->mode == want_mode
+    uint32_t want_mode;         // kernel runs only when ctl->mode == want_mode ...
+    const uint32_t *rbeg2;      // ... or, with these row ranges, when it is want_mode2
+    const uint32_t *rend2;
+    uint32_t want_mode2;        // 0xffffffff: no second mode
 };
+
+// Row ranges for the current mode, or false when the kernel has nothing to do.
+__device__ __forceinline__ bool advance_ranges(const AdvanceArgs &a, const TravCtl *c,
+                                               const uint32_t *&rbeg, const uint32_t *&rend) {
+    if (c->done) return false;
+    const uint32_t m = c->mode;
+    if (m == a.want_mode) {
+        rbeg = a.rbeg;
+        rend = a.rend;
+        return true;
+    }
+    if (m == a.want_mode2) {
+        rbeg = a.rbeg2;
+        rend = a.rend2;
+        return true;
+    }
+    return false;
+}
 
 // Per-superstep chunk expansion over the input queue.
 template <class Op>
 __global__ void __launch_bounds__(kBlock) k_advance_chunks(AdvanceArgs a, Op op) {
     TravCtl *c = a.ctl;
-    if (c->done || c->mode != a.want_mode) return;
+    const uint32_t *rbeg, *rend;
+    if (!advance_ranges(a, c, rbeg, rend)) return;
     op.begin(c);
     const uint32_t cur = c->cur;
     const uint32_t n = c->qsize[cur];
@@ -134,6 +242,15 @@ __global__ void __launch_bounds__(kBlock) k_advance_chunks(AdvanceArgs a, Op op)
     __shared__ uint32_t s_off[kBlock];
     __shared__ SV s_val[kBlock];
     __shared__ uint32_t s_warp[33];
+    constexpr uint32_t kFarStage = Op::kHasFar ? kStage : 1;
+    __shared__ uint32_t s_q[kStage], s_f[kFarStage];
+    __shared__ uint32_t s_qn, s_fn, s_qlim, s_flim, s_base;
+    if (threadIdx.x == 0) {
+        s_qn = 0;
+        s_fn = 0;
+        s_qlim = kStage;
+        s_flim = kStage;
+    }
 
     unsigned long long relaxed = 0;
     for (uint32_t chunk = blockIdx.x; (uint64_t)chunk * kBlock < n; chunk += gridDim.x) {
@@ -142,8 +259,8 @@ __global__ void __launch_bounds__(kBlock) k_advance_chunks(AdvanceArgs a, Op op)
         SV sv = 0;
         if (i < n) {
             const uint32_t u = qin[i];
-            beg = __ldg(&a.rowptr[u]);
-            deg = __ldg(&a.rowptr[u + 1]) - beg;
+            beg = __ldg(&rbeg[u]);
+            deg = __ldg(&rend[u]) - beg;
             if (deg > a.hub_degree) {
                 const uint32_t np = (deg + a.piece - 1) / a.piece;
                 const uint32_t b = atomicAdd(&c->npieces, np);
@@ -190,11 +307,14 @@ __global__ void __launch_bounds__(kBlock) k_advance_chunks(AdvanceArgs a, Op op)
                 if (act[j]) pre[j] = op.prepare(sv[j], e[j], v[j]);
 #pragma unroll
             for (int j = 0; j < kItems; j++) act[j] = act[j] ? op.apply(pre[j], v[j]) : 0;
-            warp_push_n<kItems>(act, v, 1, qout, qout_size);
-            if (Op::kHasFar) warp_push_n<kItems>(act, v, 2, far, far_size);
+            stage_push_n<kItems>(act, v, 1, s_q, &s_qn, &s_qlim, kStage, qout, qout_size);
+            if (Op::kHasFar)
+                stage_push_n<kItems>(act, v, 2, s_f, &s_fn, &s_flim, kStage, far, far_size);
 #pragma unroll
             for (int j = 0; j < kItems; j++) op.on_push(act[j] == 1, v[j]);
         }
+        stage_flush(s_q, &s_qn, &s_qlim, &s_base, qout, qout_size);
+        if (Op::kHasFar) stage_flush(s_f, &s_fn, &s_flim, &s_base, far, far_size);
         __syncthreads();
     }
     op.flush(relaxed);
@@ -204,7 +324,8 @@ __global__ void __launch_bounds__(kBlock) k_advance_chunks(AdvanceArgs a, Op op)
 template <class Op>
 __global__ void __launch_bounds__(kBlock) k_advance_pieces(AdvanceArgs a, Op op) {
     TravCtl *c = a.ctl;
-    if (c->done || c->mode != a.want_mode) return;
+    const uint32_t *rbeg, *rend;
+    if (!advance_ranges(a, c, rbeg, rend)) return;
     const uint32_t np = c->npieces;
     if (np == 0) return;
     op.begin(c);
@@ -216,10 +337,22 @@ __global__ void __launch_bounds__(kBlock) k_advance_pieces(AdvanceArgs a, Op op)
     const uint32_t lane = lane_id();
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    constexpr uint32_t kFarW = Op::kHasFar ? kWarpStage : 1;
+    __shared__ uint32_t s_q[kBlock / 32][kWarpStage], s_f[kBlock / 32][kFarW];
+    __shared__ uint32_t s_qn[kBlock / 32], s_fn[kBlock / 32];
+    __shared__ uint32_t s_qlim[kBlock / 32], s_flim[kBlock / 32];
+    const uint32_t wl = threadIdx.x >> 5;
+    if (lane == 0) {
+        s_qn[wl] = 0;
+        s_fn[wl] = 0;
+        s_qlim[wl] = kWarpStage;
+        s_flim[wl] = kWarpStage;
+    }
+    __syncwarp();
     for (uint32_t p = warp; p < np; p += nwarps) {
         const uint2 pc = a.pieces[p];
         const uint32_t u = pc.x;
-        const uint32_t rb = __ldg(&a.rowptr[u]), re = __ldg(&a.rowptr[u + 1]);
+        const uint32_t rb = __ldg(&rbeg[u]), re = __ldg(&rend[u]);
         const uint32_t b = rb + pc.y * a.piece;
         const uint32_t e_end = min(re, b + a.piece);
         const typename Op::SV sv = op.src_value(u);
@@ -238,12 +371,25 @@ __global__ void __launch_bounds__(kBlock) k_advance_pieces(AdvanceArgs a, Op op)
                 if (act[j]) pre[j] = op.prepare(sv, e[j], v[j]);
 #pragma unroll
             for (int j = 0; j < kItems; j++) act[j] = act[j] ? op.apply(pre[j], v[j]) : 0;
-            warp_push_n<kItems>(act, v, 1, qout, qout_size);
-            if (Op::kHasFar) warp_push_n<kItems>(act, v, 2, far, far_size);
+            // flush before a round could overflow the warp's buffers (the
+            // counts were last written by lane 0's shared atomics)
+            __syncwarp();
+            if (s_qn[wl] + 32 * kItems > kWarpStage)
+                warp_stage_flush(s_q[wl], &s_qn[wl], &s_qlim[wl], qout, qout_size);
+            stage_push_n<kItems>(act, v, 1, s_q[wl], &s_qn[wl], &s_qlim[wl], kWarpStage, qout,
+                                 qout_size);
+            if (Op::kHasFar) {
+                if (s_fn[wl] + 32 * kItems > kWarpStage)
+                    warp_stage_flush(s_f[wl], &s_fn[wl], &s_flim[wl], far, far_size);
+                stage_push_n<kItems>(act, v, 2, s_f[wl], &s_fn[wl], &s_flim[wl], kWarpStage, far,
+                                     far_size);
+            }
 #pragma unroll
             for (int j = 0; j < kItems; j++) op.on_push(act[j] == 1, v[j]);
         }
     }
+    warp_stage_flush(s_q[wl], &s_qn[wl], &s_qlim[wl], qout, qout_size);
+    if (Op::kHasFar) warp_stage_flush(s_f[wl], &s_fn[wl], &s_flim[wl], far, far_size);
     op.flush(0);
 }
 

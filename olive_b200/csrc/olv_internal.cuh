@@ -67,6 +67,12 @@ struct TravCtl {
     uint32_t split_lo;          // SSSP: lower edge of the bucket being split
     uint32_t fb_cur;            // BFS: which frontier bitmap holds the current level
     uint32_t fb_valid;          // BFS: that bitmap is up to date
+    uint32_t ncand[4];          // BFS pull candidates: heavy[0..1], light[2..3]
+    uint32_t cand_cur;          // BFS: candidate lists holding this level's input
+    uint32_t cand_valid;        // BFS: candidate lists hold exactly the unvisited vertices
+    uint32_t queue_stale;       // BFS: the frontier is only in the bitmap (after a pull level)
+    uint32_t heavy_done;        // SSSP: heavy edges of the current bucket relaxed
+    uint32_t bucket_lo;         // SSSP: lower distance edge of the current bucket
     void *vdata;                // per-vertex result array of the run (level / dist)
     unsigned long long m_f;         // out-edges of the input frontier
     unsigned long long m_next;      // out-edges of vertices discovered this superstep
@@ -74,6 +80,7 @@ struct TravCtl {
     unsigned long long edges_traversed;
     unsigned long long edges_relaxed;
     unsigned long long reached;
+    unsigned long long reached_pull;   // BFS: vertices found by this pull level
 };
 
 // Tunables (olv_autotune writes them; defaults are set at graph creation).
@@ -82,7 +89,7 @@ struct Tuning {
     uint32_t piece = 1024;        // edges per piece
     float alpha = 14.0f;          // push -> pull when m_f > m_unvisited / alpha
     float beta = 24.0f;           // pull -> push when n_f < V / beta
-    uint32_t sssp_delta = 0;      // 0 = derived from the weights
+    uint32_t sssp_delta = 0;      // 0 = default bucket width (64)
     float ms_alpha = 4.0f;        // msBFS: pull when active out-edges * ms_alpha > E
     int levels_per_sync = 4;      // host loop: supersteps enqueued per check
     int use_graphs = 1;           // run supersteps inside a CUDA graph
@@ -90,9 +97,16 @@ struct Tuning {
 
 struct Workspace {
     DevBuf level, q0, q1, pieces, ctl, mark, far0, far1, tmp, partials, fbits;
+    DevBuf order, cand;             // BFS pull: in-degree-sorted vertices, candidate lists
+    DevBuf pull_idx;                // BFS pull: in-edges sorted by source out-degree (desc)
+    DevBuf sssp_col, sssp_w, rowmid; // SSSP: rows split light (w <= delta) | heavy
+    uint32_t sssp_delta_built = 0;
+    uint32_t n_heavy = 0, n_light = 0;
     void release() {
         level.release(); q0.release(); q1.release(); pieces.release(); ctl.release();
-        fbits.release();
+        fbits.release(); order.release(); cand.release(); pull_idx.release();
+        sssp_col.release(); sssp_w.release(); rowmid.release();
+        sssp_delta_built = 0;
         mark.release(); far0.release(); far1.release(); tmp.release(); partials.release();
     }
 };
@@ -128,6 +142,8 @@ struct olv_graph {
 };
 
 namespace olv {
+// Resident CTAs of kBlock threads for `kernel` on all SMs (a persistent grid).
+int resident_blocks(const olv_graph *g, const void *kernel, int *blocks);
 void release_pr_state(olv_graph *g);
 void release_ms_state(olv_graph *g);
 void release_wpr_state(olv_graph *g);

@@ -27,7 +27,7 @@
 namespace olv {
 
 constexpr uint32_t kNnz = 2048;      // entries staged per row block
-constexpr uint32_t kRows = 2048;     // rows per row block at most
+constexpr uint32_t kRows = 256;      // rows per row block at most (one per thread)
 constexpr uint32_t kSeg = 4096;      // entries per segment of a long row
 constexpr uint32_t kShort = 32;      // rows up to this length are summed by one thread
 constexpr int kGather = kNnz / kBlock;
@@ -145,7 +145,7 @@ k_row_segments(const uint32_t *__restrict__ idx, const uint2 *__restrict__ seg_r
 }
 
 template <class Op>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, 8)
 k_row_blocks(const uint32_t *__restrict__ ptr, const uint32_t *__restrict__ idx,
              const uint32_t *__restrict__ blocks, const uint32_t *__restrict__ segbase,
              const float2 *__restrict__ segs, Op op, double *__restrict__ partials) {

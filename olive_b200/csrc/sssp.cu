@@ -6,13 +6,22 @@
 // (cond/update, SSSP.cu:66-76).  Distances are unique, so the result equals
 // serial Dijkstra bit for bit; 0x7fffffff marks unreached vertices.
 //
-// B200 formulation: the same atomicMin relaxation, ordered by a near/far split
-// (a two-bucket delta-stepping) so that most vertices are relaxed once.  The
-// near queue holds vertices whose tentative distance is below `threshold`; an
-// improvement at or above it goes to the far pile (deduplicated per pile
-// generation).  When the near queue drains, one split pass raises the
-// threshold by delta and moves the far vertices under it to the near queue.
-// Supersteps (relax or split) run as one CUDA graph, as for BFS.
+// B200 formulation: the same atomicMin relaxation, ordered as delta-stepping
+// with a near queue and a far pile, and light/heavy edges (Meyer & Sanders):
+//   * each row is stored light edges first (w <= delta), then heavy ones
+//     (built once per graph and delta, k_partition_rows);
+//   * the near queue holds vertices with tentative distance below
+//     `threshold`; relax supersteps follow only their light edges, and an
+//     improvement at or above the threshold goes to the far pile
+//     (deduplicated per pile generation);
+//   * when the near queue drains, every vertex of the bucket [bucket_lo,
+//     threshold) has its final distance: one heavy superstep collects them
+//     and relaxes their heavy edges once (all such relaxations land at or
+//     above the threshold, in the far pile);
+//   * one split pass then raises the threshold by delta and moves the far
+//     vertices under it to the near queue.
+// Heavy edges are thus relaxed once per reached vertex; only light edges can
+// be relaxed again.  Supersteps run as one CUDA graph, as for BFS.
 #include "olv_advance.cuh"
 #include "olv_graphexec.cuh"
 #include "olv_internal.cuh"
@@ -24,6 +33,47 @@ __global__ void k_fill_i32(int32_t *__restrict__ a, uint32_t n, int32_t x);
 
 constexpr uint32_t kModeRelax = 0;
 constexpr uint32_t kModeSplit = 2;
+constexpr uint32_t kModeHeavy = 3;
+constexpr uint32_t kDefaultDelta = 64;
+
+// Stable partition of every row into light (w <= delta) then heavy edges; one
+// warp per row, two passes (count, then write in order).
+__global__ void k_partition_rows(const uint32_t *__restrict__ rowptr,
+                                 const uint32_t *__restrict__ col, const uint32_t *__restrict__ w,
+                                 uint32_t V, uint32_t delta, uint32_t *__restrict__ pcol,
+                                 uint32_t *__restrict__ pw, uint32_t *__restrict__ rowmid) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    for (uint64_t u = warp; u < V; u += nwarps) {
+        const uint32_t b = rowptr[u], e = rowptr[u + 1];
+        uint32_t nl = 0;
+        for (uint32_t base = b; base < e; base += 32) {
+            const uint32_t i = base + lane;
+            nl += __popc(__ballot_sync(0xffffffffu, i < e && w[i] <= delta));
+        }
+        uint32_t lo = b, hi = b + nl;
+        for (uint32_t base = b; base < e; base += 32) {
+            const uint32_t i = base + lane;
+            const bool ok = i < e;
+            const uint32_t wi = ok ? w[i] : 0, ci = ok ? col[i] : 0;
+            const bool light = ok && wi <= delta;
+            const unsigned ml = __ballot_sync(0xffffffffu, light);
+            const unsigned mh = __ballot_sync(0xffffffffu, ok && !light);
+            if (light) {
+                pcol[lo + __popc(ml & lt)] = ci;
+                pw[lo + __popc(ml & lt)] = wi;
+            } else if (ok) {
+                pcol[hi + __popc(mh & lt)] = ci;
+                pw[hi + __popc(mh & lt)] = wi;
+            }
+            lo += __popc(ml);
+            hi += __popc(mh);
+        }
+        if (lane == 0) rowmid[u] = b + nl;
+    }
+}
 
 struct SsspOp {
     using SV = uint32_t;
@@ -71,6 +121,8 @@ struct SsspOp {
     }
 };
 
+__device__ void sssp_begin(TravCtl *c);
+
 __global__ void k_sssp_init(TravCtl *c, uint32_t *dist, uint32_t *q0, uint32_t src,
                             uint32_t delta) {
     TravCtl t = {};
@@ -80,15 +132,27 @@ __global__ void k_sssp_init(TravCtl *c, uint32_t *dist, uint32_t *q0, uint32_t s
     t.delta = delta;
     t.epoch = 1;
     t.far_min = 0xffffffffu;
+    t.heavy_done = 0;
+    t.bucket_lo = 0;
     *c = t;
     dist[src] = 0;
     q0[0] = src;
+    sssp_begin(c);
 }
 
-__global__ void k_sssp_begin(TravCtl *c) {
+// Choose the next superstep's mode (relax light edges, relax a settled
+// bucket's heavy edges, or split the far pile) and reset its counters.
+__device__ void sssp_begin(TravCtl *c) {
     if (c->done) return;
     if (c->qsize[c->cur] > 0) {
         c->mode = kModeRelax;
+        c->qsize[c->cur ^ 1] = 0;
+        c->npieces = 0;
+        return;
+    }
+    if (!c->heavy_done) {   // bucket settled: collect it and relax its heavy edges
+        c->mode = kModeHeavy;
+        c->qsize[c->cur] = 0;
         c->qsize[c->cur ^ 1] = 0;
         c->npieces = 0;
         return;
@@ -97,9 +161,10 @@ __global__ void k_sssp_begin(TravCtl *c) {
         c->done = 1;
         return;
     }
-    // near queue drained: next bucket starts at max(threshold, smallest far distance)
+    // next bucket starts at max(threshold, smallest far distance)
     c->mode = kModeSplit;
     c->split_lo = c->threshold;   // far entries below it were settled already
+    c->bucket_lo = c->threshold;
     uint32_t lo = c->threshold > c->far_min ? c->threshold : c->far_min;
     uint64_t t = (uint64_t)lo + c->delta;
     c->threshold = t > (uint64_t)kInf ? (uint32_t)kInf : (uint32_t)t;
@@ -107,13 +172,30 @@ __global__ void k_sssp_begin(TravCtl *c) {
     c->far_min = 0xffffffffu;
 }
 
+
+// Heavy superstep, step 1: the vertices of the settled bucket
+// [bucket_lo, threshold) become the input queue.
+__device__ void sssp_collect(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1) {
+    const uint32_t *dist = static_cast<const uint32_t *>(c->vdata);
+    const uint32_t lo = c->bucket_lo, hi = c->threshold;
+    uint32_t *q = c->cur ? q1 : q0;
+    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V;
+         base += (uint64_t)gridDim.x * kBlock) {
+        const uint64_t v = base + threadIdx.x;
+        bool in = false;
+        if (v < V) {
+            const uint32_t d = __ldcg(&dist[v]);
+            in = d >= lo && d < hi;
+        }
+        warp_push(in, (uint32_t)v, q, &c->qsize[c->cur]);
+    }
+}
+
 // Split the far pile: stale entries (distance below the old threshold) are
 // dropped, entries under the new threshold become the near queue, the rest
 // move to the other far buffer under the next generation.
-__global__ void __launch_bounds__(kBlock)
-k_sssp_split(TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0, uint32_t *far1,
-             uint32_t *farmark) {
-    if (c->done || c->mode != kModeSplit) return;
+__device__ void sssp_split(TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0,
+                           uint32_t *far1, uint32_t *farmark) {
     const uint32_t *dist = static_cast<const uint32_t *>(c->vdata);
     const uint32_t fc = c->far_cur;
     const uint32_t n = c->far_size[fc];
@@ -154,18 +236,35 @@ __global__ void k_sssp_end(TravCtl *c, cudaGraphConditionalHandle h, int use_con
     if (!c->done) {
         if (c->mode == kModeRelax) {
             c->cur ^= 1;
+        } else if (c->mode == kModeHeavy) {
+            c->qsize[c->cur] = 0;
+            c->heavy_done = 1;
         } else {
             c->far_cur ^= 1;
             c->epoch++;
+            c->heavy_done = 0;
         }
         c->steps++;
-        if (c->qsize[c->cur] == 0 && c->far_size[c->far_cur] == 0) c->done = 1;
+        if (c->qsize[c->cur] == 0 && c->far_size[c->far_cur] == 0 && c->heavy_done) c->done = 1;
         if (c->steps > max_steps) {
             c->err = 2;
             c->done = 1;
         }
+        sssp_begin(c);   // mode and counters of the next superstep
     }
     if (use_cond) cudaGraphSetConditional(h, c->done ? 0u : 1u);
+}
+
+// The superstep's dense pass: collect the settled bucket (heavy mode) or split
+// the far pile (split mode); nothing in relax mode.
+__global__ void __launch_bounds__(kBlock)
+k_sssp_aux(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0, uint32_t *far1,
+           uint32_t *farmark) {
+    if (c->done) return;
+    if (c->mode == kModeHeavy)
+        sssp_collect(V, c, q0, q1);
+    else if (c->mode == kModeSplit)
+        sssp_split(c, q0, q1, far0, far1, farmark);
 }
 
 // Sum of out-degrees and count of reached vertices (the GTEPS basis).
@@ -186,7 +285,23 @@ __global__ void k_reached_edges(const uint32_t *__restrict__ rowptr,
 // ------------------------------------------------------------------ host --
 static uint32_t sssp_delta(olv_graph *g) {
     if (g->tune.sssp_delta) return g->tune.sssp_delta;
-    return 256;
+    return kDefaultDelta;
+}
+
+// Rows split light | heavy for the current delta (built once per delta).
+static int sssp_partition(olv_graph *g) {
+    Workspace &ws = g->ws;
+    const uint32_t delta = sssp_delta(g);
+    if (ws.sssp_delta_built == delta && ws.rowmid.p) return OLV_OK;
+    OLV_TRY(ws.sssp_col.ensure(g->E * 4 + 16));
+    OLV_TRY(ws.sssp_w.ensure(g->E * 4 + 16));
+    OLV_TRY(ws.rowmid.ensure((size_t)g->V * 4 + 16));
+    k_partition_rows<<<g->num_sms * 16, kBlock, 0, g->stream>>>(
+        g->rowptr.as<uint32_t>(), g->col.as<uint32_t>(), g->w.as<uint32_t>(), g->V, delta,
+        ws.sssp_col.as<uint32_t>(), ws.sssp_w.as<uint32_t>(), ws.rowmid.as<uint32_t>());
+    OLV_CUDA(cudaGetLastError());
+    ws.sssp_delta_built = delta;
+    return OLV_OK;
 }
 
 template <class Sink>
@@ -194,9 +309,10 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
                           int use_cond) {
     Workspace &ws = g->ws;
     TravCtl *ctl = ws.ctl.as<TravCtl>();
-    AdvanceArgs a;
-    a.rowptr = g->rowptr.as<uint32_t>();
-    a.col = g->col.as<uint32_t>();
+    AdvanceArgs a;   // light edges: [rowptr[u], rowmid[u])
+    a.rbeg = g->rowptr.as<uint32_t>();
+    a.rend = ws.rowmid.as<uint32_t>();
+    a.col = ws.sssp_col.as<uint32_t>();
     a.ctl = ctl;
     a.q0 = ws.q0.as<uint32_t>();
     a.q1 = ws.q1.as<uint32_t>();
@@ -206,22 +322,28 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     a.hub_degree = g->tune.hub_degree;
     a.piece = g->tune.piece;
     a.want_mode = kModeRelax;
+    AdvanceArgs ah = a;   // heavy edges: [rowmid[u], rowptr[u+1])
+    ah.rbeg = ws.rowmid.as<uint32_t>();
+    ah.rend = g->rowptr.as<uint32_t>() + 1;
     SsspOp op = {};
-    op.w = g->w.as<uint32_t>();
+    op.w = ws.sssp_w.as<uint32_t>();
     op.mark = ws.mark.as<uint32_t>();
     op.farmark = ws.mark.as<uint32_t>() + g->V;
     uint32_t *q0 = a.q0, *q1 = a.q1, *far0 = a.far0, *far1 = a.far1, *farmark = op.farmark;
     // a correct run needs far fewer supersteps; the bound only stops a runaway loop
     uint32_t max_steps = (uint32_t)(3ULL * g->V + 1000 > 0xfffffff0ULL ? 0xfffffff0ULL
                                                                     : 3ULL * g->V + 1000);
-    const int nb = g->persist_blocks;
-    void *a_begin[] = {&ctl};
-    OLV_TRY(sink((const void *)k_sssp_begin, dim3(1), dim3(1), a_begin));
+    int nb = 0;   // the relax kernel's own residency (it holds more registers than BFS's)
+    OLV_TRY(resident_blocks(g, (const void *)k_advance_chunks<SsspOp>, &nb));
+    uint32_t V = g->V;
+    a.rbeg2 = ah.rbeg;
+    a.rend2 = ah.rend;
+    a.want_mode2 = kModeHeavy;
+    void *a_aux[] = {&V, &ctl, &q0, &q1, &far0, &far1, &farmark};
+    OLV_TRY(sink((const void *)k_sssp_aux, dim3(nb), dim3(kBlock), a_aux));
     void *a_adv[] = {&a, &op};
     OLV_TRY(sink((const void *)k_advance_chunks<SsspOp>, dim3(nb), dim3(kBlock), a_adv));
     OLV_TRY(sink((const void *)k_advance_pieces<SsspOp>, dim3(nb), dim3(kBlock), a_adv));
-    void *a_split[] = {&ctl, &q0, &q1, &far0, &far1, &farmark};
-    OLV_TRY(sink((const void *)k_sssp_split, dim3(nb), dim3(kBlock), a_split));
     void *a_end[] = {&ctl, &h, &use_cond, &max_steps};
     OLV_TRY(sink((const void *)k_sssp_end, dim3(1), dim3(1), a_end));
     return OLV_OK;
@@ -247,6 +369,7 @@ int sssp_workspace(olv_graph *g) {
 }
 
 int run_sssp_device(olv_graph *g, uint32_t src, uint32_t *dist_dev) {
+    OLV_TRY(sssp_partition(g));
     cudaStream_t s = g->stream;
     TravCtl *ctl = g->ws.ctl.as<TravCtl>();
     OLV_CUDA(cudaMemsetAsync(g->ws.mark.p, 0, (size_t)g->V * 8, s));

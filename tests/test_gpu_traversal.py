@@ -257,3 +257,25 @@ def test_msbfs_bad_arguments(ob):
             g.msbfs(np.arange(65, dtype=np.uint32) % 16)
         with pytest.raises(ob.OliveError):
             g.msbfs(np.array([16], np.uint32))
+
+
+# -------------------------------------------------------------- autotune --
+def test_autotune_keeps_results_and_roundtrips(ob, tmp_path):
+    with ob.Graph.rmat(14, 16, 3, weights=True, wseed=4) as g:
+        rp, cl, w = g.csr()
+        hub, _ = g.max_degree_vertex()
+        path = str(tmp_path / "tune.json")
+        best = g.autotune(path, reps=1)
+        assert best["hub_degree"] in (256, 1024, 4096)
+        np.testing.assert_array_equal(g.bfs(hub), oracle.bfs(rp, cl, hub)[0])
+        np.testing.assert_array_equal(g.sssp(hub), oracle.dijkstra(rp, cl, w, hub)[0])
+        txt = open(path).read()
+        assert '"key"' in txt and "sssp_delta" in txt
+    with ob.Graph.rmat(14, 16, 3, weights=True, wseed=4) as g2:
+        g2.tune(hub_degree=4096, sssp_delta=16)
+        assert g2.autotune_load(path)
+        assert g2.tune() == best
+    with ob.Graph.rmat(13, 16, 3) as g3:       # another graph: table not applied
+        before = g3.tune()
+        assert not g3.autotune_load(path)
+        assert g3.tune() == before
