@@ -103,43 +103,71 @@ __global__ void k_bfs_begin(TravCtl *c, uint32_t V, float alpha, float beta) {
     c->npieces = 0;
     c->m_next = 0;
     c->reached_pull = 0;
-    c->ncand[0] = 0;   // pull overflow list
+    c->ncand[0] = 0;   // pull candidate list
+    c->ncand[1] = 0;   // pull overflow list
     if (c->mode == 0 && c->queue_stale) c->qsize[c->cur] = 0;   // rebuilt from the bitmap
 }
 
-// Pull-level preparation (pull levels only), two independent index ranges:
-//   - bitmap of the current frontier (level == L), one ballot per warp, when the
-//     previous level was a push level;
-//   - zero the next frontier's bitmap.
+// Pull lists, built once per graph by bfs_pull_lists.
 struct PullLists {
     uint32_t V;
     const uint32_t *pidx;      // in-edges, highest out-degree source first
+    const uint32_t *first;     // pidx[colptr[v]] (v's likeliest parent), or kNoParent
     const uint32_t *order;     // vertices by in-degree (heavy: in-degree > kPullHeavy)
     uint32_t n_heavy, n_light;
-    uint32_t *cand;            // pull overflow list (V entries)
+    uint32_t *cand;            // vertices whose first probe failed (V entries)
+    uint32_t *ovf;             // candidates with in-edges left after the group pass
     uint32_t *fb0, *fb1;
     uint32_t words;            // words per bitmap
 };
 
 constexpr uint32_t kPullHeavy = 128;   // in-degree split of the sorted vertex list
+constexpr uint32_t kNoParent = 0xffffffffu;
+constexpr uint32_t kGroupProbe = 8;    // in-edges 1..8 probed by the candidate pass
 
+// Four consecutive vertices per thread: v0 = 4 * quad.  Loads level[v0..v0+3]
+// as one int4 when the array is 16-byte aligned and the quad is complete, else
+// one int at a time; vertices >= V read as visited (0).
+__device__ __forceinline__ int4 load_quad_level(const int32_t *level, uint64_t v0, uint32_t V,
+                                                bool vec) {
+    if (vec && v0 + 3 < V) return __ldcg(reinterpret_cast<const int4 *>(level + v0));
+    int4 r = make_int4(0, 0, 0, 0);
+    if (v0 < V) r.x = __ldcg(level + v0);
+    if (v0 + 1 < V) r.y = __ldcg(level + v0 + 1);
+    if (v0 + 2 < V) r.z = __ldcg(level + v0 + 2);
+    if (v0 + 3 < V) r.w = __ldcg(level + v0 + 3);
+    return r;
+}
 
+// The 32-bit bitmap word of the 8 quads held by lanes 8k..8k+7: each lane
+// contributes its 4-bit nibble; lane 8k gets the whole word.
+__device__ __forceinline__ uint32_t quad_word(uint32_t nibble) {
+    uint32_t w = nibble << ((lane_id() & 7) * 4);
+    w |= __shfl_xor_sync(0xffffffffu, w, 1);
+    w |= __shfl_xor_sync(0xffffffffu, w, 2);
+    w |= __shfl_xor_sync(0xffffffffu, w, 4);
+    return w;
+}
+
+// Pull-level preparation, when the previous level was a push level: the
+// current frontier's bitmap (level == L) from the level array, one whole word
+// per 8 lanes.
 __global__ void __launch_bounds__(kBlock)
 k_bfs_pull_prep(uint32_t V, TravCtl *c, PullLists p) {
-    if (c->done || c->mode != 1) return;
+    if (c->done || c->mode != 1 || c->fb_valid) return;
     const int32_t *level = static_cast<const int32_t *>(c->vdata);
     const int L = (int)c->level;
     uint32_t *fcur = c->fb_cur ? p.fb1 : p.fb0;
-    uint32_t *fnext = c->fb_cur ? p.fb0 : p.fb1;
-    const uint64_t stride = (uint64_t)gridDim.x * kBlock;
-    if (!c->fb_valid)
-        for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V; base += stride) {
-            const uint64_t v = base + threadIdx.x;
-            const unsigned word = __ballot_sync(0xffffffffu, v < V && __ldcg(&level[v]) == L);
-            if (lane_id() == 0) fcur[v >> 5] = word;
-        }
-    for (uint64_t w = blockIdx.x * (uint64_t)kBlock + threadIdx.x; w < p.words; w += stride)
-        fnext[w] = 0;
+    const bool vec = ((uintptr_t)level & 15) == 0;
+    const uint64_t nw = ((uint64_t)V + 31) / 32, nquad = nw * 8;
+    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < nquad;
+         base += (uint64_t)gridDim.x * kBlock) {
+        const uint64_t qd = base + threadIdx.x;
+        const int4 lv = load_quad_level(level, qd * 4, V, vec);
+        const uint32_t nib = (lv.x == L) | (lv.y == L) << 1 | (lv.z == L) << 2 | (lv.w == L) << 3;
+        const uint32_t w = quad_word(nib);
+        if ((lane_id() & 7) == 0 && qd < nquad) fcur[qd >> 3] = w;
+    }
 }
 
 // The current frontier as a queue, from its bitmap, when a push level follows
@@ -180,68 +208,168 @@ __device__ __forceinline__ bool in_bitmap(const uint32_t *__restrict__ fb, uint3
     return (__ldg(&fb[u >> 5]) >> (u & 31)) & 1u;
 }
 
-// Pull, pass 1: every unvisited vertex probes its first kProbe1 in-edges (the
-// in-edge lists are ordered by source out-degree, so the likeliest parents
-// come first) against the frontier bitmap, kParents at a time.  A vertex that
-// finds a parent gets level L+1, a bit in the next bitmap and a queue slot;
-// one that has more in-edges left goes to the overflow list.  Every thread
-// does at most kProbe1 probes, so the lanes of a warp finish together.
-constexpr int kParents = 4;
-constexpr uint32_t kProbe1 = 8;
-
-
+// Pull, pass 1.  Each thread takes four consecutive vertices and does one
+// probe per unvisited one: its first in-edge (first[v], the in-neighbour of
+// highest out-degree, the one a BFS reaches earliest) against the frontier
+// bitmap.  Every load is a coalesced vector load except the bitmap probe,
+// which hits a 2 MB bitmap held in L2; the four vertices' loads are issued
+// together.  A vertex whose first probe fails and that has more in-edges goes
+// to the candidate list.  Lanes 8k..8k+7 own one 32-vertex word of the next
+// bitmap and store it whole, so the next bitmap needs no clearing and no
+// atomics in this pass.
 __global__ void __launch_bounds__(kBlock)
 k_bfs_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowptr,
-           TravCtl *c, uint32_t *q0, uint32_t *q1, PullLists p) {
+           TravCtl *c, PullLists p) {
     if (c->done || c->mode != 1) return;
+    int32_t *level = static_cast<int32_t *>(c->vdata);
+    const int L = (int)c->level;
+    const uint32_t V = p.V;
+    const uint32_t *__restrict__ fin = c->fb_cur ? p.fb1 : p.fb0;
+    uint32_t *fout = c->fb_cur ? p.fb0 : p.fb1;
+    const bool vec = ((uintptr_t)level & 15) == 0;
+    const uint32_t wl = threadIdx.x >> 5;
+    __shared__ uint32_t s_c[kBlock / 32][kWarpStage];
+    __shared__ uint32_t s_cn[kBlock / 32], s_clim[kBlock / 32];
+    if (lane_id() == 0) {
+        s_cn[wl] = 0;
+        s_clim[wl] = kWarpStage;
+    }
+    __syncwarp();
+    unsigned long long acc = 0, nfound = 0;
+    const uint64_t nw = ((uint64_t)V + 31) / 32, nquad = nw * 8;
+    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < nquad;
+         base += (uint64_t)gridDim.x * kBlock) {
+        const uint64_t qd = base + threadIdx.x;
+        const uint64_t v0 = qd * 4;
+        const int4 lv = load_quad_level(level, v0, V, vec);
+        uint32_t um = (lv.x == kInf) | (lv.y == kInf) << 1 | (lv.z == kInf) << 2 |
+                      (lv.w == kInf) << 3;
+        uint32_t fm = 0, cm = 0;
+        if (um) {
+            uint4 f;
+            if (v0 + 3 < V) {
+                f = __ldg(reinterpret_cast<const uint4 *>(p.first + v0));
+            } else {
+                f = make_uint4(kNoParent, kNoParent, kNoParent, kNoParent);
+                if (v0 < V) f.x = __ldg(p.first + v0);
+                if (v0 + 1 < V) f.y = __ldg(p.first + v0 + 1);
+                if (v0 + 2 < V) f.z = __ldg(p.first + v0 + 2);
+            }
+            const uint32_t fa[4] = {f.x, f.y, f.z, f.w};
+            bool hit[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                hit[j] = ((um >> j) & 1) && fa[j] != kNoParent && in_bitmap(fin, fa[j]);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (hit[j]) fm |= 1u << j;
+                else if (((um >> j) & 1) && fa[j] != kNoParent) cm |= 1u << j;
+            }
+        }
+        if (fm) {
+            // rowptr[v0..v0+4]: out-degrees of the new frontier vertices
+            uint32_t r[5];
+#pragma unroll
+            for (int j = 0; j < 5; j++) r[j] = (fm >> j & 1) || (j > 0 && (fm >> (j - 1) & 1))
+                                                   ? __ldg(&rowptr[v0 + j]) : 0;
+            int4 out = lv;
+            if (fm & 1) out.x = L + 1;
+            if (fm & 2) out.y = L + 1;
+            if (fm & 4) out.z = L + 1;
+            if (fm & 8) out.w = L + 1;
+            if (vec && v0 + 3 < V) {
+                *reinterpret_cast<int4 *>(level + v0) = out;
+            } else {
+                if (fm & 1) level[v0] = L + 1;
+                if (fm & 2) level[v0 + 1] = L + 1;
+                if (fm & 4) level[v0 + 2] = L + 1;
+                if (fm & 8) level[v0 + 3] = L + 1;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (fm >> j & 1) acc += r[j + 1] - r[j];
+            nfound += __popc(fm);
+        }
+        if (cm) {
+            // candidates with one in-edge have no other parent to try
+            uint32_t cp[5];
+#pragma unroll
+            for (int j = 0; j < 5; j++) cp[j] = (cm >> j & 1) || (j > 0 && (cm >> (j - 1) & 1))
+                                                    ? __ldg(&colptr[v0 + j]) : 0;
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if ((cm >> j & 1) && cp[j + 1] - cp[j] < 2) cm &= ~(1u << j);
+        }
+        const uint32_t w = quad_word(fm);
+        if ((lane_id() & 7) == 0 && qd < nquad) fout[qd >> 3] = w;
+        int act[4];
+        uint32_t vv[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            act[j] = (cm >> j) & 1;
+            vv[j] = (uint32_t)(v0 + j);
+        }
+        __syncwarp();
+        if (s_cn[wl] + 32 * 4 > kWarpStage)
+            warp_stage_flush(s_c[wl], &s_cn[wl], &s_clim[wl], p.cand, &c->ncand[0]);
+        stage_push_n<4>(act, vv, 1, s_c[wl], &s_cn[wl], &s_clim[wl], kWarpStage, p.cand,
+                        &c->ncand[0]);
+    }
+    warp_stage_flush(s_c[wl], &s_cn[wl], &s_clim[wl], p.cand, &c->ncand[0]);
+    warp_add64(acc, &c->m_next);
+    // the next frontier lives in the bitmap; only its size is counted here
+    warp_add64(nfound, &c->reached_pull);
+}
+
+// Pull, pass 2: eight lanes per candidate probe in-edges 1..8 at once (one
+// 32-byte sector of the in-edge list).  A candidate with in-edges left after
+// that goes to the overflow list.
+__global__ void __launch_bounds__(kBlock)
+k_bfs_pull_cand(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowptr,
+                TravCtl *c, PullLists p) {
+    if (c->done || c->mode != 1) return;
+    const uint32_t n = c->ncand[0];
+    if (n == 0) return;
     int32_t *level = static_cast<int32_t *>(c->vdata);
     const int L = (int)c->level;
     const uint32_t *__restrict__ fin = c->fb_cur ? p.fb1 : p.fb0;
     uint32_t *fout = c->fb_cur ? p.fb0 : p.fb1;
-    uint32_t *ovf = p.cand;
-    const uint32_t lane = lane_id();
+    const uint32_t lane = lane_id(), sub = lane & 7, grp = lane & 24;
+    const uint32_t gwarp = (blockIdx.x * kBlock + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * kBlock) >> 5;
     unsigned long long acc = 0, nfound = 0;
-    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < p.V;
-         base += (uint64_t)gridDim.x * kBlock) {
-        const uint32_t v = (uint32_t)base + threadIdx.x;
-        bool found = false, more = false;
-        if (v < p.V && level[v] == kInf) {
-            const uint32_t b = __ldg(&colptr[v]), e = __ldg(&colptr[v + 1]);
-            const uint32_t e1 = e - b > kProbe1 ? b + kProbe1 : e;
-            for (uint32_t k = b; k < e1 && !found; k += kParents) {
-                uint32_t u[kParents];
-#pragma unroll
-                for (int j = 0; j < kParents; j++)
-                    u[j] = k + j < e1 ? __ldg(&p.pidx[k + j]) : 0xffffffffu;
-#pragma unroll
-                for (int j = 0; j < kParents; j++)
-                    if (u[j] != 0xffffffffu && in_bitmap(fin, u[j])) found = true;
-            }
-            if (found) {
-                level[v] = L + 1;
-                acc += __ldg(&rowptr[v + 1]) - __ldg(&rowptr[v]);
-            } else {
-                more = e1 < e;
-            }
+    for (uint64_t base = (uint64_t)gwarp * 4; base < n; base += (uint64_t)nwarps * 4) {
+        const uint64_t i = base + (lane >> 3);
+        const bool valid = i < n;
+        uint32_t v = 0, b = 0, e = 0;
+        if (valid) {
+            v = p.cand[i];
+            b = __ldg(&colptr[v]) + 1;
+            e = __ldg(&colptr[v + 1]);
         }
-        const unsigned word = __ballot_sync(0xffffffffu, found);
-        if (lane == 0 && word) atomicOr(&fout[v >> 5], word);
-        nfound += found;
-        warp_push(more, v, ovf, &c->ncand[0]);
+        const uint32_t j = b + sub;
+        const bool hit = valid && j < e && in_bitmap(fin, __ldg(&p.pidx[j]));
+        const uint32_t gm = (__ballot_sync(0xffffffffu, hit) >> grp) & 0xffu;
+        const bool more = valid && !gm && e > b + kGroupProbe;
+        if (valid && gm && sub == 0) {
+            level[v] = L + 1;
+            atomicOr(&fout[v >> 5], 1u << (v & 31));
+            acc += __ldg(&rowptr[v + 1]) - __ldg(&rowptr[v]);
+            nfound++;
+        }
+        warp_push(more && sub == 0, v, p.ovf, &c->ncand[1]);
     }
     warp_add64(acc, &c->m_next);
-    // the next frontier lives in the bitmap; only its size is counted here
-    // (one atomic per warp at the end, not one per iteration)
     warp_add64(nfound, &c->reached_pull);
 }
 
-// Pull, pass 2: one warp per overflow vertex scans the rest of its in-edges,
+// Pull, pass 3: one warp per overflow vertex scans the rest of its in-edges,
 // 32 per probe, and stops at the first parent.
 __global__ void __launch_bounds__(kBlock)
 k_bfs_pull_overflow(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowptr,
-                    TravCtl *c, uint32_t *q0, uint32_t *q1, PullLists p) {
+                    TravCtl *c, PullLists p) {
     if (c->done || c->mode != 1) return;
-    const uint32_t n = c->ncand[0];
+    const uint32_t n = c->ncand[1];
     if (n == 0) return;
     int32_t *level = static_cast<int32_t *>(c->vdata);
     const int L = (int)c->level;
@@ -252,8 +380,8 @@ k_bfs_pull_overflow(const uint32_t *__restrict__ colptr, const uint32_t *__restr
     const uint32_t nwarps = (gridDim.x * kBlock) >> 5;
     unsigned long long acc = 0, nfound = 0;
     for (uint32_t i = gwarp; i < n; i += nwarps) {
-        const uint32_t v = p.cand[i];
-        const uint32_t b = __ldg(&colptr[v]) + kProbe1, e = __ldg(&colptr[v + 1]);
+        const uint32_t v = p.ovf[i];
+        const uint32_t b = __ldg(&colptr[v]) + 1 + kGroupProbe, e = __ldg(&colptr[v + 1]);
         bool found = false;
         for (uint32_t base = b; base < e; base += 32) {
             const uint32_t j = base + lane;
@@ -358,6 +486,18 @@ __global__ void k_pull_keys(const uint32_t *__restrict__ colptr, const uint32_t 
     }
 }
 
+// first[v] = v's first in-edge in pull order (its highest out-degree
+// in-neighbour), kNoParent for a vertex without in-edges.
+__global__ void k_first_parent(const uint32_t *__restrict__ colptr,
+                               const uint32_t *__restrict__ pidx, uint32_t V,
+                               uint32_t *__restrict__ first) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+         v += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t b = colptr[v], e = colptr[v + 1];
+        first[v] = b < e ? pidx[b] : kNoParent;
+    }
+}
+
 // Vertices with in-edges, sorted by in-degree (descending, ties by id), split
 // into heavy and light lists for the pull kernel, and the in-edge lists
 // reordered so each vertex first probes its highest out-degree in-neighbours
@@ -389,7 +529,9 @@ int bfs_pull_lists(olv_graph *g) {
     OLV_CUDA(cudaStreamSynchronize(s));
     w.n_heavy = h[0];
     w.n_light = h[1];
-    OLV_TRY(w.cand.ensure((size_t)V * 4 + 16));   // pull overflow list
+    OLV_TRY(w.cand.ensure((size_t)V * 4 + 16));    // pull candidate list
+    OLV_TRY(w.cand2.ensure((size_t)V * 4 + 16));   // pull overflow list
+    OLV_TRY(w.pull_first.ensure((size_t)V * 4 + 16));
     key.release();
     val.release();
     key2.release();
@@ -415,8 +557,12 @@ int bfs_pull_lists(olv_graph *g) {
                                                  k1.as<unsigned long long>(),
                                                  g->rowidx.as<uint32_t>(),
                                                  w.pull_idx.as<uint32_t>(), (int64_t)E, 0, 64, s));
-        OLV_CUDA(cudaStreamSynchronize(s));
     }
+    k_first_parent<<<g->num_sms * 8, kBlock, 0, s>>>(g->colptr.as<uint32_t>(),
+                                                    w.pull_idx.as<uint32_t>(), V,
+                                                    w.pull_first.as<uint32_t>());
+    OLV_CUDA(cudaGetLastError());
+    OLV_CUDA(cudaStreamSynchronize(s));
     return OLV_OK;
 }
 
@@ -457,7 +603,9 @@ static int bfs_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle h
     pl.order = g->ws.order.as<uint32_t>();
     pl.n_heavy = g->ws.n_heavy;
     pl.n_light = g->ws.n_light;
+    pl.first = g->ws.pull_first.as<uint32_t>();
     pl.cand = g->ws.cand.as<uint32_t>();
+    pl.ovf = g->ws.cand2.as<uint32_t>();
     pl.words = ((uint32_t)V + 31) / 32 + 8;
     pl.fb0 = g->ws.fbits.as<uint32_t>();
     pl.fb1 = pl.fb0 + pl.words;
@@ -470,8 +618,9 @@ static int bfs_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle h
     OLV_TRY(sink((const void *)k_advance_pieces<BfsPushOp>, dim3(nb), dim3(kBlock), a_adv));
     void *a_prep[] = {&V, &ctl, &pl};
     OLV_TRY(sink((const void *)k_bfs_pull_prep, dim3(nb), dim3(kBlock), a_prep));
-    void *a_pull[] = {&colptr, &rowptr, &ctl, &q0, &q1, &pl};
+    void *a_pull[] = {&colptr, &rowptr, &ctl, &pl};
     OLV_TRY(sink((const void *)k_bfs_pull, dim3(nb), dim3(kBlock), a_pull));
+    OLV_TRY(sink((const void *)k_bfs_pull_cand, dim3(nb), dim3(kBlock), a_pull));
     OLV_TRY(sink((const void *)k_bfs_pull_overflow, dim3(nb), dim3(kBlock), a_pull));
     void *a_end[] = {&ctl, &h, &use_cond, &V};
     OLV_TRY(sink((const void *)k_bfs_end, dim3(1), dim3(1), a_end));

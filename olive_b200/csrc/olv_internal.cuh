@@ -67,9 +67,7 @@ struct TravCtl {
     uint32_t split_lo;          // SSSP: lower edge of the bucket being split
     uint32_t fb_cur;            // BFS: which frontier bitmap holds the current level
     uint32_t fb_valid;          // BFS: that bitmap is up to date
-    uint32_t ncand[4];          // BFS pull candidates: heavy[0..1], light[2..3]
-    uint32_t cand_cur;          // BFS: candidate lists holding this level's input
-    uint32_t cand_valid;        // BFS: candidate lists hold exactly the unvisited vertices
+    uint32_t ncand[4];          // BFS pull: [0] candidates, [1] overflow
     uint32_t queue_stale;       // BFS: the frontier is only in the bitmap (after a pull level)
     uint32_t heavy_done;        // SSSP: heavy edges of the current bucket relaxed
     uint32_t bucket_lo;         // SSSP: lower distance edge of the current bucket
@@ -97,14 +95,16 @@ struct Tuning {
 
 struct Workspace {
     DevBuf level, q0, q1, pieces, ctl, mark, far0, far1, tmp, partials, fbits;
-    DevBuf order, cand;             // BFS pull: in-degree-sorted vertices, candidate lists
+    DevBuf order, cand, cand2;      // BFS pull: in-degree-sorted vertices, candidate lists
+    DevBuf pull_first;              // BFS pull: each vertex's first in-edge in pull order
     DevBuf pull_idx;                // BFS pull: in-edges sorted by source out-degree (desc)
     DevBuf sssp_col, sssp_w, rowmid; // SSSP: rows split light (w <= delta) | heavy
     uint32_t sssp_delta_built = 0;
     uint32_t n_heavy = 0, n_light = 0;
     void release() {
         level.release(); q0.release(); q1.release(); pieces.release(); ctl.release();
-        fbits.release(); order.release(); cand.release(); pull_idx.release();
+        fbits.release(); order.release(); cand.release(); cand2.release(); pull_idx.release();
+        pull_first.release();
         sssp_col.release(); sssp_w.release(); rowmid.release();
         sssp_delta_built = 0;
         mark.release(); far0.release(); far1.release(); tmp.release(); partials.release();

@@ -173,29 +173,67 @@ __device__ void sssp_begin(TravCtl *c) {
 }
 
 
+// Per-warp staging of queue appends in shared memory (one buffer per warp and
+// output list), flushed to the global list with one atomic per flush.
+struct WarpStage {
+    uint32_t *buf, *n, *lim;
+    __device__ __forceinline__ void init() {
+        if (lane_id() == 0) {
+            *n = 0;
+            *lim = kWarpStage;
+        }
+        __syncwarp();
+    }
+    // make room for up to `room` entries (warp-uniform)
+    __device__ __forceinline__ void reserve(uint32_t room, uint32_t *q, uint32_t *qsize) {
+        __syncwarp();
+        if (*n + room > kWarpStage) warp_stage_flush(buf, n, lim, q, qsize);
+    }
+};
+
 // Heavy superstep, step 1: the vertices of the settled bucket
-// [bucket_lo, threshold) become the input queue.
-__device__ void sssp_collect(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1) {
+// [bucket_lo, threshold) become the input queue.  Four vertices per thread.
+__device__ void sssp_collect(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1,
+                             WarpStage st) {
     const uint32_t *dist = static_cast<const uint32_t *>(c->vdata);
     const uint32_t lo = c->bucket_lo, hi = c->threshold;
     uint32_t *q = c->cur ? q1 : q0;
-    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V;
+    uint32_t *qsize = &c->qsize[c->cur];
+    const bool vec = ((uintptr_t)dist & 15) == 0;
+    const uint64_t nquad = ((uint64_t)V + 3) / 4;
+    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < nquad;
          base += (uint64_t)gridDim.x * kBlock) {
-        const uint64_t v = base + threadIdx.x;
-        bool in = false;
-        if (v < V) {
-            const uint32_t d = __ldcg(&dist[v]);
-            in = d >= lo && d < hi;
+        const uint64_t v0 = (base + threadIdx.x) * 4;
+        uint32_t d[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu};
+        if (vec && v0 + 3 < V) {
+            const uint4 x = __ldcg(reinterpret_cast<const uint4 *>(dist + v0));
+            d[0] = x.x;
+            d[1] = x.y;
+            d[2] = x.z;
+            d[3] = x.w;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (v0 + j < V) d[j] = __ldcg(dist + v0 + j);
         }
-        warp_push(in, (uint32_t)v, q, &c->qsize[c->cur]);
+        int act[4];
+        uint32_t vv[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            act[j] = d[j] >= lo && d[j] < hi;   // vertices >= V hold 0xffffffff
+            vv[j] = (uint32_t)(v0 + j);
+        }
+        st.reserve(32 * 4, q, qsize);
+        stage_push_n<4>(act, vv, 1, st.buf, st.n, st.lim, kWarpStage, q, qsize);
     }
+    warp_stage_flush(st.buf, st.n, st.lim, q, qsize);
 }
 
 // Split the far pile: stale entries (distance below the old threshold) are
 // dropped, entries under the new threshold become the near queue, the rest
 // move to the other far buffer under the next generation.
 __device__ void sssp_split(TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0,
-                           uint32_t *far1, uint32_t *farmark) {
+                           uint32_t *far1, uint32_t *farmark, WarpStage sn, WarpStage sf) {
     const uint32_t *dist = static_cast<const uint32_t *>(c->vdata);
     const uint32_t fc = c->far_cur;
     const uint32_t n = c->far_size[fc];
@@ -209,24 +247,28 @@ __device__ void sssp_split(TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far
     for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < n;
          base += (uint64_t)gridDim.x * kBlock) {
         const uint64_t i = base + threadIdx.x;
-        bool to_near = false, keep = false;
-        uint32_t v = 0;
+        int act[1] = {0};
+        uint32_t v[1] = {0};
         if (i < n) {
-            v = fin[i];
-            const uint32_t d = __ldcg(&dist[v]);
+            v[0] = fin[i];
+            const uint32_t d = __ldcg(&dist[v[0]]);
             if (d >= lo) {
                 if (d < hi) {
-                    to_near = true;
+                    act[0] = 1;
                 } else {
-                    keep = true;
-                    farmark[v] = next_epoch;
+                    act[0] = 2;
+                    farmark[v[0]] = next_epoch;
                     fmin = d < fmin ? d : fmin;
                 }
             }
         }
-        warp_push(to_near, v, qn, qn_size);
-        warp_push(keep, v, fout, fout_size);
+        sn.reserve(32, qn, qn_size);
+        stage_push_n<1>(act, v, 1, sn.buf, sn.n, sn.lim, kWarpStage, qn, qn_size);
+        sf.reserve(32, fout, fout_size);
+        stage_push_n<1>(act, v, 2, sf.buf, sf.n, sf.lim, kWarpStage, fout, fout_size);
     }
+    warp_stage_flush(sn.buf, sn.n, sn.lim, qn, qn_size);
+    warp_stage_flush(sf.buf, sf.n, sf.lim, fout, fout_size);
     const uint32_t m = __reduce_min_sync(0xffffffffu, fmin);
     if (lane_id() == 0 && m != 0xffffffffu) atomicMin(&c->far_min, m);
 }
@@ -261,10 +303,20 @@ __global__ void __launch_bounds__(kBlock)
 k_sssp_aux(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0, uint32_t *far1,
            uint32_t *farmark) {
     if (c->done) return;
-    if (c->mode == kModeHeavy)
-        sssp_collect(V, c, q0, q1);
-    else if (c->mode == kModeSplit)
-        sssp_split(c, q0, q1, far0, far1, farmark);
+    const uint32_t mode = c->mode;
+    if (mode != kModeHeavy && mode != kModeSplit) return;
+    __shared__ uint32_t s_a[kBlock / 32][kWarpStage], s_b[kBlock / 32][kWarpStage];
+    __shared__ uint32_t s_an[kBlock / 32], s_alim[kBlock / 32];
+    __shared__ uint32_t s_bn[kBlock / 32], s_blim[kBlock / 32];
+    const uint32_t wl = threadIdx.x >> 5;
+    WarpStage sa{s_a[wl], &s_an[wl], &s_alim[wl]};
+    WarpStage sb{s_b[wl], &s_bn[wl], &s_blim[wl]};
+    sa.init();
+    sb.init();
+    if (mode == kModeHeavy)
+        sssp_collect(V, c, q0, q1, sa);
+    else
+        sssp_split(c, q0, q1, far0, far1, farmark, sa, sb);
 }
 
 // Sum of out-degrees and count of reached vertices (the GTEPS basis).
