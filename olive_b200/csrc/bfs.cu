@@ -31,6 +31,7 @@ namespace olv {
 
 struct BfsPushOp {
     using SV = uint32_t;
+    static constexpr int kMinBlocks = 1;   // CTAs per SM the advance must fit
     static constexpr bool kHasFar = false;
     const uint32_t *rowptr;
     int32_t *level;
@@ -51,9 +52,18 @@ struct BfsPushOp {
     __device__ __forceinline__ Pre prepare(uint32_t, uint32_t, uint32_t v) const {
         return Pre{__ldcg(&level[v])};
     }
-    __device__ __forceinline__ int apply(const Pre &p, uint32_t v) {
-        if (p.lvl != kInf) return 0;
-        return atomicCAS(&level[v], kInf, next) == kInf ? 1 : 0;
+    // claims first (all issued before any result is used), then the outcomes
+    template <int N>
+    __device__ __forceinline__ void apply_n(const Pre (&p)[N], const uint32_t (&v)[N],
+                                            int (&act)[N]) {
+        int r[N];
+#pragma unroll
+        for (int j = 0; j < N; j++) {
+            act[j] = act[j] && p[j].lvl == kInf;
+            r[j] = act[j] ? atomicCAS(&level[v[j]], kInf, next) : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < N; j++) act[j] = act[j] && r[j] == kInf;
     }
     __device__ __forceinline__ void on_push(bool p, uint32_t v) {
         if (p) acc += __ldg(&rowptr[v + 1]) - __ldg(&rowptr[v]);

@@ -49,6 +49,7 @@ struct MsState {
 
 struct MsPushOp {
     using SV = unsigned long long;
+    static constexpr int kMinBlocks = 1;   // CTAs per SM the advance must fit
     static constexpr bool kHasFar = false;
     const unsigned long long *cur;
     const unsigned long long *visit;
@@ -61,9 +62,14 @@ struct MsPushOp {
     __device__ __forceinline__ Pre prepare(SV sv, uint32_t, uint32_t v) const {
         return Pre{sv & ~__ldg(&visit[v])};
     }
-    __device__ __forceinline__ int apply(const Pre &p, uint32_t v) {
-        if (p.bits) atomicOr(&next[v], p.bits);
-        return 0;
+    template <int N>
+    __device__ __forceinline__ void apply_n(const Pre (&p)[N], const uint32_t (&v)[N],
+                                            int (&act)[N]) {
+#pragma unroll
+        for (int j = 0; j < N; j++) {
+            if (act[j] && p[j].bits) atomicOr(&next[v[j]], p[j].bits);
+            act[j] = 0;
+        }
     }
     __device__ __forceinline__ void on_push(bool, uint32_t) {}
     __device__ __forceinline__ void flush(unsigned long long) {}

@@ -224,7 +224,7 @@ __device__ __forceinline__ bool advance_ranges(const AdvanceArgs &a, const TravC
 
 // Per-superstep chunk expansion over the input queue.
 template <class Op>
-__global__ void __launch_bounds__(kBlock) k_advance_chunks(AdvanceArgs a, Op op) {
+__global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_chunks(AdvanceArgs a, Op op) {
     TravCtl *c = a.ctl;
     const uint32_t *rbeg, *rend;
     if (!advance_ranges(a, c, rbeg, rend)) return;
@@ -305,8 +305,7 @@ __global__ void __launch_bounds__(kBlock) k_advance_chunks(AdvanceArgs a, Op op)
 #pragma unroll
             for (int j = 0; j < kItems; j++)
                 if (act[j]) pre[j] = op.prepare(sv[j], e[j], v[j]);
-#pragma unroll
-            for (int j = 0; j < kItems; j++) act[j] = act[j] ? op.apply(pre[j], v[j]) : 0;
+            op.template apply_n<kItems>(pre, v, act);
             stage_push_n<kItems>(act, v, 1, s_q, &s_qn, &s_qlim, kStage, qout, qout_size);
             if (Op::kHasFar)
                 stage_push_n<kItems>(act, v, 2, s_f, &s_fn, &s_flim, kStage, far, far_size);
@@ -322,7 +321,7 @@ __global__ void __launch_bounds__(kBlock) k_advance_chunks(AdvanceArgs a, Op op)
 
 // Hub pieces: one warp per piece of up to a.piece edges.
 template <class Op>
-__global__ void __launch_bounds__(kBlock) k_advance_pieces(AdvanceArgs a, Op op) {
+__global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_pieces(AdvanceArgs a, Op op) {
     TravCtl *c = a.ctl;
     const uint32_t *rbeg, *rend;
     if (!advance_ranges(a, c, rbeg, rend)) return;
@@ -369,8 +368,7 @@ __global__ void __launch_bounds__(kBlock) k_advance_pieces(AdvanceArgs a, Op op)
 #pragma unroll
             for (int j = 0; j < kItems; j++)
                 if (act[j]) pre[j] = op.prepare(sv, e[j], v[j]);
-#pragma unroll
-            for (int j = 0; j < kItems; j++) act[j] = act[j] ? op.apply(pre[j], v[j]) : 0;
+            op.template apply_n<kItems>(pre, v, act);
             // flush before a round could overflow the warp's buffers (the
             // counts were last written by lane 0's shared atomics)
             __syncwarp();

@@ -76,6 +76,7 @@ __global__ void k_partition_rows(const uint32_t *__restrict__ rowptr,
 }
 
 struct SsspOp {
+    static constexpr int kMinBlocks = 4;   // CTAs per SM the advance must fit (<= 64 registers)
     using SV = uint32_t;
     static constexpr bool kHasFar = true;
     const uint32_t *w;
@@ -104,14 +105,45 @@ struct SsspOp {
         if (nd < du || nd > (uint32_t)kInf) nd = (uint32_t)kInf;   // saturate
         return Pre{nd, __ldcg(&dist[v])};
     }
-    __device__ __forceinline__ int apply(const Pre &p, uint32_t v) {
-        const uint32_t nd = p.nd;
-        if (nd >= p.cur) return 0;
-        const uint32_t old = atomicMin(&dist[v], nd);
-        if (nd >= old) return 0;
-        if (nd < threshold) return atomicExch(&mark[v], stamp) != stamp ? 1 : 0;
-        fmin = nd < fmin ? nd : fmin;
-        return atomicExch(&farmark[v], epoch) != epoch ? 2 : 0;
+    // All of a thread's relaxations first, as reductions (no value returned, so
+    // they pipeline), then one dedupe exchange per improved target, also all
+    // issued before any result is used.  An edge counts as improving when its
+    // candidate beats the distance loaded in prepare; a concurrent smaller
+    // write makes the push redundant, never wrong: every decrease is made by a
+    // thread that saw nd < dist and queues v (once per superstep through the
+    // near mark, once per pile generation through the far mark), and a far
+    // entry whose vertex ends up under the threshold is dropped by the split.
+    template <int N>
+    __device__ __forceinline__ void apply_n(const Pre (&p)[N], const uint32_t (&v)[N],
+                                            int (&act)[N]) {
+        bool cand[N];
+#pragma unroll
+        for (int j = 0; j < N; j++) {
+            cand[j] = act[j] && p[j].nd < p[j].cur;
+            if (cand[j]) atomicMin(&dist[v[j]], p[j].nd);
+        }
+        uint32_t old[N];
+#pragma unroll
+        for (int j = 0; j < N; j++) {
+            old[j] = 0;
+            if (cand[j]) {
+                if (p[j].nd < threshold) {
+                    old[j] = atomicExch(&mark[v[j]], stamp);
+                } else {
+                    fmin = p[j].nd < fmin ? p[j].nd : fmin;
+                    old[j] = atomicExch(&farmark[v[j]], epoch);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < N; j++) {
+            if (!cand[j])
+                act[j] = 0;
+            else if (p[j].nd < threshold)
+                act[j] = old[j] != stamp ? 1 : 0;
+            else
+                act[j] = old[j] != epoch ? 2 : 0;
+        }
     }
     __device__ __forceinline__ void on_push(bool, uint32_t) {}
     __device__ __forceinline__ void flush(unsigned long long relaxed) {
