@@ -71,15 +71,18 @@ struct PrOp {
         base = (float)ctl->base;
     }
     __device__ __forceinline__ float term(uint32_t, uint32_t j) const { return __ldg(&cin[j]); }
-    __device__ __forceinline__ void finish(uint32_t v, float s, float c, double &res,
+    struct Row {
+        float old;       // rank before this iteration
+        uint32_t deg;    // out-degree
+    };
+    __device__ __forceinline__ Row row(uint32_t v) const { return Row{rank[v], __ldg(&outdeg[v])}; }
+    __device__ __forceinline__ void finish(uint32_t v, float s, float c, const Row &r, double &res,
                                            double &dang) const {
         const float nr = pr_update(s, c, a_hi, a_lo, base);
-        const float old = rank[v];
         rank[v] = nr;
-        res += fabs((double)nr - (double)old);
-        const uint32_t d = outdeg[v];
-        if (d) {
-            cout[v] = __fdiv_rn(nr, (float)d);
+        res += fabs((double)nr - (double)r.old);
+        if (r.deg) {
+            cout[v] = __fdiv_rn(nr, (float)r.deg);
         } else {
             cout[v] = 0.0f;
             dang += (double)nr;
@@ -204,7 +207,7 @@ static int pr_iteration(olv_graph *g, PrPlan &p, float *rank, Sink &&sink,
     op.base = 0;
     OLV_TRY(row_pass(p.rows, g->colptr.as<uint32_t>(), g->rowidx.as<uint32_t>(), op, sink));
     const double *cpart = p.rows.partials.as<double>();
-    uint32_t nparts = p.rows.nblocks;
+    uint32_t nparts = p.rows.nparts;
     void *a_red[] = {&ctl, &cpart, &nparts, &h, &use_cond};
     OLV_TRY(sink((const void *)k_pr_reduce, dim3(1), dim3(kRedThreads), a_red));
     return OLV_OK;

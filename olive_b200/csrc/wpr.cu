@@ -40,7 +40,12 @@ struct WsumOp {   // W_u = sum of out-weights (CSR)
     float *W;
     __device__ __forceinline__ void begin() {}
     __device__ __forceinline__ float term(uint32_t e, uint32_t) const { return __ldg(&w[e]); }
-    __device__ __forceinline__ void finish(uint32_t u, float s, float c, double &, double &) const {
+    struct Row {
+        uint32_t unused;
+    };
+    __device__ __forceinline__ Row row(uint32_t) const { return Row{0}; }
+    __device__ __forceinline__ void finish(uint32_t u, float s, float c, const Row &, double &,
+                                           double &) const {
         W[u] = s + c;
     }
 };
@@ -63,14 +68,17 @@ struct WfwdOp {   // r'[v] = (1-alpha) p[v] + alpha sum_{u->v} w_uv r[u]/W_u
     __device__ __forceinline__ float term(uint32_t e, uint32_t u) const {
         return __ldg(&wc[e]) * __ldg(&sin[u]);
     }
-    __device__ __forceinline__ void finish(uint32_t v, float s, float c, double &res,
+    struct Row {
+        float tp, r, W;
+    };
+    __device__ __forceinline__ Row row(uint32_t v) const { return Row{tp[v], r[v], W[v]}; }
+    __device__ __forceinline__ void finish(uint32_t v, float s, float c, const Row &q, double &res,
                                            double &) const {
-        const float t = fmaf(a_lo, s, fmaf(a_hi, c, tp[v]));
+        const float t = fmaf(a_lo, s, fmaf(a_hi, c, q.tp));
         const float nr = fmaf(a_hi, s, t);
-        res += fabs((double)nr - (double)r[v]);
+        res += fabs((double)nr - (double)q.r);
         r[v] = nr;
-        const float Wv = W[v];
-        sout[v] = Wv > 0.0f ? __fdiv_rn(nr, Wv) : 0.0f;
+        sout[v] = q.W > 0.0f ? __fdiv_rn(nr, q.W) : 0.0f;
     }
 };
 
@@ -92,12 +100,15 @@ struct WadjOp {   // lambda'[u] = g[u] + alpha sum_{u->v} w_uv lambda[v] / W_u
     __device__ __forceinline__ float term(uint32_t e, uint32_t v) const {
         return __ldg(&w[e]) * __ldg(&lin[v]);
     }
-    __device__ __forceinline__ void finish(uint32_t u, float s, float c, double &res,
+    struct Row {
+        float W, g, lam;
+    };
+    __device__ __forceinline__ Row row(uint32_t u) const { return Row{W[u], gv[u], lin[u]}; }
+    __device__ __forceinline__ void finish(uint32_t u, float s, float c, const Row &q, double &res,
                                            double &) const {
-        const float Wu = W[u];
-        const float tu = Wu > 0.0f ? __fdiv_rn(s + c, Wu) : 0.0f;
-        const float nl = fmaf(a_hi, tu, fmaf(a_lo, tu, gv[u]));
-        res += fabs((double)nl - (double)lin[u]);
+        const float tu = q.W > 0.0f ? __fdiv_rn(s + c, q.W) : 0.0f;
+        const float nl = fmaf(a_hi, tu, fmaf(a_lo, tu, q.g));
+        res += fabs((double)nl - (double)q.lam);
         lout[u] = nl;
         t[u] = tu;
     }
@@ -112,10 +123,14 @@ struct WtOp {     // t_u from the final lambda, and dL/dp = (1-alpha) lambda
     __device__ __forceinline__ float term(uint32_t e, uint32_t v) const {
         return __ldg(&w[e]) * __ldg(&lam[v]);
     }
-    __device__ __forceinline__ void finish(uint32_t u, float s, float c, double &, double &) const {
-        const float Wu = W[u];
-        t[u] = Wu > 0.0f ? __fdiv_rn(s + c, Wu) : 0.0f;
-        if (dp) dp[u] = one_minus_alpha * lam[u];
+    struct Row {
+        float W, lam;
+    };
+    __device__ __forceinline__ Row row(uint32_t u) const { return Row{W[u], lam[u]}; }
+    __device__ __forceinline__ void finish(uint32_t u, float s, float c, const Row &q, double &,
+                                           double &) const {
+        t[u] = q.W > 0.0f ? __fdiv_rn(s + c, q.W) : 0.0f;
+        if (dp) dp[u] = one_minus_alpha * q.lam;
     }
 };
 
@@ -281,7 +296,7 @@ extern "C" int olv_wpr_forward(olv_graph *g, const float *w, const float *p, dou
     op.sin = nullptr;
     op.sout = nullptr;
     const double *cpart = pl.csc.partials.as<double>();
-    uint32_t nparts = pl.csc.nblocks;
+    uint32_t nparts = pl.csc.nparts;
     auto body = [&](auto &&sink, cudaGraphConditionalHandle h, int use_cond) {
         OLV_TRY(row_pass(pl.csc, g->colptr.as<uint32_t>(), g->rowidx.as<uint32_t>(), op, sink));
         void *a_fold[] = {&ctl, &cpart, &nparts, &h, &use_cond};
@@ -369,7 +384,7 @@ extern "C" int olv_wpr_backward(olv_wpr_ctx *c, const float *gvec, int max_it, d
     op.lin = nullptr;
     op.lout = nullptr;
     const double *cpart = pl.csr.partials.as<double>();
-    uint32_t nparts = pl.csr.nblocks;
+    uint32_t nparts = pl.csr.nparts;
     auto body = [&](auto &&sink, cudaGraphConditionalHandle h, int use_cond) {
         OLV_TRY(row_pass(pl.csr, g->rowptr.as<uint32_t>(), g->col.as<uint32_t>(), op, sink));
         void *a_fold[] = {&ctl, &cpart, &nparts, &h, &use_cond};
