@@ -59,6 +59,7 @@ struct MsPushOp {
     };
     __device__ __forceinline__ void begin(TravCtl *) {}
     __device__ __forceinline__ SV src_value(uint32_t u) const { return cur[u]; }
+    __device__ __forceinline__ void on_input(uint32_t) const {}
     __device__ __forceinline__ Pre prepare(SV sv, uint32_t, uint32_t v) const {
         return Pre{sv & ~__ldg(&visit[v])};
     }

@@ -14,9 +14,13 @@
 //   void begin(TravCtl *c)                          load per-superstep values
 //   SV src_value(uint32_t u)                        value carried from the source
 //   Pre prepare(SV sv, uint32_t e, uint32_t v)      plain loads for one edge
-//   int apply(const Pre &p, uint32_t v)             0: nothing, 1: push v to the
-//                                                   output queue, 2: push to the
-//                                                   secondary (far) queue
+//   void apply_n<N>(const Pre (&p)[N], const uint32_t (&v)[N], int (&act)[N])
+//                                                   the atomics of a thread's N edges
+//                                                   (all issued before any result is
+//                                                   used); act[j] becomes 0: nothing,
+//                                                   1: push v to the output queue,
+//                                                   2: push to the secondary (far) queue
+//   void on_input(uint32_t u)                       once per input queue entry
 //   void on_push(bool pushed, uint32_t v)           after each warp-wide push
 //   void flush(unsigned long long relaxed)          once per thread at the end
 #pragma once
@@ -259,6 +263,7 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_chunks(Advan
         SV sv = 0;
         if (i < n) {
             const uint32_t u = qin[i];
+            op.on_input(u);
             beg = __ldg(&rbeg[u]);
             deg = __ldg(&rend[u]) - beg;
             if (deg > a.hub_degree) {
@@ -300,7 +305,7 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_chunks(Advan
             }
 #pragma unroll
             for (int j = 0; j < kItems; j++)
-                if (act[j]) v[j] = __ldg(&a.col[e[j]]);
+                if (act[j]) v[j] = __ldcs(&a.col[e[j]]);   // streamed once: evict first
             typename Op::Pre pre[kItems];
 #pragma unroll
             for (int j = 0; j < kItems; j++)
@@ -362,7 +367,7 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_pieces(Advan
             for (int j = 0; j < kItems; j++) {
                 e[j] = base + j * 32 + lane;
                 act[j] = e[j] < e_end;
-                v[j] = act[j] ? __ldg(&a.col[e[j]]) : 0;
+                v[j] = act[j] ? __ldcs(&a.col[e[j]]) : 0;   // streamed once: evict first
             }
             typename Op::Pre pre[kItems];
 #pragma unroll

@@ -80,17 +80,27 @@ struct SsspOp {
     using SV = uint32_t;
     static constexpr bool kHasFar = true;
     const uint32_t *w;
-    uint32_t *mark;       // stamp of the superstep that last queued v as near
-    uint32_t *farmark;    // far-pile generation that holds v
+    // Dedupe bitmaps, 2 MB each at 16M vertices, so they stay in L2.  Near:
+    // superstep t sets bits in nmark<t & 1> for the vertices it queues; those
+    // vertices are superstep t+1's input queue, which clears them again
+    // (on_input), so the bitmap is empty when superstep t+2 reuses it.  Far:
+    // fmark<epoch & 1> holds the vertices of the current pile generation; the
+    // split clears each pile entry's bit and sets the next generation's bit
+    // for the entries it keeps.
+    uint32_t *nmark0, *nmark1;
+    uint32_t *fmark0, *fmark1;
     uint32_t *dist;
-    uint32_t stamp, epoch, threshold, fmin;
+    uint32_t *nbits, *nprev, *fbits;
+    uint32_t threshold, fmin;
     unsigned long long *relaxed_ctr;
     uint32_t *far_min;
 
     __device__ __forceinline__ void begin(TravCtl *c) {
         dist = static_cast<uint32_t *>(c->vdata);
-        stamp = c->steps + 1;
-        epoch = c->epoch;
+        const uint32_t stamp = c->steps + 1;
+        nbits = (stamp & 1) ? nmark1 : nmark0;
+        nprev = (stamp & 1) ? nmark0 : nmark1;
+        fbits = (c->epoch & 1) ? fmark1 : fmark0;
         threshold = c->threshold;
         relaxed_ctr = &c->edges_relaxed;
         far_min = &c->far_min;
@@ -101,7 +111,7 @@ struct SsspOp {
     };
     __device__ __forceinline__ uint32_t src_value(uint32_t u) const { return __ldcg(&dist[u]); }
     __device__ __forceinline__ Pre prepare(uint32_t du, uint32_t e, uint32_t v) const {
-        uint32_t nd = du + __ldg(&w[e]);
+        uint32_t nd = du + __ldcs(&w[e]);   // streamed once: evict first
         if (nd < du || nd > (uint32_t)kInf) nd = (uint32_t)kInf;   // saturate
         return Pre{nd, __ldcg(&dist[v])};
     }
@@ -127,23 +137,27 @@ struct SsspOp {
         for (int j = 0; j < N; j++) {
             old[j] = 0;
             if (cand[j]) {
+                const uint32_t bit = 1u << (v[j] & 31);
                 if (p[j].nd < threshold) {
-                    old[j] = atomicExch(&mark[v[j]], stamp);
+                    old[j] = atomicOr(&nbits[v[j] >> 5], bit);
                 } else {
                     fmin = p[j].nd < fmin ? p[j].nd : fmin;
-                    old[j] = atomicExch(&farmark[v[j]], epoch);
+                    old[j] = atomicOr(&fbits[v[j] >> 5], bit);
                 }
             }
         }
 #pragma unroll
         for (int j = 0; j < N; j++) {
-            if (!cand[j])
+            const bool fresh = !((old[j] >> (v[j] & 31)) & 1u);
+            if (!cand[j] || !fresh)
                 act[j] = 0;
-            else if (p[j].nd < threshold)
-                act[j] = old[j] != stamp ? 1 : 0;
             else
-                act[j] = old[j] != epoch ? 2 : 0;
+                act[j] = p[j].nd < threshold ? 1 : 2;
         }
+    }
+    // the input vertex was queued (and marked) by the previous superstep
+    __device__ __forceinline__ void on_input(uint32_t u) const {
+        atomicAnd(&nprev[u >> 5], ~(1u << (u & 31)));
     }
     __device__ __forceinline__ void on_push(bool, uint32_t) {}
     __device__ __forceinline__ void flush(unsigned long long relaxed) {
@@ -205,6 +219,11 @@ __device__ void sssp_begin(TravCtl *c) {
 }
 
 
+// The two far-pile generation bitmaps (kernel argument by value).
+struct FarMarks {
+    uint32_t *m0, *m1;
+};
+
 // Per-warp staging of queue appends in shared memory (one buffer per warp and
 // output list), flushed to the global list with one atomic per flush.
 struct WarpStage {
@@ -265,7 +284,7 @@ __device__ void sssp_collect(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1,
 // dropped, entries under the new threshold become the near queue, the rest
 // move to the other far buffer under the next generation.
 __device__ void sssp_split(TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0,
-                           uint32_t *far1, uint32_t *farmark, WarpStage sn, WarpStage sf) {
+                           uint32_t *far1, FarMarks fm, WarpStage sn, WarpStage sf) {
     const uint32_t *dist = static_cast<const uint32_t *>(c->vdata);
     const uint32_t fc = c->far_cur;
     const uint32_t n = c->far_size[fc];
@@ -274,7 +293,9 @@ __device__ void sssp_split(TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far
     uint32_t *fout_size = &c->far_size[fc ^ 1];
     uint32_t *qn = c->cur ? q1 : q0;
     uint32_t *qn_size = &c->qsize[c->cur];
-    const uint32_t lo = c->split_lo, hi = c->threshold, next_epoch = c->epoch + 1;
+    const uint32_t lo = c->split_lo, hi = c->threshold;
+    uint32_t *fcur = (c->epoch & 1) ? fm.m1 : fm.m0;
+    uint32_t *fnext = (c->epoch & 1) ? fm.m0 : fm.m1;
     uint32_t fmin = 0xffffffffu;
     for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < n;
          base += (uint64_t)gridDim.x * kBlock) {
@@ -283,13 +304,15 @@ __device__ void sssp_split(TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far
         uint32_t v[1] = {0};
         if (i < n) {
             v[0] = fin[i];
+            const uint32_t bit = 1u << (v[0] & 31);
+            atomicAnd(&fcur[v[0] >> 5], ~bit);   // this generation's pile is consumed
             const uint32_t d = __ldcg(&dist[v[0]]);
             if (d >= lo) {
                 if (d < hi) {
                     act[0] = 1;
                 } else {
                     act[0] = 2;
-                    farmark[v[0]] = next_epoch;
+                    atomicOr(&fnext[v[0] >> 5], bit);
                     fmin = d < fmin ? d : fmin;
                 }
             }
@@ -333,7 +356,7 @@ __global__ void k_sssp_end(TravCtl *c, cudaGraphConditionalHandle h, int use_con
 // the far pile (split mode); nothing in relax mode.
 __global__ void __launch_bounds__(kBlock)
 k_sssp_aux(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0, uint32_t *far1,
-           uint32_t *farmark) {
+           FarMarks fm) {
     if (c->done) return;
     const uint32_t mode = c->mode;
     if (mode != kModeHeavy && mode != kModeSplit) return;
@@ -348,7 +371,7 @@ k_sssp_aux(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0, u
     if (mode == kModeHeavy)
         sssp_collect(V, c, q0, q1, sa);
     else
-        sssp_split(c, q0, q1, far0, far1, farmark, sa, sb);
+        sssp_split(c, q0, q1, far0, far1, fm, sa, sb);
 }
 
 // Sum of out-degrees and count of reached vertices (the GTEPS basis).
@@ -367,6 +390,9 @@ __global__ void k_reached_edges(const uint32_t *__restrict__ rowptr,
 }
 
 // ------------------------------------------------------------------ host --
+// words of one dedupe bitmap (rounded up to 64 words = 256 bytes)
+static size_t mark_words(uint32_t V) { return (((size_t)V + 31) / 32 + 63) & ~(size_t)63; }
+
 static uint32_t sssp_delta(olv_graph *g) {
     if (g->tune.sssp_delta) return g->tune.sssp_delta;
     return kDefaultDelta;
@@ -411,9 +437,16 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     ah.rend = g->rowptr.as<uint32_t>() + 1;
     SsspOp op = {};
     op.w = ws.sssp_w.as<uint32_t>();
-    op.mark = ws.mark.as<uint32_t>();
-    op.farmark = ws.mark.as<uint32_t>() + g->V;
-    uint32_t *q0 = a.q0, *q1 = a.q1, *far0 = a.far0, *far1 = a.far1, *farmark = op.farmark;
+    const size_t words = mark_words(g->V);
+    uint32_t *mk = ws.mark.as<uint32_t>();
+    op.nmark0 = mk;
+    op.nmark1 = mk + words;
+    op.fmark0 = mk + 2 * words;
+    op.fmark1 = mk + 3 * words;
+    FarMarks fm;
+    fm.m0 = op.fmark0;
+    fm.m1 = op.fmark1;
+    uint32_t *q0 = a.q0, *q1 = a.q1, *far0 = a.far0, *far1 = a.far1;
     // a correct run needs far fewer supersteps; the bound only stops a runaway loop
     uint32_t max_steps = (uint32_t)(3ULL * g->V + 1000 > 0xfffffff0ULL ? 0xfffffff0ULL
                                                                     : 3ULL * g->V + 1000);
@@ -423,7 +456,7 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     a.rbeg2 = ah.rbeg;
     a.rend2 = ah.rend;
     a.want_mode2 = kModeHeavy;
-    void *a_aux[] = {&V, &ctl, &q0, &q1, &far0, &far1, &farmark};
+    void *a_aux[] = {&V, &ctl, &q0, &q1, &far0, &far1, &fm};
     OLV_TRY(sink((const void *)k_sssp_aux, dim3(nb), dim3(kBlock), a_aux));
     void *a_adv[] = {&a, &op};
     OLV_TRY(sink((const void *)k_advance_chunks<SsspOp>, dim3(nb), dim3(kBlock), a_adv));
@@ -448,7 +481,7 @@ int sssp_workspace(olv_graph *g) {
     const size_t V = g->V;
     OLV_TRY(g->ws.far0.ensure(V * 4 + 16));
     OLV_TRY(g->ws.far1.ensure(V * 4 + 16));
-    OLV_TRY(g->ws.mark.ensure(V * 8 + 16));
+    OLV_TRY(g->ws.mark.ensure(4 * mark_words(V) * 4));
     return OLV_OK;
 }
 
@@ -456,7 +489,7 @@ int run_sssp_device(olv_graph *g, uint32_t src, uint32_t *dist_dev) {
     OLV_TRY(sssp_partition(g));
     cudaStream_t s = g->stream;
     TravCtl *ctl = g->ws.ctl.as<TravCtl>();
-    OLV_CUDA(cudaMemsetAsync(g->ws.mark.p, 0, (size_t)g->V * 8, s));
+    OLV_CUDA(cudaMemsetAsync(g->ws.mark.p, 0, 4 * mark_words(g->V) * 4, s));
     k_fill_i32<<<g->num_sms * 8, kBlock, 0, s>>>((int32_t *)dist_dev, g->V, kInf);
     k_sssp_init<<<1, 1, 0, s>>>(ctl, dist_dev, g->ws.q0.as<uint32_t>(), src, sssp_delta(g));
     OLV_CUDA(cudaGetLastError());
