@@ -259,7 +259,7 @@ def run_ours(a, rank, world, local_rank):
     elif a.workload == "bfs":
         per_step = 2 + 9 * st.iterations
     elif a.workload == "msbfs":
-        per_step = 2 + 7 * st.iterations + 1
+        per_step = 2 + 6 * st.iterations + 1
     else:   # pagerank: segments (when the graph has long rows), blocks, fold per iteration
         per_step = 2 + 3 * st.iterations
     launches = per_step * a.steps

@@ -11,10 +11,13 @@
 //   pull  (large frontier): each vertex with unvisited bits ORs cur[] over its
 //         in-edges, stopping once every missing source is found;
 //   apply (dense pass): new = next & ~visit; visit |= new; cur = new; the
-//         level of each new (source, vertex) pair is written straight into
-//         the [n][V] output; vertices with new bits form the next active queue.
-// A final pass writes 0x7fffffff for pairs never reached, so every output
-// element is written exactly once.  Levels run in a CUDA graph as for BFS.
+//         new-bit mask of level L is kept in slot L of a per-level mask store
+//         (levels past the store write their pairs straight into the output);
+//         vertices with new bits form the next active queue.
+// A final pass turns the stored masks into the [n][V] int32 output, one
+// vertex per lane, so each source's row goes out as full 128-byte lines and
+// every output element is written once.  Levels run in a CUDA
+// graph as for BFS.
 #include <string.h>
 
 #include <vector>
@@ -30,9 +33,11 @@ int bfs_pull_lists(olv_graph *g);
 
 constexpr uint32_t kMsHeavy = 128;     // in-degree above which pieces are used (same split as BFS)
 constexpr uint32_t kMsPiece = 2048;    // in-edges per heavy piece
+constexpr uint32_t kMsSlots = 16;      // levels whose new-bit masks are stored (0 .. 15)
 
 struct MsState {
     DevBuf masks;     // visit | cur | next, V words each
+    DevBuf store;     // new-bit masks of levels 0 .. kMsSlots-1, V words each
     DevBuf srcs;
     DevBuf pieces;    // (vertex, first in-edge, end) of heavy vertices' in-edge pieces
     uint32_t npieces = 0;
@@ -41,6 +46,7 @@ struct MsState {
     uint32_t graph_n = 0;
     ~MsState() {
         masks.release();
+        store.release();
         srcs.release();
         pieces.release();
         graph.destroy();
@@ -93,7 +99,7 @@ __device__ __forceinline__ void write_levels_warp(int32_t *levels, uint64_t V, u
 
 __global__ void k_ms_init(TravCtl *c, int32_t *levels, const uint32_t *srcs, int n, uint32_t V,
                           const uint32_t *rowptr, unsigned long long *visit,
-                          unsigned long long *cur, uint32_t *q0) {
+                          unsigned long long *cur, uint32_t *q0, unsigned long long *store0) {
     __shared__ unsigned long long s_edges;
     if (threadIdx.x == 0) {
         TravCtl t = {};
@@ -107,7 +113,7 @@ __global__ void k_ms_init(TravCtl *c, int32_t *levels, const uint32_t *srcs, int
         const unsigned long long bit = 1ULL << threadIdx.x;
         const unsigned long long old = atomicOr(&cur[u], bit);
         atomicOr(&visit[u], bit);
-        levels[(uint64_t)threadIdx.x * V + u] = 0;
+        atomicOr(&store0[u], bit);   // level 0
         const uint32_t d = rowptr[u + 1] - rowptr[u];
         atomicAdd(&s_edges, (unsigned long long)d);
         if (old == 0) {
@@ -127,7 +133,6 @@ __global__ void k_ms_begin(TravCtl *c, unsigned long long E, float alpha) {
         return;
     }
     c->mode = ((double)c->m_f * alpha > (double)E) ? 1u : 0u;
-    if (c->mode == 0 && c->level > 0) c->qsize[c->cur] = 0;   // rebuilt by k_ms_queue
     c->qsize[c->cur ^ 1] = 0;
     c->npieces = 0;
     c->m_next = 0;
@@ -193,61 +198,78 @@ k_ms_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowi
 __global__ void __launch_bounds__(kBlock)
 k_ms_apply(uint32_t V, TravCtl *c, const uint32_t *__restrict__ rowptr,
            unsigned long long *__restrict__ visit, unsigned long long *__restrict__ cur,
-           unsigned long long *__restrict__ next) {
+           unsigned long long *__restrict__ next, unsigned long long *__restrict__ store,
+           uint32_t *q0, uint32_t *q1) {
     if (c->done) return;
     int32_t *levels = static_cast<int32_t *>(c->vdata);
-    const int32_t lv = (int32_t)c->level + 1;
-    unsigned long long m_next = 0, traversed = 0, nact = 0;
-    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V;
-         base += (uint64_t)gridDim.x * kBlock) {
-        const uint64_t v = base + threadIdx.x;
-        bool act = false;
-        unsigned long long bits = 0;
-        if (v < V) {
-            const unsigned long long nx = next[v], oc = cur[v];
-            unsigned long long nw = 0;
-            if (nx) {
-                const unsigned long long vis = visit[v];
-                nw = nx & ~vis;
-                next[v] = 0;
-                if (nw) {
-                    visit[v] = vis | nw;
-                    const uint32_t d = __ldg(&rowptr[v + 1]) - __ldg(&rowptr[v]);
-                    m_next += d;
-                    traversed += (unsigned long long)d * __popcll(nw);
-                    act = true;
-                }
-            }
-            if (oc != nw) cur[v] = nw;
-            bits = nw;
-        }
-        write_levels_warp(levels, V, (uint32_t)v, bits, lv);
-        nact += act;
+    // vertices with new bits form the next level's queue (per-warp staging)
+    uint32_t *q = c->cur ? q0 : q1;
+    uint32_t *qsize = &c->qsize[c->cur ^ 1];
+    __shared__ uint32_t s_q[kBlock / 32][kWarpStage];
+    __shared__ uint32_t s_n[kBlock / 32], s_lim[kBlock / 32];
+    const uint32_t wl = threadIdx.x >> 5;
+    if (lane_id() == 0) {
+        s_n[wl] = 0;
+        s_lim[wl] = kWarpStage;
     }
-    // the next frontier is the dense cur[] array; only its size is counted here
+    __syncwarp();
+    const int32_t lv = (int32_t)c->level + 1;
+    // slot lv of the mask store, or direct writes past the store
+    unsigned long long *slot = (uint32_t)lv < kMsSlots ? store + (uint64_t)lv * V : nullptr;
+    unsigned long long m_next = 0, traversed = 0, nact = 0;
+    // kApply vertices per thread, strided by the grid so each load stays coalesced;
+    // all their next/cur loads are issued before any is used
+    constexpr int kApply = 4;
+    const uint64_t stride = (uint64_t)gridDim.x * kBlock;
+    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V; base += stride * kApply) {
+        unsigned long long nx[kApply], oc[kApply];
+#pragma unroll
+        for (int k = 0; k < kApply; k++) {
+            const uint64_t v = base + k * stride + threadIdx.x;
+            nx[k] = v < V ? next[v] : 0ULL;
+            oc[k] = v < V ? cur[v] : 0ULL;
+        }
+#pragma unroll
+        for (int k = 0; k < kApply; k++) {
+            const uint64_t v = base + k * stride + threadIdx.x;
+            unsigned long long nw = 0;
+            bool act = false;
+            if (v < V) {
+                if (nx[k]) {
+                    const unsigned long long vis = visit[v];
+                    nw = nx[k] & ~vis;
+                    next[v] = 0;
+                    if (nw) {
+                        visit[v] = vis | nw;
+                        const uint32_t d = __ldg(&rowptr[v + 1]) - __ldg(&rowptr[v]);
+                        m_next += d;
+                        traversed += (unsigned long long)d * __popcll(nw);
+                        act = true;
+                    }
+                }
+                if (oc[k] != nw) cur[v] = nw;
+                if (slot) __stcs(&slot[v], nw);
+            }
+            // warp-uniform: base, k and stride are the same for the whole warp
+            if (!slot && base + k * stride < V) write_levels_warp(levels, V, (uint32_t)v, nw, lv);
+            nact += act;
+            int pa[1] = {act};
+            uint32_t pv[1] = {(uint32_t)v};
+            __syncwarp();
+            if (s_n[wl] + 32 > kWarpStage) warp_stage_flush(s_q[wl], &s_n[wl], &s_lim[wl], q, qsize);
+            stage_push_n<1>(pa, pv, 1, s_q[wl], &s_n[wl], &s_lim[wl], kWarpStage, q, qsize);
+        }
+    }
+    warp_stage_flush(s_q[wl], &s_n[wl], &s_lim[wl], q, qsize);
     warp_add64(m_next, &c->m_next);
     warp_add64(traversed, &c->edges_traversed);
     warp_add64(nact, &c->reached_pull);
-}
-
-// Queue of the active vertices (cur != 0) for a push level.
-__global__ void __launch_bounds__(kBlock)
-k_ms_queue(uint32_t V, TravCtl *c, const unsigned long long *__restrict__ cur, uint32_t *q0,
-           uint32_t *q1) {
-    if (c->done || c->mode != 0 || c->level == 0) return;   // level 0: init wrote the queue
-    uint32_t *q = c->cur ? q1 : q0;
-    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V;
-         base += (uint64_t)gridDim.x * kBlock) {
-        const uint64_t v = base + threadIdx.x;
-        warp_push(v < V && cur[v] != 0, (uint32_t)v, q, &c->qsize[c->cur]);
-    }
 }
 
 __global__ void k_ms_end(TravCtl *c, cudaGraphConditionalHandle h, int use_cond, uint32_t V) {
     if (!c->done) {
         if (c->mode) c->pull_steps++;
         c->m_f = c->m_next;
-        c->qsize[c->cur ^ 1] = (uint32_t)c->reached_pull;
         c->cur ^= 1;
         c->level++;
         c->steps++;
@@ -260,23 +282,48 @@ __global__ void k_ms_end(TravCtl *c, cudaGraphConditionalHandle h, int use_cond,
     if (use_cond) cudaGraphSetConditional(h, c->done ? 0u : 1u);
 }
 
-// 0x7fffffff for every (source, vertex) pair the traversal did not reach;
-// counts reached pairs.
+// The [n][V] output from the stored level masks.  Each source's bit is set
+// in at most one slot, so OR-ing the slot masks by the bits of the slot index
+// gives four masks whose bit q spells source q's level (levels 0..15) with no
+// per-bit loop.  A lane holds one vertex; for each source q it writes
+// 0x7fffffff (never reached), the stored level, or nothing (a level past the
+// store, written by apply), and the 32 lanes' stores form one 128-byte line of
+// row q.  Also counts the reached pairs.
+static_assert(kMsSlots == 16, "four level bits");
 __global__ void __launch_bounds__(kBlock)
-k_ms_finish(uint32_t V, unsigned long long srcmask, TravCtl *c,
-            const unsigned long long *__restrict__ visit) {
+k_ms_levels(uint32_t V, int n, unsigned long long srcmask, TravCtl *c,
+            const unsigned long long *__restrict__ visit,
+            const unsigned long long *__restrict__ store) {
     int32_t *levels = static_cast<int32_t *>(c->vdata);
+    const uint32_t nst = c->level + 1 < kMsSlots ? c->level + 1 : kMsSlots;
     unsigned long long reached = 0;
-    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V;
-         base += (uint64_t)gridDim.x * kBlock) {
-        const uint64_t v = base + threadIdx.x;
-        unsigned long long miss = 0;
-        if (v < V) {
-            const unsigned long long vis = visit[v] & srcmask;
-            reached += __popcll(vis);
-            miss = ~vis & srcmask;
+    for (uint64_t v = blockIdx.x * (uint64_t)kBlock + threadIdx.x; v < V;
+         v += (uint64_t)gridDim.x * kBlock) {
+        const unsigned long long vis = visit[v] & srcmask;
+        reached += __popcll(vis);
+        unsigned long long m[kMsSlots];
+#pragma unroll
+        for (uint32_t L = 0; L < kMsSlots; L++)
+            m[L] = L < nst ? __ldcs(&store[(uint64_t)L * V + v]) : 0ULL;
+        unsigned long long b0 = 0, b1 = 0, b2 = 0, b3 = 0, any = 0;
+#pragma unroll
+        for (uint32_t L = 0; L < kMsSlots; L++) {
+            any |= m[L];
+            if (L & 1) b0 |= m[L];
+            if (L & 2) b1 |= m[L];
+            if (L & 4) b2 |= m[L];
+            if (L & 8) b3 |= m[L];
         }
-        write_levels_warp(levels, V, (uint32_t)v, miss, kInf);
+#pragma unroll
+        for (int q = 0; q < 64; q++) {
+            if (q >= n) break;
+            const int32_t lvl = (int32_t)(((b0 >> q) & 1ULL) | (((b1 >> q) & 1ULL) << 1) |
+                                          (((b2 >> q) & 1ULL) << 2) | (((b3 >> q) & 1ULL) << 3));
+            if (!((vis >> q) & 1ULL))
+                __stcs(&levels[(uint64_t)q * V + v], kInf);
+            else if ((any >> q) & 1ULL)
+                __stcs(&levels[(uint64_t)q * V + v], lvl);
+        }
     }
     warp_add64(reached, &c->reached);
 }
@@ -322,9 +369,6 @@ static int ms_superstep(olv_graph *g, MsState &ms, Sink &&sink, cudaGraphConditi
     OLV_TRY(resident_blocks(g, (const void *)k_advance_chunks<MsPushOp>, &nb));
     void *a_begin[] = {&ctl, &E, &alpha};
     OLV_TRY(sink((const void *)k_ms_begin, dim3(1), dim3(1), a_begin));
-    const unsigned long long *ccur2 = cur;
-    void *a_q[] = {&V, &ctl, &ccur2, &q0, &q1};
-    OLV_TRY(sink((const void *)k_ms_queue, dim3(nb), dim3(kBlock), a_q));
     void *a_adv[] = {&a, &op};
     OLV_TRY(sink((const void *)k_advance_chunks<MsPushOp>, dim3(nb), dim3(kBlock), a_adv));
     OLV_TRY(sink((const void *)k_advance_pieces<MsPushOp>, dim3(nb), dim3(kBlock), a_adv));
@@ -332,7 +376,8 @@ static int ms_superstep(olv_graph *g, MsState &ms, Sink &&sink, cudaGraphConditi
     uint32_t npcs = ms.npieces;
     void *a_pull[] = {&colptr, &rowidx, &V, &srcmask, &cctl, &cvisit, &ccur, &next, &pcs, &npcs};
     OLV_TRY(sink((const void *)k_ms_pull, dim3(nb), dim3(kBlock), a_pull));
-    void *a_apply[] = {&V, &ctl, &rowptr, &visit, &cur, &next};
+    unsigned long long *store = ms.store.as<unsigned long long>();
+    void *a_apply[] = {&V, &ctl, &rowptr, &visit, &cur, &next, &store, &q0, &q1};
     OLV_TRY(sink((const void *)k_ms_apply, dim3(nb), dim3(kBlock), a_apply));
     void *a_end[] = {&ctl, &h, &use_cond, &V};
     OLV_TRY(sink((const void *)k_ms_end, dim3(1), dim3(1), a_end));
@@ -394,6 +439,7 @@ extern "C" int olv_msbfs(olv_graph *g, const uint32_t *srcs, int n, int32_t *lev
     OLV_TRY(ms_pieces(g, ms));
     const size_t V = g->V;
     OLV_TRY(ms.masks.ensure(V * 24 + 64));
+    OLV_TRY(ms.store.ensure((size_t)kMsSlots * V * 8 + 64));
     OLV_TRY(ms.srcs.ensure(64 * 4));
     const bool dev_out = is_device_ptr(levels_out);
     const size_t out_bytes = (size_t)n * V * 4;
@@ -408,8 +454,10 @@ extern "C" int olv_msbfs(olv_graph *g, const uint32_t *srcs, int n, int32_t *lev
     OLV_CUDA(cudaEventRecord(g->ev0, s));
     OLV_CUDA(cudaMemcpyAsync(ms.srcs.p, hs.data(), n * 4, cudaMemcpyHostToDevice, s));
     OLV_CUDA(cudaMemsetAsync(ms.masks.p, 0, V * 24, s));
+    OLV_CUDA(cudaMemsetAsync(ms.store.p, 0, V * 8, s));   // slot 0: the sources
     k_ms_init<<<1, 64, 0, s>>>(ctl, levels, ms.srcs.as<uint32_t>(), n, g->V,
-                               g->rowptr.as<uint32_t>(), visit, visit + V, g->ws.q0.as<uint32_t>());
+                               g->rowptr.as<uint32_t>(), visit, visit + V, g->ws.q0.as<uint32_t>(),
+                               ms.store.as<unsigned long long>());
     OLV_CUDA(cudaGetLastError());
     bool launched = false;
     if (g->tune.use_graphs) {
@@ -441,7 +489,8 @@ extern "C" int olv_msbfs(olv_graph *g, const uint32_t *srcs, int n, int32_t *lev
             if (g->host_ctl->done) break;
         }
     }
-    k_ms_finish<<<g->persist_blocks, kBlock, 0, s>>>(g->V, srcmask, ctl, visit);
+    k_ms_levels<<<g->num_sms * 8, kBlock, 0, s>>>(g->V, n, srcmask, ctl, visit,
+                                                  ms.store.as<unsigned long long>());
     OLV_CUDA(cudaGetLastError());
     OLV_CUDA(cudaEventRecord(g->ev1, s));
     OLV_CUDA(cudaMemcpyAsync(g->host_ctl, ctl, sizeof(TravCtl), cudaMemcpyDeviceToHost, s));
