@@ -10,6 +10,10 @@ backward solve of 100 sweeps; batch: 512 ER graphs, BFS plus K=32 PPR, with
 engine's host-loop mode, `use_graphs=0`) so that a kernel profiler sees each
 launch: kernels inside CUDA graphs with conditional nodes are not profiled
 node by node.  The kernels are the same as in the graph mode.
+
+The solves run between cudaProfilerStart and cudaProfilerStop, so
+`ncu --profile-from-start off` sees the solve kernels only (no graph
+generation, CSC build or sort).
 """
 import argparse
 import sys
@@ -37,9 +41,12 @@ def main():
         seeds = np.stack([rng.integers(0, ni, K) for ni in n]).astype(np.uint32)
         lv = torch.empty(g.V, dtype=torch.int32, device="cuda")
         pr = torch.empty((g.V, K), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
         for _ in range(a.runs):
             g.batch(off, seeds, K=K, alpha=0.85, max_it=50, tol=1e-7, levels_out=lv, ppr_out=pr)
         torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
         print(a.workload, g.last_stats.as_dict(), file=sys.stderr)
         g.close()
         return
@@ -63,13 +70,18 @@ def main():
         gv = torch.from_numpy(rng.standard_normal(g.V).astype(np.float32)).cuda()
         dw = torch.empty(g.E, dtype=torch.float32, device="cuda")
         dp = torch.empty(g.V, dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
         for _ in range(a.runs):
             g.wpr_forward(p, w=w, max_it=100, out=out)
             g.wpr_backward(gv, max_it=100, dw_out=dw, dp_out=dp)
         torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
         print(a.workload, g.last_stats.as_dict(), file=sys.stderr)
         g.close()
         return
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
     for _ in range(a.runs):
         if a.workload == "bfs":
             g.bfs(hub, out=out)
@@ -80,6 +92,7 @@ def main():
         else:
             g.pagerank(0.85, 50, 1e-7, out=out)
     torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
     print(a.workload, g.last_stats.as_dict(), file=sys.stderr)
     g.close()
 
