@@ -12,10 +12,13 @@
 //   PPR: K <= 32 personalised PageRank vectors with one-hot seeds (the
 //     oracle's orc_ppr definition: dangling mass returns to the seed), pulled
 //     over the in-edges with one warp per vertex and lane k = vector k, so
-//     each in-edge reads one 128-byte row.  Sums run in CSC order per lane
-//     and cross-warp reductions in a fixed order, so results do not depend on
-//     which CTA runs the item or when.  Stops after max_it iterations or when
-//     every vector's L1 change (FP64) is below tol.
+//     each in-edge reads one 128-byte row, scaled by the source's inverse
+//     out-degree (computed once per item).  A warp keeps eight rows in
+//     flight; sums still run in CSC order per lane, the dangling mass is
+//     summed while the new vectors are written, and cross-warp reductions
+//     run in a fixed order, so results do not depend on which CTA runs the
+//     item or when.  Stops after max_it iterations or when every vector's L1
+//     change (FP64) is below tol.
 #include <algorithm>
 #include <numeric>
 #include <vector>
@@ -40,6 +43,7 @@ struct BatchArgs {
     double tol;
     int32_t *levels;             // [V]
     float *ppr, *ppr_tmp;        // [V][K]
+    float *inv_deg;              // [V] 1 / out-degree (0: dangling), written per PPR item
     uint32_t *counter;           // work queue head
     uint32_t *ppr_iters;         // [count]
     unsigned long long *stats;   // [0] BFS edges traversed, [1] PPR edge visits, [2] error bits
@@ -103,6 +107,10 @@ __device__ void cta_bfs(const BatchArgs &a, uint32_t inst, uint32_t *bm) {
     __syncthreads();
 }
 
+// Rows gathered per round of one warp's in-edge walk: the loads of a round
+// are issued together, then folded in CSC order.
+constexpr int kPprRound = 8;
+
 __device__ void cta_ppr(const BatchArgs &a, uint32_t inst) {
     const uint32_t base = a.inst_off[inst], n = a.inst_off[inst + 1] - base;
     const int K = a.K;
@@ -115,20 +123,25 @@ __device__ void cta_ppr(const BatchArgs &a, uint32_t inst) {
     __shared__ float s_dang[32];
     __shared__ int s_stop;
     float *r0 = a.ppr + (size_t)base * K, *r1 = a.ppr_tmp + (size_t)base * K;
-    for (uint32_t v = wid; v < n; v += kBatchWarps)
-        if (lk) r0[(size_t)v * K + lane] = (v == seed) ? 1.0f : 0.0f;
+    float *inv = a.inv_deg + base;   // 1 / out-degree, 0 for a dangling vertex
+    // Start vectors, the instance's inverse out-degrees, and the dangling mass
+    // of the start vectors.  Dangling mass is always summed in the same order:
+    // each warp over its vertices (v = wid, wid + W, ...), then warps 0..W-1.
+    float dpart = 0.0f;
+    for (uint32_t v = wid; v < n; v += kBatchWarps) {
+        const uint32_t deg = a.rowptr[base + v + 1] - a.rowptr[base + v];
+        if (lane == 0) inv[v] = deg ? __fdiv_rn(1.0f, (float)deg) : 0.0f;
+        const float x = (v == seed) ? 1.0f : 0.0f;
+        if (lk) r0[(size_t)v * K + lane] = x;
+        if (!deg) dpart += x;
+    }
+    s_d[wid][lane] = dpart;
     __syncthreads();
     int it = 0;
     unsigned long long visits = 0;
     while (it < a.max_it) {
         const float *src = (it & 1) ? r1 : r0;
         float *dst = (it & 1) ? r0 : r1;
-        // dangling mass of each vector, fixed order: per warp, then warp 0..W-1
-        float d = 0.0f;
-        for (uint32_t u = wid; u < n; u += kBatchWarps)
-            if (a.rowptr[base + u + 1] == a.rowptr[base + u] && lk) d += src[(size_t)u * K + lane];
-        s_d[wid][lane] = d;
-        __syncthreads();
         if (wid == 0) {
             float t = 0.0f;
             for (int w = 0; w < kBatchWarps; w++) t += s_d[w][lane];
@@ -137,17 +150,39 @@ __device__ void cta_ppr(const BatchArgs &a, uint32_t inst) {
         __syncthreads();
         const float dk = s_dang[lane];
         double res = 0.0;
+        dpart = 0.0f;
         for (uint32_t v = wid; v < n; v += kBatchWarps) {
             const uint32_t b = a.colptr[base + v], e = a.colptr[base + v + 1];
             float acc = 0.0f;
-            for (uint32_t i = b; i < e; i++) {
-                const uint32_t u = a.rowidx[i];
-                if (u - base >= n) {   // edge enters from outside the instance
-                    if (lane == 0) atomicOr((unsigned int *)&a.stats[2], 2u);
-                    continue;
+            // 32 in-edges at a time: lane j fetches source j and its inverse
+            // degree, then the warp gathers the sources' rows kPprRound at a
+            // time (lane k = vector k) and folds them in CSC order.  Padding
+            // slots carry weight 0 and add exactly 0.
+            for (uint32_t c0 = b; c0 < e; c0 += 32) {
+                const uint32_t cnt = min(32u, e - c0);
+                uint32_t u = 0;
+                float w = 0.0f;
+                if (lane < cnt) {
+                    u = a.rowidx[c0 + lane] - base;
+                    if (u >= n) {   // edge enters from outside the instance
+                        atomicOr((unsigned int *)&a.stats[2], 2u);
+                        u = 0;
+                    } else {
+                        w = inv[u];
+                    }
                 }
-                const float deg = (float)(a.rowptr[u + 1] - a.rowptr[u]);
-                if (lk) acc += __fdiv_rn(src[(size_t)(u - base) * K + lane], deg);
+                for (uint32_t t = 0; t < cnt; t += kPprRound) {
+                    float x[kPprRound], ww[kPprRound];
+#pragma unroll
+                    for (int j = 0; j < kPprRound; j++) {
+                        const uint32_t uj = __shfl_sync(0xffffffffu, u, (t + j) & 31);
+                        ww[j] = __shfl_sync(0xffffffffu, w, (t + j) & 31);
+                        x[j] = (lk && t + j < cnt) ? src[(size_t)uj * K + lane] : 0.0f;
+                    }
+#pragma unroll
+                    for (int j = 0; j < kPprRound; j++)
+                        if (t + j < cnt) acc = fmaf(x[j], ww[j], acc);
+                }
             }
             visits += e - b;
             if (lk) {
@@ -155,8 +190,10 @@ __device__ void cta_ppr(const BatchArgs &a, uint32_t inst) {
                 const float nv = fmaf(alpha, acc, tele);
                 res += fabs((double)nv - (double)src[(size_t)v * K + lane]);
                 dst[(size_t)v * K + lane] = nv;
+                if (inv[v] == 0.0f) dpart += nv;
             }
         }
+        s_d[wid][lane] = dpart;
         s_res[wid][lane] = res;
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -201,9 +238,9 @@ __global__ void __launch_bounds__(kBatchThreads) k_batch(BatchArgs a) {
 }
 
 struct BatchState {
-    DevBuf off, order, seeds, tmp, counter, iters, stats, levels, ppr;
+    DevBuf off, order, seeds, tmp, inv, counter, iters, stats, levels, ppr;
     ~BatchState() {
-        off.release(); order.release(); seeds.release(); tmp.release(); counter.release();
+        off.release(); order.release(); seeds.release(); tmp.release(); inv.release(); counter.release();
         iters.release(); stats.release(); levels.release(); ppr.release();
     }
 };
@@ -273,6 +310,7 @@ extern "C" int olv_batch_run(olv_graph *g, const uint32_t *inst_offsets, int cou
         OLV_CUDA(cudaMemcpyAsync(bs.seeds.p, hseeds.data(), hseeds.size() * 4,
                                  cudaMemcpyHostToDevice, s));
         OLV_TRY(bs.tmp.ensure(V * K * 4));
+        OLV_TRY(bs.inv.ensure(V * 4));
         if (!dev_pr) OLV_TRY(bs.ppr.ensure(V * K * 4));
     }
     BatchArgs a;
@@ -294,6 +332,7 @@ extern "C" int olv_batch_run(olv_graph *g, const uint32_t *inst_offsets, int cou
     a.levels = levels_out ? (dev_lv ? levels_out : bs.levels.as<int32_t>()) : nullptr;
     a.ppr = ppr_out ? (dev_pr ? ppr_out : bs.ppr.as<float>()) : nullptr;
     a.ppr_tmp = bs.tmp.as<float>();
+    a.inv_deg = bs.inv.as<float>();
     a.counter = bs.counter.as<uint32_t>();
     a.ppr_iters = bs.iters.as<uint32_t>();
     a.stats = bs.stats.as<unsigned long long>();
