@@ -375,10 +375,15 @@ static int ms_superstep(olv_graph *g, MsState &ms, Sink &&sink, cudaGraphConditi
     const uint4 *pcs = ms.pieces.as<uint4>();
     uint32_t npcs = ms.npieces;
     void *a_pull[] = {&colptr, &rowidx, &V, &srcmask, &cctl, &cvisit, &ccur, &next, &pcs, &npcs};
-    OLV_TRY(sink((const void *)k_ms_pull, dim3(nb), dim3(kBlock), a_pull));
+    // the pull and apply passes are latency bound: each runs at its own full
+    // residency (the advance is held to fewer CTAs by its registers)
+    int nb_pull = 0, nb_apply = 0;
+    OLV_TRY(resident_blocks(g, (const void *)k_ms_pull, &nb_pull));
+    OLV_TRY(resident_blocks(g, (const void *)k_ms_apply, &nb_apply));
+    OLV_TRY(sink((const void *)k_ms_pull, dim3(nb_pull), dim3(kBlock), a_pull));
     unsigned long long *store = ms.store.as<unsigned long long>();
     void *a_apply[] = {&V, &ctl, &rowptr, &visit, &cur, &next, &store, &q0, &q1};
-    OLV_TRY(sink((const void *)k_ms_apply, dim3(nb), dim3(kBlock), a_apply));
+    OLV_TRY(sink((const void *)k_ms_apply, dim3(nb_apply), dim3(kBlock), a_apply));
     void *a_end[] = {&ctl, &h, &use_cond, &V};
     OLV_TRY(sink((const void *)k_ms_end, dim3(1), dim3(1), a_end));
     return OLV_OK;
