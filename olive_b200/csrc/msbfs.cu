@@ -144,7 +144,8 @@ constexpr int kMsParents = 4;
 // Pull.  Heavy vertices' in-edges come as pieces of kMsPiece edges, one warp
 // per piece, ORed into next[v] with atomicOr (OR is order-free).  Light
 // vertices (in-degree 1..kMsHeavy) are scanned by one thread each over
-// consecutive ids.  Both stop once every missing source is found.
+// consecutive ids, eight in-edges per round from two 16-byte index loads.
+// Both stop once every missing source is found.
 __global__ void __launch_bounds__(kBlock)
 k_ms_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowidx, uint32_t V,
           unsigned long long srcmask, const TravCtl *c, const unsigned long long *__restrict__ visit,
@@ -181,14 +182,18 @@ k_ms_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowi
         if (e - b > kMsHeavy || e == b) continue;
         const unsigned long long todo = ~visit[v] & srcmask;
         if (!todo) continue;
+        // in-edges read as aligned 16-byte blocks (the index array is padded
+        // to a multiple of 4 entries), two blocks per round; entries outside
+        // [b, e) are skipped
         unsigned long long acc = 0;
-        for (uint32_t i = b; i < e; i += kMsParents) {
-            uint32_t u[kMsParents];
+        for (uint32_t blk = b & ~3u; blk < e; blk += 8) {
+            const uint4 x0 = __ldg(reinterpret_cast<const uint4 *>(rowidx + blk));
+            const uint4 x1 = blk + 4 < e ? __ldg(reinterpret_cast<const uint4 *>(rowidx + blk + 4))
+                                         : make_uint4(0, 0, 0, 0);
+            const uint32_t u[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
 #pragma unroll
-            for (int j = 0; j < kMsParents; j++) u[j] = i + j < e ? __ldg(&rowidx[i + j]) : 0xffffffffu;
-#pragma unroll
-            for (int j = 0; j < kMsParents; j++)
-                if (u[j] != 0xffffffffu) acc |= __ldg(&cur[u[j]]);
+            for (int j = 0; j < 8; j++)
+                if (blk + j >= b && blk + j < e) acc |= __ldg(&cur[u[j]]);
             if ((acc & todo) == todo) break;
         }
         if (acc & todo) atomicOr(&next[v], acc & todo);
@@ -288,9 +293,31 @@ __global__ void k_ms_end(TravCtl *c, cudaGraphConditionalHandle h, int use_cond,
 // per-bit loop.  A lane holds one vertex; for each source q it writes
 // 0x7fffffff (never reached), the stored level, or nothing (a level past the
 // store, written by apply), and the 32 lanes' stores form one 128-byte line of
-// row q.  Also counts the reached pairs.
+// row q.  The masks are kept as 32-bit halves so that every source's bits
+// come out with constant shifts (the source loop is unrolled).  Also counts
+// the reached pairs.
 static_assert(kMsSlots == 16, "four level bits");
-__global__ void __launch_bounds__(kBlock)
+
+// Row q of the output for sources q0 .. q0+31 of one vertex, from 32-bit
+// halves of the level-bit masks (b0..b3), the stored-level mask and the
+// visit mask.  `out` points at row q0, column v.
+template <int Q0>
+__device__ __forceinline__ void ms_write_half(int32_t *out, uint64_t V, int n, uint32_t b0,
+                                              uint32_t b1, uint32_t b2, uint32_t b3, uint32_t any,
+                                              uint32_t vis) {
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+        if (Q0 + j >= n) break;
+        const int32_t lvl = (int32_t)(((b0 >> j) & 1u) | (((b1 >> j) & 1u) << 1) |
+                                      (((b2 >> j) & 1u) << 2) | (((b3 >> j) & 1u) << 3));
+        const bool reached = (vis >> j) & 1u;
+        const bool stored = (any >> j) & 1u;
+        if (!reached || stored) __stcs(out, reached ? lvl : kInf);
+        out += V;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock, 4)
 k_ms_levels(uint32_t V, int n, unsigned long long srcmask, TravCtl *c,
             const unsigned long long *__restrict__ visit,
             const unsigned long long *__restrict__ store) {
@@ -314,16 +341,13 @@ k_ms_levels(uint32_t V, int n, unsigned long long srcmask, TravCtl *c,
             if (L & 4) b2 |= m[L];
             if (L & 8) b3 |= m[L];
         }
-#pragma unroll
-        for (int q = 0; q < 64; q++) {
-            if (q >= n) break;
-            const int32_t lvl = (int32_t)(((b0 >> q) & 1ULL) | (((b1 >> q) & 1ULL) << 1) |
-                                          (((b2 >> q) & 1ULL) << 2) | (((b3 >> q) & 1ULL) << 3));
-            if (!((vis >> q) & 1ULL))
-                __stcs(&levels[(uint64_t)q * V + v], kInf);
-            else if ((any >> q) & 1ULL)
-                __stcs(&levels[(uint64_t)q * V + v], lvl);
-        }
+        int32_t *out = levels + v;
+        ms_write_half<0>(out, V, n, (uint32_t)b0, (uint32_t)b1, (uint32_t)b2, (uint32_t)b3,
+                         (uint32_t)any, (uint32_t)vis);
+        if (n > 32)
+            ms_write_half<32>(out + 32 * (uint64_t)V, V, n, (uint32_t)(b0 >> 32),
+                              (uint32_t)(b1 >> 32), (uint32_t)(b2 >> 32), (uint32_t)(b3 >> 32),
+                              (uint32_t)(any >> 32), (uint32_t)(vis >> 32));
     }
     warp_add64(reached, &c->reached);
 }
