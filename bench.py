@@ -102,6 +102,29 @@ def peaks():
     return PEAK_FALLBACK_GBS, "fallback 6.65 TB/s"
 
 
+# Committed ncu launch-list summaries (profiles/*.md) of each default workload:
+# their `traffic_bytes` line is the DRAM read + write of one solve as the
+# profiler measured it (sum over the solve's launches; ncu flushes the caches
+# before each launch, so this is a cold-cache upper bound of the warm run).
+PROFILE_OF = {("sssp", 24): "sssp_rmat24.md", ("bfs", 24): "bfs_rmat24.md",
+              ("pagerank", 22): "pagerank_rmat22.md", ("msbfs", 24): "msbfs_rmat24.md",
+              ("wpr", 20): "wpr_rmat20.md", ("batch", 0): "batch_er512.md"}
+
+
+def profile_traffic(workload, scale, seed, key="traffic_bytes"):
+    """(bytes, source) from the committed profile summary of this workload
+    (default size, seed 1), or (None, None)."""
+    name = PROFILE_OF.get((workload, scale)) if seed == 1 else None
+    path = os.path.join(ROOT, "profiles", name) if name else None
+    if not path or not os.path.exists(path):
+        return None, None
+    for line in open(path):
+        if line.startswith(key + ":"):
+            return int(float(line.split(":", 1)[1].split()[0])), (
+                f"profiles/{name} ({key}: ncu launch list, cold cache per launch)")
+    return None, None
+
+
 class ClockSampler:
     """nvidia-smi clock/throttle samples taken while the timed region runs."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -246,8 +269,10 @@ def run_ours(a, rank, world, local_rank):
     peak, peak_src = peaks()
     kern_ms = float(np.median(dev_ms))
     achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
+    traffic, traffic_src = profile_traffic(a.workload, a.scale, a.seed)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": None,
+                "frac": round(achieved / peak, 4), "traffic": traffic,
+                "traffic_source": traffic_src,
                 "kernel": f"whole {a.workload} solve (all kernels of one call, CUDA graph)",
                 "algorithmic_bytes": int(alg_bytes), "bytes_formula": bytes_formula,
                 "peak_source": peak_src, "kernel_ms": round(kern_ms, 4)}
@@ -476,9 +501,11 @@ def run_wpr(a, rank, world, local_rank):
     value = world * units / (ms_f * 1e-3) / 1e9
     peak, peak_src = peaks()
     alg = (12 * E + 20 * V) * it
+    traffic, traffic_src = profile_traffic("wpr", a.scale, a.seed, "traffic_bytes_forward")
     roofline = {"bound": "hbm", "achieved": round(alg / (ms_f * 1e-3) / 1e9, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(alg / (ms_f * 1e-3) / 1e9 / peak, 4),
-                "traffic": None, "kernel": "forward solve (100 pull sweeps, CUDA graph)",
+                "traffic": traffic, "traffic_source": traffic_src,
+                "kernel": "forward solve (100 pull sweeps, CUDA graph)",
                 "algorithmic_bytes": int(alg),
                 "bytes_formula": "(12 B/edge: CSC index, weight, r/W gather + 20 B/vertex) per sweep",
                 "peak_source": peak_src}
@@ -570,8 +597,10 @@ def run_batch(a, rank, world, local_rank):
     peak, peak_src = peaks()
     _, _, iters = g.batch(off, seeds, K=K, max_it=50, tol=1e-7, levels_out=lv, ppr_out=pr)
     alg = 8 * st.edges_traversed + 4 * st.edges_relaxed + (4 + 8 * K) * V * 1
+    traffic, traffic_src = profile_traffic("batch", a.scale, a.seed)
     roofline = {"bound": "hbm", "achieved": round(alg / (ms * 1e-3) / 1e9, 1), "peak": peak,
-                "unit": "GB/s", "frac": round(alg / (ms * 1e-3) / 1e9 / peak, 4), "traffic": None,
+                "unit": "GB/s", "frac": round(alg / (ms * 1e-3) / 1e9 / peak, 4),
+                "traffic": traffic, "traffic_source": traffic_src,
                 "kernel": "k_batch (one persistent launch)", "algorithmic_bytes": int(alg),
                 "bytes_formula": "8 B/BFS edge + 4 B per PPR edge-vector visit (128 B row per "
                                  "in-edge for K=32) + (4 + 8K) B/vertex"}

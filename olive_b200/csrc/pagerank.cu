@@ -9,13 +9,17 @@
 // (PageRank.cu:51-61, common.h:141-150), refills the V accumulators on the host
 // every iteration (oliver.h:127) and copies all vertex values back to sum the
 // residual on the host (oliver.h:176-183).  Here:
-//   * each iteration is one pull kernel over the in-edges (CSC).  Vertices are
-//     cut into row blocks of at most kNnz in-edges; a CTA stages its block's
-//     contributions in shared memory and each thread sums whole rows in CSC
+//   * the solve runs on a relabelled copy of the reverse graph (CSC): vertices
+//     renumbered by in-degree, longest rows first (olv_rowtiles.cuh), built
+//     once per graph.  Ranks, contributions r/outdeg and out-degrees live in
+//     the new order; the ranks are mapped back to the caller's ids once, at
+//     the end of the solve;
+//   * each iteration is one pull pass over the in-edges: a group of 1..32
+//     lanes per row (by row length) sums the row's contributions in a fixed
 //     order with compensated (two-sum) FP32 arithmetic, so results do not
-//     depend on scheduling and carry ~1 rounding per vertex;  a row longer
-//     than kNnz gets a CTA of its own and a fixed-shape tree;
-//   * the same kernel writes the next iteration's contributions r/outdeg and
+//     depend on scheduling and carry ~1 rounding per vertex; rows longer than
+//     kTileLong are summed in fixed segments first;
+//   * the same pass writes the next iteration's contributions r/outdeg and
 //     per-CTA FP64 partial sums of |r' - r| and of the dangling mass;
 //   * a one-CTA kernel folds the partials in a fixed order (FP64), decides
 //     convergence on the device and sets the loop condition of the CUDA graph
@@ -26,7 +30,7 @@
 #include "olv_advance.cuh"
 #include "olv_graphexec.cuh"
 #include "olv_internal.cuh"
-#include "olv_rowsum.cuh"
+#include "olv_rowtiles.cuh"
 
 namespace olv {
 
@@ -159,29 +163,45 @@ __global__ void k_pr_ctl_init(PrCtl *ctl, const unsigned long long *ndang, uint3
     *ctl = c;
 }
 
-__global__ void k_outdeg(const uint32_t *__restrict__ rowptr, uint32_t V, uint32_t *d) {
+// out-degree of every vertex, in the relabelled order
+__global__ void k_outdeg_perm(const uint32_t *__restrict__ rowptr,
+                              const uint32_t *__restrict__ perm, uint32_t V, uint32_t *d) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < V;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = perm[i];
+        d[i] = rowptr[v + 1] - rowptr[v];
+    }
+}
+
+// rank[v] = rank of v's new id (coalesced writes, gathers from an L2-sized array)
+__global__ void k_pr_unpermute(const float *__restrict__ rank_new,
+                               const uint32_t *__restrict__ newid, uint32_t V,
+                               float *__restrict__ rank) {
     for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
          v += (uint64_t)gridDim.x * blockDim.x)
-        d[v] = rowptr[v + 1] - rowptr[v];
+        rank[v] = rank_new[newid[v]];
 }
 
 // ------------------------------------------------------------------ host --
 struct PrPlan {
-    RowPlan rows;
-    DevBuf outdeg, contrib, ctl, dang;
+    TilePlan tp;
+    DevBuf outdeg, contrib, rank, ctl, dang;   // outdeg, contrib, rank: new order
     float a_hi = 0, a_lo = 0;
     ~PrPlan() {
-        rows.release(); outdeg.release(); contrib.release(); ctl.release(); dang.release();
+        tp.release(); outdeg.release(); contrib.release(); rank.release(); ctl.release();
+        dang.release();
     }
 };
 
 static int build_pr_plan(olv_graph *g, PrPlan &p) {
     const uint32_t V = g->V;
-    OLV_TRY(build_row_plan(g->colptr.as<uint32_t>(), V, g->stream, p.rows));
+    OLV_TRY(build_tile_plan(g->colptr.as<uint32_t>(), g->rowidx.as<uint32_t>(), V, g->stream,
+                            p.tp));
     OLV_TRY(p.outdeg.ensure((size_t)V * 4 + 16));
-    k_outdeg<<<g->num_sms * 8, kBlock, 0, g->stream>>>(g->rowptr.as<uint32_t>(), V,
-                                                      p.outdeg.as<uint32_t>());
+    k_outdeg_perm<<<g->num_sms * 8, kBlock, 0, g->stream>>>(
+        g->rowptr.as<uint32_t>(), p.tp.perm.as<uint32_t>(), V, p.outdeg.as<uint32_t>());
     OLV_TRY(p.contrib.ensure((size_t)V * 8 + 32));
+    OLV_TRY(p.rank.ensure((size_t)V * 4 + 16));
     OLV_TRY(p.ctl.ensure(sizeof(PrCtl)));
     OLV_TRY(p.dang.ensure(16));
     OLV_CUDA(cudaGetLastError());
@@ -190,24 +210,24 @@ static int build_pr_plan(olv_graph *g, PrPlan &p) {
 }
 
 template <class Sink>
-static int pr_iteration(olv_graph *g, PrPlan &p, float *rank, Sink &&sink,
-                        cudaGraphConditionalHandle h, int use_cond) {
+static int pr_iteration(olv_graph *g, PrPlan &p, Sink &&sink, cudaGraphConditionalHandle h,
+                        int use_cond) {
     PrCtl *ctl = p.ctl.as<PrCtl>();
     PrOp op;
     op.done = &ctl->done;
     op.ctl = ctl;
     op.c0 = p.contrib.as<float>();
     op.c1 = p.contrib.as<float>() + g->V;
-    op.rank = rank;
+    op.rank = p.rank.as<float>();
     op.outdeg = p.outdeg.as<uint32_t>();
     op.a_hi = p.a_hi;
     op.a_lo = p.a_lo;
     op.cin = nullptr;
     op.cout = nullptr;
     op.base = 0;
-    OLV_TRY(row_pass(p.rows, g->colptr.as<uint32_t>(), g->rowidx.as<uint32_t>(), op, sink));
-    const double *cpart = p.rows.partials.as<double>();
-    uint32_t nparts = p.rows.nparts;
+    OLV_TRY(tile_pass(p.tp, op, sink));
+    const double *cpart = p.tp.partials.as<double>();
+    uint32_t nparts = kRowCTAs;
     void *a_red[] = {&ctl, &cpart, &nparts, &h, &use_cond};
     OLV_TRY(sink((const void *)k_pr_reduce, dim3(1), dim3(kRedThreads), a_red));
     return OLV_OK;
@@ -220,7 +240,6 @@ using namespace olv;
 struct PrState {
     PrPlan plan;
     WhileGraph graph;
-    float *graph_rank = nullptr;
 };
 
 static PrState *pr_state(olv_graph *g) { return static_cast<PrState *>(g->pr_state); }
@@ -260,10 +279,11 @@ extern "C" int olv_pagerank(olv_graph *g, double alpha, int max_it, double tol, 
     const bool dev_out = is_device_ptr(rank_out);
     if (!dev_out) OLV_TRY(g->ws.level.ensure((size_t)g->V * 4 + 16));
     float *rank = dev_out ? rank_out : g->ws.level.as<float>();
+    float *rank_new = p.rank.as<float>();
 
     OLV_CUDA(cudaEventRecord(g->ev0, s));
     OLV_CUDA(cudaMemsetAsync(p.dang.p, 0, 8, s));
-    k_pr_init<<<g->num_sms * 8, kBlock, 0, s>>>(p.outdeg.as<uint32_t>(), g->V, rank,
+    k_pr_init<<<g->num_sms * 8, kBlock, 0, s>>>(p.outdeg.as<uint32_t>(), g->V, rank_new,
                                                p.contrib.as<float>(),
                                                p.dang.as<unsigned long long>());
     k_pr_ctl_init<<<1, 1, 0, s>>>(p.ctl.as<PrCtl>(), p.dang.as<unsigned long long>(), g->V, ad,
@@ -272,14 +292,13 @@ extern "C" int olv_pagerank(olv_graph *g, double alpha, int max_it, double tol, 
     OLV_CUDA(cudaGetLastError());
     bool launched = false;
     if (g->tune.use_graphs && max_it > 0) {
-        if (!ps->graph.ready || ps->graph_rank != rank) {
+        if (!ps->graph.ready) {
             int r = ps->graph.begin();
             auto sink = [&](const void *f, dim3 gr, dim3 bl, void **args) {
                 return ps->graph.add(f, gr, bl, args);
             };
-            if (r == OLV_OK) r = pr_iteration(g, p, rank, sink, ps->graph.handle, 1);
+            if (r == OLV_OK) r = pr_iteration(g, p, sink, ps->graph.handle, 1);
             if (r == OLV_OK) r = ps->graph.finish();
-            ps->graph_rank = rank;
             if (r != OLV_OK) ps->graph.destroy();
         }
         if (ps->graph.ready) {
@@ -292,8 +311,11 @@ extern "C" int olv_pagerank(olv_graph *g, double alpha, int max_it, double tol, 
             OLV_CUDA(cudaLaunchKernel(f, gr, bl, args, 0, s));
             return OLV_OK;
         };
-        for (int it = 0; it < max_it; it++) OLV_TRY(pr_iteration(g, p, rank, launch, 0, 0));
+        for (int it = 0; it < max_it; it++) OLV_TRY(pr_iteration(g, p, launch, 0, 0));
     }
+    k_pr_unpermute<<<g->num_sms * 8, kBlock, 0, s>>>(rank_new, p.tp.newid.as<uint32_t>(), g->V,
+                                                    rank);
+    OLV_CUDA(cudaGetLastError());
     OLV_CUDA(cudaEventRecord(g->ev1, s));
     PrCtl hc;
     OLV_CUDA(cudaMemcpyAsync(&hc, p.ctl.p, sizeof(PrCtl), cudaMemcpyDeviceToHost, s));
