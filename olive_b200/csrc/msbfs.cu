@@ -10,10 +10,12 @@
 //         advance of olv_advance.cuh with a 64-bit source value;
 //   pull  (large frontier): each vertex with unvisited bits ORs cur[] over its
 //         in-edges, stopping once every missing source is found;
-//   apply (dense pass): new = next & ~visit; visit |= new; cur = new; the
-//         new-bit mask of level L is kept in slot L of a per-level mask store
-//         (levels past the store write their pairs straight into the output);
-//         vertices with new bits form the next active queue.
+//   apply (dense pass): new = next & ~visit; visit |= new; the new-bit mask
+//         of level L+1 is written to slot L+1 of a per-level mask store, and
+//         that slot is the next level's cur (no separate cur array is read or
+//         cleared); levels past the store use two spare cur arrays and write
+//         their pairs straight into the output; vertices with new bits form
+//         the next active queue.
 // A final pass turns the stored masks into the [n][V] int32 output, one
 // vertex per lane, so each source's row goes out as full 128-byte lines and
 // every output element is written once.  Levels run in a CUDA
@@ -36,7 +38,7 @@ constexpr uint32_t kMsPiece = 2048;    // in-edges per heavy piece
 constexpr uint32_t kMsSlots = 16;      // levels whose new-bit masks are stored (0 .. 15)
 
 struct MsState {
-    DevBuf masks;     // visit | cur | next, V words each
+    DevBuf masks;     // visit | next | cur A | cur B, V words each (A, B: levels >= kMsSlots)
     DevBuf store;     // new-bit masks of levels 0 .. kMsSlots-1, V words each
     DevBuf srcs;
     DevBuf pieces;    // (vertex, first in-edge, end) of heavy vertices' in-edge pieces
@@ -53,17 +55,28 @@ struct MsState {
     }
 };
 
+// The frontier mask of level L: slot L of the mask store, or one of two
+// spare arrays for the levels past the store.
+struct MsCur {
+    unsigned long long *store, *cx0, *cx1;
+    uint32_t V;
+    __device__ __forceinline__ unsigned long long *at(uint32_t L) const {
+        return L < kMsSlots ? store + (uint64_t)L * V : ((L & 1) ? cx1 : cx0);
+    }
+};
+
 struct MsPushOp {
     using SV = unsigned long long;
     static constexpr int kMinBlocks = 1;   // CTAs per SM the advance must fit
     static constexpr bool kHasFar = false;
+    MsCur cm;
     const unsigned long long *cur;
     const unsigned long long *visit;
     unsigned long long *next;
     struct Pre {
         unsigned long long bits;
     };
-    __device__ __forceinline__ void begin(TravCtl *) {}
+    __device__ __forceinline__ void begin(TravCtl *c) { cur = cm.at(c->level); }
     __device__ __forceinline__ SV src_value(uint32_t u) const { return cur[u]; }
     __device__ __forceinline__ void on_input(uint32_t) const {}
     __device__ __forceinline__ Pre prepare(SV sv, uint32_t, uint32_t v) const {
@@ -98,8 +111,8 @@ __device__ __forceinline__ void write_levels_warp(int32_t *levels, uint64_t V, u
 }
 
 __global__ void k_ms_init(TravCtl *c, int32_t *levels, const uint32_t *srcs, int n, uint32_t V,
-                          const uint32_t *rowptr, unsigned long long *visit,
-                          unsigned long long *cur, uint32_t *q0, unsigned long long *store0) {
+                          const uint32_t *rowptr, unsigned long long *visit, uint32_t *q0,
+                          unsigned long long *store0) {
     __shared__ unsigned long long s_edges;
     if (threadIdx.x == 0) {
         TravCtl t = {};
@@ -111,9 +124,8 @@ __global__ void k_ms_init(TravCtl *c, int32_t *levels, const uint32_t *srcs, int
     if ((int)threadIdx.x < n) {
         const uint32_t u = srcs[threadIdx.x];
         const unsigned long long bit = 1ULL << threadIdx.x;
-        const unsigned long long old = atomicOr(&cur[u], bit);
+        const unsigned long long old = atomicOr(&store0[u], bit);   // level 0 = cur of level 0
         atomicOr(&visit[u], bit);
-        atomicOr(&store0[u], bit);   // level 0
         const uint32_t d = rowptr[u + 1] - rowptr[u];
         atomicAdd(&s_edges, (unsigned long long)d);
         if (old == 0) {
@@ -149,9 +161,10 @@ constexpr int kMsParents = 4;
 __global__ void __launch_bounds__(kBlock)
 k_ms_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowidx, uint32_t V,
           unsigned long long srcmask, const TravCtl *c, const unsigned long long *__restrict__ visit,
-          const unsigned long long *__restrict__ cur, unsigned long long *__restrict__ next,
-          const uint4 *__restrict__ pieces, uint32_t npieces) {
+          MsCur cm, unsigned long long *__restrict__ next, const uint4 *__restrict__ pieces,
+          uint32_t npieces) {
     if (c->done || c->mode != 1) return;
+    const unsigned long long *__restrict__ cur = cm.at(c->level);
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -202,9 +215,8 @@ k_ms_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowi
 
 __global__ void __launch_bounds__(kBlock)
 k_ms_apply(uint32_t V, TravCtl *c, const uint32_t *__restrict__ rowptr,
-           unsigned long long *__restrict__ visit, unsigned long long *__restrict__ cur,
-           unsigned long long *__restrict__ next, unsigned long long *__restrict__ store,
-           uint32_t *q0, uint32_t *q1) {
+           unsigned long long *__restrict__ visit, MsCur cm,
+           unsigned long long *__restrict__ next, uint32_t *q0, uint32_t *q1) {
     if (c->done) return;
     int32_t *levels = static_cast<int32_t *>(c->vdata);
     // vertices with new bits form the next level's queue (per-warp staging)
@@ -219,20 +231,21 @@ k_ms_apply(uint32_t V, TravCtl *c, const uint32_t *__restrict__ rowptr,
     }
     __syncwarp();
     const int32_t lv = (int32_t)c->level + 1;
-    // slot lv of the mask store, or direct writes past the store
-    unsigned long long *slot = (uint32_t)lv < kMsSlots ? store + (uint64_t)lv * V : nullptr;
+    // the next level's cur: slot lv of the mask store, or a spare array (and
+    // direct writes of the level into the output) past the store
+    unsigned long long *__restrict__ ncur = cm.at((uint32_t)lv);
+    const bool past = (uint32_t)lv >= kMsSlots;
     unsigned long long m_next = 0, traversed = 0, nact = 0;
     // kApply vertices per thread, strided by the grid so each load stays coalesced;
     // all their next/cur loads are issued before any is used
     constexpr int kApply = 4;
     const uint64_t stride = (uint64_t)gridDim.x * kBlock;
     for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V; base += stride * kApply) {
-        unsigned long long nx[kApply], oc[kApply];
+        unsigned long long nx[kApply];
 #pragma unroll
         for (int k = 0; k < kApply; k++) {
             const uint64_t v = base + k * stride + threadIdx.x;
             nx[k] = v < V ? next[v] : 0ULL;
-            oc[k] = v < V ? cur[v] : 0ULL;
         }
 #pragma unroll
         for (int k = 0; k < kApply; k++) {
@@ -252,11 +265,10 @@ k_ms_apply(uint32_t V, TravCtl *c, const uint32_t *__restrict__ rowptr,
                         act = true;
                     }
                 }
-                if (oc[k] != nw) cur[v] = nw;
-                if (slot) __stcs(&slot[v], nw);
+                ncur[v] = nw;
             }
             // warp-uniform: base, k and stride are the same for the whole warp
-            if (!slot && base + k * stride < V) write_levels_warp(levels, V, (uint32_t)v, nw, lv);
+            if (past && base + k * stride < V) write_levels_warp(levels, V, (uint32_t)v, nw, lv);
             nact += act;
             int pa[1] = {act};
             uint32_t pv[1] = {(uint32_t)v};
@@ -361,8 +373,12 @@ static int ms_superstep(olv_graph *g, MsState &ms, Sink &&sink, cudaGraphConditi
     unsigned long long E = g->E;
     float alpha = g->tune.ms_alpha;
     unsigned long long *visit = ms.masks.as<unsigned long long>();
-    unsigned long long *cur = visit + V;
-    unsigned long long *next = cur + V;
+    unsigned long long *next = visit + V;
+    MsCur cm;
+    cm.store = ms.store.as<unsigned long long>();
+    cm.cx0 = visit + 2 * (size_t)V;
+    cm.cx1 = visit + 3 * (size_t)V;
+    cm.V = V;
     AdvanceArgs a;
     a.rbeg = g->rowptr.as<uint32_t>();
     a.rend = g->rowptr.as<uint32_t>() + 1;
@@ -378,7 +394,8 @@ static int ms_superstep(olv_graph *g, MsState &ms, Sink &&sink, cudaGraphConditi
     a.rbeg2 = a.rend2 = nullptr;
     a.want_mode2 = 0xffffffffu;
     MsPushOp op;
-    op.cur = cur;
+    op.cm = cm;
+    op.cur = nullptr;
     op.visit = visit;
     op.next = next;
     const uint32_t *colptr = g->colptr.as<uint32_t>();
@@ -387,7 +404,7 @@ static int ms_superstep(olv_graph *g, MsState &ms, Sink &&sink, cudaGraphConditi
                                               : g->rowidx.as<uint32_t>();
     const uint32_t *rowptr = g->rowptr.as<uint32_t>();
     const TravCtl *cctl = ctl;
-    const unsigned long long *cvisit = visit, *ccur = cur;
+    const unsigned long long *cvisit = visit;
     uint32_t *q0 = a.q0, *q1 = a.q1;
     int nb = 0;
     OLV_TRY(resident_blocks(g, (const void *)k_advance_chunks<MsPushOp>, &nb));
@@ -398,15 +415,14 @@ static int ms_superstep(olv_graph *g, MsState &ms, Sink &&sink, cudaGraphConditi
     OLV_TRY(sink((const void *)k_advance_pieces<MsPushOp>, dim3(nb), dim3(kBlock), a_adv));
     const uint4 *pcs = ms.pieces.as<uint4>();
     uint32_t npcs = ms.npieces;
-    void *a_pull[] = {&colptr, &rowidx, &V, &srcmask, &cctl, &cvisit, &ccur, &next, &pcs, &npcs};
+    void *a_pull[] = {&colptr, &rowidx, &V, &srcmask, &cctl, &cvisit, &cm, &next, &pcs, &npcs};
     // the pull and apply passes are latency bound: each runs at its own full
     // residency (the advance is held to fewer CTAs by its registers)
     int nb_pull = 0, nb_apply = 0;
     OLV_TRY(resident_blocks(g, (const void *)k_ms_pull, &nb_pull));
     OLV_TRY(resident_blocks(g, (const void *)k_ms_apply, &nb_apply));
     OLV_TRY(sink((const void *)k_ms_pull, dim3(nb_pull), dim3(kBlock), a_pull));
-    unsigned long long *store = ms.store.as<unsigned long long>();
-    void *a_apply[] = {&V, &ctl, &rowptr, &visit, &cur, &next, &store, &q0, &q1};
+    void *a_apply[] = {&V, &ctl, &rowptr, &visit, &cm, &next, &q0, &q1};
     OLV_TRY(sink((const void *)k_ms_apply, dim3(nb_apply), dim3(kBlock), a_apply));
     void *a_end[] = {&ctl, &h, &use_cond, &V};
     OLV_TRY(sink((const void *)k_ms_end, dim3(1), dim3(1), a_end));
@@ -467,7 +483,7 @@ extern "C" int olv_msbfs(olv_graph *g, const uint32_t *srcs, int n, int32_t *lev
     MsState &ms = *ms_state(g);
     OLV_TRY(ms_pieces(g, ms));
     const size_t V = g->V;
-    OLV_TRY(ms.masks.ensure(V * 24 + 64));
+    OLV_TRY(ms.masks.ensure(V * 32 + 64));
     OLV_TRY(ms.store.ensure((size_t)kMsSlots * V * 8 + 64));
     OLV_TRY(ms.srcs.ensure(64 * 4));
     const bool dev_out = is_device_ptr(levels_out);
@@ -482,10 +498,10 @@ extern "C" int olv_msbfs(olv_graph *g, const uint32_t *srcs, int n, int32_t *lev
 
     OLV_CUDA(cudaEventRecord(g->ev0, s));
     OLV_CUDA(cudaMemcpyAsync(ms.srcs.p, hs.data(), n * 4, cudaMemcpyHostToDevice, s));
-    OLV_CUDA(cudaMemsetAsync(ms.masks.p, 0, V * 24, s));
+    OLV_CUDA(cudaMemsetAsync(ms.masks.p, 0, V * 16, s));   // visit, next
     OLV_CUDA(cudaMemsetAsync(ms.store.p, 0, V * 8, s));   // slot 0: the sources
     k_ms_init<<<1, 64, 0, s>>>(ctl, levels, ms.srcs.as<uint32_t>(), n, g->V,
-                               g->rowptr.as<uint32_t>(), visit, visit + V, g->ws.q0.as<uint32_t>(),
+                               g->rowptr.as<uint32_t>(), visit, g->ws.q0.as<uint32_t>(),
                                ms.store.as<unsigned long long>());
     OLV_CUDA(cudaGetLastError());
     bool launched = false;
