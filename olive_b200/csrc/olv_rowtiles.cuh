@@ -31,6 +31,7 @@ constexpr uint32_t kTileLong = 2048;   // rows longer than this are segmented
 constexpr uint32_t kTileSeg = 2048;    // entries per segment of a long row
 constexpr int kTileU = 4;              // entries per lane per round (loads in flight)
 constexpr uint32_t kNoSeg = 0xffffffu;
+constexpr uint32_t kTileCTAs = 148 * 8;  // fixed grid of the tile pass (fixed partial order)
 
 // Relabelled structure and its tiles.  tiles[t] = (first row, lg | first
 // segment << 8): the tile covers rows first .. first + (32 >> lg) - 1 with
@@ -116,7 +117,7 @@ inline int build_tile_plan(const uint32_t *ptr_dev, const uint32_t *idx_dev, uin
     OLV_TRY(p.tiles.ensure(tiles.size() * 8 + 16));
     OLV_TRY(p.seg_range.ensure(ranges.size() * 8 + 16));
     OLV_TRY(p.segs.ensure(ranges.size() * 8 + 16));
-    OLV_TRY(p.partials.ensure((size_t)kRowCTAs * 16 + 16));
+    OLV_TRY(p.partials.ensure((size_t)kTileCTAs * 16 + 16));
     OLV_CUDA(cudaMemcpyAsync(p.perm.p, perm.data(), (size_t)n * 4, cudaMemcpyHostToDevice, s));
     OLV_CUDA(cudaMemcpyAsync(p.newid.p, newid.data(), (size_t)n * 4, cudaMemcpyHostToDevice, s));
     OLV_CUDA(cudaMemcpyAsync(p.ptr.p, ptr.data(), ((size_t)n + 1) * 4, cudaMemcpyHostToDevice, s));
@@ -133,7 +134,7 @@ inline int build_tile_plan(const uint32_t *ptr_dev, const uint32_t *idx_dev, uin
 }
 
 template <class Op>
-__global__ void __launch_bounds__(kBlock, 6)
+__global__ void __launch_bounds__(kBlock, 8)
 k_row_tiles(const uint32_t *__restrict__ ptr, const uint32_t *__restrict__ idx,
             const uint2 *__restrict__ tiles, uint32_t ntiles, uint32_t nrows,
             const float2 *__restrict__ segs, Op op, double *__restrict__ partials) {
@@ -144,8 +145,10 @@ k_row_tiles(const uint32_t *__restrict__ ptr, const uint32_t *__restrict__ idx,
     const uint32_t gw = (blockIdx.x * kBlock + threadIdx.x) >> 5;
     const uint32_t nw = (gridDim.x * kBlock) >> 5;
     double res = 0.0, aux = 0.0;
+    uint2 tdn = gw < ntiles ? tiles[gw] : make_uint2(0, 0);
     for (uint32_t t = gw; t < ntiles; t += nw) {
-        const uint2 td = tiles[t];
+        const uint2 td = tdn;   // the next tile's descriptor is fetched one tile ahead
+        if (t + nw < ntiles) tdn = tiles[t + nw];
         const uint32_t lg = td.y & 7u, G = 1u << lg;
         const uint32_t r = td.x + (lane >> lg);
         const uint32_t sub = lane & (G - 1);
@@ -234,7 +237,7 @@ int tile_pass(const TilePlan &p, Op &op, Sink &&sink) {
     }
     uint32_t ntiles = p.ntiles, n = p.n;
     void *a_t[] = {&ptr, &idx, &tiles, &ntiles, &n, &csegs, &op, &partials};
-    OLV_TRY(sink((const void *)k_row_tiles<Op>, dim3(kRowCTAs), dim3(kBlock), a_t));
+    OLV_TRY(sink((const void *)k_row_tiles<Op>, dim3(kTileCTAs), dim3(kBlock), a_t));
     return OLV_OK;
 }
 

@@ -227,7 +227,7 @@ static int pr_iteration(olv_graph *g, PrPlan &p, Sink &&sink, cudaGraphCondition
     op.base = 0;
     OLV_TRY(tile_pass(p.tp, op, sink));
     const double *cpart = p.tp.partials.as<double>();
-    uint32_t nparts = kRowCTAs;
+    uint32_t nparts = kTileCTAs;
     void *a_red[] = {&ctl, &cpart, &nparts, &h, &use_cond};
     OLV_TRY(sink((const void *)k_pr_reduce, dim3(1), dim3(kRedThreads), a_red));
     return OLV_OK;
