@@ -19,6 +19,12 @@
 // row updates produce are also summed in a fixed order.
 //
 // The Op interface is that of olv_rowsum.cuh; row ids are the new ids.
+//
+// A plan can also keep the neighbour ids (relabel = false): only the rows are
+// reordered, `pos` maps each entry to its position in the original structure
+// (to permute per-entry values such as edge weights), and PermOp hands the
+// original row id to an Op whose per-vertex arrays stay in the original
+// order.
 #pragma once
 #include <algorithm>
 #include <vector>
@@ -41,36 +47,76 @@ struct TilePlan {
     DevBuf perm;      // new id -> old id
     DevBuf newid;     // old id -> new id
     DevBuf ptr;       // [n + 1] row offsets in the new order
-    DevBuf idx;       // neighbour new ids, rows in the new order (padded to 4 entries)
+    DevBuf idx;       // neighbour (new or original) ids, rows in the new order
+    DevBuf pos;       // relabel = false: original position of every entry
     DevBuf tiles, seg_range, segs, partials;
     uint32_t n = 0, ntiles = 0, nsegs = 0;
     void release() {
-        perm.release(); newid.release(); ptr.release(); idx.release(); tiles.release();
+        perm.release(); newid.release(); ptr.release(); idx.release(); pos.release();
+        tiles.release();
         seg_range.release(); segs.release(); partials.release();
     }
 };
 
-// idx[ptr[i] + k] = newid[old_idx[old_ptr[perm[i]] + k]], one warp per row.
-__global__ void k_relabel_rows(const uint32_t *__restrict__ old_ptr,
+// idx[ptr[i] + k] = newid[old_idx[old_ptr[perm[i]] + k]] (or the original id
+// when newid is null, recording the entry's original position), one warp per
+// row.
+static __global__ void k_relabel_rows(const uint32_t *__restrict__ old_ptr,
                                const uint32_t *__restrict__ old_idx,
                                const uint32_t *__restrict__ perm, const uint32_t *__restrict__ newid,
                                const uint32_t *__restrict__ ptr, uint32_t n,
-                               uint32_t *__restrict__ idx) {
+                               uint32_t *__restrict__ idx, uint32_t *__restrict__ pos) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t w = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = w; i < n; i += nw) {
         const uint32_t v = perm[i];
         const uint32_t b = old_ptr[v], e = old_ptr[v + 1], o = ptr[i];
-        for (uint32_t k = lane; k < e - b; k += 32) idx[o + k] = newid[old_idx[b + k]];
+        for (uint32_t k = lane; k < e - b; k += 32) {
+            const uint32_t j = old_idx[b + k];
+            idx[o + k] = newid ? newid[j] : j;
+            if (pos) pos[o + k] = b + k;
+        }
     }
 }
+
+// out[k] = in[pos[k]]: per-entry values in a plan's entry order.
+static __global__ void k_permute_entries(const float *__restrict__ in, const uint32_t *__restrict__ pos,
+                                  uint64_t n, float *__restrict__ out) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n;
+         k += (uint64_t)gridDim.x * blockDim.x)
+        out[k] = in[pos[k]];
+}
+
+// An Op over a row-reordered plan (relabel = false): row r of the plan is
+// vertex perm[r] of the Op's arrays; entry values come from arrays already
+// permuted to the plan's entry order.
+template <class Op>
+struct PermOp {
+    Op op;
+    const uint32_t *perm;
+    const uint32_t *done;
+    __device__ __forceinline__ void begin() { op.begin(); }
+    __device__ __forceinline__ float term(uint32_t e, uint32_t j) const { return op.term(e, j); }
+    struct Row {
+        typename Op::Row r;
+        uint32_t v;
+    };
+    __device__ __forceinline__ Row row(uint32_t r) const {
+        const uint32_t v = __ldg(&perm[r]);
+        return Row{op.row(v), v};
+    }
+    __device__ __forceinline__ void finish(uint32_t, float s, float c, const Row &q, double &res,
+                                           double &aux) const {
+        op.finish(q.v, s, c, q.r, res, aux);
+    }
+};
 
 // Build the plan from a device row-offset array (n rows) and its neighbour
 // array.  The relabelling is a stable counting sort by row length
 // (descending), done on the host once per graph.
 inline int build_tile_plan(const uint32_t *ptr_dev, const uint32_t *idx_dev, uint32_t n,
-                           cudaStream_t s, TilePlan &p) {
+                           cudaStream_t s, TilePlan &p, bool relabel = true) {
     std::vector<uint32_t> cp((size_t)n + 1);
     OLV_CUDA(cudaMemcpyAsync(cp.data(), ptr_dev, ((size_t)n + 1) * 4, cudaMemcpyDeviceToHost, s));
     OLV_CUDA(cudaStreamSynchronize(s));
@@ -114,6 +160,7 @@ inline int build_tile_plan(const uint32_t *ptr_dev, const uint32_t *idx_dev, uin
     OLV_TRY(p.newid.ensure((size_t)n * 4 + 16));
     OLV_TRY(p.ptr.ensure(((size_t)n + 1) * 4));
     OLV_TRY(p.idx.ensure(E * 4 + 16));
+    if (!relabel) OLV_TRY(p.pos.ensure(E * 4 + 16));
     OLV_TRY(p.tiles.ensure(tiles.size() * 8 + 16));
     OLV_TRY(p.seg_range.ensure(ranges.size() * 8 + 16));
     OLV_TRY(p.segs.ensure(ranges.size() * 8 + 16));
@@ -126,8 +173,9 @@ inline int build_tile_plan(const uint32_t *ptr_dev, const uint32_t *idx_dev, uin
         OLV_CUDA(cudaMemcpyAsync(p.seg_range.p, ranges.data(), ranges.size() * 8,
                                  cudaMemcpyHostToDevice, s));
     k_relabel_rows<<<1184, kBlock, 0, s>>>(ptr_dev, idx_dev, p.perm.as<uint32_t>(),
-                                          p.newid.as<uint32_t>(), p.ptr.as<uint32_t>(), n,
-                                          p.idx.as<uint32_t>());
+                                          relabel ? p.newid.as<uint32_t>() : nullptr,
+                                          p.ptr.as<uint32_t>(), n, p.idx.as<uint32_t>(),
+                                          relabel ? nullptr : p.pos.as<uint32_t>());
     OLV_CUDA(cudaGetLastError());
     OLV_CUDA(cudaStreamSynchronize(s));
     return OLV_OK;

@@ -7,11 +7,17 @@
 //   dL/dw_uv = alpha r_u (lambda_v - t_u) / W_u,   t_u = sum_x P_ux lambda_x
 //   dL/dp    = (1-alpha) lambda                     for L = sum_v g_v r_v.
 // Both solves are Jacobi sweeps with deterministic compensated FP32 row sums
-// (olv_rowsum.cuh) and FP64 residual norms, run as CUDA graphs; the gradient
-// is implicit at the fixed point, so memory is O(V + E) with no tape.
+// and FP64 residual norms, run as CUDA graphs; the gradient is implicit at the
+// fixed point, so memory is O(V + E) with no tape.
+//
+// The row sums run on row-reordered copies of the CSC (forward) and the CSR
+// (adjoint, W, t): rows sorted by length so that a group of 1..32 lanes per
+// row fits every row of a warp (olv_rowtiles.cuh); neighbour ids and all
+// per-vertex arrays keep the caller's numbering, and the edge weights are
+// permuted into each copy's entry order at the start of every forward solve.
 #include "olv_graphexec.cuh"
 #include "olv_internal.cuh"
-#include "olv_rowsum.cuh"
+#include "olv_rowtiles.cuh"
 
 struct olv_wpr_ctx {
     olv_graph *g = nullptr;
@@ -26,10 +32,15 @@ struct olv_wpr_ctx {
 namespace olv {
 
 struct WprPlans {
-    RowPlan csc, csr;
+    RowPlan csr;               // row blocks of the CSR (gradient kernels)
+    TilePlan tcsc, tcsr;       // row-reordered CSC and CSR (row sums)
+    DevBuf wc, wr;             // weights in tcsc / tcsr entry order
     ~WprPlans() {
-        csc.release();
         csr.release();
+        tcsc.release();
+        tcsr.release();
+        wc.release();
+        wr.release();
     }
 };
 
@@ -205,8 +216,15 @@ static WprPlans *wpr_plans(olv_graph *g) { return static_cast<WprPlans *>(g->wpr
 static int ensure_wpr_plans(olv_graph *g) {
     if (g->wpr_state) return OLV_OK;
     WprPlans *p = new WprPlans();
-    int r = build_row_plan(g->colptr.as<uint32_t>(), g->V, g->stream, p->csc);
-    if (r == OLV_OK) r = build_row_plan(g->rowptr.as<uint32_t>(), g->V, g->stream, p->csr);
+    int r = build_row_plan(g->rowptr.as<uint32_t>(), g->V, g->stream, p->csr);
+    if (r == OLV_OK)
+        r = build_tile_plan(g->colptr.as<uint32_t>(), g->rowidx.as<uint32_t>(), g->V, g->stream,
+                            p->tcsc, false);
+    if (r == OLV_OK)
+        r = build_tile_plan(g->rowptr.as<uint32_t>(), g->col.as<uint32_t>(), g->V, g->stream,
+                            p->tcsr, false);
+    if (r == OLV_OK) r = p->wc.ensure(g->E * 4 + 16);
+    if (r == OLV_OK) r = p->wr.ensure(g->E * 4 + 16);
     if (r != OLV_OK) {
         delete p;
         return r;
@@ -267,25 +285,34 @@ extern "C" int olv_wpr_forward(olv_graph *g, const float *w, const float *p, dou
     OLV_TRY(copy_vec_in(c->gbuf, p, V, s));   // p staged in gbuf during the forward
     IterCtl *ctl = c->ctl.as<IterCtl>();
     OLV_CUDA(cudaEventRecord(g->ev0, s));
+    // the weights in the entry orders of the two row-reordered copies
+    k_permute_entries<<<g->num_sms * 8, kBlock, 0, s>>>(g->csc_w.as<float>(),
+                                                       pl.tcsc.pos.as<uint32_t>(), g->E,
+                                                       pl.wc.as<float>());
+    k_permute_entries<<<g->num_sms * 8, kBlock, 0, s>>>(g->w.as<float>(),
+                                                       pl.tcsr.pos.as<uint32_t>(), g->E,
+                                                       pl.wr.as<float>());
     // W = row sums of the weights (one pass, same deterministic engine)
     {
         k_iter_init<<<1, 1, 0, s>>>(ctl, 1, 0.0);   // done = 0 for the single pass
-        WsumOp op{&ctl->done, g->w.as<float>(), c->W.as<float>()};
+        PermOp<WsumOp> op{WsumOp{&ctl->done, pl.wr.as<float>(), c->W.as<float>()},
+                          pl.tcsr.perm.as<uint32_t>(), &ctl->done};
         auto launch = [&](const void *f, dim3 gr, dim3 bl, void **args) {
             OLV_CUDA(cudaLaunchKernel(f, gr, bl, args, 0, s));
             return OLV_OK;
         };
-        OLV_TRY(row_pass(pl.csr, g->rowptr.as<uint32_t>(), g->col.as<uint32_t>(), op, launch));
+        OLV_TRY(tile_pass(pl.tcsr, op, launch));
     }
     k_wpr_init<<<g->num_sms * 8, kBlock, 0, s>>>(g->V, c->gbuf.as<float>(), c->W.as<float>(),
                                                 (float)alpha, c->tp.as<float>(), c->r.as<float>(),
                                                 c->s2.as<float>());
     k_iter_init<<<1, 1, 0, s>>>(ctl, (uint32_t)max_it, tol);
     OLV_CUDA(cudaGetLastError());
-    WfwdOp op;
+    WfwdOp fop;
+    WfwdOp &op = fop;
     op.done = &ctl->done;
     op.ctl = ctl;
-    op.wc = g->csc_w.as<float>();
+    op.wc = pl.wc.as<float>();
     op.s0 = c->s2.as<float>();
     op.s1 = c->s2.as<float>() + V;
     op.W = c->W.as<float>();
@@ -295,10 +322,11 @@ extern "C" int olv_wpr_forward(olv_graph *g, const float *w, const float *p, dou
     op.a_lo = c->a_lo;
     op.sin = nullptr;
     op.sout = nullptr;
-    const double *cpart = pl.csc.partials.as<double>();
-    uint32_t nparts = pl.csc.nparts;
+    PermOp<WfwdOp> pop{fop, pl.tcsc.perm.as<uint32_t>(), &ctl->done};
+    const double *cpart = pl.tcsc.partials.as<double>();
+    uint32_t nparts = kTileCTAs;
     auto body = [&](auto &&sink, cudaGraphConditionalHandle h, int use_cond) {
-        OLV_TRY(row_pass(pl.csc, g->colptr.as<uint32_t>(), g->rowidx.as<uint32_t>(), op, sink));
+        OLV_TRY(tile_pass(pl.tcsc, pop, sink));
         void *a_fold[] = {&ctl, &cpart, &nparts, &h, &use_cond};
         return sink((const void *)k_iter_fold, dim3(1), dim3(kFoldThreads), a_fold);
     };
@@ -370,10 +398,11 @@ extern "C" int olv_wpr_backward(olv_wpr_ctx *c, const float *gvec, int max_it, d
     k_copy_f32<<<g->num_sms * 8, kBlock, 0, s>>>(c->gbuf.as<float>(), c->lam2.as<float>(), g->V);
     k_iter_init<<<1, 1, 0, s>>>(ctl, (uint32_t)max_it, tol);
     OLV_CUDA(cudaGetLastError());
-    WadjOp op;
+    WadjOp aop;
+    WadjOp &op = aop;
     op.done = &ctl->done;
     op.ctl = ctl;
-    op.w = g->w.as<float>();
+    op.w = pl.wr.as<float>();
     op.l0 = c->lam2.as<float>();
     op.l1 = c->lam2.as<float>() + V;
     op.W = c->W.as<float>();
@@ -383,10 +412,11 @@ extern "C" int olv_wpr_backward(olv_wpr_ctx *c, const float *gvec, int max_it, d
     op.a_lo = c->a_lo;
     op.lin = nullptr;
     op.lout = nullptr;
-    const double *cpart = pl.csr.partials.as<double>();
-    uint32_t nparts = pl.csr.nparts;
+    PermOp<WadjOp> pop{aop, pl.tcsr.perm.as<uint32_t>(), &ctl->done};
+    const double *cpart = pl.tcsr.partials.as<double>();
+    uint32_t nparts = kTileCTAs;
     auto body = [&](auto &&sink, cudaGraphConditionalHandle h, int use_cond) {
-        OLV_TRY(row_pass(pl.csr, g->rowptr.as<uint32_t>(), g->col.as<uint32_t>(), op, sink));
+        OLV_TRY(tile_pass(pl.tcsr, pop, sink));
         void *a_fold[] = {&ctl, &cpart, &nparts, &h, &use_cond};
         return sink((const void *)k_iter_fold, dim3(1), dim3(kFoldThreads), a_fold);
     };
@@ -422,13 +452,14 @@ extern "C" int olv_wpr_backward(olv_wpr_ctx *c, const float *gvec, int max_it, d
     const float *lam = c->lam2.as<float>() + ((hc.iter & 1) ? V : 0);
     {
         k_iter_init<<<1, 1, 0, s>>>(ctl, 1, 0.0);
-        WtOp top{&ctl->done, g->w.as<float>(), lam, c->W.as<float>(), c->t.as<float>(), dp,
-                 (float)(1.0 - c->alpha)};
+        PermOp<WtOp> top{WtOp{&ctl->done, pl.wr.as<float>(), lam, c->W.as<float>(),
+                              c->t.as<float>(), dp, (float)(1.0 - c->alpha)},
+                         pl.tcsr.perm.as<uint32_t>(), &ctl->done};
         auto launch = [&](const void *f, dim3 gr, dim3 bl, void **args) {
             OLV_CUDA(cudaLaunchKernel(f, gr, bl, args, 0, s));
             return OLV_OK;
         };
-        OLV_TRY(row_pass(pl.csr, g->rowptr.as<uint32_t>(), g->col.as<uint32_t>(), top, launch));
+        OLV_TRY(tile_pass(pl.tcsr, top, launch));
     }
     k_wpr_grad_blocks<<<pl.csr.nblocks, kBlock, 0, s>>>(
         g->rowptr.as<uint32_t>(), g->col.as<uint32_t>(), pl.csr.blocks.as<uint32_t>(),
