@@ -35,9 +35,17 @@ namespace olv {
 
 constexpr uint32_t kTileLong = 2048;   // rows longer than this are segmented
 constexpr uint32_t kTileSeg = 2048;    // entries per segment of a long row
-constexpr int kTileU = 4;              // entries per lane per round (loads in flight)
+#ifndef OLV_TILE_U
+#define OLV_TILE_U 8
+#endif
+#ifndef OLV_TILE_MINB
+#define OLV_TILE_MINB 6
+#endif
+constexpr int kTileU = OLV_TILE_U;     // entries per lane per round (loads in flight)
+constexpr int kTileMinBlocks = OLV_TILE_MINB;   // resident CTAs per SM of the tile pass
 constexpr uint32_t kNoSeg = 0xffffffu;
-constexpr uint32_t kTileCTAs = 148 * 8;  // fixed grid of the tile pass (fixed partial order)
+constexpr uint32_t kTileCTAs = 148 * kTileMinBlocks;  // fixed grid of the tile pass
+                                                      // (fixed partial order), one wave
 
 // Relabelled structure and its tiles.  tiles[t] = (first row, lg | first
 // segment << 8): the tile covers rows first .. first + (32 >> lg) - 1 with
@@ -182,7 +190,7 @@ inline int build_tile_plan(const uint32_t *ptr_dev, const uint32_t *idx_dev, uin
 }
 
 template <class Op>
-__global__ void __launch_bounds__(kBlock, 8)
+__global__ void __launch_bounds__(kBlock, kTileMinBlocks)
 k_row_tiles(const uint32_t *__restrict__ ptr, const uint32_t *__restrict__ idx,
             const uint2 *__restrict__ tiles, uint32_t ntiles, uint32_t nrows,
             const float2 *__restrict__ segs, Op op, double *__restrict__ partials) {
