@@ -105,7 +105,10 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
  *   "sssp_delta"  SSSP bucket width, 0 = default                    (0)
  *   "ms_alpha"    msBFS pull when active out-edges * ms_alpha > E   (4)
  *   "use_graphs"  run supersteps inside CUDA graphs (1) or a host loop (0)
- *   "levels_per_sync" host loop: supersteps enqueued per check      (4)  */
+ *   "levels_per_sync" host loop: supersteps enqueued per check      (4)
+ *   "batch_cluster" olv_batch_run: PPR items on thread-block clusters of
+ *                 8 or 16 CTAs (1 = the largest the GPU runs), or one CTA per
+ *                 item (0); the float results depend on the choice       (1) */
 int olv_tune_set(olv_graph *g, const char *key, double value);
 int olv_tune_get(const olv_graph *g, const char *key, double *value);
 /* Autotuner: coordinate descent over hub_degree, alpha, beta (BFS) and, on

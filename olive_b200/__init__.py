@@ -216,7 +216,7 @@ class Graph:
             _check(lib().olv_tune_set(self._h, k.encode(), float(v)), f"olv_tune_set({k})")
         out = {}
         for k in ("hub_degree", "piece", "alpha", "beta", "sssp_delta", "ms_alpha",
-                  "use_graphs", "levels_per_sync"):
+                  "use_graphs", "levels_per_sync", "batch_cluster"):
             d = _D()
             _check(lib().olv_tune_get(self._h, k.encode(), ctypes.byref(d)), "olv_tune_get")
             out[k] = d.value

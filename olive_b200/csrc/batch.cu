@@ -23,8 +23,12 @@
 #include <numeric>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "olv_advance.cuh"
 #include "olv_internal.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace olv {
 
@@ -111,37 +115,117 @@ __device__ void cta_bfs(const BatchArgs &a, uint32_t inst, uint32_t *bm) {
 // are issued together, then folded in CSC order.
 constexpr int kPprRound = 8;
 
+// What one warp sees of a PPR item.
+struct PprView {
+    uint32_t base, n, seed;
+    int K;
+    bool lk;          // lane < K: the lane carries vector `lane`
+    float alpha;
+    float *r0, *r1;   // the item's vectors, ping-pong
+    float *inv;       // 1 / out-degree, 0 for a dangling vertex
+};
+
+__device__ __forceinline__ PprView ppr_view(const BatchArgs &a, uint32_t inst, uint32_t lane) {
+    PprView p;
+    p.base = a.inst_off[inst];
+    p.n = a.inst_off[inst + 1] - p.base;
+    p.K = a.K;
+    p.lk = (int)lane < p.K;
+    p.seed = p.lk ? a.seeds[(size_t)inst * p.K + lane] : 0xffffffffu;
+    p.alpha = a.alpha;
+    p.r0 = a.ppr + (size_t)p.base * p.K;
+    p.r1 = a.ppr_tmp + (size_t)p.base * p.K;
+    p.inv = a.inv_deg + p.base;
+    return p;
+}
+
+// Start vectors and inverse out-degrees of the vertices v = w0, w0 + nw, ...;
+// returns this warp's dangling mass of the start vectors (per lane), summed
+// in vertex order.
+__device__ __forceinline__ float ppr_init_warp(const BatchArgs &a, const PprView &p, uint32_t lane,
+                                               uint32_t w0, uint32_t nw) {
+    float dpart = 0.0f;
+    for (uint32_t v = w0; v < p.n; v += nw) {
+        const uint32_t deg = a.rowptr[p.base + v + 1] - a.rowptr[p.base + v];
+        if (lane == 0) p.inv[v] = deg ? __fdiv_rn(1.0f, (float)deg) : 0.0f;
+        const float x = (v == p.seed) ? 1.0f : 0.0f;
+        if (p.lk) p.r0[(size_t)v * p.K + lane] = x;
+        if (!deg) dpart += x;
+    }
+    return dpart;
+}
+
+// One sweep over the vertices v = w0, w0 + nw, ... (one warp each): pull
+// src over the in-edges, write dst; accumulates the warp's dangling mass of
+// the new vectors, its FP64 L1 change and its in-edge visits.
+__device__ __forceinline__ void ppr_sweep_warp(const BatchArgs &a, const PprView &p, uint32_t lane,
+                                               uint32_t w0, uint32_t nw, const float *src,
+                                               float *dst, float dk, float &dpart, double &res,
+                                               unsigned long long &visits) {
+    const uint32_t base = p.base, n = p.n;
+    const int K = p.K;
+    for (uint32_t v = w0; v < n; v += nw) {
+        const uint32_t b = a.colptr[base + v], e = a.colptr[base + v + 1];
+        float acc = 0.0f;
+        // 32 in-edges at a time: lane j fetches source j and its inverse
+        // degree, then the warp gathers the sources' rows kPprRound at a
+        // time (lane k = vector k) and folds them in CSC order.  Padding
+        // slots carry weight 0 and add exactly 0.
+        for (uint32_t c0 = b; c0 < e; c0 += 32) {
+            const uint32_t cnt = min(32u, e - c0);
+            uint32_t u = 0;
+            float w = 0.0f;
+            if (lane < cnt) {
+                u = a.rowidx[c0 + lane] - base;
+                if (u >= n) {   // edge enters from outside the instance
+                    atomicOr((unsigned int *)&a.stats[2], 2u);
+                    u = 0;
+                } else {
+                    w = p.inv[u];
+                }
+            }
+            for (uint32_t t = 0; t < cnt; t += kPprRound) {
+                float x[kPprRound], ww[kPprRound];
+#pragma unroll
+                for (int j = 0; j < kPprRound; j++) {
+                    const uint32_t uj = __shfl_sync(0xffffffffu, u, (t + j) & 31);
+                    ww[j] = __shfl_sync(0xffffffffu, w, (t + j) & 31);
+                    x[j] = (p.lk && t + j < cnt) ? src[(size_t)uj * K + lane] : 0.0f;
+                }
+#pragma unroll
+                for (int j = 0; j < kPprRound; j++)
+                    if (t + j < cnt) acc = fmaf(x[j], ww[j], acc);
+            }
+        }
+        visits += e - b;
+        if (p.lk) {
+            const float tele = (v == p.seed) ? fmaf(p.alpha, dk, 1.0f - p.alpha) : 0.0f;
+            const float nv = fmaf(p.alpha, acc, tele);
+            res += fabs((double)nv - (double)src[(size_t)v * K + lane]);
+            dst[(size_t)v * K + lane] = nv;
+            if (p.inv[v] == 0.0f) dpart += nv;
+        }
+    }
+}
+
 __device__ void cta_ppr(const BatchArgs &a, uint32_t inst) {
-    const uint32_t base = a.inst_off[inst], n = a.inst_off[inst + 1] - base;
-    const int K = a.K;
     const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const bool lk = (int)lane < K;
-    const uint32_t seed = lk ? a.seeds[(size_t)inst * K + lane] : 0xffffffffu;
-    const float alpha = a.alpha;
+    const PprView p = ppr_view(a, inst, lane);
+    const uint32_t n = p.n;
+    const int K = p.K;
     __shared__ float s_d[kBatchWarps][32];
     __shared__ double s_res[kBatchWarps][32];
     __shared__ float s_dang[32];
     __shared__ int s_stop;
-    float *r0 = a.ppr + (size_t)base * K, *r1 = a.ppr_tmp + (size_t)base * K;
-    float *inv = a.inv_deg + base;   // 1 / out-degree, 0 for a dangling vertex
-    // Start vectors, the instance's inverse out-degrees, and the dangling mass
-    // of the start vectors.  Dangling mass is always summed in the same order:
-    // each warp over its vertices (v = wid, wid + W, ...), then warps 0..W-1.
-    float dpart = 0.0f;
-    for (uint32_t v = wid; v < n; v += kBatchWarps) {
-        const uint32_t deg = a.rowptr[base + v + 1] - a.rowptr[base + v];
-        if (lane == 0) inv[v] = deg ? __fdiv_rn(1.0f, (float)deg) : 0.0f;
-        const float x = (v == seed) ? 1.0f : 0.0f;
-        if (lk) r0[(size_t)v * K + lane] = x;
-        if (!deg) dpart += x;
-    }
-    s_d[wid][lane] = dpart;
+    // Dangling mass is always summed in the same order: each warp over its
+    // vertices (v = wid, wid + W, ...), then warps 0..W-1.
+    s_d[wid][lane] = ppr_init_warp(a, p, lane, wid, kBatchWarps);
     __syncthreads();
     int it = 0;
     unsigned long long visits = 0;
     while (it < a.max_it) {
-        const float *src = (it & 1) ? r1 : r0;
-        float *dst = (it & 1) ? r0 : r1;
+        const float *src = (it & 1) ? p.r1 : p.r0;
+        float *dst = (it & 1) ? p.r0 : p.r1;
         if (wid == 0) {
             float t = 0.0f;
             for (int w = 0; w < kBatchWarps; w++) t += s_d[w][lane];
@@ -150,49 +234,8 @@ __device__ void cta_ppr(const BatchArgs &a, uint32_t inst) {
         __syncthreads();
         const float dk = s_dang[lane];
         double res = 0.0;
-        dpart = 0.0f;
-        for (uint32_t v = wid; v < n; v += kBatchWarps) {
-            const uint32_t b = a.colptr[base + v], e = a.colptr[base + v + 1];
-            float acc = 0.0f;
-            // 32 in-edges at a time: lane j fetches source j and its inverse
-            // degree, then the warp gathers the sources' rows kPprRound at a
-            // time (lane k = vector k) and folds them in CSC order.  Padding
-            // slots carry weight 0 and add exactly 0.
-            for (uint32_t c0 = b; c0 < e; c0 += 32) {
-                const uint32_t cnt = min(32u, e - c0);
-                uint32_t u = 0;
-                float w = 0.0f;
-                if (lane < cnt) {
-                    u = a.rowidx[c0 + lane] - base;
-                    if (u >= n) {   // edge enters from outside the instance
-                        atomicOr((unsigned int *)&a.stats[2], 2u);
-                        u = 0;
-                    } else {
-                        w = inv[u];
-                    }
-                }
-                for (uint32_t t = 0; t < cnt; t += kPprRound) {
-                    float x[kPprRound], ww[kPprRound];
-#pragma unroll
-                    for (int j = 0; j < kPprRound; j++) {
-                        const uint32_t uj = __shfl_sync(0xffffffffu, u, (t + j) & 31);
-                        ww[j] = __shfl_sync(0xffffffffu, w, (t + j) & 31);
-                        x[j] = (lk && t + j < cnt) ? src[(size_t)uj * K + lane] : 0.0f;
-                    }
-#pragma unroll
-                    for (int j = 0; j < kPprRound; j++)
-                        if (t + j < cnt) acc = fmaf(x[j], ww[j], acc);
-                }
-            }
-            visits += e - b;
-            if (lk) {
-                const float tele = (v == seed) ? fmaf(alpha, dk, 1.0f - alpha) : 0.0f;
-                const float nv = fmaf(alpha, acc, tele);
-                res += fabs((double)nv - (double)src[(size_t)v * K + lane]);
-                dst[(size_t)v * K + lane] = nv;
-                if (inv[v] == 0.0f) dpart += nv;
-            }
-        }
+        float dpart = 0.0f;
+        ppr_sweep_warp(a, p, lane, wid, kBatchWarps, src, dst, dk, dpart, res, visits);
         s_d[wid][lane] = dpart;
         s_res[wid][lane] = res;
         __syncthreads();
@@ -211,7 +254,7 @@ __device__ void cta_ppr(const BatchArgs &a, uint32_t inst) {
     }
     if (it & 1) {   // result is in the scratch copy
         for (uint32_t v = wid; v < n; v += kBatchWarps)
-            if (lk) r0[(size_t)v * K + lane] = r1[(size_t)v * K + lane];
+            if (p.lk) p.r0[(size_t)v * K + lane] = p.r1[(size_t)v * K + lane];
     }
     if (threadIdx.x == 0) a.ppr_iters[inst] = it;
     if (lane == 0 && visits) atomicAdd(&a.stats[1], visits * (unsigned long long)K);
@@ -237,6 +280,158 @@ __global__ void __launch_bounds__(kBatchThreads) k_batch(BatchArgs a) {
     }
 }
 
+// ---- cluster version ------------------------------------------------------
+// The same items, with every PPR item run by a whole thread-block cluster
+// (16 CTAs of 1024 threads where the GPU allows it, else 8): the cluster's
+// 512 (256) warps split the instance's vertices, and the per-iteration
+// reductions go through distributed shared memory with one cluster barrier
+// per iteration.  Only a handful of instances are in flight at a time, so
+// their PPR vectors (2 x V_i x 128 B each) stay in L2 and the 128-byte row
+// gathers, eight per vertex per iteration, hit L2 instead of DRAM.  BFS items
+// still take one CTA each, before the PPR items.  Results depend on the
+// cluster size (it fixes the order of the dangling-mass sums), never on
+// scheduling: a solo run with the same cluster size is bitwise equal.
+constexpr int kClusterThreads = 1024;
+constexpr int kClusterWarps = kClusterThreads / 32;
+
+struct ClusterShared {
+    float d[kClusterWarps][32];      // per-warp dangling mass
+    double res[kClusterWarps][32];   // per-warp L1 change
+    float dc[2][32];                 // CTA dangling mass, by iteration parity
+    double rc[2][32];                // CTA L1 change, by iteration parity
+    int stop;
+};
+
+__device__ void cluster_ppr(const BatchArgs &a, uint32_t inst, cg::cluster_group &cl,
+                            ClusterShared &sh) {
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint32_t C = cl.num_blocks(), crank = cl.block_rank();
+    const uint32_t gw = crank * kClusterWarps + wid, nw = C * kClusterWarps;
+    const PprView p = ppr_view(a, inst, lane);
+    const int K = p.K;
+    // dangling mass: each warp in vertex order, then warps 0..31 of a CTA,
+    // then CTAs 0..C-1 (every CTA forms the same sum)
+    sh.d[wid][lane] = ppr_init_warp(a, p, lane, gw, nw);
+    __syncthreads();
+    if (wid == 0) {
+        float t = 0.0f;
+        for (int w = 0; w < kClusterWarps; w++) t += sh.d[w][lane];
+        sh.dc[0][lane] = t;
+    }
+    cl.sync();
+    int it = 0;
+    unsigned long long visits = 0;
+    while (it < a.max_it) {
+        const int pb = it & 1;
+        float dk = 0.0f;
+        for (uint32_t r = 0; r < C; r++) dk += cl.map_shared_rank(&sh.dc[pb][0], r)[lane];
+        const float *src = pb ? p.r1 : p.r0;
+        float *dst = pb ? p.r0 : p.r1;
+        double res = 0.0;
+        float dpart = 0.0f;
+        ppr_sweep_warp(a, p, lane, gw, nw, src, dst, dk, dpart, res, visits);
+        sh.d[wid][lane] = dpart;
+        sh.res[wid][lane] = res;
+        __syncthreads();
+        if (wid == 0) {
+            float t = 0.0f;
+            double q = 0.0;
+            for (int w = 0; w < kClusterWarps; w++) {
+                t += sh.d[w][lane];
+                q += sh.res[w][lane];
+            }
+            sh.dc[pb ^ 1][lane] = t;
+            sh.rc[pb ^ 1][lane] = q;
+        }
+        // orders this sweep's writes (vectors and partials) before every
+        // CTA's reads of the next sweep, cluster wide
+        cl.sync();
+        if (wid == 0) {   // stop test: the same on every CTA
+            double tot = 0.0;
+            for (uint32_t r = 0; r < C; r++) tot += cl.map_shared_rank(&sh.rc[pb ^ 1][0], r)[lane];
+            double mx = (int)lane < K ? tot : 0.0;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            if (lane == 0) sh.stop = mx < a.tol;
+        }
+        __syncthreads();
+        it++;
+        if (sh.stop) break;
+    }
+    if (it & 1) {   // result is in the scratch copy
+        for (uint32_t v = gw; v < p.n; v += nw)
+            if (p.lk) p.r0[(size_t)v * K + lane] = p.r1[(size_t)v * K + lane];
+    }
+    if (crank == 0 && threadIdx.x == 0) a.ppr_iters[inst] = it;
+    if (lane == 0 && visits) atomicAdd(&a.stats[1], visits * (unsigned long long)K);
+}
+
+__global__ void __launch_bounds__(kClusterThreads, 1) k_batch_cluster(BatchArgs a) {
+    __shared__ uint32_t bm[3 * (kBatchMaxV / 32)];
+    __shared__ ClusterShared sh;
+    __shared__ uint32_t s_item;
+    cg::cluster_group cl = cg::this_cluster();
+    if (a.do_bfs) {   // BFS items: one CTA each (counter[0])
+        for (;;) {
+            if (threadIdx.x == 0) s_item = atomicAdd(&a.counter[0], 1u);
+            __syncthreads();
+            const uint32_t item = s_item;
+            __syncthreads();
+            if (item >= (uint32_t)a.count) break;
+            cta_bfs(a, a.order[item], bm);
+        }
+    }
+    if (a.do_ppr) {   // PPR items: one cluster each (counter[1], taken by CTA 0)
+        for (;;) {
+            if (cl.block_rank() == 0 && threadIdx.x == 0) s_item = atomicAdd(&a.counter[1], 1u);
+            cl.sync();
+            const uint32_t item = *cl.map_shared_rank(&s_item, 0);
+            if (item >= (uint32_t)a.count) break;
+            cluster_ppr(a, a.order[item], cl, sh);
+        }
+    }
+    cl.sync();   // no CTA leaves while another may still read its shared memory
+}
+
+// Launch k_batch_cluster with `want` CTAs per cluster (8 or 16), or with the
+// largest size the GPU runs when want = 1; one CTA per SM.  *launched =
+// false when no wanted size is available.
+static int launch_batch_cluster(const BatchArgs &a, int num_sms, cudaStream_t s, int want,
+                                bool *launched, int *cluster_size) {
+    *launched = false;
+    if (cudaFuncSetAttribute(k_batch_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+        cudaSuccess)
+        cudaGetLastError();
+    for (int C : {16, 8}) {
+        if (want != 1 && want != C) continue;
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = C;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(C * std::max(1, num_sms / C));
+        cfg.blockDim = dim3(kClusterThreads);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = s;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int ncl = 0;
+        if (cudaOccupancyMaxActiveClusters(&ncl, k_batch_cluster, &cfg) != cudaSuccess || ncl < 1) {
+            cudaGetLastError();
+            continue;
+        }
+        cfg.gridDim = dim3(C * std::min(ncl, std::max(1, num_sms / C)));
+        OLV_CUDA(cudaLaunchKernelEx(&cfg, k_batch_cluster, a));
+        *launched = true;
+        *cluster_size = C;
+        return OLV_OK;
+    }
+    return OLV_OK;
+}
+
+// Device buffers of olv_batch_run, kept with the graph between calls (they
+// only grow), so a call allocates nothing once the sizes have been seen.
 struct BatchState {
     DevBuf off, order, seeds, tmp, inv, counter, iters, stats, levels, ppr;
     ~BatchState() {
@@ -244,6 +439,11 @@ struct BatchState {
         iters.release(); stats.release(); levels.release(); ppr.release();
     }
 };
+
+void release_batch_state(olv_graph *g) {
+    delete static_cast<BatchState *>(g->batch_state);
+    g->batch_state = nullptr;
+}
 
 }  // namespace olv
 
@@ -292,7 +492,8 @@ extern "C" int olv_batch_run(olv_graph *g, const uint32_t *inst_offsets, int cou
     std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
         return off[x + 1] - off[x] > off[y + 1] - off[y];
     });
-    BatchState bs;
+    if (!g->batch_state) g->batch_state = new BatchState();
+    BatchState &bs = *static_cast<BatchState *>(g->batch_state);
     cudaStream_t s = g->stream;
     const size_t V = off[count];
     OLV_TRY(bs.off.ensure((count + 1) * 4));
@@ -336,13 +537,19 @@ extern "C" int olv_batch_run(olv_graph *g, const uint32_t *inst_offsets, int cou
     a.counter = bs.counter.as<uint32_t>();
     a.ppr_iters = bs.iters.as<uint32_t>();
     a.stats = bs.stats.as<unsigned long long>();
-    int per_sm = 0;
-    OLV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, kBatchThreads, 0));
-    const int grid = std::max(1, per_sm) * g->num_sms;
     OLV_CUDA(cudaEventRecord(g->ev0, s));
     OLV_CUDA(cudaMemsetAsync(bs.counter.p, 0, 16, s));
     OLV_CUDA(cudaMemsetAsync(bs.stats.p, 0, 32, s));
-    k_batch<<<grid, kBatchThreads, 0, s>>>(a);
+    bool launched = false;
+    int csize = 0;
+    if (g->tune.batch_cluster)
+        OLV_TRY(launch_batch_cluster(a, g->num_sms, s, g->tune.batch_cluster, &launched, &csize));
+    if (!launched) {   // one CTA per item
+        int per_sm = 0;
+        OLV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, kBatchThreads, 0));
+        const int grid = std::max(1, per_sm) * g->num_sms;
+        k_batch<<<grid, kBatchThreads, 0, s>>>(a);
+    }
     OLV_CUDA(cudaGetLastError());
     OLV_CUDA(cudaEventRecord(g->ev1, s));
     unsigned long long hst[3];

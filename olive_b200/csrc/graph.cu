@@ -440,6 +440,7 @@ int olv_graph_destroy(olv_graph *g) {
     release_pr_state(g);
     release_ms_state(g);
     release_wpr_state(g);
+    release_batch_state(g);
     for (WhileGraph **wg : {&g->bfs_graph, &g->sssp_graph}) {
         if (*wg) {
             (*wg)->destroy();
@@ -513,6 +514,10 @@ int olv_tune_set(olv_graph *g, const char *key, double value) {
         t.ms_alpha = (float)value;
     } else if (!strcmp(key, "use_graphs")) {
         t.use_graphs = value != 0;
+    } else if (!strcmp(key, "batch_cluster")) {
+        OLV_CHECK_ARG(value == 0 || value == 1 || value == 8 || value == 16,
+                      "olv_tune_set: batch_cluster must be 0, 1, 8 or 16");
+        t.batch_cluster = (int)value;
     } else if (!strcmp(key, "levels_per_sync")) {
         OLV_CHECK_ARG(value >= 1 && value <= 1024, "olv_tune_set: levels_per_sync out of range");
         t.levels_per_sync = (int)value;
@@ -537,6 +542,7 @@ int olv_tune_get(const olv_graph *g, const char *key, double *value) {
     else if (!strcmp(key, "sssp_delta")) *value = t.sssp_delta;
     else if (!strcmp(key, "ms_alpha")) *value = t.ms_alpha;
     else if (!strcmp(key, "use_graphs")) *value = t.use_graphs;
+    else if (!strcmp(key, "batch_cluster")) *value = t.batch_cluster;
     else if (!strcmp(key, "levels_per_sync")) *value = t.levels_per_sync;
     else {
         set_error("olv_tune_get: unknown key '%s'", key);

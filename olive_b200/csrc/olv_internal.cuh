@@ -91,6 +91,7 @@ struct Tuning {
     float ms_alpha = 4.0f;        // msBFS: pull when active out-edges * ms_alpha > E
     int levels_per_sync = 4;      // host loop: supersteps enqueued per check
     int use_graphs = 1;           // run supersteps inside a CUDA graph
+    int batch_cluster = 1;        // batch PPR items run by thread-block clusters
 };
 
 struct Workspace {
@@ -139,6 +140,7 @@ struct olv_graph {
     void *pr_state = nullptr;            // PageRank plan + graph (pagerank.cu)
     void *ms_state = nullptr;            // multi-source BFS masks + graph (msbfs.cu)
     void *wpr_state = nullptr;           // weighted PageRank row plans (wpr.cu)
+    void *batch_state = nullptr;         // batch buffers kept between calls (batch.cu)
 };
 
 namespace olv {
@@ -147,4 +149,5 @@ int resident_blocks(const olv_graph *g, const void *kernel, int *blocks);
 void release_pr_state(olv_graph *g);
 void release_ms_state(olv_graph *g);
 void release_wpr_state(olv_graph *g);
+void release_batch_state(olv_graph *g);
 }

@@ -30,6 +30,8 @@ def main():
     ap.add_argument("--runs", type=int, default=2)
     ap.add_argument("--graphs", action="store_true", help="keep CUDA-graph mode")
     ap.add_argument("--count", type=int, default=512, help="batch: number of ER graphs")
+    ap.add_argument("--batch-cluster", type=int, default=1,
+                    help="batch: PPR items on thread-block clusters (1) or one CTA each (0)")
     a = ap.parse_args()
     import torch
 
@@ -37,6 +39,7 @@ def main():
     if a.workload == "batch":
         count, K = a.count, 32
         g, off = ob.Graph.er_batch(count, 1024, 65536, 8, seed=1)
+        g.tune(batch_cluster=a.batch_cluster)
         n = np.diff(off.astype(np.int64))
         rng = np.random.default_rng(11)
         seeds = np.stack([rng.integers(0, ni, K) for ni in n]).astype(np.uint32)

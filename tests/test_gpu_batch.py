@@ -111,3 +111,25 @@ def test_batch_rejects_non_block_diagonal(ob):
     with ob.Graph.from_csr(rp, cl) as g:
         with pytest.raises(ob.OliveError, match="block-diagonal"):
             g.batch(np.array([0, 200, 400], np.uint32), np.zeros((2, 4), np.uint32), max_it=3)
+
+
+@pytest.mark.parametrize("cluster", [0, 1, 8])
+def test_batch_cluster_and_cta_paths_vs_oracle(ob, small_batch, cluster):
+    """Both ways of running the PPR items (one thread-block cluster per item,
+    or one CTA per item) agree with the FP64 oracle; each is deterministic."""
+    g, off, rp, cl = small_batch
+    K = 32
+    seeds = draw_seeds(off, K, 5)
+    g.tune(batch_cluster=cluster)
+    try:
+        lv, pr, iters = g.batch(off, seeds, alpha=0.85, max_it=20, tol=0.0)
+        lv2, pr2, _ = g.batch(off, seeds, alpha=0.85, max_it=20, tol=0.0)
+    finally:
+        g.tune(batch_cluster=1)
+    assert pr.tobytes() == pr2.tobytes() and lv.tobytes() == lv2.tobytes()
+    for i in (0, 7, 23):
+        lrp, lcl = instance_csr(rp, cl, off, i)
+        np.testing.assert_array_equal(lv[off[i]:off[i + 1]], oracle.bfs(lrp, lcl, 0)[0])
+        pref, _ = oracle.ppr(lrp, lcl, seeds[i], 0.85, 20, 0.0)
+        np.testing.assert_allclose(pr[off[i]:off[i + 1]].astype(np.float64), pref,
+                                   rtol=2e-5, atol=2e-7)
