@@ -103,7 +103,7 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
  *   "alpha"       BFS push->pull when m_f * alpha > m_unvisited     (14)
  *   "beta"        BFS pull->push when n_f * beta < V                (24)
  *   "sssp_delta"  SSSP bucket width, 0 = default                    (0)
- *   "ms_alpha"    msBFS pull when active out-edges * ms_alpha > E   (4)
+ *   "ms_alpha"    msBFS pull when active out-edges * ms_alpha > E   (20)
  *   "use_graphs"  run supersteps inside CUDA graphs (1) or a host loop (0)
  *   "levels_per_sync" host loop: supersteps enqueued per check      (4)
  *   "batch_cluster" olv_batch_run: PPR items on thread-block clusters of

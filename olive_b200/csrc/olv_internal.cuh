@@ -88,7 +88,7 @@ struct Tuning {
     float alpha = 14.0f;          // push -> pull when m_f > m_unvisited / alpha
     float beta = 24.0f;           // pull -> push when n_f < V / beta
     uint32_t sssp_delta = 0;      // 0 = default bucket width (64)
-    float ms_alpha = 4.0f;        // msBFS: pull when active out-edges * ms_alpha > E
+    float ms_alpha = 20.0f;       // msBFS: pull when active out-edges * ms_alpha > E
     int levels_per_sync = 4;      // host loop: supersteps enqueued per check
     int use_graphs = 1;           // run supersteps inside a CUDA graph
     int batch_cluster = 1;        // batch PPR items run by thread-block clusters

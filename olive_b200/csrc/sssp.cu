@@ -75,8 +75,11 @@ __global__ void k_partition_rows(const uint32_t *__restrict__ rowptr,
     }
 }
 
+#ifndef OLV_SSSP_MINB
+#define OLV_SSSP_MINB 4   // 4: <= 64 registers
+#endif
 struct SsspOp {
-    static constexpr int kMinBlocks = 4;   // CTAs per SM the advance must fit (<= 64 registers)
+    static constexpr int kMinBlocks = OLV_SSSP_MINB;   // CTAs per SM the advance must fit
     using SV = uint32_t;
     static constexpr bool kHasFar = true;
     const uint32_t *w;
