@@ -208,6 +208,87 @@ __device__ __forceinline__ void ppr_sweep_warp(const BatchArgs &a, const PprView
     }
 }
 
+// The same sweep for K = 32 with 16-byte rows per lane: lane l holds vectors
+// 4(l & 7) .. 4(l & 7) + 3 of in-edge slot l >> 3, so one load instruction of
+// the warp fetches the rows of four in-edges and a round keeps eight in
+// flight.  Each slot folds its edges in CSC order; the four slot sums are
+// then added by a fixed shuffle tree (the same sum on every lane) and handed
+// back to lane k = vector k for the update.  Needs 16-byte aligned vectors.
+// Used by the cluster kernel, whose rows come from L2 (the one-CTA-per-item
+// kernel is bound by DRAM traffic and keeps the 4-byte path).
+__device__ __forceinline__ void ppr_sweep_warp_v4(const BatchArgs &a, const PprView &p,
+                                                  uint32_t lane, uint32_t w0, uint32_t nw,
+                                                  const float *src, float *dst, float dk,
+                                                  float &dpart, double &res,
+                                                  unsigned long long &visits) {
+    constexpr unsigned kFull = 0xffffffffu;
+    const uint32_t base = p.base, n = p.n;
+    const uint32_t slot = lane >> 3, quad = lane & 7;
+    const float4 *src4 = reinterpret_cast<const float4 *>(src);
+    for (uint32_t v = w0; v < n; v += nw) {
+        const uint32_t b = a.colptr[base + v], e = a.colptr[base + v + 1];
+        float4 acc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        for (uint32_t c0 = b; c0 < e; c0 += 32) {
+            const uint32_t cnt = min(32u, e - c0);
+            uint32_t u = 0;
+            float w = 0.0f;
+            if (lane < cnt) {
+                u = a.rowidx[c0 + lane] - base;
+                if (u >= n) {   // edge enters from outside the instance
+                    atomicOr((unsigned int *)&a.stats[2], 2u);
+                    u = 0;
+                } else {
+                    w = p.inv[u];
+                }
+            }
+            for (uint32_t t = 0; t < cnt; t += 8) {
+                float4 x[2];
+                float wj[2];
+#pragma unroll
+                for (int r = 0; r < 2; r++) {
+                    const uint32_t i = t + 4 * r + slot;
+                    const uint32_t uj = __shfl_sync(kFull, u, i & 31);
+                    wj[r] = __shfl_sync(kFull, w, i & 31);
+                    x[r] = i < cnt ? src4[(size_t)uj * 8 + quad] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                }
+#pragma unroll
+                for (int r = 0; r < 2; r++) {
+                    if (t + 4 * r + slot < cnt) {
+                        acc.x = fmaf(x[r].x, wj[r], acc.x);
+                        acc.y = fmaf(x[r].y, wj[r], acc.y);
+                        acc.z = fmaf(x[r].z, wj[r], acc.z);
+                        acc.w = fmaf(x[r].w, wj[r], acc.w);
+                    }
+                }
+            }
+        }
+        // slots 0+1 and 2+3, then the two pairs (commutative adds: every
+        // lane of a quad ends with the same sum)
+#pragma unroll
+        for (int o = 8; o <= 16; o <<= 1) {
+            acc.x += __shfl_xor_sync(kFull, acc.x, o);
+            acc.y += __shfl_xor_sync(kFull, acc.y, o);
+            acc.z += __shfl_xor_sync(kFull, acc.z, o);
+            acc.w += __shfl_xor_sync(kFull, acc.w, o);
+        }
+        const uint32_t from = lane >> 2, comp = lane & 3;
+        const float ax = __shfl_sync(kFull, acc.x, from), ay = __shfl_sync(kFull, acc.y, from);
+        const float az = __shfl_sync(kFull, acc.z, from), aw = __shfl_sync(kFull, acc.w, from);
+        const float sum = comp == 0 ? ax : comp == 1 ? ay : comp == 2 ? az : aw;
+        visits += e - b;
+        const float tele = (v == p.seed) ? fmaf(p.alpha, dk, 1.0f - p.alpha) : 0.0f;
+        const float nv = fmaf(p.alpha, sum, tele);
+        res += fabs((double)nv - (double)src[(size_t)v * 32 + lane]);
+        dst[(size_t)v * 32 + lane] = nv;
+        if (p.inv[v] == 0.0f) dpart += nv;
+    }
+}
+
+// Whether an item's sweeps can use the 16-byte row path.
+__device__ __forceinline__ bool ppr_v4(const BatchArgs &a) {
+    return a.K == 32 && ((reinterpret_cast<uintptr_t>(a.ppr) | reinterpret_cast<uintptr_t>(a.ppr_tmp)) & 15) == 0;
+}
+
 __device__ void cta_ppr(const BatchArgs &a, uint32_t inst) {
     const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const PprView p = ppr_view(a, inst, lane);
@@ -329,7 +410,10 @@ __device__ void cluster_ppr(const BatchArgs &a, uint32_t inst, cg::cluster_group
         float *dst = pb ? p.r0 : p.r1;
         double res = 0.0;
         float dpart = 0.0f;
-        ppr_sweep_warp(a, p, lane, gw, nw, src, dst, dk, dpart, res, visits);
+        if (ppr_v4(a))
+            ppr_sweep_warp_v4(a, p, lane, gw, nw, src, dst, dk, dpart, res, visits);
+        else
+            ppr_sweep_warp(a, p, lane, gw, nw, src, dst, dk, dpart, res, visits);
         sh.d[wid][lane] = dpart;
         sh.res[wid][lane] = res;
         __syncthreads();
