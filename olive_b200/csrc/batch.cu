@@ -208,32 +208,56 @@ __device__ __forceinline__ void ppr_sweep_warp(const BatchArgs &a, const PprView
     }
 }
 
-// The same sweep for K = 32 with 16-byte rows per lane: lane l holds vectors
-// 4(l & 7) .. 4(l & 7) + 3 of in-edge slot l >> 3, so one load instruction of
-// the warp fetches the rows of four in-edges and a round keeps eight in
-// flight.  Each slot folds its edges in CSC order; the four slot sums are
-// then added by a fixed shuffle tree (the same sum on every lane) and handed
-// back to lane k = vector k for the update.  Needs 16-byte aligned vectors.
-// Used by the cluster kernel, whose rows come from L2 (the one-CTA-per-item
-// kernel is bound by DRAM traffic and keeps the 4-byte path).
-__device__ __forceinline__ void ppr_sweep_warp_v4(const BatchArgs &a, const PprView &p,
-                                                  uint32_t lane, uint32_t w0, uint32_t nw,
-                                                  const float *src, float *dst, float dk,
-                                                  float &dpart, double &res,
-                                                  unsigned long long &visits) {
+// K = 32 sweep with four vertices per warp: slot s = lane >> 3 (8 lanes)
+// takes vertex 4g + s of vertex group g (g = w0, w0 + nw, ...), lane quad q =
+// lane & 7 holds vectors 4q .. 4q+3 of it as one float4.  A round gathers
+// two in-edges of each of the four vertices (one 16-byte load per lane per
+// in-edge), so the per-vertex work -- offsets, sources, update, residual --
+// is shared by four vertices per instruction.  Each vertex's in-edges are
+// folded in CSC order; the warp's dangling mass and L1 change are combined
+// over the slots by a fixed shuffle tree and returned in the lane-per-vector
+// layout, like ppr_sweep_warp.  `visits` gets the warp's in-edge visits.
+// Needs 16-byte aligned vectors.  Used by the cluster kernel, whose rows come
+// from L2 (the one-CTA-per-item kernel is bound by DRAM traffic and keeps the
+// 4-byte path).
+__device__ __forceinline__ void ppr_sweep_warp_q(const BatchArgs &a, const PprView &p,
+                                                 uint32_t lane, uint32_t w0, uint32_t nw,
+                                                 const float *src, float *dst, float dk,
+                                                 float &dpart, double &res,
+                                                 unsigned long long &visits) {
     constexpr unsigned kFull = 0xffffffffu;
     const uint32_t base = p.base, n = p.n;
     const uint32_t slot = lane >> 3, quad = lane & 7;
     const float4 *src4 = reinterpret_cast<const float4 *>(src);
-    for (uint32_t v = w0; v < n; v += nw) {
-        const uint32_t b = a.colptr[base + v], e = a.colptr[base + v + 1];
+    float4 *dst4 = reinterpret_cast<float4 *>(dst);
+    uint32_t seed4[4];
+    float dk4[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        seed4[c] = __shfl_sync(kFull, p.seed, 4 * quad + c);
+        dk4[c] = __shfl_sync(kFull, dk, 4 * quad + c);
+    }
+    float dp4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    double rs4[4] = {0.0, 0.0, 0.0, 0.0};
+    unsigned long long vq = 0;
+    for (uint32_t g = w0; 4 * g < n; g += nw) {
+        const uint32_t v = 4 * g + slot;
+        const bool valid = v < n;
+        uint32_t b = 0, deg = 0;
+        if (valid) {
+            b = a.colptr[base + v];
+            deg = a.colptr[base + v + 1] - b;
+        }
+        uint32_t maxdeg = deg;
+        maxdeg = max(maxdeg, __shfl_xor_sync(kFull, maxdeg, 8));
+        maxdeg = max(maxdeg, __shfl_xor_sync(kFull, maxdeg, 16));
         float4 acc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        for (uint32_t c0 = b; c0 < e; c0 += 32) {
-            const uint32_t cnt = min(32u, e - c0);
+        for (uint32_t c0 = 0; c0 < maxdeg; c0 += 8) {
+            // lane quad q of a slot holds in-edge c0 + q of the slot's vertex
             uint32_t u = 0;
             float w = 0.0f;
-            if (lane < cnt) {
-                u = a.rowidx[c0 + lane] - base;
+            if (c0 + quad < deg) {
+                u = a.rowidx[b + c0 + quad] - base;
                 if (u >= n) {   // edge enters from outside the instance
                     atomicOr((unsigned int *)&a.stats[2], 2u);
                     u = 0;
@@ -241,19 +265,21 @@ __device__ __forceinline__ void ppr_sweep_warp_v4(const BatchArgs &a, const PprV
                     w = p.inv[u];
                 }
             }
-            for (uint32_t t = 0; t < cnt; t += 8) {
+            const uint32_t cend = min(8u, maxdeg - c0);
+            for (uint32_t t = 0; t < cend; t += 2) {
                 float4 x[2];
                 float wj[2];
 #pragma unroll
                 for (int r = 0; r < 2; r++) {
-                    const uint32_t i = t + 4 * r + slot;
-                    const uint32_t uj = __shfl_sync(kFull, u, i & 31);
-                    wj[r] = __shfl_sync(kFull, w, i & 31);
-                    x[r] = i < cnt ? src4[(size_t)uj * 8 + quad] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    const uint32_t i = t + r;
+                    const uint32_t uj = __shfl_sync(kFull, u, slot * 8 + (i & 7));
+                    wj[r] = __shfl_sync(kFull, w, slot * 8 + (i & 7));
+                    x[r] = c0 + i < deg ? src4[(size_t)uj * 8 + quad]
+                                        : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 }
 #pragma unroll
                 for (int r = 0; r < 2; r++) {
-                    if (t + 4 * r + slot < cnt) {
+                    if (c0 + t + r < deg) {
                         acc.x = fmaf(x[r].x, wj[r], acc.x);
                         acc.y = fmaf(x[r].y, wj[r], acc.y);
                         acc.z = fmaf(x[r].z, wj[r], acc.z);
@@ -262,26 +288,48 @@ __device__ __forceinline__ void ppr_sweep_warp_v4(const BatchArgs &a, const PprV
                 }
             }
         }
-        // slots 0+1 and 2+3, then the two pairs (commutative adds: every
-        // lane of a quad ends with the same sum)
+        if (quad == 0) vq += deg;
+        if (valid) {
+            const float4 old = src4[(size_t)v * 8 + quad];
+            const float a4[4] = {acc.x, acc.y, acc.z, acc.w};
+            const float o4[4] = {old.x, old.y, old.z, old.w};
+            float nv[4];
+            const bool dang = p.inv[v] == 0.0f;
 #pragma unroll
-        for (int o = 8; o <= 16; o <<= 1) {
-            acc.x += __shfl_xor_sync(kFull, acc.x, o);
-            acc.y += __shfl_xor_sync(kFull, acc.y, o);
-            acc.z += __shfl_xor_sync(kFull, acc.z, o);
-            acc.w += __shfl_xor_sync(kFull, acc.w, o);
+            for (int c = 0; c < 4; c++) {
+                const float tele = (v == seed4[c]) ? fmaf(p.alpha, dk4[c], 1.0f - p.alpha) : 0.0f;
+                nv[c] = fmaf(p.alpha, a4[c], tele);
+                rs4[c] += fabs((double)nv[c] - (double)o4[c]);
+                if (dang) dp4[c] += nv[c];
+            }
+            dst4[(size_t)v * 8 + quad] = make_float4(nv[0], nv[1], nv[2], nv[3]);
         }
-        const uint32_t from = lane >> 2, comp = lane & 3;
-        const float ax = __shfl_sync(kFull, acc.x, from), ay = __shfl_sync(kFull, acc.y, from);
-        const float az = __shfl_sync(kFull, acc.z, from), aw = __shfl_sync(kFull, acc.w, from);
-        const float sum = comp == 0 ? ax : comp == 1 ? ay : comp == 2 ? az : aw;
-        visits += e - b;
-        const float tele = (v == p.seed) ? fmaf(p.alpha, dk, 1.0f - p.alpha) : 0.0f;
-        const float nv = fmaf(p.alpha, sum, tele);
-        res += fabs((double)nv - (double)src[(size_t)v * 32 + lane]);
-        dst[(size_t)v * 32 + lane] = nv;
-        if (p.inv[v] == 0.0f) dpart += nv;
     }
+    // slots 0+1 and 2+3, then the pairs; back to lane k = vector k
+#pragma unroll
+    for (int o = 8; o <= 16; o <<= 1) {
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            dp4[c] += __shfl_xor_sync(kFull, dp4[c], o);
+            rs4[c] += __shfl_xor_sync(kFull, rs4[c], o);
+        }
+        vq += __shfl_xor_sync(kFull, vq, o);
+    }
+    const uint32_t from = lane >> 2, comp = lane & 3;
+    float dsel = 0.0f;
+    double rsel = 0.0;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const float dc = __shfl_sync(kFull, dp4[c], from);
+        const double rc = __shfl_sync(kFull, rs4[c], from);
+        if (comp == (uint32_t)c) {
+            dsel = dc;
+            rsel = rc;
+        }
+    }
+    dpart += dsel;
+    res += rsel;
+    visits += vq;
 }
 
 // Whether an item's sweeps can use the 16-byte row path.
@@ -411,7 +459,7 @@ __device__ void cluster_ppr(const BatchArgs &a, uint32_t inst, cg::cluster_group
         double res = 0.0;
         float dpart = 0.0f;
         if (ppr_v4(a))
-            ppr_sweep_warp_v4(a, p, lane, gw, nw, src, dst, dk, dpart, res, visits);
+            ppr_sweep_warp_q(a, p, lane, gw, nw, src, dst, dk, dpart, res, visits);
         else
             ppr_sweep_warp(a, p, lane, gw, nw, src, dst, dk, dpart, res, visits);
         sh.d[wid][lane] = dpart;
