@@ -312,20 +312,32 @@ static_assert(kMsSlots == 16, "four level bits");
 
 // Row q of the output for sources q0 .. q0+31 of one vertex, from 32-bit
 // halves of the level-bit masks (b0..b3), the stored-level mask and the
-// visit mask.  `out` points at row q0, column v.
+// visit mask.  `out` points at row q0, column v.  For each group of eight
+// sources the four planes' bytes are packed into one word W (b3, b2, b1, b0
+// from the low byte up); a source's level is then (((W >> j) & 0x01010101)
+// * 0x08040201) >> 24: the multiply lines the four bits up at bits 24..27
+// (8 b3 + 4 b2 + 2 b1 + b0), with no carries since no two partial products
+// share a bit.
 template <int Q0>
 __device__ __forceinline__ void ms_write_half(int32_t *out, uint64_t V, int n, uint32_t b0,
                                               uint32_t b1, uint32_t b2, uint32_t b3, uint32_t any,
                                               uint32_t vis) {
 #pragma unroll
-    for (int j = 0; j < 32; j++) {
-        if (Q0 + j >= n) break;
-        const int32_t lvl = (int32_t)(((b0 >> j) & 1u) | (((b1 >> j) & 1u) << 1) |
-                                      (((b2 >> j) & 1u) << 2) | (((b3 >> j) & 1u) << 3));
-        const bool reached = (vis >> j) & 1u;
-        const bool stored = (any >> j) & 1u;
-        if (!reached || stored) __stcs(out, reached ? lvl : kInf);
-        out += V;
+    for (int m = 0; m < 4; m++) {
+        if (Q0 + 8 * m >= n) break;
+        const uint32_t sel = (uint32_t)m | ((4u + m) << 4);
+        const uint32_t lo = __byte_perm(b3, b2, sel);   // [b3.m, b2.m, -, -]
+        const uint32_t hi = __byte_perm(b1, b0, sel);   // [b1.m, b0.m, -, -]
+        const uint32_t W = __byte_perm(lo, hi, 0x5410);
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            if (Q0 + 8 * m + j >= n) break;
+            const int32_t lvl = (int32_t)((((W >> j) & 0x01010101u) * 0x08040201u) >> 24);
+            const bool reached = (vis >> (8 * m + j)) & 1u;
+            const bool stored = (any >> (8 * m + j)) & 1u;
+            if (!reached || stored) __stcs(out, reached ? lvl : kInf);
+            out += V;
+        }
     }
 }
 

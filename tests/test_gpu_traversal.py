@@ -250,6 +250,19 @@ def test_msbfs_fixtures_duplicates_and_device_output(ob):
             np.testing.assert_array_equal(o[1], z["bfs_levels"][0])
 
 
+@pytest.mark.parametrize("rows,cols,n", [(37, 29, 64), (11, 3, 40), (128, 128, 33)])
+def test_msbfs_long_diameter_grids(ob, rows, cols, n):
+    """Grids: levels far past the 16 stored level slots, V not a multiple of 32."""
+    rp, cl = oracle.grid_csr(rows, cols)
+    V = rows * cols
+    srcs = np.random.default_rng(rows).choice(V, min(n, V), replace=False).astype(np.uint32)
+    with ob.Graph.from_csr(rp, cl) as g:
+        lv = g.msbfs(srcs)
+        for s in range(len(srcs)):
+            ref, _ = oracle.bfs(rp, cl, int(srcs[s]))
+            np.testing.assert_array_equal(lv[s], ref, err_msg=f"row {s}")
+
+
 def test_msbfs_bad_arguments(ob):
     rp, cl = oracle.grid_csr(4, 4)
     with ob.Graph.from_csr(rp, cl) as g:
