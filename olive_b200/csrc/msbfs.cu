@@ -376,6 +376,115 @@ k_ms_levels(uint32_t V, int n, unsigned long long srcmask, TravCtl *c,
     warp_add64(reached, &c->reached);
 }
 
+// The same output with one thread per four consecutive vertices, each row's
+// four levels written as one 16-byte store (a warp writes 512 contiguous
+// bytes of a row).  Needs V % 4 == 0 and a 16-byte aligned output.
+__device__ __forceinline__ uint32_t ms_pack_planes(uint32_t b0, uint32_t b1, uint32_t b2,
+                                                   uint32_t b3, uint32_t m) {
+    const uint32_t sel = m | ((4u + m) << 4);
+    return __byte_perm(__byte_perm(b3, b2, sel), __byte_perm(b1, b0, sel), 0x5410);
+}
+
+template <int Q0>
+__device__ __forceinline__ void ms_write_half4(int32_t *out, uint64_t V, int n,
+                                               const uint32_t (&b0)[4], const uint32_t (&b1)[4],
+                                               const uint32_t (&b2)[4], const uint32_t (&b3)[4],
+                                               const uint32_t (&any)[4], const uint32_t (&vis)[4]) {
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+        if (Q0 + 8 * m >= n) break;
+        uint32_t W[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) W[k] = ms_pack_planes(b0[k], b1[k], b2[k], b3[k], m);
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            if (Q0 + 8 * m + j >= n) break;
+            int32_t val[4];
+            bool skip = false;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int32_t lvl = (int32_t)((((W[k] >> j) & 0x01010101u) * 0x08040201u) >> 24);
+                const bool reached = (vis[k] >> (8 * m + j)) & 1u;
+                const bool stored = (any[k] >> (8 * m + j)) & 1u;
+                val[k] = reached ? lvl : kInf;
+                skip |= reached && !stored;
+            }
+            if (!skip) {
+                __stcs(reinterpret_cast<int4 *>(out), make_int4(val[0], val[1], val[2], val[3]));
+            } else {   // a level past the store, written by apply: leave it
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const bool reached = (vis[k] >> (8 * m + j)) & 1u;
+                    const bool stored = (any[k] >> (8 * m + j)) & 1u;
+                    if (!reached || stored) __stcs(out + k, val[k]);
+                }
+            }
+            out += V;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBlock, 3)
+k_ms_levels4(uint32_t V, int n, unsigned long long srcmask, TravCtl *c,
+             const unsigned long long *__restrict__ visit,
+             const unsigned long long *__restrict__ store) {
+    int32_t *levels = static_cast<int32_t *>(c->vdata);
+    const uint32_t nst = c->level + 1 < kMsSlots ? c->level + 1 : kMsSlots;
+    unsigned long long reached = 0;
+    const uint64_t nq = V / 4;
+    for (uint64_t t = blockIdx.x * (uint64_t)kBlock + threadIdx.x; t < nq;
+         t += (uint64_t)gridDim.x * kBlock) {
+        const uint64_t v0 = 4 * t;
+        const ulonglong2 va = __ldcs(reinterpret_cast<const ulonglong2 *>(visit + v0));
+        const ulonglong2 vb = __ldcs(reinterpret_cast<const ulonglong2 *>(visit + v0 + 2));
+        unsigned long long vis[4] = {va.x & srcmask, va.y & srcmask, vb.x & srcmask, vb.y & srcmask};
+        unsigned long long B0[4] = {0, 0, 0, 0}, B1[4] = {0, 0, 0, 0}, B2[4] = {0, 0, 0, 0},
+                           B3[4] = {0, 0, 0, 0}, AN[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (uint32_t L = 0; L < kMsSlots; L++) {
+            if (L >= nst) break;
+            const unsigned long long *sl = store + (uint64_t)L * V + v0;
+            const ulonglong2 x = __ldcs(reinterpret_cast<const ulonglong2 *>(sl));
+            const ulonglong2 y = __ldcs(reinterpret_cast<const ulonglong2 *>(sl + 2));
+            const unsigned long long mk[4] = {x.x, x.y, y.x, y.y};
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                AN[k] |= mk[k];
+                if (L & 1) B0[k] |= mk[k];
+                if (L & 2) B1[k] |= mk[k];
+                if (L & 4) B2[k] |= mk[k];
+                if (L & 8) B3[k] |= mk[k];
+            }
+        }
+        uint32_t b0[4], b1[4], b2[4], b3[4], an[4], vs[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            reached += __popcll(vis[k]);
+            b0[k] = (uint32_t)B0[k];
+            b1[k] = (uint32_t)B1[k];
+            b2[k] = (uint32_t)B2[k];
+            b3[k] = (uint32_t)B3[k];
+            an[k] = (uint32_t)AN[k];
+            vs[k] = (uint32_t)vis[k];
+        }
+        int32_t *out = levels + v0;
+        ms_write_half4<0>(out, V, n, b0, b1, b2, b3, an, vs);
+        if (n > 32) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                b0[k] = (uint32_t)(B0[k] >> 32);
+                b1[k] = (uint32_t)(B1[k] >> 32);
+                b2[k] = (uint32_t)(B2[k] >> 32);
+                b3[k] = (uint32_t)(B3[k] >> 32);
+                an[k] = (uint32_t)(AN[k] >> 32);
+                vs[k] = (uint32_t)(vis[k] >> 32);
+            }
+            ms_write_half4<32>(out + 32 * (uint64_t)V, V, n, b0, b1, b2, b3, an, vs);
+        }
+    }
+    warp_add64(reached, &c->reached);
+}
+
 // ------------------------------------------------------------------ host --
 template <class Sink>
 static int ms_superstep(olv_graph *g, MsState &ms, Sink &&sink, cudaGraphConditionalHandle h,
@@ -546,8 +655,12 @@ extern "C" int olv_msbfs(olv_graph *g, const uint32_t *srcs, int n, int32_t *lev
             if (g->host_ctl->done) break;
         }
     }
-    k_ms_levels<<<g->num_sms * 8, kBlock, 0, s>>>(g->V, n, srcmask, ctl, visit,
-                                                  ms.store.as<unsigned long long>());
+    if (g->V % 4 == 0 && ((uintptr_t)levels & 15) == 0)   // 16-byte rows of four vertices
+        k_ms_levels4<<<g->num_sms * 6, kBlock, 0, s>>>(g->V, n, srcmask, ctl, visit,
+                                                       ms.store.as<unsigned long long>());
+    else
+        k_ms_levels<<<g->num_sms * 8, kBlock, 0, s>>>(g->V, n, srcmask, ctl, visit,
+                                                      ms.store.as<unsigned long long>());
     OLV_CUDA(cudaGetLastError());
     OLV_CUDA(cudaEventRecord(g->ev1, s));
     OLV_CUDA(cudaMemcpyAsync(g->host_ctl, ctl, sizeof(TravCtl), cudaMemcpyDeviceToHost, s));
