@@ -346,7 +346,9 @@ k_ms_levels(uint32_t V, int n, unsigned long long srcmask, TravCtl *c,
             const unsigned long long *__restrict__ visit,
             const unsigned long long *__restrict__ store) {
     int32_t *levels = static_cast<int32_t *>(c->vdata);
-    const uint32_t nst = c->level + 1 < kMsSlots ? c->level + 1 : kMsSlots;
+    // slots 0 .. level-1: the run ended because level `level` found no new
+    // vertex, so its slot is all zeros and is not read
+    const uint32_t nst = c->level < kMsSlots ? c->level : kMsSlots;
     unsigned long long reached = 0;
     for (uint64_t v = blockIdx.x * (uint64_t)kBlock + threadIdx.x; v < V;
          v += (uint64_t)gridDim.x * kBlock) {
@@ -429,7 +431,9 @@ k_ms_levels4(uint32_t V, int n, unsigned long long srcmask, TravCtl *c,
              const unsigned long long *__restrict__ visit,
              const unsigned long long *__restrict__ store) {
     int32_t *levels = static_cast<int32_t *>(c->vdata);
-    const uint32_t nst = c->level + 1 < kMsSlots ? c->level + 1 : kMsSlots;
+    // slots 0 .. level-1: the run ended because level `level` found no new
+    // vertex, so its slot is all zeros and is not read
+    const uint32_t nst = c->level < kMsSlots ? c->level : kMsSlots;
     unsigned long long reached = 0;
     const uint64_t nq = V / 4;
     for (uint64_t t = blockIdx.x * (uint64_t)kBlock + threadIdx.x; t < nq;
@@ -655,12 +659,16 @@ extern "C" int olv_msbfs(olv_graph *g, const uint32_t *srcs, int n, int32_t *lev
             if (g->host_ctl->done) break;
         }
     }
-    if (g->V % 4 == 0 && ((uintptr_t)levels & 15) == 0)   // 16-byte rows of four vertices
-        k_ms_levels4<<<g->num_sms * 6, kBlock, 0, s>>>(g->V, n, srcmask, ctl, visit,
-                                                       ms.store.as<unsigned long long>());
-    else
+    if (g->V % 4 == 0 && ((uintptr_t)levels & 15) == 0) {   // 16-byte rows of four vertices
+        int nb4 = 0;
+        OLV_TRY(resident_blocks(g, (const void *)k_ms_levels4, &nb4));
+        k_ms_levels4<<<nb4, kBlock, 0, s>>>(g->V, n, srcmask, ctl, visit,
+                                            ms.store.as<unsigned long long>());
+    }
+    else {
         k_ms_levels<<<g->num_sms * 8, kBlock, 0, s>>>(g->V, n, srcmask, ctl, visit,
                                                       ms.store.as<unsigned long long>());
+    }
     OLV_CUDA(cudaGetLastError());
     OLV_CUDA(cudaEventRecord(g->ev1, s));
     OLV_CUDA(cudaMemcpyAsync(g->host_ctl, ctl, sizeof(TravCtl), cudaMemcpyDeviceToHost, s));
