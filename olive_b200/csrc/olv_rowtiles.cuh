@@ -34,7 +34,10 @@
 namespace olv {
 
 constexpr uint32_t kTileLong = 2048;   // rows longer than this are segmented
-constexpr uint32_t kTileSeg = 2048;    // entries per segment of a long row
+#ifndef OLV_TILE_SEG
+#define OLV_TILE_SEG 512
+#endif
+constexpr uint32_t kTileSeg = OLV_TILE_SEG;   // entries per segment of a long row
 #ifndef OLV_TILE_U
 #define OLV_TILE_U 8
 #endif
