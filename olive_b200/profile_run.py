@@ -45,6 +45,7 @@ def main():
         seeds = np.stack([rng.integers(0, ni, K) for ni in n]).astype(np.uint32)
         lv = torch.empty(g.V, dtype=torch.int32, device="cuda")
         pr = torch.empty((g.V, K), dtype=torch.float32, device="cuda")
+        g.batch(off, seeds, K=K, alpha=0.85, max_it=50, tol=1e-7, levels_out=lv, ppr_out=pr)
         torch.cuda.synchronize()
         torch.cuda.profiler.start()
         for _ in range(a.runs):
@@ -74,6 +75,8 @@ def main():
         gv = torch.from_numpy(rng.standard_normal(g.V).astype(np.float32)).cuda()
         dw = torch.empty(g.E, dtype=torch.float32, device="cuda")
         dp = torch.empty(g.V, dtype=torch.float32, device="cuda")
+        g.wpr_forward(p, w=w, max_it=100, out=out)   # builds the row plans
+        g.wpr_backward(gv, max_it=100, dw_out=dw, dp_out=dp)
         torch.cuda.synchronize()
         torch.cuda.profiler.start()
         for _ in range(a.runs):
