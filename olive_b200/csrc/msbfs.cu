@@ -40,6 +40,7 @@ constexpr uint32_t kMsSlots = 16;      // levels whose new-bit masks are stored 
 struct MsState {
     DevBuf masks;     // visit | next | cur A | cur B, V words each (A, B: levels >= kMsSlots)
     DevBuf store;     // new-bit masks of levels 0 .. kMsSlots-1, V words each
+    DevBuf touched;   // vertices first touched by a tracked push level
     DevBuf srcs;
     DevBuf pieces;    // (vertex, first in-edge, end) of heavy vertices' in-edge pieces
     uint32_t npieces = 0;
@@ -49,6 +50,7 @@ struct MsState {
     ~MsState() {
         masks.release();
         store.release();
+        touched.release();
         srcs.release();
         pieces.release();
         graph.destroy();
@@ -73,23 +75,60 @@ struct MsPushOp {
     const unsigned long long *cur;
     const unsigned long long *visit;
     unsigned long long *next;
+    uint32_t *touched;          // first-touched vertices of a tracked level
+    uint32_t *ntouched;
+    uint32_t track;
     struct Pre {
         unsigned long long bits;
     };
-    __device__ __forceinline__ void begin(TravCtl *c) { cur = cm.at(c->level); }
+    __device__ __forceinline__ void begin(TravCtl *c) {
+        cur = cm.at(c->level);
+        track = c->ms_track;
+        ntouched = &c->ms_touched;
+    }
     __device__ __forceinline__ SV src_value(uint32_t u) const { return cur[u]; }
     __device__ __forceinline__ void on_input(uint32_t) const {}
     __device__ __forceinline__ Pre prepare(SV sv, uint32_t, uint32_t v) const {
         return Pre{sv & ~__ldg(&visit[v])};
     }
+    // OR the source bits into next[v]; on a tracked level, also list every v
+    // whose next mask was zero before (once per vertex and level), with one
+    // list atomic per warp.  All 32 lanes call it.
     template <int N>
     __device__ __forceinline__ void apply_n(const Pre (&p)[N], const uint32_t (&v)[N],
                                             int (&act)[N]) {
+        if (!track) {
+#pragma unroll
+            for (int j = 0; j < N; j++) {
+                if (act[j] && p[j].bits) atomicOr(&next[v[j]], p[j].bits);
+                act[j] = 0;
+            }
+            return;
+        }
+        bool first[N];
+        uint32_t cnt = 0;
 #pragma unroll
         for (int j = 0; j < N; j++) {
-            if (act[j] && p[j].bits) atomicOr(&next[v[j]], p[j].bits);
+            first[j] = false;
+            if (act[j] && p[j].bits) first[j] = atomicOr(&next[v[j]], p[j].bits) == 0ULL;
+            cnt += first[j];
             act[j] = 0;
         }
+        const uint32_t lane = lane_id();
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (uint32_t)o) incl += t;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        if (!total) return;
+        uint32_t base = 0;
+        if (lane == 31) base = atomicAdd(ntouched, total);
+        base = __shfl_sync(0xffffffffu, base, 31) + incl - cnt;
+#pragma unroll
+        for (int j = 0; j < N; j++)
+            if (first[j]) touched[base++] = v[j];
     }
     __device__ __forceinline__ void on_push(bool, uint32_t) {}
     __device__ __forceinline__ void flush(unsigned long long) {}
@@ -117,6 +156,10 @@ __global__ void k_ms_init(TravCtl *c, int32_t *levels, const uint32_t *srcs, int
     if (threadIdx.x == 0) {
         TravCtl t = {};
         t.vdata = levels;
+        t.ms_sparse_from = 0xffffffffu;
+        t.ms_cur_dense = 1;                  // slot 0 is cleared and holds the sources
+        t.ms_new_prev = (unsigned long long)n;   // level 0: the sources
+        t.ms_new_prev2 = 0;
         *c = t;
         s_edges = 0;
     }
@@ -144,11 +187,25 @@ __global__ void k_ms_begin(TravCtl *c, unsigned long long E, float alpha) {
         c->done = 1;
         return;
     }
-    c->mode = ((double)c->m_f * alpha > (double)E) ? 1u : 0u;
+    // after a sparse level the frontier array is valid only at queued
+    // vertices, which a push reads and a pull would not: push
+    c->mode = (c->ms_cur_dense && (double)c->m_f * alpha > (double)E) ? 1u : 0u;
+    // a push on a shrinking frontier lists the vertices it touches, so that a
+    // small level can be applied sparsely
+    c->ms_track = c->mode == 0 && c->ms_new_prev < c->ms_new_prev2;
+    c->ms_touched = 0;
     c->qsize[c->cur ^ 1] = 0;
     c->npieces = 0;
     c->m_next = 0;
     c->reached_pull = 0;
+}
+
+// A tracked push level that touched at most V/64 vertices is applied
+// sparsely: only its touched vertices are visited, their new bits become the
+// next frontier at those vertices only, and their levels are written
+// straight into the output (no store slot for this or any later level).
+__device__ __forceinline__ bool ms_sparse_level(const TravCtl *c, uint32_t V) {
+    return c->ms_track && c->ms_touched <= V / 64;
 }
 
 constexpr int kMsParents = 4;
@@ -217,7 +274,7 @@ __global__ void __launch_bounds__(kBlock)
 k_ms_apply(uint32_t V, TravCtl *c, const uint32_t *__restrict__ rowptr,
            unsigned long long *__restrict__ visit, MsCur cm,
            unsigned long long *__restrict__ next, uint32_t *q0, uint32_t *q1) {
-    if (c->done) return;
+    if (c->done || ms_sparse_level(c, V)) return;
     int32_t *levels = static_cast<int32_t *>(c->vdata);
     // vertices with new bits form the next level's queue (per-warp staging)
     uint32_t *q = c->cur ? q0 : q1;
@@ -234,7 +291,7 @@ k_ms_apply(uint32_t V, TravCtl *c, const uint32_t *__restrict__ rowptr,
     // the next level's cur: slot lv of the mask store, or a spare array (and
     // direct writes of the level into the output) past the store
     unsigned long long *__restrict__ ncur = cm.at((uint32_t)lv);
-    const bool past = (uint32_t)lv >= kMsSlots;
+    const bool past = (uint32_t)lv >= kMsSlots || (uint32_t)lv >= c->ms_sparse_from;
     unsigned long long m_next = 0, traversed = 0, nact = 0;
     // kApply vertices per thread, strided by the grid so each load stays coalesced;
     // all their next/cur loads are issued before any is used
@@ -283,9 +340,77 @@ k_ms_apply(uint32_t V, TravCtl *c, const uint32_t *__restrict__ rowptr,
     warp_add64(nact, &c->reached_pull);
 }
 
+// Sparse apply of a small push level: one thread per touched vertex (the
+// vertices whose next mask the push made nonzero).  New bits join visit,
+// become the next frontier at that vertex, and their level is written into
+// each source's row directly; the vertex joins the next queue.
+__global__ void __launch_bounds__(kBlock)
+k_ms_apply_sparse(uint32_t V, TravCtl *c, const uint32_t *__restrict__ rowptr,
+                  unsigned long long *__restrict__ visit, MsCur cm,
+                  unsigned long long *__restrict__ next, uint32_t *q0, uint32_t *q1,
+                  const uint32_t *__restrict__ touched) {
+    if (c->done || !ms_sparse_level(c, V)) return;
+    int32_t *levels = static_cast<int32_t *>(c->vdata);
+    uint32_t *q = c->cur ? q0 : q1;
+    uint32_t *qsize = &c->qsize[c->cur ^ 1];
+    __shared__ uint32_t s_q[kBlock / 32][kWarpStage];
+    __shared__ uint32_t s_n[kBlock / 32], s_lim[kBlock / 32];
+    const uint32_t wl = threadIdx.x >> 5;
+    if (lane_id() == 0) {
+        s_n[wl] = 0;
+        s_lim[wl] = kWarpStage;
+    }
+    __syncwarp();
+    const int32_t lv = (int32_t)c->level + 1;
+    unsigned long long *__restrict__ ncur = cm.at((uint32_t)lv);
+    const uint32_t nt = c->ms_touched;
+    unsigned long long m_next = 0, traversed = 0, nact = 0;
+    const uint32_t stride = gridDim.x * kBlock;
+    for (uint32_t base = blockIdx.x * kBlock; base < nt; base += stride) {   // warp-uniform
+        const uint32_t i = base + threadIdx.x;
+        bool act = false;
+        uint32_t v = 0;
+        if (i < nt) {
+            v = touched[i];
+            const unsigned long long nx = next[v];
+            next[v] = 0;
+            const unsigned long long vis = visit[v];
+            const unsigned long long nw = nx & ~vis;
+            if (nw) {
+                visit[v] = vis | nw;
+                ncur[v] = nw;
+                const uint32_t d = __ldg(&rowptr[v + 1]) - __ldg(&rowptr[v]);
+                m_next += d;
+                traversed += (unsigned long long)d * __popcll(nw);
+                act = true;
+                for (unsigned long long b = nw; b; b &= b - 1)
+                    levels[(uint64_t)(__ffsll((long long)b) - 1) * V + v] = lv;
+            }
+        }
+        nact += act;
+        int pa[1] = {act};
+        uint32_t pv[1] = {v};
+        __syncwarp();
+        if (s_n[wl] + 32 > kWarpStage) warp_stage_flush(s_q[wl], &s_n[wl], &s_lim[wl], q, qsize);
+        stage_push_n<1>(pa, pv, 1, s_q[wl], &s_n[wl], &s_lim[wl], kWarpStage, q, qsize);
+    }
+    warp_stage_flush(s_q[wl], &s_n[wl], &s_lim[wl], q, qsize);
+    warp_add64(m_next, &c->m_next);
+    warp_add64(traversed, &c->edges_traversed);
+    warp_add64(nact, &c->reached_pull);
+}
+
 __global__ void k_ms_end(TravCtl *c, cudaGraphConditionalHandle h, int use_cond, uint32_t V) {
     if (!c->done) {
         if (c->mode) c->pull_steps++;
+        if (ms_sparse_level(c, V)) {
+            c->ms_cur_dense = 0;
+            if (c->ms_sparse_from == 0xffffffffu) c->ms_sparse_from = c->level + 1;
+        } else {
+            c->ms_cur_dense = 1;
+        }
+        c->ms_new_prev2 = c->ms_new_prev;
+        c->ms_new_prev = c->reached_pull;
         c->m_f = c->m_next;
         c->cur ^= 1;
         c->level++;
@@ -348,7 +473,8 @@ k_ms_levels(uint32_t V, int n, unsigned long long srcmask, TravCtl *c,
     int32_t *levels = static_cast<int32_t *>(c->vdata);
     // slots 0 .. level-1: the run ended because level `level` found no new
     // vertex, so its slot is all zeros and is not read
-    const uint32_t nst = c->level < kMsSlots ? c->level : kMsSlots;
+    uint32_t nst = c->level < kMsSlots ? c->level : kMsSlots;
+    if (nst > c->ms_sparse_from) nst = c->ms_sparse_from;   // later levels were written directly
     unsigned long long reached = 0;
     for (uint64_t v = blockIdx.x * (uint64_t)kBlock + threadIdx.x; v < V;
          v += (uint64_t)gridDim.x * kBlock) {
@@ -433,7 +559,8 @@ k_ms_levels4(uint32_t V, int n, unsigned long long srcmask, TravCtl *c,
     int32_t *levels = static_cast<int32_t *>(c->vdata);
     // slots 0 .. level-1: the run ended because level `level` found no new
     // vertex, so its slot is all zeros and is not read
-    const uint32_t nst = c->level < kMsSlots ? c->level : kMsSlots;
+    uint32_t nst = c->level < kMsSlots ? c->level : kMsSlots;
+    if (nst > c->ms_sparse_from) nst = c->ms_sparse_from;   // later levels were written directly
     unsigned long long reached = 0;
     const uint64_t nq = V / 4;
     for (uint64_t t = blockIdx.x * (uint64_t)kBlock + threadIdx.x; t < nq;
@@ -521,6 +648,9 @@ static int ms_superstep(olv_graph *g, MsState &ms, Sink &&sink, cudaGraphConditi
     MsPushOp op;
     op.cm = cm;
     op.cur = nullptr;
+    op.touched = ms.touched.as<uint32_t>();
+    op.ntouched = nullptr;
+    op.track = 0;
     op.visit = visit;
     op.next = next;
     const uint32_t *colptr = g->colptr.as<uint32_t>();
@@ -549,6 +679,9 @@ static int ms_superstep(olv_graph *g, MsState &ms, Sink &&sink, cudaGraphConditi
     OLV_TRY(sink((const void *)k_ms_pull, dim3(nb_pull), dim3(kBlock), a_pull));
     void *a_apply[] = {&V, &ctl, &rowptr, &visit, &cm, &next, &q0, &q1};
     OLV_TRY(sink((const void *)k_ms_apply, dim3(nb_apply), dim3(kBlock), a_apply));
+    const uint32_t *touched = ms.touched.as<uint32_t>();
+    void *a_sparse[] = {&V, &ctl, &rowptr, &visit, &cm, &next, &q0, &q1, &touched};
+    OLV_TRY(sink((const void *)k_ms_apply_sparse, dim3(g->num_sms * 2), dim3(kBlock), a_sparse));
     void *a_end[] = {&ctl, &h, &use_cond, &V};
     OLV_TRY(sink((const void *)k_ms_end, dim3(1), dim3(1), a_end));
     return OLV_OK;
@@ -610,6 +743,7 @@ extern "C" int olv_msbfs(olv_graph *g, const uint32_t *srcs, int n, int32_t *lev
     const size_t V = g->V;
     OLV_TRY(ms.masks.ensure(V * 32 + 64));
     OLV_TRY(ms.store.ensure((size_t)kMsSlots * V * 8 + 64));
+    OLV_TRY(ms.touched.ensure(V * 4 + 64));
     OLV_TRY(ms.srcs.ensure(64 * 4));
     const bool dev_out = is_device_ptr(levels_out);
     const size_t out_bytes = (size_t)n * V * 4;

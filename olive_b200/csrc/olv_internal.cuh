@@ -71,6 +71,11 @@ struct TravCtl {
     uint32_t queue_stale;       // BFS: the frontier is only in the bitmap (after a pull level)
     uint32_t heavy_done;        // SSSP: heavy edges of the current bucket relaxed
     uint32_t bucket_lo;         // SSSP: lower distance edge of the current bucket
+    uint32_t ms_track;          // msBFS: this push level records first-touched vertices
+    uint32_t ms_touched;        // msBFS: vertices first touched by this level's push
+    uint32_t ms_sparse_from;    // msBFS: first level applied sparsely (no store slot)
+    uint32_t ms_cur_dense;      // msBFS: the frontier array is valid at every vertex
+    unsigned long long ms_new_prev, ms_new_prev2;   // msBFS: vertices found one / two levels ago
     void *vdata;                // per-vertex result array of the run (level / dist)
     unsigned long long m_f;         // out-edges of the input frontier
     unsigned long long m_next;      // out-edges of vertices discovered this superstep
