@@ -149,9 +149,11 @@ __device__ __forceinline__ void write_levels_warp(int32_t *levels, uint64_t V, u
     }
 }
 
+__device__ void ms_begin(TravCtl *c, unsigned long long E, float alpha);
+
 __global__ void k_ms_init(TravCtl *c, int32_t *levels, const uint32_t *srcs, int n, uint32_t V,
                           const uint32_t *rowptr, unsigned long long *visit, uint32_t *q0,
-                          unsigned long long *store0) {
+                          unsigned long long *store0, unsigned long long E, float alpha) {
     __shared__ unsigned long long s_edges;
     if (threadIdx.x == 0) {
         TravCtl t = {};
@@ -178,10 +180,14 @@ __global__ void k_ms_init(TravCtl *c, int32_t *levels, const uint32_t *srcs, int
         }
     }
     __syncthreads();
-    if (threadIdx.x == 0) c->edges_traversed = s_edges;
+    if (threadIdx.x == 0) {
+        c->edges_traversed = s_edges;
+        ms_begin(c, E, alpha);   // the first superstep's mode
+    }
 }
 
-__global__ void k_ms_begin(TravCtl *c, unsigned long long E, float alpha) {
+// Mode and counters of the next superstep (called by k_ms_init and k_ms_end).
+__device__ void ms_begin(TravCtl *c, unsigned long long E, float alpha) {
     if (c->done) return;
     if (c->qsize[c->cur] == 0) {
         c->done = 1;
@@ -273,8 +279,9 @@ k_ms_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowi
 __global__ void __launch_bounds__(kBlock)
 k_ms_apply(uint32_t V, TravCtl *c, const uint32_t *__restrict__ rowptr,
            unsigned long long *__restrict__ visit, MsCur cm,
-           unsigned long long *__restrict__ next, uint32_t *q0, uint32_t *q1) {
-    if (c->done || ms_sparse_level(c, V)) return;
+           unsigned long long *__restrict__ next, uint32_t *q0, uint32_t *q1,
+           const uint32_t *__restrict__ touched) {
+    if (c->done) return;
     int32_t *levels = static_cast<int32_t *>(c->vdata);
     // vertices with new bits form the next level's queue (per-warp staging)
     uint32_t *q = c->cur ? q0 : q1;
@@ -293,8 +300,49 @@ k_ms_apply(uint32_t V, TravCtl *c, const uint32_t *__restrict__ rowptr,
     unsigned long long *__restrict__ ncur = cm.at((uint32_t)lv);
     const bool past = (uint32_t)lv >= kMsSlots || (uint32_t)lv >= c->ms_sparse_from;
     unsigned long long m_next = 0, traversed = 0, nact = 0;
-    // kApply vertices per thread, strided by the grid so each load stays coalesced;
-    // all their next/cur loads are issued before any is used
+    if (ms_sparse_level(c, V)) {
+        // sparse: one thread per touched vertex (the vertices whose next mask
+        // the push made nonzero); new bits join visit, become the next
+        // frontier at that vertex, and their level goes straight into each
+        // source's row
+        const uint32_t nt = c->ms_touched;
+        const uint32_t sstride = gridDim.x * kBlock;
+        for (uint32_t b = blockIdx.x * kBlock; b < nt; b += sstride) {   // warp-uniform
+            const uint32_t i = b + threadIdx.x;
+            bool act = false;
+            uint32_t v = 0;
+            if (i < nt) {
+                v = touched[i];
+                const unsigned long long nx = next[v];
+                next[v] = 0;
+                const unsigned long long vis = visit[v];
+                const unsigned long long nw = nx & ~vis;
+                if (nw) {
+                    visit[v] = vis | nw;
+                    ncur[v] = nw;
+                    const uint32_t d = __ldg(&rowptr[v + 1]) - __ldg(&rowptr[v]);
+                    m_next += d;
+                    traversed += (unsigned long long)d * __popcll(nw);
+                    act = true;
+                    for (unsigned long long bb = nw; bb; bb &= bb - 1)
+                        levels[(uint64_t)(__ffsll((long long)bb) - 1) * V + v] = lv;
+                }
+            }
+            nact += act;
+            int pa[1] = {act};
+            uint32_t pv[1] = {v};
+            __syncwarp();
+            if (s_n[wl] + 32 > kWarpStage) warp_stage_flush(s_q[wl], &s_n[wl], &s_lim[wl], q, qsize);
+            stage_push_n<1>(pa, pv, 1, s_q[wl], &s_n[wl], &s_lim[wl], kWarpStage, q, qsize);
+        }
+        warp_stage_flush(s_q[wl], &s_n[wl], &s_lim[wl], q, qsize);
+        warp_add64(m_next, &c->m_next);
+        warp_add64(traversed, &c->edges_traversed);
+        warp_add64(nact, &c->reached_pull);
+        return;
+    }
+    // dense: kApply vertices per thread, strided by the grid so each load stays
+    // coalesced; all their next loads are issued before any is used
     constexpr int kApply = 4;
     const uint64_t stride = (uint64_t)gridDim.x * kBlock;
     for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < V; base += stride * kApply) {
@@ -340,67 +388,8 @@ k_ms_apply(uint32_t V, TravCtl *c, const uint32_t *__restrict__ rowptr,
     warp_add64(nact, &c->reached_pull);
 }
 
-// Sparse apply of a small push level: one thread per touched vertex (the
-// vertices whose next mask the push made nonzero).  New bits join visit,
-// become the next frontier at that vertex, and their level is written into
-// each source's row directly; the vertex joins the next queue.
-__global__ void __launch_bounds__(kBlock)
-k_ms_apply_sparse(uint32_t V, TravCtl *c, const uint32_t *__restrict__ rowptr,
-                  unsigned long long *__restrict__ visit, MsCur cm,
-                  unsigned long long *__restrict__ next, uint32_t *q0, uint32_t *q1,
-                  const uint32_t *__restrict__ touched) {
-    if (c->done || !ms_sparse_level(c, V)) return;
-    int32_t *levels = static_cast<int32_t *>(c->vdata);
-    uint32_t *q = c->cur ? q0 : q1;
-    uint32_t *qsize = &c->qsize[c->cur ^ 1];
-    __shared__ uint32_t s_q[kBlock / 32][kWarpStage];
-    __shared__ uint32_t s_n[kBlock / 32], s_lim[kBlock / 32];
-    const uint32_t wl = threadIdx.x >> 5;
-    if (lane_id() == 0) {
-        s_n[wl] = 0;
-        s_lim[wl] = kWarpStage;
-    }
-    __syncwarp();
-    const int32_t lv = (int32_t)c->level + 1;
-    unsigned long long *__restrict__ ncur = cm.at((uint32_t)lv);
-    const uint32_t nt = c->ms_touched;
-    unsigned long long m_next = 0, traversed = 0, nact = 0;
-    const uint32_t stride = gridDim.x * kBlock;
-    for (uint32_t base = blockIdx.x * kBlock; base < nt; base += stride) {   // warp-uniform
-        const uint32_t i = base + threadIdx.x;
-        bool act = false;
-        uint32_t v = 0;
-        if (i < nt) {
-            v = touched[i];
-            const unsigned long long nx = next[v];
-            next[v] = 0;
-            const unsigned long long vis = visit[v];
-            const unsigned long long nw = nx & ~vis;
-            if (nw) {
-                visit[v] = vis | nw;
-                ncur[v] = nw;
-                const uint32_t d = __ldg(&rowptr[v + 1]) - __ldg(&rowptr[v]);
-                m_next += d;
-                traversed += (unsigned long long)d * __popcll(nw);
-                act = true;
-                for (unsigned long long b = nw; b; b &= b - 1)
-                    levels[(uint64_t)(__ffsll((long long)b) - 1) * V + v] = lv;
-            }
-        }
-        nact += act;
-        int pa[1] = {act};
-        uint32_t pv[1] = {v};
-        __syncwarp();
-        if (s_n[wl] + 32 > kWarpStage) warp_stage_flush(s_q[wl], &s_n[wl], &s_lim[wl], q, qsize);
-        stage_push_n<1>(pa, pv, 1, s_q[wl], &s_n[wl], &s_lim[wl], kWarpStage, q, qsize);
-    }
-    warp_stage_flush(s_q[wl], &s_n[wl], &s_lim[wl], q, qsize);
-    warp_add64(m_next, &c->m_next);
-    warp_add64(traversed, &c->edges_traversed);
-    warp_add64(nact, &c->reached_pull);
-}
-
-__global__ void k_ms_end(TravCtl *c, cudaGraphConditionalHandle h, int use_cond, uint32_t V) {
+__global__ void k_ms_end(TravCtl *c, cudaGraphConditionalHandle h, int use_cond, uint32_t V,
+                         unsigned long long E, float alpha) {
     if (!c->done) {
         if (c->mode) c->pull_steps++;
         if (ms_sparse_level(c, V)) {
@@ -420,6 +409,7 @@ __global__ void k_ms_end(TravCtl *c, cudaGraphConditionalHandle h, int use_cond,
             c->err = 1;
             c->done = 1;
         }
+        ms_begin(c, E, alpha);   // the next superstep's mode and counters
     }
     if (use_cond) cudaGraphSetConditional(h, c->done ? 0u : 1u);
 }
@@ -663,8 +653,6 @@ static int ms_superstep(olv_graph *g, MsState &ms, Sink &&sink, cudaGraphConditi
     uint32_t *q0 = a.q0, *q1 = a.q1;
     int nb = 0;
     OLV_TRY(resident_blocks(g, (const void *)k_advance_chunks<MsPushOp>, &nb));
-    void *a_begin[] = {&ctl, &E, &alpha};
-    OLV_TRY(sink((const void *)k_ms_begin, dim3(1), dim3(1), a_begin));
     void *a_adv[] = {&a, &op};
     OLV_TRY(sink((const void *)k_advance_chunks<MsPushOp>, dim3(nb), dim3(kBlock), a_adv));
     OLV_TRY(sink((const void *)k_advance_pieces<MsPushOp>, dim3(nb), dim3(kBlock), a_adv));
@@ -677,12 +665,10 @@ static int ms_superstep(olv_graph *g, MsState &ms, Sink &&sink, cudaGraphConditi
     OLV_TRY(resident_blocks(g, (const void *)k_ms_pull, &nb_pull));
     OLV_TRY(resident_blocks(g, (const void *)k_ms_apply, &nb_apply));
     OLV_TRY(sink((const void *)k_ms_pull, dim3(nb_pull), dim3(kBlock), a_pull));
-    void *a_apply[] = {&V, &ctl, &rowptr, &visit, &cm, &next, &q0, &q1};
-    OLV_TRY(sink((const void *)k_ms_apply, dim3(nb_apply), dim3(kBlock), a_apply));
     const uint32_t *touched = ms.touched.as<uint32_t>();
-    void *a_sparse[] = {&V, &ctl, &rowptr, &visit, &cm, &next, &q0, &q1, &touched};
-    OLV_TRY(sink((const void *)k_ms_apply_sparse, dim3(g->num_sms * 2), dim3(kBlock), a_sparse));
-    void *a_end[] = {&ctl, &h, &use_cond, &V};
+    void *a_apply[] = {&V, &ctl, &rowptr, &visit, &cm, &next, &q0, &q1, &touched};
+    OLV_TRY(sink((const void *)k_ms_apply, dim3(nb_apply), dim3(kBlock), a_apply));
+    void *a_end[] = {&ctl, &h, &use_cond, &V, &E, &alpha};
     OLV_TRY(sink((const void *)k_ms_end, dim3(1), dim3(1), a_end));
     return OLV_OK;
 }
@@ -761,7 +747,8 @@ extern "C" int olv_msbfs(olv_graph *g, const uint32_t *srcs, int n, int32_t *lev
     OLV_CUDA(cudaMemsetAsync(ms.store.p, 0, V * 8, s));   // slot 0: the sources
     k_ms_init<<<1, 64, 0, s>>>(ctl, levels, ms.srcs.as<uint32_t>(), n, g->V,
                                g->rowptr.as<uint32_t>(), visit, g->ws.q0.as<uint32_t>(),
-                               ms.store.as<unsigned long long>());
+                               ms.store.as<unsigned long long>(), (unsigned long long)g->E,
+                               g->tune.ms_alpha);
     OLV_CUDA(cudaGetLastError());
     bool launched = false;
     if (g->tune.use_graphs) {
