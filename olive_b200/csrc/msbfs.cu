@@ -78,6 +78,7 @@ struct MsPushOp {
     uint32_t *touched;          // first-touched vertices of a tracked level
     uint32_t *ntouched;
     uint32_t track;
+    uint32_t filter;            // drop source bits the target already has
     struct Pre {
         unsigned long long bits;
     };
@@ -85,11 +86,14 @@ struct MsPushOp {
         cur = cm.at(c->level);
         track = c->ms_track;
         ntouched = &c->ms_touched;
+        // in the first two levels almost no target has been visited yet:
+        // skip the visit gather per edge and let apply drop known bits
+        filter = c->level >= 2;
     }
     __device__ __forceinline__ SV src_value(uint32_t u) const { return cur[u]; }
     __device__ __forceinline__ void on_input(uint32_t) const {}
     __device__ __forceinline__ Pre prepare(SV sv, uint32_t, uint32_t v) const {
-        return Pre{sv & ~__ldg(&visit[v])};
+        return Pre{filter ? sv & ~__ldg(&visit[v]) : sv};
     }
     // OR the source bits into next[v]; on a tracked level, also list every v
     // whose next mask was zero before (once per vertex and level), with one
@@ -641,6 +645,7 @@ static int ms_superstep(olv_graph *g, MsState &ms, Sink &&sink, cudaGraphConditi
     op.touched = ms.touched.as<uint32_t>();
     op.ntouched = nullptr;
     op.track = 0;
+    op.filter = 1;
     op.visit = visit;
     op.next = next;
     const uint32_t *colptr = g->colptr.as<uint32_t>();
