@@ -7,19 +7,24 @@
 // holds it this level), next (sources reaching it next level).  A level is
 //   push  (few active vertices): for each active u and out-edge u->v,
 //         atomicOr(next[v], cur[u] & ~visit[v])   -- the shared chunk/piece
-//         advance of olv_advance.cuh with a 64-bit source value;
+//         advance of olv_advance.cuh with a 64-bit source value (in the first
+//         two levels without the visit gather: apply drops known bits);
 //   pull  (large frontier): each vertex with unvisited bits ORs cur[] over its
 //         in-edges, stopping once every missing source is found;
-//   apply (dense pass): new = next & ~visit; visit |= new; the new-bit mask
-//         of level L+1 is written to slot L+1 of a per-level mask store, and
+//   apply, dense: new = next & ~visit; visit |= new; the new-bit mask of
+//         level L+1 is written to slot L+1 of a per-level mask store, and
 //         that slot is the next level's cur (no separate cur array is read or
 //         cleared); levels past the store use two spare cur arrays and write
 //         their pairs straight into the output; vertices with new bits form
-//         the next active queue.
+//         the next active queue;
+//   apply, sparse (a small push level on a shrinking frontier): the push
+//         lists the vertices it touches and only they are visited; their
+//         levels go straight into the output and every later level is
+//         written the same way (the store is not read past that level).
 // A final pass turns the stored masks into the [n][V] int32 output, one
-// vertex per lane, so each source's row goes out as full 128-byte lines and
-// every output element is written once.  Levels run in a CUDA
-// graph as for BFS.
+// thread per four vertices, so each source's row goes out in 16-byte stores
+// and every output element is written once.  Levels run in a CUDA graph as
+// for BFS.
 #include <string.h>
 
 #include <vector>
