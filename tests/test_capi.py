@@ -67,3 +67,13 @@ def test_argument_errors_need_no_gpu():
     assert rc == -1
     rc = L.olv_graph_create_rmat(0, 16, 1, 0, 0, ctypes.byref(out))
     assert rc == -1
+
+
+def test_no_unresolved_library_symbols():
+    """Every symbol the library's own translation units reference is defined
+    in it (a kernel declared in one .cu file and defined with another
+    signature elsewhere would only fail when first called)."""
+    nm = subprocess.run(["nm", "-D", "-C", "--undefined-only", ob.LIB_PATH], capture_output=True,
+                        text=True, check=True).stdout
+    own = [ln for ln in nm.splitlines() if "olv::" in ln or " olv_" in ln]
+    assert not own, own
