@@ -208,6 +208,11 @@ __device__ __forceinline__ void ppr_sweep_warp(const BatchArgs &a, const PprView
     }
 }
 
+#ifndef OLV_QROUND
+#define OLV_QROUND 4
+#endif
+constexpr int kQRound = OLV_QROUND;   // in-edges per vertex gathered per round
+
 // K = 32 sweep with four vertices per warp: slot s = lane >> 3 (8 lanes)
 // takes vertex 4g + s of vertex group g (g = w0, w0 + nw, ...), lane quad q =
 // lane & 7 holds vectors 4q .. 4q+3 of it as one float4.  A round gathers
@@ -266,11 +271,11 @@ __device__ __forceinline__ void ppr_sweep_warp_q(const BatchArgs &a, const PprVi
                 }
             }
             const uint32_t cend = min(8u, maxdeg - c0);
-            for (uint32_t t = 0; t < cend; t += 2) {
-                float4 x[2];
-                float wj[2];
+            for (uint32_t t = 0; t < cend; t += kQRound) {
+                float4 x[kQRound];
+                float wj[kQRound];
 #pragma unroll
-                for (int r = 0; r < 2; r++) {
+                for (int r = 0; r < kQRound; r++) {
                     const uint32_t i = t + r;
                     const uint32_t uj = __shfl_sync(kFull, u, slot * 8 + (i & 7));
                     wj[r] = __shfl_sync(kFull, w, slot * 8 + (i & 7));
@@ -278,7 +283,7 @@ __device__ __forceinline__ void ppr_sweep_warp_q(const BatchArgs &a, const PprVi
                                         : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 }
 #pragma unroll
-                for (int r = 0; r < 2; r++) {
+                for (int r = 0; r < kQRound; r++) {
                     if (c0 + t + r < deg) {
                         acc.x = fmaf(x[r].x, wj[r], acc.x);
                         acc.y = fmaf(x[r].y, wj[r], acc.y);
