@@ -224,6 +224,10 @@ __device__ __forceinline__ bool ms_sparse_level(const TravCtl *c, uint32_t V) {
 }
 
 constexpr int kMsParents = 4;
+#ifndef OLV_MS_BLOCKS
+#define OLV_MS_BLOCKS 2
+#endif
+constexpr int kMsBlocks = OLV_MS_BLOCKS;   // 16-byte in-edge blocks per light-vertex round
 
 // Pull.  Heavy vertices' in-edges come as pieces of kMsPiece edges, one warp
 // per piece, ORed into next[v] with atomicOr (OR is order-free).  Light
@@ -268,16 +272,23 @@ k_ms_pull(const uint32_t *__restrict__ colptr, const uint32_t *__restrict__ rowi
         const unsigned long long todo = ~visit[v] & srcmask;
         if (!todo) continue;
         // in-edges read as aligned 16-byte blocks (the index array is padded
-        // to a multiple of 4 entries), two blocks per round; entries outside
-        // [b, e) are skipped
+        // to a multiple of 4 entries), kMsBlocks blocks per round; entries
+        // outside [b, e) are skipped
         unsigned long long acc = 0;
-        for (uint32_t blk = b & ~3u; blk < e; blk += 8) {
-            const uint4 x0 = __ldg(reinterpret_cast<const uint4 *>(rowidx + blk));
-            const uint4 x1 = blk + 4 < e ? __ldg(reinterpret_cast<const uint4 *>(rowidx + blk + 4))
-                                         : make_uint4(0, 0, 0, 0);
-            const uint32_t u[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
+        for (uint32_t blk = b & ~3u; blk < e; blk += 4 * kMsBlocks) {
+            uint32_t u[4 * kMsBlocks];
 #pragma unroll
-            for (int j = 0; j < 8; j++)
+            for (int k = 0; k < kMsBlocks; k++) {
+                const uint4 x = (k == 0 || blk + 4 * k < e)
+                                    ? __ldg(reinterpret_cast<const uint4 *>(rowidx + blk + 4 * k))
+                                    : make_uint4(0, 0, 0, 0);
+                u[4 * k] = x.x;
+                u[4 * k + 1] = x.y;
+                u[4 * k + 2] = x.z;
+                u[4 * k + 3] = x.w;
+            }
+#pragma unroll
+            for (int j = 0; j < 4 * kMsBlocks; j++)
                 if (blk + j >= b && blk + j < e) acc |= __ldg(&cur[u[j]]);
             if ((acc & todo) == todo) break;
         }
