@@ -103,6 +103,9 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
  *   "alpha"       BFS push->pull when m_f * alpha > m_unvisited     (14)
  *   "beta"        BFS pull->push when n_f * beta < V                (24)
  *   "sssp_delta"  SSSP bucket width, 0 = default                    (0)
+ *   "sssp_pull"   SSSP: a settled bucket's heavy edges may be relaxed by
+ *                 a pull over the in-edges of the unsettled vertices when
+ *                 that reads fewer edges (1) or always by push (0)       (1)
  *   "ms_alpha"    msBFS pull when active out-edges * ms_alpha > E   (20)
  *   "use_graphs"  run supersteps inside CUDA graphs (1) or a host loop (0)
  *   "levels_per_sync" host loop: supersteps enqueued per check      (4)

@@ -509,6 +509,8 @@ int olv_tune_set(olv_graph *g, const char *key, double value) {
     } else if (!strcmp(key, "sssp_delta")) {
         OLV_CHECK_ARG(value >= 0 && value < 2147483647.0, "olv_tune_set: bad sssp_delta");
         t.sssp_delta = (uint32_t)value;
+    } else if (!strcmp(key, "sssp_pull")) {
+        t.sssp_pull = value != 0;
     } else if (!strcmp(key, "ms_alpha")) {
         OLV_CHECK_ARG(value > 0, "olv_tune_set: ms_alpha must be > 0");
         t.ms_alpha = (float)value;
@@ -540,6 +542,7 @@ int olv_tune_get(const olv_graph *g, const char *key, double *value) {
     else if (!strcmp(key, "alpha")) *value = t.alpha;
     else if (!strcmp(key, "beta")) *value = t.beta;
     else if (!strcmp(key, "sssp_delta")) *value = t.sssp_delta;
+    else if (!strcmp(key, "sssp_pull")) *value = t.sssp_pull;
     else if (!strcmp(key, "ms_alpha")) *value = t.ms_alpha;
     else if (!strcmp(key, "use_graphs")) *value = t.use_graphs;
     else if (!strcmp(key, "batch_cluster")) *value = t.batch_cluster;

@@ -71,6 +71,12 @@ struct TravCtl {
     uint32_t queue_stale;       // BFS: the frontier is only in the bitmap (after a pull level)
     uint32_t heavy_done;        // SSSP: heavy edges of the current bucket relaxed
     uint32_t bucket_lo;         // SSSP: lower distance edge of the current bucket
+    uint32_t pull_pending;      // SSSP: the settled bucket's heavy edges go by a pull pass
+    uint32_t aux_done;          // SSSP: CTAs of the collect pass that finished
+    uint32_t bl_size;           // SSSP: entries in the bucket list
+    uint32_t bl_over;           // SSSP: the bucket list overflowed (collect densely)
+    unsigned long long heavy_work;  // SSSP: heavy out-edges of the collected bucket
+    unsigned long long settled_in;  // SSSP: in-edges of all settled vertices
     uint32_t ms_track;          // msBFS: this push level records first-touched vertices
     uint32_t ms_touched;        // msBFS: vertices first touched by this level's push
     uint32_t ms_sparse_from;    // msBFS: first level applied sparsely (no store slot)
@@ -93,6 +99,7 @@ struct Tuning {
     float alpha = 14.0f;          // push -> pull when m_f > m_unvisited / alpha
     float beta = 24.0f;           // pull -> push when n_f < V / beta
     uint32_t sssp_delta = 0;      // 0 = default bucket width (64)
+    int sssp_pull = 1;            // SSSP: a bucket's heavy edges may go by an in-edge pull
     float ms_alpha = 20.0f;       // msBFS: pull when active out-edges * ms_alpha > E
     int levels_per_sync = 4;      // host loop: supersteps enqueued per check
     int use_graphs = 1;           // run supersteps inside a CUDA graph
@@ -105,13 +112,15 @@ struct Workspace {
     DevBuf pull_first;              // BFS pull: each vertex's first in-edge in pull order
     DevBuf pull_idx;                // BFS pull: in-edges sorted by source out-degree (desc)
     DevBuf sssp_col, sssp_w, rowmid; // SSSP: rows split light (w <= delta) | heavy
+    DevBuf blist;                   // SSSP: inputs of the current bucket's relax supersteps
+    DevBuf hdin;                    // SSSP: per vertex (heavy out-degree, in-degree)
     uint32_t sssp_delta_built = 0;
     uint32_t n_heavy = 0, n_light = 0;
     void release() {
         level.release(); q0.release(); q1.release(); pieces.release(); ctl.release();
         fbits.release(); order.release(); cand.release(); cand2.release(); pull_idx.release();
         pull_first.release();
-        sssp_col.release(); sssp_w.release(); rowmid.release();
+        sssp_col.release(); sssp_w.release(); rowmid.release(); blist.release(); hdin.release();
         sssp_delta_built = 0;
         mark.release(); far0.release(); far1.release(); tmp.release(); partials.release();
     }

@@ -22,6 +22,23 @@
 //     vertices under it to the near queue.
 // Heavy edges are thus relaxed once per reached vertex; only light edges can
 // be relaxed again.  Supersteps run as one CUDA graph, as for BFS.
+//
+// Direction choice for the heavy step.  On scale-free graphs the first
+// bucket settles the well-connected core, and its heavy out-edges are most
+// of the graph's edges, while the vertices left unsettled are the periphery
+// with few in-edges (RMAT-22 from the hub: 47.2 M heavy out-edges against
+// 1.75 M in-edges of unsettled vertices).  The collect pass therefore also
+// sums the heavy out-degree of the bucket and, over all buckets so far, the
+// in-degree of the settled vertices; its last CTA picks a pull superstep
+// when E - settled in-edges + V/2 (a dense pass reads about a vertex per two
+// edges' worth of bytes) is below the heavy out-edge count.  The pull visits
+// every vertex at or above the threshold and takes the minimum of dist[u] + w
+// over its in-edges whose source is settled (dist[u] < threshold).  Every
+// light edge of a settled vertex and every edge of an earlier bucket was
+// relaxed already, so this minimum improves a vertex exactly where the push
+// over the bucket's heavy edges would, and by the same value; each vertex is
+// written by its own thread, and its new distance (at or above the
+// threshold) does not pass the `dist[u] < threshold` filter of any reader.
 #include "olv_advance.cuh"
 #include "olv_graphexec.cuh"
 #include "olv_internal.cuh"
@@ -34,7 +51,21 @@ __global__ void k_fill_i32(int32_t *__restrict__ a, uint32_t n, int32_t x);
 constexpr uint32_t kModeRelax = 0;
 constexpr uint32_t kModeSplit = 2;
 constexpr uint32_t kModeHeavy = 3;
+constexpr uint32_t kModePull = 4;
 constexpr uint32_t kDefaultDelta = 64;
+
+// Arrays the collect and pull passes read besides the queues.
+struct SsspAux {
+    const uint32_t *rowptr, *rowmid;   // CSR rows, light | heavy split
+    const uint32_t *colptr, *rowidx;   // CSC: in-edges and their sources
+    const uint32_t *cw;                // CSC weights
+    const uint2 *hdin;                 // per vertex: (heavy out-degree, in-degree)
+    uint32_t *blist;                   // bucket list: the bucket's relax inputs, in order
+    uint32_t *cmark;                   // bitmap: vertices collected so far this run
+    uint32_t bl_cap;                   // bucket list capacity (entries)
+    unsigned long long E;
+    int pull;                          // pull supersteps allowed
+};
 
 // Stable partition of every row into light (w <= delta) then heavy edges; one
 // warp per row, two passes (count, then write in order).
@@ -200,10 +231,12 @@ __device__ void sssp_begin(TravCtl *c) {
         return;
     }
     if (!c->heavy_done) {   // bucket settled: collect it and relax its heavy edges
-        c->mode = kModeHeavy;
+        c->mode = c->pull_pending ? kModePull : kModeHeavy;
         c->qsize[c->cur] = 0;
         c->qsize[c->cur ^ 1] = 0;
         c->npieces = 0;
+        c->heavy_work = 0;
+        c->aux_done = 0;
         return;
     }
     if (c->far_size[c->far_cur] == 0) {
@@ -246,41 +279,244 @@ struct WarpStage {
 };
 
 // Heavy superstep, step 1: the vertices of the settled bucket
-// [bucket_lo, threshold) become the input queue.  Four vertices per thread.
+// [bucket_lo, threshold) become the input queue.  Every such vertex was the
+// input of one of the bucket's relax supersteps (it entered the bucket from
+// the far pile through the split, or by a light relaxation), so when the
+// bucket list (those inputs, kept by the aux pass) is short, the collect
+// reads the list, dropping repeats with a bitmap of the vertices collected so
+// far in the run (a vertex is collected once: later buckets start above its
+// distance); otherwise it reads every vertex's distance, four per thread.
+// With pull supersteps allowed, the collected vertices' heavy out-degrees and
+// in-degrees are summed into heavy_work and settled_in for the direction
+// choice.
 __device__ void sssp_collect(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1,
-                             WarpStage st) {
+                             const SsspAux &x, WarpStage st) {
+    unsigned long long hw = 0, si = 0;
     const uint32_t *dist = static_cast<const uint32_t *>(c->vdata);
     const uint32_t lo = c->bucket_lo, hi = c->threshold;
     uint32_t *q = c->cur ? q1 : q0;
     uint32_t *qsize = &c->qsize[c->cur];
+    const uint32_t nl = c->bl_size;
+    const bool from_list = !c->bl_over && (uint64_t)nl * 8 < V;
+    const uint64_t nquad = from_list ? ((uint64_t)nl + 3) / 4 : ((uint64_t)V + 3) / 4;
     const bool vec = ((uintptr_t)dist & 15) == 0;
-    const uint64_t nquad = ((uint64_t)V + 3) / 4;
     for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < nquad;
          base += (uint64_t)gridDim.x * kBlock) {
-        const uint64_t v0 = (base + threadIdx.x) * 4;
-        uint32_t d[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu};
-        if (vec && v0 + 3 < V) {
-            const uint4 x = __ldcg(reinterpret_cast<const uint4 *>(dist + v0));
-            d[0] = x.x;
-            d[1] = x.y;
-            d[2] = x.z;
-            d[3] = x.w;
-        } else {
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-                if (v0 + j < V) d[j] = __ldcg(dist + v0 + j);
-        }
         int act[4];
         uint32_t vv[4];
+        uint32_t d[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu};
+        if (from_list) {   // entries base*4 + j*kBlock + t: coalesced per j
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            act[j] = d[j] >= lo && d[j] < hi;   // vertices >= V hold 0xffffffff
-            vv[j] = (uint32_t)(v0 + j);
+            for (int j = 0; j < 4; j++) {
+                const uint64_t i = base * 4 + (uint64_t)j * kBlock + threadIdx.x;
+                vv[j] = i < nl ? x.blist[i] : 0u;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const uint64_t i = base * 4 + (uint64_t)j * kBlock + threadIdx.x;
+                if (i < nl) d[j] = __ldcg(dist + vv[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                act[j] = d[j] >= lo && d[j] < hi;
+                if (act[j]) {
+                    const uint32_t bit = 1u << (vv[j] & 31);
+                    if (atomicOr(&x.cmark[vv[j] >> 5], bit) & bit) act[j] = 0;   // a repeat
+                }
+            }
+        } else {
+            const uint64_t v0 = (base + threadIdx.x) * 4;
+            if (vec && v0 + 3 < V) {
+                const uint4 d4 = __ldcg(reinterpret_cast<const uint4 *>(dist + v0));
+                d[0] = d4.x;
+                d[1] = d4.y;
+                d[2] = d4.z;
+                d[3] = d4.w;
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    if (v0 + j < V) d[j] = __ldcg(dist + v0 + j);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                act[j] = d[j] >= lo && d[j] < hi;   // vertices >= V hold 0xffffffff
+                vv[j] = (uint32_t)(v0 + j);
+            }
+        }
+        if (x.pull) {
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (act[j]) {
+                    const uint2 h = x.hdin[vv[j]];
+                    hw += h.x;
+                    si += h.y;
+                }
         }
         st.reserve(32 * 4, q, qsize);
         stage_push_n<4>(act, vv, 1, st.buf, st.n, st.lim, kWarpStage, q, qsize);
     }
     warp_stage_flush(st.buf, st.n, st.lim, q, qsize);
+    if (x.pull) {
+        warp_add64(hw, &c->heavy_work);
+        warp_add64(si, &c->settled_in);
+    }
+}
+
+// The collect pass's last CTA to finish chooses push or pull for the heavy
+// edges of the bucket (all CTAs' sums are in by then: each CTA fences its
+// atomics before counting itself done).  Pull empties the collected queue,
+// so the push kernels of this superstep find no work, and marks the pull
+// superstep to follow.
+__device__ void sssp_choose(uint32_t V, TravCtl *c, const SsspAux &x) {
+    __shared__ uint32_t s_last;
+    __threadfence();   // this thread's sums are visible before the CTA counts itself done
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(&c->aux_done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last || threadIdx.x != 0) return;
+    __threadfence();
+    const unsigned long long hw = atomicAdd(&c->heavy_work, 0ull);
+    const unsigned long long si = atomicAdd(&c->settled_in, 0ull);
+    const unsigned long long pull_edges = (x.E > si ? x.E - si : 0ull) + V / 2;
+    if (pull_edges < hw) {
+        c->pull_pending = 1;
+        c->qsize[c->cur] = 0;
+    }
+}
+
+// Relaxation candidate of in-edge i: dist[u] + w when u is settled
+// (dist[u] < hi), else no candidate.
+__device__ __forceinline__ uint32_t pull_cand(uint32_t du, uint32_t w, uint32_t hi) {
+    if (du >= hi) return 0xffffffffu;
+    uint32_t nd = du + w;
+    if (nd < du || nd > (uint32_t)kInf) nd = (uint32_t)kInf;   // saturate
+    return nd;
+}
+
+// Pull superstep: every vertex at or above the threshold takes the minimum
+// candidate over its in-edges; improved vertices go to the far pile (once
+// per pile generation).  Each CTA iteration covers 1024 vertices, four per
+// thread (16-byte distance and column-pointer loads); the chunk's in-degrees
+// are scanned across the CTA, its threads then take the chunk's in-edges in
+// order, kPullItems per thread in flight (owner vertex by binary search over
+// the scan), and fold candidates into a shared per-vertex minimum.
+constexpr int kPullItems = 4;
+constexpr uint32_t kPullChunk = 4 * kBlock;
+__device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1, FarMarks fm,
+                          const SsspAux &x, WarpStage sf) {
+    uint32_t *dist = static_cast<uint32_t *>(c->vdata);
+    const uint32_t hi = c->threshold;
+    uint32_t *far = c->far_cur ? far1 : far0;
+    uint32_t *far_size = &c->far_size[c->far_cur];
+    uint32_t *fbits = (c->epoch & 1) ? fm.m1 : fm.m0;
+    __shared__ uint32_t s_off[kPullChunk + 1], s_beg[kPullChunk], s_best[kPullChunk], s_warp[33];
+    const bool vec = ((uintptr_t)dist & 15) == 0 && ((uintptr_t)x.colptr & 15) == 0;
+    const uint32_t lane = lane_id();
+    uint32_t fmin = 0xffffffffu;
+    unsigned long long scanned = 0;
+    for (uint64_t base = (uint64_t)blockIdx.x * kPullChunk; base < V;
+         base += (uint64_t)gridDim.x * kPullChunk) {
+        const uint64_t v0 = base + 4 * (uint64_t)threadIdx.x;
+        uint32_t d[4] = {0u, 0u, 0u, 0u}, b[4] = {0u, 0u, 0u, 0u}, e[4] = {0u, 0u, 0u, 0u};
+        if (vec && v0 + 4 <= V) {
+            const uint4 d4 = __ldcg(reinterpret_cast<const uint4 *>(dist + v0));
+            d[0] = d4.x;
+            d[1] = d4.y;
+            d[2] = d4.z;
+            d[3] = d4.w;
+            if (d[0] >= hi || d[1] >= hi || d[2] >= hi || d[3] >= hi) {
+                const uint4 c4 = *reinterpret_cast<const uint4 *>(x.colptr + v0);
+                const uint32_t c5 = x.colptr[v0 + 4];
+                if (d[0] >= hi) { b[0] = c4.x; e[0] = c4.y; }
+                if (d[1] >= hi) { b[1] = c4.y; e[1] = c4.z; }
+                if (d[2] >= hi) { b[2] = c4.z; e[2] = c4.w; }
+                if (d[3] >= hi) { b[3] = c4.w; e[3] = c5; }
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (v0 + j < V) {
+                    d[j] = __ldcg(dist + v0 + j);
+                    if (d[j] >= hi) {
+                        b[j] = x.colptr[v0 + j];
+                        e[j] = x.colptr[v0 + j + 1];
+                    }
+                }
+        }
+        // vertices past V keep d = 0 < hi and no in-edges
+        const uint32_t t01 = (e[0] - b[0]) + (e[1] - b[1]);
+        const uint32_t t = t01 + (e[2] - b[2]) + (e[3] - b[3]);
+        uint32_t total;
+        const uint32_t off = block_exclusive_scan(t, &total, s_warp);
+        const uint32_t r0 = 4 * threadIdx.x;
+        s_off[r0] = off;
+        s_off[r0 + 1] = off + (e[0] - b[0]);
+        s_off[r0 + 2] = off + t01;
+        s_off[r0 + 3] = off + t01 + (e[2] - b[2]);
+        if (threadIdx.x == kBlock - 1) s_off[kPullChunk] = total;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            s_beg[r0 + j] = b[j];
+            s_best[r0 + j] = d[j];
+        }
+        __syncthreads();
+        for (uint32_t k0 = threadIdx.x; k0 < total; k0 += kBlock * kPullItems) {
+            uint32_t own[kPullItems], u[kPullItems], w[kPullItems], du[kPullItems];
+#pragma unroll
+            for (int j = 0; j < kPullItems; j++) {
+                const uint32_t k = k0 + j * kBlock;
+                own[j] = kPullChunk;
+                u[j] = 0;
+                w[j] = 0;
+                if (k < total) {
+                    uint32_t lo = 0;   // last vertex with s_off[vertex] <= k
+#pragma unroll
+                    for (uint32_t step = kPullChunk / 2; step > 0; step >>= 1)
+                        if (s_off[lo + step] <= k) lo += step;
+                    own[j] = lo;
+                    const uint32_t i = s_beg[lo] + (k - s_off[lo]);
+                    u[j] = x.rowidx[i];
+                    w[j] = x.cw[i];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kPullItems; j++)
+                du[j] = own[j] < kPullChunk ? __ldcg(&dist[u[j]]) : 0xffffffffu;
+#pragma unroll
+            for (int j = 0; j < kPullItems; j++) {
+                if (own[j] < kPullChunk) {
+                    const uint32_t nd = pull_cand(du[j], w[j], hi);
+                    if (nd < s_best[own[j]]) atomicMin(&s_best[own[j]], nd);
+                }
+            }
+        }
+        __syncthreads();
+        scanned += t;
+        int act[4];
+        uint32_t va[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const uint32_t best = s_best[r0 + j];
+            va[j] = (uint32_t)(v0 + j);
+            act[j] = 0;
+            if (best < d[j]) {   // only vertices at or above the threshold with in-edges
+                dist[va[j]] = best;
+                const uint32_t bit = 1u << (va[j] & 31);
+                if (!(atomicOr(&fbits[va[j] >> 5], bit) & bit)) act[j] = 2;
+                fmin = best < fmin ? best : fmin;
+            }
+        }
+        sf.reserve(32 * 4, far, far_size);
+        stage_push_n<4>(act, va, 2, sf.buf, sf.n, sf.lim, kWarpStage, far, far_size);
+        __syncthreads();   // s_off / s_beg / s_best are rewritten by the next chunk
+    }
+    warp_stage_flush(sf.buf, sf.n, sf.lim, far, far_size);
+    const uint32_t m = __reduce_min_sync(0xffffffffu, fmin);
+    if (lane == 0 && m != 0xffffffffu) atomicMin(&c->far_min, m);
+    warp_add64(scanned, &c->edges_relaxed);
 }
 
 // Split the far pile: stale entries (distance below the old threshold) are
@@ -332,14 +568,28 @@ __device__ void sssp_split(TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far
 }
 
 __global__ void k_sssp_end(TravCtl *c, cudaGraphConditionalHandle h, int use_cond,
-                           uint32_t max_steps) {
+                           uint32_t max_steps, uint32_t bl_cap) {
     if (!c->done) {
         if (c->mode == kModeRelax) {
+            // the aux pass appended this superstep's input to the bucket list
+            // under the same capacity test
+            const uint32_t n = c->qsize[c->cur];
+            if (!c->bl_over) {
+                if ((uint64_t)c->bl_size + n <= bl_cap)
+                    c->bl_size += n;
+                else
+                    c->bl_over = 1;
+            }
             c->cur ^= 1;
         } else if (c->mode == kModeHeavy) {
             c->qsize[c->cur] = 0;
+            c->heavy_done = c->pull_pending ? 0 : 1;   // pending: the pull superstep is next
+        } else if (c->mode == kModePull) {
+            c->pull_pending = 0;
             c->heavy_done = 1;
         } else {
+            c->bl_size = 0;   // a new bucket: its list starts empty
+            c->bl_over = 0;
             c->far_cur ^= 1;
             c->epoch++;
             c->heavy_done = 0;
@@ -355,14 +605,25 @@ __global__ void k_sssp_end(TravCtl *c, cudaGraphConditionalHandle h, int use_con
     if (use_cond) cudaGraphSetConditional(h, c->done ? 0u : 1u);
 }
 
-// The superstep's dense pass: collect the settled bucket (heavy mode) or split
-// the far pile (split mode); nothing in relax mode.
+// The superstep's dense pass: collect the settled bucket (heavy mode), pull
+// over the unsettled vertices' in-edges (pull mode) or split the far pile
+// (split mode); nothing in relax mode.
 __global__ void __launch_bounds__(kBlock)
 k_sssp_aux(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0, uint32_t *far1,
-           FarMarks fm) {
+           FarMarks fm, SsspAux x) {
     if (c->done) return;
     const uint32_t mode = c->mode;
-    if (mode != kModeHeavy && mode != kModeSplit) return;
+    if (mode == kModeRelax) {   // append this superstep's input to the bucket list
+        const uint32_t n = c->qsize[c->cur];
+        if (c->bl_over || (uint64_t)c->bl_size + n > x.bl_cap) return;   // k_sssp_end: overflow
+        const uint32_t *qin = c->cur ? q1 : q0;
+        uint32_t *dst = x.blist + c->bl_size;
+        for (uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x; i < n;
+             i += (uint64_t)gridDim.x * kBlock)
+            dst[i] = qin[i];
+        return;
+    }
+    if (mode != kModeHeavy && mode != kModeSplit && mode != kModePull) return;
     __shared__ uint32_t s_a[kBlock / 32][kWarpStage], s_b[kBlock / 32][kWarpStage];
     __shared__ uint32_t s_an[kBlock / 32], s_alim[kBlock / 32];
     __shared__ uint32_t s_bn[kBlock / 32], s_blim[kBlock / 32];
@@ -371,10 +632,14 @@ k_sssp_aux(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0, u
     WarpStage sb{s_b[wl], &s_bn[wl], &s_blim[wl]};
     sa.init();
     sb.init();
-    if (mode == kModeHeavy)
-        sssp_collect(V, c, q0, q1, sa);
-    else
+    if (mode == kModeHeavy) {
+        sssp_collect(V, c, q0, q1, x, sa);
+        if (x.pull) sssp_choose(V, c, x);
+    } else if (mode == kModePull) {
+        sssp_pull(V, c, far0, far1, fm, x, sb);
+    } else {
         sssp_split(c, q0, q1, far0, far1, fm, sa, sb);
+    }
 }
 
 // Sum of out-degrees and count of reached vertices (the GTEPS basis).
@@ -395,10 +660,23 @@ __global__ void k_reached_edges(const uint32_t *__restrict__ rowptr,
 // ------------------------------------------------------------------ host --
 // words of one dedupe bitmap (rounded up to 64 words = 256 bytes)
 static size_t mark_words(uint32_t V) { return (((size_t)V + 31) / 32 + 63) & ~(size_t)63; }
+// bitmaps: near marks x2, far-pile generation marks x2, collected vertices
+constexpr size_t kMarks = 5;
 
 static uint32_t sssp_delta(olv_graph *g) {
     if (g->tune.sssp_delta) return g->tune.sssp_delta;
     return kDefaultDelta;
+}
+
+// Per vertex (heavy out-degree, in-degree): what the collect pass sums for the
+// push/pull choice, one 8-byte load per collected vertex.
+__global__ void k_heavy_in_degrees(const uint32_t *__restrict__ rowptr,
+                                   const uint32_t *__restrict__ rowmid,
+                                   const uint32_t *__restrict__ colptr, uint32_t V,
+                                   uint2 *__restrict__ hdin) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+         v += (uint64_t)gridDim.x * blockDim.x)
+        hdin[v] = make_uint2(rowptr[v + 1] - rowmid[v], colptr[v + 1] - colptr[v]);
 }
 
 // Rows split light | heavy for the current delta (built once per delta).
@@ -409,9 +687,13 @@ static int sssp_partition(olv_graph *g) {
     OLV_TRY(ws.sssp_col.ensure(g->E * 4 + 16));
     OLV_TRY(ws.sssp_w.ensure(g->E * 4 + 16));
     OLV_TRY(ws.rowmid.ensure((size_t)g->V * 4 + 16));
+    OLV_TRY(ws.hdin.ensure((size_t)g->V * 8 + 16));
     k_partition_rows<<<g->num_sms * 16, kBlock, 0, g->stream>>>(
         g->rowptr.as<uint32_t>(), g->col.as<uint32_t>(), g->w.as<uint32_t>(), g->V, delta,
         ws.sssp_col.as<uint32_t>(), ws.sssp_w.as<uint32_t>(), ws.rowmid.as<uint32_t>());
+    k_heavy_in_degrees<<<g->num_sms * 8, kBlock, 0, g->stream>>>(
+        g->rowptr.as<uint32_t>(), ws.rowmid.as<uint32_t>(), g->colptr.as<uint32_t>(), g->V,
+        ws.hdin.as<uint2>());
     OLV_CUDA(cudaGetLastError());
     ws.sssp_delta_built = delta;
     return OLV_OK;
@@ -459,12 +741,25 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     a.rbeg2 = ah.rbeg;
     a.rend2 = ah.rend;
     a.want_mode2 = kModeHeavy;
-    void *a_aux[] = {&V, &ctl, &q0, &q1, &far0, &far1, &fm};
+    SsspAux x;
+    x.rowptr = g->rowptr.as<uint32_t>();
+    x.rowmid = ws.rowmid.as<uint32_t>();
+    x.colptr = g->colptr.as<uint32_t>();
+    x.rowidx = g->rowidx.as<uint32_t>();
+    x.cw = g->csc_w.as<uint32_t>();
+    x.E = g->E;
+    x.hdin = ws.hdin.as<uint2>();
+    x.blist = ws.blist.as<uint32_t>();
+    x.cmark = mk + 4 * words;
+    x.bl_cap = V;
+    x.pull = g->tune.sssp_pull && x.cw != nullptr;
+    void *a_aux[] = {&V, &ctl, &q0, &q1, &far0, &far1, &fm, &x};
     OLV_TRY(sink((const void *)k_sssp_aux, dim3(nb), dim3(kBlock), a_aux));
     void *a_adv[] = {&a, &op};
     OLV_TRY(sink((const void *)k_advance_chunks<SsspOp>, dim3(nb), dim3(kBlock), a_adv));
     OLV_TRY(sink((const void *)k_advance_pieces<SsspOp>, dim3(nb), dim3(kBlock), a_adv));
-    void *a_end[] = {&ctl, &h, &use_cond, &max_steps};
+    uint32_t bl_cap = x.bl_cap;
+    void *a_end[] = {&ctl, &h, &use_cond, &max_steps, &bl_cap};
     OLV_TRY(sink((const void *)k_sssp_end, dim3(1), dim3(1), a_end));
     return OLV_OK;
 }
@@ -484,7 +779,8 @@ int sssp_workspace(olv_graph *g) {
     const size_t V = g->V;
     OLV_TRY(g->ws.far0.ensure(V * 4 + 16));
     OLV_TRY(g->ws.far1.ensure(V * 4 + 16));
-    OLV_TRY(g->ws.mark.ensure(4 * mark_words(V) * 4));
+    OLV_TRY(g->ws.blist.ensure(V * 4 + 16));
+    OLV_TRY(g->ws.mark.ensure(kMarks * mark_words(V) * 4));
     return OLV_OK;
 }
 
@@ -492,7 +788,7 @@ int run_sssp_device(olv_graph *g, uint32_t src, uint32_t *dist_dev) {
     OLV_TRY(sssp_partition(g));
     cudaStream_t s = g->stream;
     TravCtl *ctl = g->ws.ctl.as<TravCtl>();
-    OLV_CUDA(cudaMemsetAsync(g->ws.mark.p, 0, 4 * mark_words(g->V) * 4, s));
+    OLV_CUDA(cudaMemsetAsync(g->ws.mark.p, 0, kMarks * mark_words(g->V) * 4, s));
     k_fill_i32<<<g->num_sms * 8, kBlock, 0, s>>>((int32_t *)dist_dev, g->V, kInf);
     k_sssp_init<<<1, 1, 0, s>>>(ctl, dist_dev, g->ws.q0.as<uint32_t>(), src, sssp_delta(g));
     OLV_CUDA(cudaGetLastError());

@@ -143,9 +143,13 @@ def test_sssp_unit_weights_equal_reference_bfs(ob, path):
                                           z["bfs_levels"][i].astype(np.int64))
 
 
-@pytest.mark.parametrize("scale,seed", [(12, 1), (16, 2)])
-def test_sssp_rmat_vs_dijkstra(ob, scale, seed):
+@pytest.mark.parametrize("pull", [0, 1])
+@pytest.mark.parametrize("scale,seed", [(12, 1), (16, 2), (18, 3)])
+def test_sssp_rmat_vs_dijkstra(ob, scale, seed, pull):
+    """Heavy edges by push only (pull=0) or by the in-edge pull where it reads
+    fewer edges (pull=1, the default): the same distances either way."""
     with ob.Graph.rmat(scale, 16, seed, weights=True, wseed=seed + 10) as g:
+        g.tune(sssp_pull=pull)
         rp, cl, w = g.csr()
         np.testing.assert_array_equal(w, oracle.uint_weights(len(cl), seed + 10))
         hub, _ = g.max_degree_vertex()
@@ -155,7 +159,61 @@ def test_sssp_rmat_vs_dijkstra(ob, scale, seed):
             np.testing.assert_array_equal(g.sssp(s), ref)
             st = g.last_stats
             assert st.edges_traversed == e_ref and st.vertices_reached == nset
-            assert st.edges_relaxed >= st.edges_traversed
+            if not pull:   # push relaxes every out-edge of a reached vertex at least once
+                assert st.edges_relaxed >= st.edges_traversed
+        if pull and scale >= 16:
+            # the pull reads far fewer edges than the push from the hub
+            g.sssp(hub)
+            relaxed_pull = g.last_stats.edges_relaxed
+            g.tune(sssp_pull=0)
+            g.sssp(hub)
+            assert relaxed_pull < g.last_stats.edges_relaxed
+
+
+def _core_graph(n_core=300, n_tail=40, seed=5):
+    """Source -> core by light edges, a complete core of heavy edges (most of
+    E, all landing on settled vertices), core -> four targets with 300 heavy
+    in-edges each (warp-read in-rows) and -> tail vertices with 3 in-edges
+    each (thread-read in-rows); targets and tail lead on into later buckets,
+    and two unreachable vertices point at a target."""
+    rng = np.random.default_rng(seed)
+    src = 0
+    core = np.arange(1, n_core + 1)
+    tgt = np.arange(n_core + 1, n_core + 5)
+    tail = np.arange(n_core + 5, n_core + 5 + n_tail)
+    far = np.arange(tail[-1] + 1, tail[-1] + 1 + 50)
+    unr = np.array([far[-1] + 1, far[-1] + 2])
+    V = int(unr[-1]) + 1
+    e = []
+    e += [(src, int(c), int(rng.integers(1, 20))) for c in core]
+    e += [(int(a), int(b), int(rng.integers(100, 400))) for a in core for b in core if a != b]
+    e += [(int(a), int(t), int(rng.integers(65, 900))) for t in tgt for a in core]
+    e += [(int(a), int(t), int(rng.integers(65, 900))) for t in tail
+          for a in rng.choice(core, 3, replace=False)]
+    e += [(int(t), int(f), int(rng.integers(1, 300))) for t in np.concatenate([tgt, tail])
+          for f in rng.choice(far, 4, replace=False)]
+    e += [(int(f), int(rng.choice(far)), int(rng.integers(1, 100))) for f in far]
+    e += [(int(u), int(tgt[0]), 1) for u in unr]
+    e.sort()
+    a = np.array(e, dtype=np.int64)
+    rp = np.zeros(V + 1, np.uint32)
+    np.add.at(rp, a[:, 0] + 1, 1)
+    return np.cumsum(rp).astype(np.uint32), a[:, 1].astype(np.uint32), a[:, 2].astype(np.uint32)
+
+
+@pytest.mark.parametrize("pull", [0, 1])
+def test_sssp_pull_superstep_long_and_short_in_rows(ob, pull):
+    rp, cl, w = _core_graph()
+    ref, e_ref, _, nset = oracle.dijkstra(rp, cl, w, 0)
+    with ob.Graph.from_csr(rp, cl, w) as g:
+        g.tune(sssp_pull=pull)
+        np.testing.assert_array_equal(g.sssp(0), ref)
+        st = g.last_stats
+        assert st.edges_traversed == e_ref and st.vertices_reached == nset
+        if pull:   # the core's heavy edges were not relaxed one by one
+            assert st.edges_relaxed < (len(cl) * 3) // 4
+        for s in (1, 7):
+            np.testing.assert_array_equal(g.sssp(s), oracle.dijkstra(rp, cl, w, s)[0])
 
 
 def test_sssp_needs_weights(ob):
