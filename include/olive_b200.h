@@ -141,8 +141,10 @@ int olv_bfs(olv_graph *g, uint32_t src, int32_t *level_out, olv_stats *st);
 int olv_bfs_noalloc(const uint32_t *rowptr, const uint32_t *col, uint32_t V, uint64_t E,
                     uint32_t src, int32_t *level_out, void *stream, olv_stats *st);
 /* SSSP distances with non-negative uint32 weights: the frontier Bellman-Ford of
- * SSSP.cu:106-174 (atomicMin relaxation) with near/far bucketing.  uint32
- * distance, 0x7fffffff unreached.  Needs an OLV_W_U32 graph.                   */
+ * SSSP.cu:106-174 (atomicMin relaxation) with near/far bucketing; a bucket's
+ * heavy edges go by push or, where it reads fewer edges, by a pull over the
+ * unsettled vertices' in-edges (tune key "sssp_pull").  uint32 distance,
+ * 0x7fffffff unreached.  Needs an OLV_W_U32 graph.                             */
 int olv_sssp(olv_graph *g, uint32_t src, uint32_t *dist_out, olv_stats *st);
 /* Multi-source BFS (no reference counterpart): n <= 64 sources advanced
  * together with one 64-bit mask per vertex.  levels_out is [n][V] int32
