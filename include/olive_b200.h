@@ -60,7 +60,7 @@ typedef struct olv_stats {
     uint32_t pull_steps;        /* BFS levels run bottom-up                             */
     uint64_t vertices_reached;  /* BFS/SSSP: vertices with a finite result              */
     uint64_t edges_traversed;   /* sum of out-degrees of reached vertices (GTEPS basis)  */
-    uint64_t edges_relaxed;     /* SSSP: edges actually relaxed (>= edges_traversed)     */
+    uint64_t edges_relaxed;     /* SSSP: out-edges pushed plus in-edges pulled          */
     double   residual;          /* PageRank: last L1 residual (FP64)                     */
     double   device_ms;         /* device time of the call (CUDA events)                */
 } olv_stats;
@@ -98,8 +98,10 @@ int olv_set_stream(olv_graph *g, void *stream);
 int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
 /* Engine tunables by name (no reference counterpart; the reference fixed its
  * launch shape in util::kernelConfig, utils.h:56-72, and the app's -g flag):
- *   "hub_degree"  rows longer than this are split into pieces       (1024)
- *   "piece"       edges per piece                                   (1024)
+ *   "hub_degree"  BFS: rows longer than this are split into pieces  (1024)
+ *   "piece"       BFS: edges per piece                              (1024)
+ *   "sssp_hub_degree", "sssp_piece"  the same for SSSP's relax
+ *                 supersteps (smaller pieces even out the CTAs' work) (256)
  *   "alpha"       BFS push->pull when m_f * alpha > m_unvisited     (14)
  *   "beta"        BFS pull->push when n_f * beta < V                (24)
  *   "sssp_delta"  SSSP bucket width, 0 = default                    (0)
@@ -115,7 +117,8 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
 int olv_tune_set(olv_graph *g, const char *key, double value);
 int olv_tune_get(const olv_graph *g, const char *key, double *value);
 /* Autotuner: coordinate descent over hub_degree, alpha, beta (BFS) and, on
- * uint32-weighted graphs, sssp_delta and piece (SSSP), each candidate timed
+ * uint32-weighted graphs, sssp_delta, sssp_hub_degree and sssp_piece (SSSP),
+ * each candidate timed
  * `reps` times from the highest out-degree vertex; the fastest values are
  * applied to the handle and, if json_path is not NULL, written to a JSON table
  * keyed by GPU name and graph shape.  olv_autotune_load applies such a table

@@ -71,7 +71,8 @@ extern "C" int olv_autotune(olv_graph *g, const char *json_path, int reps) {
     };
     if (g->weight_type == OLV_W_U32) {
         plan.push_back({"sssp_delta", {16, 32, 64, 128, 256, 512, 1024}, run_sssp});
-        plan.push_back({"piece", {256, 1024, 4096}, run_sssp});
+        plan.push_back({"sssp_hub_degree", {128, 256, 1024}, run_sssp});
+        plan.push_back({"sssp_piece", {256, 1024}, run_sssp});
     }
     std::string log;
     for (auto &c : plan) {
@@ -117,7 +118,8 @@ extern "C" int olv_autotune_load(olv_graph *g, const char *json_path, int *appli
     fclose(f);
     const std::string want = "\"key\": \"" + tune_key(g) + "\"";
     if (text.find(want) == std::string::npos) return OLV_OK;   // table is for another graph/GPU
-    const char *keys[] = {"hub_degree", "piece", "alpha", "beta", "sssp_delta", "ms_alpha"};
+    const char *keys[] = {"hub_degree", "piece",      "alpha",           "beta",
+                          "sssp_delta", "sssp_piece", "sssp_hub_degree", "ms_alpha"};
     for (const char *k : keys) {
         const std::string pat = std::string("\"") + k + "\":";
         size_t pos = text.find(pat);

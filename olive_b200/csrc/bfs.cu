@@ -450,7 +450,12 @@ int traversal_workspace(olv_graph *g, bool pieces) {
     OLV_TRY(w.ctl.ensure(sizeof(TravCtl)));
     OLV_TRY(w.fbits.ensure(2 * (((size_t)V + 31) / 32 + 8) * 4));
     if (pieces) {
-        const uint64_t np = g->E / g->tune.piece + g->E / g->tune.hub_degree + 16;
+        // hub pieces of one superstep: at most E/piece + (rows over hub_degree),
+        // for the BFS and the SSSP settings alike
+        const Tuning &t = g->tune;
+        const uint64_t piece = t.piece < t.sssp_piece ? t.piece : t.sssp_piece;
+        const uint64_t hub = t.hub_degree < t.sssp_hub_degree ? t.hub_degree : t.sssp_hub_degree;
+        const uint64_t np = g->E / piece + g->E / hub + 16;
         OLV_TRY(w.pieces.ensure(np * sizeof(uint2)));
     }
     if (g->persist_blocks == 0) {

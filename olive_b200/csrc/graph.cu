@@ -500,6 +500,14 @@ int olv_tune_set(olv_graph *g, const char *key, double value) {
         OLV_CHECK_ARG(value >= 32 && value <= 1e9, "olv_tune_set: piece out of range");
         t.piece = (uint32_t)value;
         g->ws.pieces.release();
+    } else if (!strcmp(key, "sssp_hub_degree")) {
+        OLV_CHECK_ARG(value >= 32 && value <= 1e9, "olv_tune_set: sssp_hub_degree out of range");
+        t.sssp_hub_degree = (uint32_t)value;
+        g->ws.pieces.release();
+    } else if (!strcmp(key, "sssp_piece")) {
+        OLV_CHECK_ARG(value >= 32 && value <= 1e9, "olv_tune_set: sssp_piece out of range");
+        t.sssp_piece = (uint32_t)value;
+        g->ws.pieces.release();
     } else if (!strcmp(key, "alpha")) {
         OLV_CHECK_ARG(value > 0, "olv_tune_set: alpha must be > 0");
         t.alpha = (float)value;
@@ -543,6 +551,8 @@ int olv_tune_get(const olv_graph *g, const char *key, double *value) {
     else if (!strcmp(key, "beta")) *value = t.beta;
     else if (!strcmp(key, "sssp_delta")) *value = t.sssp_delta;
     else if (!strcmp(key, "sssp_pull")) *value = t.sssp_pull;
+    else if (!strcmp(key, "sssp_hub_degree")) *value = t.sssp_hub_degree;
+    else if (!strcmp(key, "sssp_piece")) *value = t.sssp_piece;
     else if (!strcmp(key, "ms_alpha")) *value = t.ms_alpha;
     else if (!strcmp(key, "use_graphs")) *value = t.use_graphs;
     else if (!strcmp(key, "batch_cluster")) *value = t.batch_cluster;

@@ -100,6 +100,8 @@ struct Tuning {
     float beta = 24.0f;           // pull -> push when n_f < V / beta
     uint32_t sssp_delta = 0;      // 0 = default bucket width (64)
     int sssp_pull = 1;            // SSSP: a bucket's heavy edges may go by an in-edge pull
+    uint32_t sssp_hub_degree = 256;   // SSSP: rows with more edges are split into pieces
+    uint32_t sssp_piece = 256;        // SSSP: edges per piece
     float ms_alpha = 20.0f;       // msBFS: pull when active out-edges * ms_alpha > E
     int levels_per_sync = 4;      // host loop: supersteps enqueued per check
     int use_graphs = 1;           // run supersteps inside a CUDA graph

@@ -714,8 +714,8 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     a.far0 = ws.far0.as<uint32_t>();
     a.far1 = ws.far1.as<uint32_t>();
     a.pieces = ws.pieces.as<uint2>();
-    a.hub_degree = g->tune.hub_degree;
-    a.piece = g->tune.piece;
+    a.hub_degree = g->tune.sssp_hub_degree;
+    a.piece = g->tune.sssp_piece;
     a.want_mode = kModeRelax;
     AdvanceArgs ah = a;   // heavy edges: [rowmid[u], rowptr[u+1])
     ah.rbeg = ws.rowmid.as<uint32_t>();

@@ -170,6 +170,18 @@ def test_sssp_rmat_vs_dijkstra(ob, scale, seed, pull):
             assert relaxed_pull < g.last_stats.edges_relaxed
 
 
+@pytest.mark.parametrize("hub,piece", [(32, 32), (4096, 4096)])
+def test_sssp_hub_pieces_vs_dijkstra(ob, hub, piece):
+    """Rows over sssp_hub_degree go to warp pieces of sssp_piece edges: every
+    split gives the same distances (32/32 puts most RMAT rows in pieces)."""
+    with ob.Graph.rmat(16, 16, 4, weights=True, wseed=9) as g:
+        g.tune(sssp_hub_degree=hub, sssp_piece=piece)
+        rp, cl, w = g.csr()
+        hubv, _ = g.max_degree_vertex()
+        for s in (hubv, 5):
+            np.testing.assert_array_equal(g.sssp(s), oracle.dijkstra(rp, cl, w, s)[0])
+
+
 def _core_graph(n_core=300, n_tail=40, seed=5):
     """Source -> core by light edges, a complete core of heavy edges (most of
     E, all landing on settled vertices), core -> four targets with 300 heavy
@@ -338,12 +350,13 @@ def test_autotune_keeps_results_and_roundtrips(ob, tmp_path):
         path = str(tmp_path / "tune.json")
         best = g.autotune(path, reps=1)
         assert best["hub_degree"] in (256, 1024, 4096)
+        assert best["sssp_hub_degree"] in (128, 256, 1024) and best["sssp_piece"] in (256, 1024)
         np.testing.assert_array_equal(g.bfs(hub), oracle.bfs(rp, cl, hub)[0])
         np.testing.assert_array_equal(g.sssp(hub), oracle.dijkstra(rp, cl, w, hub)[0])
         txt = open(path).read()
         assert '"key"' in txt and "sssp_delta" in txt
     with ob.Graph.rmat(14, 16, 3, weights=True, wseed=4) as g2:
-        g2.tune(hub_degree=4096, sssp_delta=16)
+        g2.tune(hub_degree=4096, sssp_delta=16, sssp_hub_degree=4096, sssp_piece=4096)
         assert g2.autotune_load(path)
         assert g2.tune() == best
     with ob.Graph.rmat(13, 16, 3) as g3:       # another graph: table not applied
