@@ -69,7 +69,7 @@ struct NoAllocBfsOp {
         m_next = &c->m_next;
     }
     __device__ __forceinline__ uint32_t src_value(uint32_t) const { return 0; }
-    __device__ __forceinline__ void on_input(uint32_t) const {}
+    __device__ __forceinline__ bool on_input(uint32_t) const { return true; }
     __device__ __forceinline__ Pre prepare(uint32_t, uint32_t, uint32_t v) const {
         return Pre{__ldcg(&level[v])};
     }

@@ -96,7 +96,7 @@ struct MsPushOp {
         filter = c->level >= 2;
     }
     __device__ __forceinline__ SV src_value(uint32_t u) const { return cur[u]; }
-    __device__ __forceinline__ void on_input(uint32_t) const {}
+    __device__ __forceinline__ bool on_input(uint32_t) const { return true; }
     __device__ __forceinline__ Pre prepare(SV sv, uint32_t, uint32_t v) const {
         return Pre{filter ? sv & ~__ldg(&visit[v]) : sv};
     }

@@ -20,7 +20,8 @@
 //                                                   used); act[j] becomes 0: nothing,
 //                                                   1: push v to the output queue,
 //                                                   2: push to the secondary (far) queue
-//   void on_input(uint32_t u)                       once per input queue entry
+//   bool on_input(uint32_t u)                       once per input queue entry;
+//                                                   false: skip its edges now
 //   void on_push(bool pushed, uint32_t v)           after each warp-wide push
 //   void flush(unsigned long long relaxed)          once per thread at the end
 #pragma once
@@ -263,9 +264,10 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_chunks(Advan
         SV sv = 0;
         if (i < n) {
             const uint32_t u = qin[i];
-            op.on_input(u);
-            beg = __ldg(&rbeg[u]);
-            deg = __ldg(&rend[u]) - beg;
+            if (op.on_input(u)) {
+                beg = __ldg(&rbeg[u]);
+                deg = __ldg(&rend[u]) - beg;
+            }
             if (deg > a.hub_degree) {
                 const uint32_t np = (deg + a.piece - 1) / a.piece;
                 const uint32_t b = atomicAdd(&c->npieces, np);

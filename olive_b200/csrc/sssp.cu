@@ -189,9 +189,14 @@ struct SsspOp {
                 act[j] = p[j].nd < threshold ? 1 : 2;
         }
     }
-    // the input vertex was queued (and marked) by the previous superstep
-    __device__ __forceinline__ void on_input(uint32_t u) const {
-        atomicAnd(&nprev[u >> 5], ~(1u << (u & 31)));
+    // The input vertex was queued (and marked) by the previous superstep.  If
+    // this superstep has lowered its distance again, it is already queued for
+    // the next one, which relaxes its edges from a distance no larger than
+    // today's: expanding it now would only be repeated, so it is skipped.
+    __device__ __forceinline__ bool on_input(uint32_t u) const {
+        const uint32_t bit = 1u << (u & 31);
+        atomicAnd(&nprev[u >> 5], ~bit);
+        return !(__ldcg(&nbits[u >> 5]) & bit);
     }
     __device__ __forceinline__ void on_push(bool, uint32_t) {}
     __device__ __forceinline__ void flush(unsigned long long relaxed) {
