@@ -1,0 +1,143 @@
+"""CPU model of the SSSP superstep schedule (olive_b200/csrc/sssp.cu), checked
+against Dijkstra.
+
+The device solve orders the atomicMin relaxation of SSSP.cu:54-76 as
+delta-stepping with a near queue, a far pile and light/heavy edges, and
+relaxes a settled bucket's heavy edges either by push (every heavy out-edge
+of the bucket) or by pull (every in-edge of every vertex at or above the
+threshold whose source is settled).  It collects the settled bucket either
+densely or from the list of the bucket's relax inputs.  This model runs the
+same schedule synchronously in numpy, choosing push or pull with the
+kernel's rule, and checks that both choices and both collects give Dijkstra's
+distances, that a pull never lowers a vertex below the threshold, and that
+the bucket list covers every settled vertex.  No GPU needed.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle
+
+INF = 0x7fffffff
+
+
+def _expand(rp, deg, sel, us):
+    """(u, e) for every edge of rows us whose position passes sel."""
+    cnt = deg[us]
+    tot = int(cnt.sum())
+    if tot == 0:
+        return np.empty(0, np.int64), np.empty(0, np.int64)
+    u = np.repeat(us, cnt)
+    off = np.arange(tot) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+    e = rp[u] + off
+    m = sel[e]
+    return u[m], e[m]
+
+
+def _lower(dist, v, nd):
+    """Apply candidate distances; return the improved vertices and values."""
+    imp = nd < dist[v]
+    v, nd = v[imp], nd[imp]
+    o = np.lexsort((nd, v))
+    v, nd = v[o], nd[o]
+    first = np.ones(len(v), bool)
+    first[1:] = v[1:] != v[:-1]
+    v, nd = v[first], nd[first]
+    dist[v] = nd
+    return v, nd
+
+
+def schedule(rp, col, w, src, delta, pull_mode, list_collect):
+    """pull_mode: 'never', 'always' or 'rule' (the kernel's choice:
+    E - settled in-edges + V/2 < heavy out-edges of the bucket)."""
+    rp = rp.astype(np.int64)
+    col = col.astype(np.int64)
+    w = w.astype(np.int64)
+    V, E = len(rp) - 1, len(col)
+    deg = np.diff(rp)
+    row = np.repeat(np.arange(V), deg)
+    order = np.argsort(col, kind="stable")
+    cptr = np.zeros(V + 1, np.int64)
+    np.add.at(cptr, col + 1, 1)
+    cptr = np.cumsum(cptr)
+    indeg = np.diff(cptr)
+    csrc, cw = row[order], w[order]
+    light = w <= delta
+    hdeg = np.bincount(row[~light], minlength=V)
+    dist = np.full(V, INF, np.int64)
+    dist[src] = 0
+    far = np.zeros(V, bool)
+    q = np.array([src])
+    lo, hi = 0, delta
+    settled_in, pulls = 0, 0
+    while True:
+        blist = []
+        while len(q):                       # relax supersteps: light edges
+            blist.append(q)
+            u, e = _expand(rp, deg, light, q)
+            v, nd = _lower(dist, col[e], np.minimum(dist[u] + w[e], INF))
+            far[v[nd >= hi]] = True
+            q = v[nd < hi]
+        in_bucket = np.flatnonzero((dist >= lo) & (dist < hi))
+        if list_collect:
+            listed = np.unique(np.concatenate(blist)) if blist else np.empty(0, np.int64)
+            listed = listed[(dist[listed] >= lo) & (dist[listed] < hi)]
+            np.testing.assert_array_equal(listed, in_bucket)   # the list covers the bucket
+        hw = int(hdeg[in_bucket].sum())
+        settled_in += int(indeg[in_bucket].sum())
+        pull = {"never": False, "always": True,
+                "rule": (E - settled_in) + V // 2 < hw}[pull_mode]
+        if pull:
+            pulls += 1
+            uns = np.flatnonzero(dist >= hi)
+            cnt = indeg[uns]
+            vv = np.repeat(uns, cnt)
+            off = np.arange(int(cnt.sum())) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+            ce = cptr[vv] + off
+            du = dist[csrc[ce]]
+            ok = du < hi
+            v, nd = _lower(dist, vv[ok], np.minimum(du[ok] + cw[ce][ok], INF))
+        else:
+            u, e = _expand(rp, deg, ~light, in_bucket)
+            v, nd = _lower(dist, col[e], np.minimum(dist[u] + w[e], INF))
+        assert (nd >= hi).all()          # heavy relaxations land at or above the threshold
+        far[v] = True
+        fv = np.flatnonzero(far)
+        fv = fv[dist[fv] >= hi]
+        far[:] = False
+        far[fv] = True
+        if len(fv) == 0:
+            return dist, pulls
+        lo = max(hi, int(dist[fv].min()))
+        hi = lo + delta
+        q = fv[dist[fv] < hi]
+        far[q] = False
+
+
+@pytest.mark.parametrize("scale,seed,delta", [(11, 1, 64), (12, 2, 16), (12, 3, 200)])
+@pytest.mark.parametrize("pull_mode", ["never", "always", "rule"])
+def test_schedule_matches_dijkstra_rmat(scale, seed, delta, pull_mode):
+    rp, col = oracle.rmat_csr(scale, 16, seed)
+    w = oracle.uint_weights(len(col), seed + 10)
+    deg = np.diff(rp.astype(np.int64))
+    hub = int(np.argmax(deg))
+    ref = oracle.dijkstra(rp, col, w, hub)[0].astype(np.int64)
+    dist, pulls = schedule(rp, col, w, hub, delta, pull_mode, list_collect=True)
+    np.testing.assert_array_equal(dist, ref)
+    if pull_mode == "rule" and delta == 64:
+        assert pulls >= 1   # from the hub the first bucket's heavy edges go by pull
+
+
+def test_schedule_matches_dijkstra_random_and_unit_weights():
+    rng = np.random.default_rng(3)
+    V, E = 2000, 12000
+    src = np.sort(rng.integers(0, V, E))
+    dst = rng.integers(0, V, E)
+    rp = np.zeros(V + 1, np.int64)
+    np.add.at(rp, src + 1, 1)
+    rp = np.cumsum(rp).astype(np.uint32)
+    col = dst.astype(np.uint32)
+    for w in (rng.integers(1, 1000, E).astype(np.uint32), np.ones(E, np.uint32)):
+        ref = oracle.dijkstra(rp, col, w, 0)[0].astype(np.int64)
+        for mode in ("never", "always"):
+            dist, _ = schedule(rp, col, w, 0, 32, mode, list_collect=True)
+            np.testing.assert_array_equal(dist, ref)
