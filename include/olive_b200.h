@@ -108,6 +108,9 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
  *   "sssp_pull"   SSSP: a settled bucket's heavy edges may be relaxed by
  *                 a pull over the in-edges of the unsettled vertices when
  *                 that reads fewer edges (1) or always by push (0)       (1)
+ *   "sssp_relabel" SSSP runs on vertices renumbered by in-degree, so the
+ *                 most-read distances share cache lines (1), or on the
+ *                 graph's own ids (0); results are identical            (1)
  *   "ms_alpha"    msBFS pull when active out-edges * ms_alpha > E   (20)
  *   "use_graphs"  run supersteps inside CUDA graphs (1) or a host loop (0)
  *   "levels_per_sync" host loop: supersteps enqueued per check      (4)

@@ -215,7 +215,7 @@ class Graph:
         for k, v in kw.items():
             _check(lib().olv_tune_set(self._h, k.encode(), float(v)), f"olv_tune_set({k})")
         out = {}
-        for k in ("hub_degree", "piece", "alpha", "beta", "sssp_delta", "sssp_pull",
+        for k in ("hub_degree", "piece", "alpha", "beta", "sssp_delta", "sssp_pull", "sssp_relabel",
                   "sssp_hub_degree", "sssp_piece", "ms_alpha",
                   "use_graphs", "levels_per_sync", "batch_cluster"):
             d = _D()

@@ -519,6 +519,8 @@ int olv_tune_set(olv_graph *g, const char *key, double value) {
         t.sssp_delta = (uint32_t)value;
     } else if (!strcmp(key, "sssp_pull")) {
         t.sssp_pull = value != 0;
+    } else if (!strcmp(key, "sssp_relabel")) {
+        t.sssp_relabel = value != 0;
     } else if (!strcmp(key, "ms_alpha")) {
         OLV_CHECK_ARG(value > 0, "olv_tune_set: ms_alpha must be > 0");
         t.ms_alpha = (float)value;
@@ -551,6 +553,7 @@ int olv_tune_get(const olv_graph *g, const char *key, double *value) {
     else if (!strcmp(key, "beta")) *value = t.beta;
     else if (!strcmp(key, "sssp_delta")) *value = t.sssp_delta;
     else if (!strcmp(key, "sssp_pull")) *value = t.sssp_pull;
+    else if (!strcmp(key, "sssp_relabel")) *value = t.sssp_relabel;
     else if (!strcmp(key, "sssp_hub_degree")) *value = t.sssp_hub_degree;
     else if (!strcmp(key, "sssp_piece")) *value = t.sssp_piece;
     else if (!strcmp(key, "ms_alpha")) *value = t.ms_alpha;

@@ -102,6 +102,7 @@ struct Tuning {
     int sssp_pull = 1;            // SSSP: a bucket's heavy edges may go by an in-edge pull
     uint32_t sssp_hub_degree = 256;   // SSSP: rows with more edges are split into pieces
     uint32_t sssp_piece = 256;        // SSSP: edges per piece
+    int sssp_relabel = 1;             // SSSP: run on vertices renumbered by in-degree
     float ms_alpha = 20.0f;       // msBFS: pull when active out-edges * ms_alpha > E
     int levels_per_sync = 4;      // host loop: supersteps enqueued per check
     int use_graphs = 1;           // run supersteps inside a CUDA graph
@@ -116,6 +117,12 @@ struct Workspace {
     DevBuf sssp_col, sssp_w, rowmid; // SSSP: rows split light (w <= delta) | heavy
     DevBuf blist;                   // SSSP: inputs of the current bucket's relax supersteps
     DevBuf hdin;                    // SSSP: per vertex (heavy out-degree, in-degree)
+    // SSSP: vertices renumbered by in-degree (descending): new -> old and
+    // old -> new ids, the CSR and CSC in the new ids with their weights, and
+    // the distances in the new ids
+    DevBuf sr_perm, sr_newid, sr_rowptr, sr_col, sr_w, sr_colptr, sr_rowidx, sr_cw, sr_dist;
+    int sr_built = 0;
+    int sssp_part_relabel = -1;     // SSSP: the partition above was built relabelled (1) or not
     uint32_t sssp_delta_built = 0;
     uint32_t n_heavy = 0, n_light = 0;
     void release() {
@@ -124,6 +131,11 @@ struct Workspace {
         pull_first.release();
         sssp_col.release(); sssp_w.release(); rowmid.release(); blist.release(); hdin.release();
         sssp_delta_built = 0;
+        sr_perm.release(); sr_newid.release(); sr_rowptr.release(); sr_col.release();
+        sr_w.release(); sr_colptr.release(); sr_rowidx.release(); sr_cw.release();
+        sr_dist.release();
+        sr_built = 0;
+        sssp_part_relabel = -1;
         mark.release(); far0.release(); far1.release(); tmp.release(); partials.release();
     }
 };

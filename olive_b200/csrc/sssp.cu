@@ -39,6 +39,9 @@
 // over the bucket's heavy edges would, and by the same value; each vertex is
 // written by its own thread, and its new distance (at or above the
 // threshold) does not pass the `dist[u] < threshold` filter of any reader.
+#include <algorithm>
+#include <vector>
+
 #include "olv_advance.cuh"
 #include "olv_graphexec.cuh"
 #include "olv_internal.cuh"
@@ -209,7 +212,8 @@ struct SsspOp {
 __device__ void sssp_begin(TravCtl *c);
 
 __global__ void k_sssp_init(TravCtl *c, uint32_t *dist, uint32_t *q0, uint32_t src,
-                            uint32_t delta) {
+                            uint32_t delta, const uint32_t *newid) {
+    if (newid) src = newid[src];   // relabelled run: the source's new id
     TravCtl t = {};
     t.qsize[0] = 1;
     t.vdata = dist;
@@ -684,23 +688,138 @@ __global__ void k_heavy_in_degrees(const uint32_t *__restrict__ rowptr,
         hdin[v] = make_uint2(rowptr[v + 1] - rowmid[v], colptr[v + 1] - colptr[v]);
 }
 
-// Rows split light | heavy for the current delta (built once per delta).
+// Row i of the renumbered structure is row perm[i] of the old one, its
+// entries in the same order, neighbour ids mapped through newid, weights
+// carried along.  One warp per row.
+__global__ void k_sssp_relabel(const uint32_t *__restrict__ old_ptr,
+                               const uint32_t *__restrict__ old_idx,
+                               const uint32_t *__restrict__ old_w,
+                               const uint32_t *__restrict__ perm,
+                               const uint32_t *__restrict__ newid,
+                               const uint32_t *__restrict__ new_ptr, uint32_t n,
+                               uint32_t *__restrict__ new_idx, uint32_t *__restrict__ new_w) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t w = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = w; i < n; i += nw) {
+        const uint32_t v = perm[i];
+        const uint32_t b = old_ptr[v], e = old_ptr[v + 1], o = new_ptr[i];
+        for (uint32_t k = lane; k < e - b; k += 32) {
+            new_idx[o + k] = newid[old_idx[b + k]];
+            new_w[o + k] = old_w[b + k];
+        }
+    }
+}
+
+// Distances back to the caller's ids: out[v] = dnew[newid[v]].
+__global__ void k_sssp_unrelabel(const uint32_t *__restrict__ dnew,
+                                 const uint32_t *__restrict__ newid, uint32_t V,
+                                 uint32_t *__restrict__ out) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+         v += (uint64_t)gridDim.x * blockDim.x)
+        out[v] = __ldg(&dnew[newid[v]]);
+}
+
+// Renumber the vertices by in-degree, highest first (a stable counting sort
+// on the host, once per graph), and build the CSR and CSC with weights in
+// the new ids.  The relax supersteps gather the distances of edge targets;
+// on a scale-free graph most gathers hit the high in-degree vertices, whose
+// distances then share cache lines instead of one 32-byte sector each.
+static int sssp_relabel(olv_graph *g) {
+    Workspace &ws = g->ws;
+    if (ws.sr_built) return OLV_OK;
+    const uint32_t V = g->V;
+    const uint64_t E = g->E;
+    cudaStream_t s = g->stream;
+    std::vector<uint32_t> rp((size_t)V + 1), cp((size_t)V + 1);
+    OLV_CUDA(cudaMemcpyAsync(rp.data(), g->rowptr.p, ((size_t)V + 1) * 4, cudaMemcpyDeviceToHost, s));
+    OLV_CUDA(cudaMemcpyAsync(cp.data(), g->colptr.p, ((size_t)V + 1) * 4, cudaMemcpyDeviceToHost, s));
+    OLV_CUDA(cudaStreamSynchronize(s));
+    uint32_t maxd = 0;
+    for (uint32_t v = 0; v < V; v++) maxd = std::max(maxd, cp[v + 1] - cp[v]);
+    std::vector<uint64_t> start((size_t)maxd + 2, 0);
+    for (uint32_t v = 0; v < V; v++) start[maxd - (cp[v + 1] - cp[v]) + 1]++;
+    for (size_t d = 1; d < start.size(); d++) start[d] += start[d - 1];
+    std::vector<uint32_t> perm(V), newid(V), nrp((size_t)V + 1), ncp((size_t)V + 1);
+    for (uint32_t v = 0; v < V; v++) {
+        const uint32_t i = (uint32_t)start[maxd - (cp[v + 1] - cp[v])]++;
+        perm[i] = v;
+        newid[v] = i;
+    }
+    nrp[0] = 0;
+    ncp[0] = 0;
+    for (uint32_t i = 0; i < V; i++) {
+        nrp[i + 1] = nrp[i] + (rp[perm[i] + 1] - rp[perm[i]]);
+        ncp[i + 1] = ncp[i] + (cp[perm[i] + 1] - cp[perm[i]]);
+    }
+    OLV_TRY(ws.sr_perm.ensure((size_t)V * 4 + 16));
+    OLV_TRY(ws.sr_newid.ensure((size_t)V * 4 + 16));
+    OLV_TRY(ws.sr_rowptr.ensure(((size_t)V + 1) * 4 + 16));
+    OLV_TRY(ws.sr_colptr.ensure(((size_t)V + 1) * 4 + 16));
+    OLV_TRY(ws.sr_col.ensure(E * 4 + 16));
+    OLV_TRY(ws.sr_w.ensure(E * 4 + 16));
+    OLV_TRY(ws.sr_rowidx.ensure(E * 4 + 16));
+    OLV_TRY(ws.sr_cw.ensure(E * 4 + 16));
+    OLV_TRY(ws.sr_dist.ensure((size_t)V * 4 + 16));
+    OLV_CUDA(cudaMemcpyAsync(ws.sr_perm.p, perm.data(), (size_t)V * 4, cudaMemcpyHostToDevice, s));
+    OLV_CUDA(cudaMemcpyAsync(ws.sr_newid.p, newid.data(), (size_t)V * 4, cudaMemcpyHostToDevice, s));
+    OLV_CUDA(cudaMemcpyAsync(ws.sr_rowptr.p, nrp.data(), ((size_t)V + 1) * 4, cudaMemcpyHostToDevice, s));
+    OLV_CUDA(cudaMemcpyAsync(ws.sr_colptr.p, ncp.data(), ((size_t)V + 1) * 4, cudaMemcpyHostToDevice, s));
+    if (E) {
+        k_sssp_relabel<<<g->num_sms * 16, kBlock, 0, s>>>(
+            g->rowptr.as<uint32_t>(), g->col.as<uint32_t>(), g->w.as<uint32_t>(),
+            ws.sr_perm.as<uint32_t>(), ws.sr_newid.as<uint32_t>(), ws.sr_rowptr.as<uint32_t>(), V,
+            ws.sr_col.as<uint32_t>(), ws.sr_w.as<uint32_t>());
+        k_sssp_relabel<<<g->num_sms * 16, kBlock, 0, s>>>(
+            g->colptr.as<uint32_t>(), g->rowidx.as<uint32_t>(), g->csc_w.as<uint32_t>(),
+            ws.sr_perm.as<uint32_t>(), ws.sr_newid.as<uint32_t>(), ws.sr_colptr.as<uint32_t>(), V,
+            ws.sr_rowidx.as<uint32_t>(), ws.sr_cw.as<uint32_t>());
+        OLV_CUDA(cudaGetLastError());
+    }
+    OLV_CUDA(cudaStreamSynchronize(s));   // the host vectors die here
+    ws.sr_built = 1;
+    return OLV_OK;
+}
+
+// The graph SSSP runs on: renumbered (sssp_relabel) or the handle's own.
+struct SsspCsr {
+    const uint32_t *rowptr, *col, *w, *colptr, *rowidx, *cw, *newid;
+    uint32_t *dist;   // internal distances (renumbered run), else null
+};
+static SsspCsr sssp_csr(olv_graph *g) {
+    Workspace &ws = g->ws;
+    if (g->tune.sssp_relabel && ws.sr_built)
+        return SsspCsr{ws.sr_rowptr.as<uint32_t>(), ws.sr_col.as<uint32_t>(),
+                       ws.sr_w.as<uint32_t>(),      ws.sr_colptr.as<uint32_t>(),
+                       ws.sr_rowidx.as<uint32_t>(), ws.sr_cw.as<uint32_t>(),
+                       ws.sr_newid.as<uint32_t>(),  ws.sr_dist.as<uint32_t>()};
+    return SsspCsr{g->rowptr.as<uint32_t>(), g->col.as<uint32_t>(),    g->w.as<uint32_t>(),
+                   g->colptr.as<uint32_t>(), g->rowidx.as<uint32_t>(), g->csc_w.as<uint32_t>(),
+                   nullptr,                  nullptr};
+}
+
+// Rows split light | heavy for the current delta (built once per delta and
+// numbering).
 static int sssp_partition(olv_graph *g) {
     Workspace &ws = g->ws;
     const uint32_t delta = sssp_delta(g);
-    if (ws.sssp_delta_built == delta && ws.rowmid.p) return OLV_OK;
+    if (g->tune.sssp_relabel) OLV_TRY(sssp_relabel(g));
+    const int relabel = g->tune.sssp_relabel ? 1 : 0;
+    if (ws.sssp_delta_built == delta && ws.sssp_part_relabel == relabel && ws.rowmid.p)
+        return OLV_OK;
+    const SsspCsr R = sssp_csr(g);
     OLV_TRY(ws.sssp_col.ensure(g->E * 4 + 16));
     OLV_TRY(ws.sssp_w.ensure(g->E * 4 + 16));
     OLV_TRY(ws.rowmid.ensure((size_t)g->V * 4 + 16));
     OLV_TRY(ws.hdin.ensure((size_t)g->V * 8 + 16));
     k_partition_rows<<<g->num_sms * 16, kBlock, 0, g->stream>>>(
-        g->rowptr.as<uint32_t>(), g->col.as<uint32_t>(), g->w.as<uint32_t>(), g->V, delta,
-        ws.sssp_col.as<uint32_t>(), ws.sssp_w.as<uint32_t>(), ws.rowmid.as<uint32_t>());
+        R.rowptr, R.col, R.w, g->V, delta, ws.sssp_col.as<uint32_t>(), ws.sssp_w.as<uint32_t>(),
+        ws.rowmid.as<uint32_t>());
     k_heavy_in_degrees<<<g->num_sms * 8, kBlock, 0, g->stream>>>(
-        g->rowptr.as<uint32_t>(), ws.rowmid.as<uint32_t>(), g->colptr.as<uint32_t>(), g->V,
-        ws.hdin.as<uint2>());
+        R.rowptr, ws.rowmid.as<uint32_t>(), R.colptr, g->V, ws.hdin.as<uint2>());
     OLV_CUDA(cudaGetLastError());
     ws.sssp_delta_built = delta;
+    ws.sssp_part_relabel = relabel;
     return OLV_OK;
 }
 
@@ -709,8 +828,9 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
                           int use_cond) {
     Workspace &ws = g->ws;
     TravCtl *ctl = ws.ctl.as<TravCtl>();
+    const SsspCsr R = sssp_csr(g);
     AdvanceArgs a;   // light edges: [rowptr[u], rowmid[u])
-    a.rbeg = g->rowptr.as<uint32_t>();
+    a.rbeg = R.rowptr;
     a.rend = ws.rowmid.as<uint32_t>();
     a.col = ws.sssp_col.as<uint32_t>();
     a.ctl = ctl;
@@ -724,7 +844,7 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     a.want_mode = kModeRelax;
     AdvanceArgs ah = a;   // heavy edges: [rowmid[u], rowptr[u+1])
     ah.rbeg = ws.rowmid.as<uint32_t>();
-    ah.rend = g->rowptr.as<uint32_t>() + 1;
+    ah.rend = R.rowptr + 1;
     SsspOp op = {};
     op.w = ws.sssp_w.as<uint32_t>();
     const size_t words = mark_words(g->V);
@@ -747,11 +867,11 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     a.rend2 = ah.rend;
     a.want_mode2 = kModeHeavy;
     SsspAux x;
-    x.rowptr = g->rowptr.as<uint32_t>();
+    x.rowptr = R.rowptr;
     x.rowmid = ws.rowmid.as<uint32_t>();
-    x.colptr = g->colptr.as<uint32_t>();
-    x.rowidx = g->rowidx.as<uint32_t>();
-    x.cw = g->csc_w.as<uint32_t>();
+    x.colptr = R.colptr;
+    x.rowidx = R.rowidx;
+    x.cw = R.cw;
     x.E = g->E;
     x.hdin = ws.hdin.as<uint2>();
     x.blist = ws.blist.as<uint32_t>();
@@ -793,12 +913,24 @@ int run_sssp_device(olv_graph *g, uint32_t src, uint32_t *dist_dev) {
     OLV_TRY(sssp_partition(g));
     cudaStream_t s = g->stream;
     TravCtl *ctl = g->ws.ctl.as<TravCtl>();
+    const SsspCsr R = sssp_csr(g);
+    uint32_t *dist = R.dist ? R.dist : dist_dev;   // renumbered run: internal distances
     OLV_CUDA(cudaMemsetAsync(g->ws.mark.p, 0, kMarks * mark_words(g->V) * 4, s));
-    k_fill_i32<<<g->num_sms * 8, kBlock, 0, s>>>((int32_t *)dist_dev, g->V, kInf);
-    k_sssp_init<<<1, 1, 0, s>>>(ctl, dist_dev, g->ws.q0.as<uint32_t>(), src, sssp_delta(g));
+    k_fill_i32<<<g->num_sms * 8, kBlock, 0, s>>>((int32_t *)dist, g->V, kInf);
+    k_sssp_init<<<1, 1, 0, s>>>(ctl, dist, g->ws.q0.as<uint32_t>(), src, sssp_delta(g), R.newid);
     OLV_CUDA(cudaGetLastError());
+    auto finish = [&]() -> int {
+        if (R.dist) {
+            k_sssp_unrelabel<<<g->num_sms * 8, kBlock, 0, s>>>(R.dist, R.newid, g->V, dist_dev);
+            OLV_CUDA(cudaGetLastError());
+        }
+        return OLV_OK;
+    };
     if (g->tune.use_graphs) {
-        if (sssp_graph(g) == OLV_OK) return g->sssp_graph->launch(s);
+        if (sssp_graph(g) == OLV_OK) {
+            OLV_TRY(g->sssp_graph->launch(s));
+            return finish();
+        }
         g->tune.use_graphs = 0;
     }
     auto launch = [&](const void *f, dim3 gr, dim3 bl, void **args) {
@@ -811,7 +943,7 @@ int run_sssp_device(olv_graph *g, uint32_t src, uint32_t *dist_dev) {
         OLV_CUDA(cudaStreamSynchronize(s));
         if (g->host_ctl->done) break;
     }
-    return OLV_OK;
+    return finish();
 }
 
 }  // namespace olv

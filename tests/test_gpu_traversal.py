@@ -182,6 +182,23 @@ def test_sssp_hub_pieces_vs_dijkstra(ob, hub, piece):
             np.testing.assert_array_equal(g.sssp(s), oracle.dijkstra(rp, cl, w, s)[0])
 
 
+def test_sssp_relabel_on_off_same_handle(ob):
+    """Renumbered (default) and own-id runs on one handle, toggled back and
+    forth, into host, device and unaligned device outputs."""
+    import torch
+    with ob.Graph.rmat(16, 16, 6, weights=True, wseed=3) as g:
+        rp, cl, w = g.csr()
+        hub, _ = g.max_degree_vertex()
+        ref = oracle.dijkstra(rp, cl, w, hub)[0]
+        for relabel in (1, 0, 1):
+            g.tune(sssp_relabel=relabel)
+            np.testing.assert_array_equal(g.sssp(hub), ref)
+            big = torch.empty(g.V + 1, dtype=torch.int32, device="cuda")
+            g.sssp(hub, out=big[1:])
+            np.testing.assert_array_equal(big[1:].cpu().numpy().astype(np.uint32), ref)
+        np.testing.assert_array_equal(g.sssp(7), oracle.dijkstra(rp, cl, w, 7)[0])
+
+
 def _core_graph(n_core=300, n_tail=40, seed=5):
     """Source -> core by light edges, a complete core of heavy edges (most of
     E, all landing on settled vertices), core -> four targets with 300 heavy
