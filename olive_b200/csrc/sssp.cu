@@ -39,6 +39,13 @@
 // over the bucket's heavy edges would, and by the same value; each vertex is
 // written by its own thread, and its new distance (at or above the
 // threshold) does not pass the `dist[u] < threshold` filter of any reader.
+//
+// Around that: the solve runs on vertices renumbered by in-degree (the
+// most-gathered distances share cache lines; one gather maps the result
+// back), rows over sssp_hub_degree edges go to 256-edge warp pieces, a
+// relax superstep skips an input vertex that it has already queued again,
+// and a bucket is collected from the list of its relax inputs when that
+// list is short.
 #include <algorithm>
 #include <vector>
 
