@@ -278,9 +278,10 @@ def run_ours(a, rank, world, local_rank):
                 "peak_source": peak_src, "kernel_ms": round(kern_ms, 4)}
 
     # launches of our kernels per step (kernel nodes executed by the graph):
-    # sssp: fill, init, 4 per superstep, reached count; bfs: fill, init, 9 per level
+    # sssp: fill, init, 4 per superstep, the map back to the caller's ids
+    # (renumbered run), reached count; bfs: fill, init, 9 per level
     if a.workload == "sssp":
-        per_step = 2 + 4 * st.iterations + 1
+        per_step = 2 + 4 * st.iterations + 1 + int(g.tune().get("sssp_relabel", 0))
     elif a.workload == "bfs":
         per_step = 2 + 9 * st.iterations
     elif a.workload == "msbfs":
