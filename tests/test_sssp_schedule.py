@@ -10,7 +10,9 @@ densely or from the list of the bucket's relax inputs.  This model runs the
 same schedule synchronously in numpy, choosing push or pull with the
 kernel's rule, and checks that both choices and both collects give Dijkstra's
 distances, that a pull never lowers a vertex below the threshold, and that
-the bucket list covers every settled vertex.  No GPU needed.
+the bucket list covers every settled vertex; and that the run on vertices
+renumbered by in-degree, mapped back, gives the same distances.  No GPU
+needed.
 """
 import numpy as np
 import pytest
@@ -141,3 +143,33 @@ def test_schedule_matches_dijkstra_random_and_unit_weights():
         for mode in ("never", "always"):
             dist, _ = schedule(rp, col, w, 0, 32, mode, list_collect=True)
             np.testing.assert_array_equal(dist, ref)
+
+
+def renumber_by_in_degree(rp, col, w):
+    """The renumbering the device solve runs on: vertices in descending
+    in-degree, ties in id order (a stable sort); rows keep their entry order.
+    Returns (perm, newid, rp', col', w')."""
+    rp = rp.astype(np.int64)
+    V = len(rp) - 1
+    indeg = np.bincount(col.astype(np.int64), minlength=V)
+    perm = np.argsort(-indeg, kind="stable")
+    newid = np.empty(V, np.int64)
+    newid[perm] = np.arange(V)
+    deg = np.diff(rp)[perm]
+    nrp = np.concatenate([[0], np.cumsum(deg)])
+    rows = np.concatenate([np.arange(rp[v], rp[v + 1]) for v in perm]) if V else np.empty(0, int)
+    return perm, newid, nrp.astype(np.uint32), newid[col[rows]].astype(np.uint32), w[rows]
+
+
+@pytest.mark.parametrize("scale,seed", [(10, 1), (11, 4)])
+def test_schedule_on_renumbered_graph(scale, seed):
+    rp, col = oracle.rmat_csr(scale, 16, seed)
+    w = oracle.uint_weights(len(col), seed + 10)
+    perm, newid, nrp, ncol, nw = renumber_by_in_degree(rp, col, w)
+    indeg = np.bincount(col.astype(np.int64), minlength=len(rp) - 1)
+    assert (np.diff(indeg[perm]) <= 0).all()          # highest in-degree first
+    deg = np.diff(rp.astype(np.int64))
+    for src in (int(np.argmax(deg)), int(np.flatnonzero(deg > 0)[2])):
+        ref = oracle.dijkstra(rp, col, w, src)[0].astype(np.int64)
+        dnew, _ = schedule(nrp, ncol, nw, int(newid[src]), 64, "rule", list_collect=True)
+        np.testing.assert_array_equal(dnew[newid], ref)   # mapped back: out[v] = dnew[newid[v]]
