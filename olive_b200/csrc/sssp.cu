@@ -66,7 +66,6 @@ constexpr uint32_t kDefaultDelta = 64;
 
 // Arrays the collect and pull passes read besides the queues.
 struct SsspAux {
-    const uint32_t *rowptr, *rowmid;   // CSR rows, light | heavy split
     const uint32_t *colptr, *rowidx;   // CSC: in-edges and their sources
     const uint32_t *cw;                // CSC weights
     const uint2 *hdin;                 // per vertex: (heavy out-degree, in-degree)
@@ -874,8 +873,6 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     a.rend2 = ah.rend;
     a.want_mode2 = kModeHeavy;
     SsspAux x;
-    x.rowptr = R.rowptr;
-    x.rowmid = ws.rowmid.as<uint32_t>();
     x.colptr = R.colptr;
     x.rowidx = R.rowidx;
     x.cw = R.cw;
