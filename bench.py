@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="bound of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-seconds", type=float, default=8.0,
+                    help="--impl reference: bound of one step's CPU sample")
     a = ap.parse_args()
     if a.scale is None:
         a.scale = {"pagerank": 22, "wpr": 20, "batch": 0}.get(a.workload, 24)
@@ -656,11 +658,52 @@ def run_reference(a, rank, world):
         return
     from oracle import oracle
     threads = oracle.max_threads()
+    bound = a.ref_seconds
+    vals, ms = [], []
+    if a.workload == "batch":
+        # the same 512 ER instances and PPR seeds as the GPU arm (the oracle's
+        # restatement of the batch generator), BFS from local vertex 0 plus
+        # PPR-32 per instance, instances in order until the bound
+        count, K = 512, 32
+        sizes = oracle.er_batch_sizes(count, 1024, 65536, a.seed)
+        rng = np.random.default_rng(11)
+        seeds = [rng.integers(0, ni, K).astype(np.uint32) for ni in sizes]
+        V, E = int(sizes.sum()), int(8 * sizes.sum())
+        desc = (f"oracle BFS + FP64 PPR-{K} per instance (serial, 1 core), instances in "
+                f"order; each step stopped after {bound:.0f} s; value = edge visits / s")
+        for i in range(a.warmup + a.steps):
+            visits, secs = 0, 0.0
+            for j in range(count):
+                lrp, lcl = oracle.er_batch_instance(j, int(sizes[j]), 8, a.seed)
+                t = time.perf_counter()
+                _, e = oracle.bfs(lrp, lcl, 0)
+                _, itn = oracle.ppr(lrp, lcl, seeds[j], 0.85, 50, 1e-7)
+                secs += time.perf_counter() - t
+                visits += e + itn * len(lcl) * K
+                if secs > bound:
+                    break
+            if i >= a.warmup:
+                vals.append(visits / secs / 1e9)
+                ms.append(secs * 1e3)
+        unit, cores = "G visits/s", 1
+        line = {"impl": "reference", "metric": metric_name(a.workload, a.scale),
+                "value": round(float(np.median(vals)) if vals else 0.0, 5), "unit": unit,
+                "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+                "ms_per_step": round(float(np.median(ms)) if ms else 0.0, 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64+i32", "data": "synthetic (seeded ER batch generated on the host)",
+                "config": {"workload": "batch-er512", "instances": count,
+                           "V_range": [1024, 65536], "avg_degree": 8, "K": K, "alpha": 0.85,
+                           "max_it": 50, "tol": 1e-7, "seed": a.seed, "V": V, "E": E}}
+        line["cpu_baseline"] = {"value": line["value"], "unit": unit, "cores": cores,
+                                "kind": "port", "sample": desc}
+        line["e2e"] = {"value": line["value"], "unit": unit, "h2d_bytes_per_step": 0,
+                       "d2h_bytes_per_step": 0}
+        print(json.dumps(line), flush=True)
+        return
     rp, cl = oracle.rmat_csr_par(a.scale, 16, a.seed, threads)
     V, E = len(rp) - 1, len(cl)
     src = int(np.argmax(np.diff(rp.astype(np.int64))))
-    bound = 8.0
-    vals, ms = [], []
     if a.workload == "sssp":
         w = oracle.uint_weights_par(E, 2, 1, 255, threads)
         desc = (f"CPU restatement of SSSP.cu's frontier Bellman-Ford (edgeFilter atomicMin + "
@@ -698,6 +741,22 @@ def run_reference(a, rank, world):
                 vals.append(edges / secs / 1e9)
                 ms.append(secs * 1e3)
         unit, cores = "GTEPS", 1
+    elif a.workload == "wpr":
+        # the GPU arm's inputs: lognormal weights and Dirichlet(1) p, numpy seed 7
+        rng = np.random.default_rng(7)
+        w = rng.lognormal(0.0, 1.0, E).astype(np.float32).astype(np.float64)
+        pn = rng.exponential(1.0, V)
+        p = (pn / pn.sum()).astype(np.float32).astype(np.float64)
+        desc = ("oracle FP64 weighted PageRank forward (the reference has no weighted PR; "
+                "1 core); each step 2 sweeps")
+        for i in range(a.warmup + a.steps):
+            t = time.perf_counter()
+            oracle.wpr_forward(rp, cl, w, p, 0.85, 2)
+            secs = time.perf_counter() - t
+            if i >= a.warmup:
+                vals.append(E * 2 / secs / 1e9)
+                ms.append(secs * 1e3)
+        unit, cores = "GE/s/iter", 1
     else:
         desc = ("restatement of testPageRank.cu:74-104 (serial FP64 push PageRank, plus "
                 "dangling redistribution; 1 core); each step 2 iterations")
@@ -714,9 +773,11 @@ def run_reference(a, rank, world):
             "value": round(value, 5), "unit": unit, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": round(float(np.median(ms)) if ms else 0.0, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if a.workload == "pagerank" else "u32",
+            "dtype": "f64" if a.workload in ("pagerank", "wpr") else "u32",
             "data": "synthetic (seeded RMAT, generated on the host)",
-            "config": workload_config(a, V, E, src),
+            "config": workload_config(a, V, E, src, {
+                "weights": "lognormal(0,1) FP32, numpy seed 7", "p": "Dirichlet(1)",
+                "sweeps_per_step": 2} if a.workload == "wpr" else None),
             "cpu_baseline": {"value": round(value, 5), "unit": unit, "cores": cores,
                              "kind": "port", "sample": desc},
             "e2e": {"value": round(value, 5), "unit": unit, "h2d_bytes_per_step": 0,

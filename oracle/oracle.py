@@ -126,6 +126,55 @@ def uint_weights(E, seed, lo=1, hi=255):
     return w[:E]
 
 
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+
+
+def _hash_np(seed, ctr):
+    """orc_hash over a uint64 counter array (SplitMix64 output function of
+    seed + ctr * golden ratio, arithmetic modulo 2^64)."""
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + np.asarray(ctr, np.uint64) * _GOLDEN
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+def er_instance(seed, n, m):
+    """Edges (u, v) of one ER digraph of the batch generator
+    (olive_b200/csrc/er_batch.cu; no reference counterpart): draw j gives
+    (h(seed, 2j) mod n, h(seed, 2j+1) mod n); self-loops are dropped and the
+    first m distinct pairs in draw order are kept, returned sorted by (u, v)."""
+    m = min(int(m), n * (n - 1))
+    draws = m + m // 4 + 64
+    while True:
+        j = np.arange(draws, dtype=np.uint64)
+        u = _hash_np(seed, 2 * j) % np.uint64(n)
+        v = _hash_np(seed, 2 * j + np.uint64(1)) % np.uint64(n)
+        keep = u != v
+        key = (u[keep] << np.uint64(32)) | v[keep]
+        uniq, first = np.unique(key, return_index=True)
+        if len(uniq) >= m or len(uniq) == n * (n - 1):
+            chosen = np.sort(uniq[np.argsort(first, kind="stable")[:m]])
+            return (chosen >> np.uint64(32)).astype(np.uint32), \
+                (chosen & np.uint64(0xffffffff)).astype(np.uint32)
+        draws *= 2
+
+
+def er_batch_sizes(count, vmin, vmax, seed):
+    """Vertex counts of the batch's instances (er_batch.cu er_instance_size)."""
+    h = _hash_np(np.uint64(seed) ^ np.uint64(0xa5a5a5a5), np.arange(count, dtype=np.uint64))
+    return (vmin + h % np.uint64(vmax - vmin + 1)).astype(np.int64)
+
+
+def er_batch_instance(i, n, deg, seed):
+    """Local CSR (rowptr, col) of instance i with n vertices."""
+    s = int(_hash_np(seed, np.uint64(1000003 + i)))
+    u, v = er_instance(s, n, deg * n)
+    rp = np.zeros(n + 1, np.int64)
+    np.add.at(rp, u.astype(np.int64) + 1, 1)
+    return np.cumsum(rp).astype(np.uint32), v
+
+
 def grid_csr(rows, cols):
     V = rows * cols
     rowptr = np.zeros(V + 1, np.uint32)

@@ -53,6 +53,19 @@ def test_er_generator_properties(small_batch):
         assert lcl.max() < n[i]                            # block diagonal
 
 
+def test_er_generator_equals_oracle_restatement(small_batch):
+    """The library's batch generator and the oracle's restatement (which the
+    reference arm of bench.py uses) draw the same instances."""
+    g, off, rp, cl = small_batch
+    n = np.diff(off.astype(np.int64))
+    np.testing.assert_array_equal(n, oracle.er_batch_sizes(24, 300, 3000, 3))
+    for i in range(len(n)):
+        lrp, lcl = instance_csr(rp, cl, off, i)
+        orp, ocl = oracle.er_batch_instance(i, int(n[i]), 8, 3)
+        np.testing.assert_array_equal(lrp, orp)
+        np.testing.assert_array_equal(lcl, ocl)
+
+
 def test_batch_bfs_and_ppr_vs_oracle(ob, small_batch):
     g, off, rp, cl = small_batch
     K = 32

@@ -172,3 +172,20 @@ def test_wpr_adjoint_matches_dense_solve():
         fm = g @ oracle.wpr_forward(rp, cl, wm_, p, a, 400)
         fd = (fp - fm) / (2 * h)
         assert abs(fd - dw[e]) <= 1e-6 * max(1.0, abs(fd)) + 1e-9
+
+
+def test_er_batch_restatement_properties():
+    """Oracle restatement of the batch generator: exact edge counts, no
+    self-loops or duplicates, rows sorted; a 2-vertex instance saturates."""
+    sizes = oracle.er_batch_sizes(5, 40, 700, 1)
+    assert sizes.min() >= 40 and sizes.max() <= 700
+    for i, n in enumerate(sizes):
+        rp, col = oracle.er_batch_instance(i, int(n), 8, 1)
+        assert rp[-1] == 8 * n and len(col) == 8 * n
+        src = np.repeat(np.arange(n), np.diff(rp.astype(np.int64)))
+        assert not np.any(src == col)
+        keys = src * n + col
+        assert (np.diff(keys) > 0).all()     # sorted by (u, v), no duplicates
+    rp, col = oracle.er_batch_instance(0, 2, 8, 3)
+    np.testing.assert_array_equal(rp, [0, 1, 2])
+    np.testing.assert_array_equal(col, [1, 0])
