@@ -2,7 +2,7 @@
 """Benchmark of the olive_b200 frontier engine on one node.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload sssp|bfs|pagerank] [--scale S]
+                    [--workload sssp|bfs|pagerank|msbfs|wpr|batch] [--scale S]
 
 Default workload: single-source shortest paths (frontier Bellman-Ford with
 atomicMin, SSSP.cu semantics) on an RMAT graph of scale 24, edge factor 16,
@@ -17,8 +17,11 @@ ranks' edges over the slowest rank's time.  Rank 0 prints one JSON line.
 
 --impl reference times the reference's algorithm on the host cores: the
 CPU restatement of SSSP.cu's frontier Bellman-Ford (all host threads), of
-testBFS.cu's queue BFS, or of testPageRank.cu's FP64 PageRank, on the same
-synthetic graph built on the host.
+testBFS.cu's queue BFS (once per source for msbfs), or of testPageRank.cu's
+FP64 PageRank, on the same synthetic graph built on the host; for wpr and
+batch, which have no reference counterpart, the oracle's FP64 weighted
+PageRank and BFS + PPR-32 per instance on the same inputs.  Each step's
+sample is bounded by --ref-seconds.
 """
 import argparse
 import json
