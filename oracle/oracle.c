@@ -18,6 +18,7 @@
  * on the 128x128 grid and on small RMAT graphs (tests/golden/).
  */
 #include <stdint.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #include <math.h>
@@ -643,4 +644,134 @@ int orc_max_threads(void) {
 #else
     return 1;
 #endif
+}
+
+/* ------------------------------------------------------------------------ */
+/* Shortest-path certificate (no reference counterpart; the size-independent */
+/* check used where a full serial oracle run is too slow).  For BFS levels    */
+/* (w == NULL: every edge weighs 1) or SSSP distances (weights >= 1):         */
+/*   d[src] == 0, every reached vertex other than src has d > 0;              */
+/*   every edge (u,v) with u reached satisfies d[v] <= d[u] + w(u,v);         */
+/*   every reached v != src has a tight in-edge: d[v] == d[u] + w(u,v).       */
+/* With strictly positive weights these conditions hold for the exact         */
+/* distances and for nothing else (tight edges strictly decrease d, so they   */
+/* lead back to src; the edge condition bounds d from below).  Unreached     */
+/* vertices (0x7fffffff) may have no reached in-neighbour, which the edge     */
+/* condition enforces.  Returns 0 when valid, else 1 + the offending vertex   */
+/* (an edge violation reports its target) with *what = 1 (source), 2 (edge),  */
+/* 3 (no tight in-edge).                                                      */
+/* ------------------------------------------------------------------------ */
+uint64_t orc_sp_certificate(uint32_t V, const uint32_t *rowptr, const uint32_t *col,
+                            const uint32_t *w, uint32_t src, const uint32_t *d,
+                            int nthreads, int *what) {
+    *what = 0;
+    if (V == 0) return 0;
+    if (d[src] != 0) { *what = 1; return (uint64_t)src + 1; }
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#else
+    nthreads = 1;
+#endif
+    uint8_t *tight = (uint8_t *)calloc(V, 1);
+    uint64_t bad = 0;
+    #pragma omp parallel for schedule(dynamic, 4096) num_threads(nthreads)
+    for (int64_t u = 0; u < (int64_t)V; u++) {
+        const uint64_t du = d[u];
+        if (du == ORC_INF) continue;
+        for (uint32_t e = rowptr[u]; e < rowptr[u + 1]; e++) {
+            const uint32_t v = col[e];
+            const uint64_t nd = du + (w ? w[e] : 1u);
+            if ((uint64_t)d[v] > nd) {
+                uint64_t z = 0;
+                __atomic_compare_exchange_n(&bad, &z, (uint64_t)v + 1, 0, __ATOMIC_RELAXED,
+                                            __ATOMIC_RELAXED);
+            } else if ((uint64_t)d[v] == nd) {
+                __atomic_store_n(&tight[v], (uint8_t)1, __ATOMIC_RELAXED);
+            }
+        }
+    }
+    if (bad) { free(tight); *what = 2; return bad; }
+    for (uint32_t v = 0; v < V; v++)
+        if (v != src && d[v] != ORC_INF && (d[v] == 0 || !tight[v])) {
+            free(tight);
+            *what = 3;
+            return (uint64_t)v + 1;
+        }
+    free(tight);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* orc_ppr over every instance of a block-diagonal batch (instances run in   */
+/* parallel on the host threads, each one exactly as orc_ppr runs it alone).  */
+/* inst_off[count+1] are the first global ids; seeds[count][K] local ids;     */
+/* instance i runs at most max_its[i] iterations (max_it when max_its is      */
+/* NULL); r[V][K] receives each instance's vectors at its global rows;        */
+/* iters[count] the iterations each ran.                                      */
+/* ------------------------------------------------------------------------ */
+void orc_ppr_batch(int count, const uint32_t *inst_off, const uint32_t *rowptr,
+                   const uint32_t *col, int K, const uint32_t *seeds, double alpha, int max_it,
+                   const int32_t *max_its, double tol, double *r, int32_t *iters,
+                   int nthreads) {
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#else
+    nthreads = 1;
+#endif
+    #pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+    for (int i = 0; i < count; i++) {
+        const uint32_t b = inst_off[i], n = inst_off[i + 1] - b;
+        const uint32_t e0 = rowptr[b], m = rowptr[b + n] - e0;
+        uint32_t *lrp = (uint32_t *)malloc(((size_t)n + 1) * sizeof(uint32_t));
+        uint32_t *lcl = (uint32_t *)malloc(((size_t)m + 1) * sizeof(uint32_t));
+        for (uint32_t v = 0; v <= n; v++) lrp[v] = rowptr[b + v] - e0;
+        for (uint32_t e = 0; e < m; e++) lcl[e] = col[e0 + e] - b;
+        iters[i] = orc_ppr(n, lrp, lcl, K, seeds + (size_t)i * K, alpha,
+                           max_its ? max_its[i] : max_it, tol, r + (size_t)b * K);
+        free(lrp);
+        free(lcl);
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Write a CSR as the text edge list CsrGraph::fromEdgeListFile reads        */
+/* (csrGraph.h:106-171): a '#' comment line, "V E", then "src dst" per edge   */
+/* in CSR order (sorted by source, as that loader requires).  Returns 0, or  */
+/* -1 when the file cannot be written.  Used to run the reference's own      */
+/* testBFS / testPageRank binaries on the benchmark graphs.                   */
+/* ------------------------------------------------------------------------ */
+static char *orc_utoa(char *p, uint64_t x) {
+    char t[24];
+    int n = 0;
+    do { t[n++] = (char)('0' + x % 10); x /= 10; } while (x);
+    while (n) *p++ = t[--n];
+    return p;
+}
+
+int orc_write_edge_list(const char *path, uint32_t V, const uint32_t *rowptr,
+                        const uint32_t *col) {
+    FILE *f = fopen(path, "wb");
+    if (!f) return -1;
+    const uint64_t E = rowptr[V];
+    fprintf(f, "# olive_b200 edge list\n%u %llu\n", V, (unsigned long long)E);
+    const size_t cap = 1 << 22;
+    char *buf = (char *)malloc(cap + 64);
+    size_t n = 0;
+    for (uint32_t u = 0; u < V; u++)
+        for (uint32_t e = rowptr[u]; e < rowptr[u + 1]; e++) {
+            char *p = buf + n;
+            p = orc_utoa(p, u);
+            *p++ = ' ';
+            p = orc_utoa(p, col[e]);
+            *p++ = '\n';
+            n = (size_t)(p - buf);
+            if (n >= cap) {
+                if (fwrite(buf, 1, n, f) != n) { free(buf); fclose(f); return -1; }
+                n = 0;
+            }
+        }
+    int rc = (n && fwrite(buf, 1, n, f) != n) ? -1 : 0;
+    free(buf);
+    if (fclose(f) != 0) rc = -1;
+    return rc;
 }

@@ -71,6 +71,14 @@ def lib():
         L.orc_ppr.restype = c.c_int
         L.orc_ppr.argtypes = [c.c_uint32, u32p, u32p, c.c_int, u32p, c.c_double, c.c_int,
                               c.c_double, f64p]
+        L.orc_sp_certificate.restype = c.c_uint64
+        L.orc_sp_certificate.argtypes = [c.c_uint32, u32p, u32p, u32p, c.c_uint32, u32p, c.c_int,
+                                         ctypes.POINTER(c.c_int)]
+        L.orc_ppr_batch.restype = None
+        L.orc_ppr_batch.argtypes = [c.c_int, u32p, u32p, u32p, c.c_int, u32p, c.c_double, c.c_int,
+                                    i32p, c.c_double, f64p, i32p, c.c_int]
+        L.orc_write_edge_list.restype = c.c_int
+        L.orc_write_edge_list.argtypes = [c.c_char_p, c.c_uint32, u32p, u32p]
         L.orc_wpr_forward.restype = None
         L.orc_wpr_forward.argtypes = [c.c_uint32, u32p, u32p, f64p, f64p, c.c_double, c.c_int,
                                       f64p]
@@ -260,6 +268,45 @@ def ppr(rowptr, col, seeds, alpha=0.85, max_it=50, tol=1e-7):
     return r.reshape(V, K), it
 
 
+def sp_certificate(rowptr, col, dist, src, w=None, threads=0):
+    """Check BFS levels (w None: unit weights) or SSSP distances by the
+    shortest-path certificate of orc_sp_certificate.  Returns None when the
+    certificate holds, else (vertex, reason)."""
+    rowptr, col = _u32(rowptr), _u32(col)
+    d = np.ascontiguousarray(dist).view(np.uint32) if np.asarray(dist).dtype.itemsize == 4 \
+        else _u32(dist)
+    V = len(rowptr) - 1
+    wp = None if w is None else _p(_u32(w), ctypes.c_uint32)
+    what = ctypes.c_int()
+    r = lib().orc_sp_certificate(V, _p(rowptr, ctypes.c_uint32), _p(col, ctypes.c_uint32), wp,
+                                 src, _p(d, ctypes.c_uint32), threads, ctypes.byref(what))
+    if r == 0:
+        return None
+    return int(r - 1), {1: "source not at 0", 2: "edge not relaxed",
+                        3: "no tight in-edge"}[what.value]
+
+
+def ppr_batch(rowptr, col, inst_off, seeds, alpha=0.85, max_it=50, tol=1e-7, threads=0):
+    """orc_ppr on every instance of a block-diagonal batch, instances in
+    parallel: (r [V, K] FP64, iterations [count]).  max_it may be an array of
+    per-instance iteration limits."""
+    rowptr, col, off = _u32(rowptr), _u32(col), _u32(inst_off)
+    seeds = _u32(seeds)
+    count, K = seeds.shape
+    V = int(off[-1])
+    r = np.empty((V, K), np.float64)
+    it = np.empty(count, np.int32)
+    per = None
+    if np.ndim(max_it):
+        per = np.ascontiguousarray(max_it, np.int32)
+        max_it = 0
+    lib().orc_ppr_batch(count, _p(off, ctypes.c_uint32), _p(rowptr, ctypes.c_uint32),
+                        _p(col, ctypes.c_uint32), K, _p(seeds, ctypes.c_uint32), alpha,
+                        int(max_it), None if per is None else _p(per, ctypes.c_int32), tol,
+                        _p(r, ctypes.c_double), _p(it, ctypes.c_int32), threads)
+    return r, it
+
+
 def wpr_forward(rowptr, col, w, p, alpha, iters):
     rowptr, col = _u32(rowptr), _u32(col)
     w = np.ascontiguousarray(w, np.float64)
@@ -358,6 +405,13 @@ def load_edge_list_sorted(path):
 
 def write_edge_list(path, rowptr, col, w=None):
     """Write CSR as a src-sorted edge-list file the reference loader reads."""
+    if w is None:   # the C writer (fast at 10^8 edges)
+        rowptr, col = _u32(rowptr), _u32(col)
+        rc = lib().orc_write_edge_list(str(path).encode(), len(rowptr) - 1,
+                                       _p(rowptr, ctypes.c_uint32), _p(col, ctypes.c_uint32))
+        if rc != 0:
+            raise OSError(f"cannot write {path}")
+        return
     V = len(rowptr) - 1
     E = len(col)
     src = np.repeat(np.arange(V, dtype=np.int64), np.diff(rowptr.astype(np.int64)))

@@ -189,3 +189,54 @@ def test_er_batch_restatement_properties():
     rp, col = oracle.er_batch_instance(0, 2, 8, 3)
     np.testing.assert_array_equal(rp, [0, 1, 2])
     np.testing.assert_array_equal(col, [1, 0])
+
+
+# ------------------------------------------- certificate, batched PPR, writer --
+def test_sp_certificate_accepts_exact_and_rejects_perturbed():
+    rp, cl = oracle.rmat_csr(12, 16, 3)
+    lv, _ = oracle.bfs(rp, cl, 0)
+    assert oracle.sp_certificate(rp, cl, lv, 0) is None
+    reached = np.flatnonzero((lv != oracle.INF) & (lv > 0))
+    for delta in (1, -1):
+        bad = lv.copy()
+        bad[reached[len(reached) // 2]] += delta
+        assert oracle.sp_certificate(rp, cl, bad, 0) is not None
+    w = oracle.uint_weights(len(cl), 5)
+    d, *_ = oracle.dijkstra(rp, cl, w, 0)
+    assert oracle.sp_certificate(rp, cl, d, 0, w) is None
+    bad = d.copy()
+    bad[np.flatnonzero(d == oracle.INF)[0]] = 7        # an unreachable vertex marked reached
+    assert oracle.sp_certificate(rp, cl, bad, 0, w)[1] == "no tight in-edge"
+    bad = d.copy()
+    bad[0] = 1
+    assert oracle.sp_certificate(rp, cl, bad, 0, w)[1] == "source not at 0"
+
+
+def test_ppr_batch_equals_per_instance_runs():
+    sizes = oracle.er_batch_sizes(5, 200, 900, 4)
+    parts = [oracle.er_batch_instance(i, int(n), 8, 4) for i, n in enumerate(sizes)]
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint32)
+    rp = [np.zeros(1, np.int64)]
+    base = 0
+    for lrp, _ in parts:
+        rp.append(lrp[1:].astype(np.int64) + base)
+        base += int(lrp[-1])
+    rp = np.concatenate(rp).astype(np.uint32)
+    cl = np.concatenate([lcl + off[i] for i, (_, lcl) in enumerate(parts)]).astype(np.uint32)
+    rng = np.random.default_rng(1)
+    seeds = np.stack([rng.integers(0, n, 8) for n in sizes]).astype(np.uint32)
+    r, it = oracle.ppr_batch(rp, cl, off, seeds, 0.85, 40, 1e-7)
+    for i, (lrp, lcl) in enumerate(parts):
+        ri, iti = oracle.ppr(lrp, lcl, seeds[i], 0.85, 40, 1e-7)
+        assert iti == it[i]
+        assert np.array_equal(ri, r[off[i]:off[i + 1]])
+    _, it2 = oracle.ppr_batch(rp, cl, off, seeds, 0.85, np.array([1, 2, 3, 4, 5]), 0.0)
+    assert list(it2) == [1, 2, 3, 4, 5]
+
+
+def test_edge_list_writer_round_trips_through_the_reference_loader(tmp_path):
+    rp, cl = oracle.rmat_csr(9, 8, 2)
+    path = str(tmp_path / "g.txt")
+    oracle.write_edge_list(path, rp, cl)
+    rp2, cl2 = oracle.load_edge_list_ref(path)[:2]
+    assert np.array_equal(rp2, rp) and np.array_equal(cl2, cl)
