@@ -10,7 +10,13 @@
  *   - an optional third column is stored in edgeValues (the reference
  *     parsed a constant 1 and never stored it);
  *   - the file is parsed from one buffered read instead of fscanf per line;
- *     ids >= V are reported and dropped instead of writing out of bounds.
+ *     ids >= V are reported and dropped instead of writing out of bounds;
+ *   - a file that starts with the 8 bytes "OLVCSR1\n" is a binary CSR dump
+ *     (no reference counterpart; text files of 10^8+ edges take minutes to
+ *     parse): uint64 V, uint64 E, uint64 flags (bit 0: uint32 edge values
+ *     follow), uint32 rowptr[V+1], uint32 col[E], [uint32 values[E]], all
+ *     little-endian.  The rows are taken as stored.  olv_graph_save and
+ *     olive_b200.write_csr_binary write it.
  * fromDimacsFile follows csrGraph.h:177-236: header "V E" with E undirected
  * (stored edges = 2E), then one line of 1-based neighbour ids per vertex;
  * '#' and '%' lines are comments; extra header fields are ignored.
@@ -20,6 +26,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <iostream>
 #include <vector>
 
@@ -112,6 +119,11 @@ public:
         }
         Stopwatch sw;
         sw.start();
+        if (fromBinary(fb, path)) {
+            LOG(INFO) << "It took " << sw.getElapsedMillis()
+                      << "ms to load the binary CSR graph.";
+            return;
+        }
         const char *p = fb.data.data();
         unsigned long long V = 0, E = 0;
         bool header = false;
@@ -233,6 +245,42 @@ public:
     }
 
 private:
+    // Binary CSR dump (see the file comment); false when the file is text.
+    bool fromBinary(const olive_detail::FileBuf &fb, const char *path) {
+        const size_t n = fb.data.size() - 1;   // FileBuf appends a terminator
+        const char *b = fb.data.data();
+        if (n < 32 || memcmp(b, "OLVCSR1\n", 8) != 0) return false;
+        unsigned long long hdr[3];
+        memcpy(hdr, b + 8, sizeof hdr);
+        const unsigned long long V = hdr[0], E = hdr[1], flags = hdr[2];
+        const unsigned long long need = 32 + 4 * (V + 1) + 4 * E * ((flags & 1) ? 2 : 1);
+        if (V >= 0xffffffffULL || E > 0xffffffffULL || n < need) {
+            LOG(ERROR) << "truncated or oversized binary CSR file: " << path;
+            return true;
+        }
+        initGraph((VertexId)V, (EdgeId)E);
+        memcpy(vertices, b + 32, 4 * (V + 1));
+        memcpy(edges, b + 32 + 4 * (V + 1), 4 * E);
+        if (flags & 1) {
+            const uint32_t *vals = reinterpret_cast<const uint32_t *>(b + 32 + 4 * (V + 1) + 4 * E);
+            for (unsigned long long e = 0; e < E; e++) edgeValues[e] = (EdgeValue)vals[e];
+        } else {
+            for (unsigned long long e = 0; e < E; e++) edgeValues[e] = EdgeValue(1);
+        }
+        bool ok = vertices[0] == 0 && vertices[V] == E;
+        for (unsigned long long v = 0; ok && v < V; v++) ok = vertices[v] <= vertices[v + 1];
+        for (unsigned long long e = 0; ok && e < E; e++) ok = edges[e] < V;
+        if (!ok) {
+            LOG(ERROR) << "invalid CSR in binary file " << path;
+            release();
+            vertexCount = 0;
+            edgeCount = 0;
+        } else {
+            LOG(INFO) << "Loaded binary CSR: " << V << " nodes, " << E << " edges";
+        }
+        return true;
+    }
+
     void buildFromTuples(VertexId V, const std::vector<VertexId> &src,
                          const std::vector<VertexId> &dst, const std::vector<EdgeValue> &val) {
         const size_t E = src.size();

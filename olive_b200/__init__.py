@@ -11,7 +11,7 @@ import os
 
 import numpy as np
 
-__all__ = ["Graph", "OliveError", "lib", "INF", "Stats"]
+__all__ = ["Graph", "OliveError", "lib", "INF", "Stats", "write_csr_binary"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libolive_b200.so")
@@ -23,6 +23,25 @@ DANGLING = {"uniform": 0, "leak": 1}
 
 class OliveError(RuntimeError):
     pass
+
+
+CSR_MAGIC = b"OLVCSR1\n"
+
+
+def write_csr_binary(path, rowptr, col, values=None):
+    """Write a binary CSR dump that CsrGraph::fromEdgeListFile (include/olive/
+    csrGraph.h) and olv_graph_load read: "OLVCSR1\\n", uint64 V, E, flags
+    (bit 0: uint32 edge values follow), uint32 rowptr[V+1], col[E], [values]."""
+    rowptr = np.ascontiguousarray(rowptr, np.uint32)
+    col = np.ascontiguousarray(col, np.uint32)
+    V, E = len(rowptr) - 1, len(col)
+    with open(path, "wb") as f:
+        f.write(CSR_MAGIC)
+        f.write(np.array([V, E, 0 if values is None else 1], np.uint64).tobytes())
+        rowptr.tofile(f)
+        col.tofile(f)
+        if values is not None:
+            np.ascontiguousarray(values, np.uint32).tofile(f)
 
 
 class Stats(ctypes.Structure):
