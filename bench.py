@@ -3,33 +3,52 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload sssp|bfs|pagerank|msbfs|wpr|batch] [--scale S]
+                    [--no-extras] [--no-parity]
 
 Default workload: single-source shortest paths (frontier Bellman-Ford with
 atomicMin, SSSP.cu semantics) on an RMAT graph of scale 24, edge factor 16,
 (a,b,c,d) = (.57,.19,.19,.05), uint32 weights uniform in [1,255], from the
 highest out-degree vertex.  A step is one complete solve on the resident
 graph.  The metric is GTEPS = (sum of out-degrees of reached vertices) / time.
-BFS on the same graph is measured in the same run and reported under "bfs".
+The default line also carries, as extra keys, BFS on the same graph ("bfs"),
+64-source BFS on RMAT-24 ("msbfs"), PageRank on RMAT-22 ("pagerank"),
+weighted PageRank forward + adjoint on RMAT-20 ("wpr") and the 512-graph ER
+batch ("batch"), each with its own timing, roofline fraction and parity check.
+
+Parity: every line checks the GPU result of its last step against the CPU
+oracle on rank 0 ("parity" key): SSSP against a complete serial Dijkstra,
+BFS against the restated testBFS queue BFS, msBFS rows against 64 solo GPU
+runs and the oracle, PageRank / weighted PageRank against the FP64 oracle
+after the same iterations, the batch against per-instance oracle runs.
 
 One process per GPU (torchrun); every rank runs its own replica of the
 workload (the traversal does not shard: "replicas only"), `value` sums the
-ranks' edges over the slowest rank's time.  Rank 0 prints one JSON line.
+ranks' work over the slowest rank's time.  Rank 0 prints one JSON line.
 
---impl reference times the reference's algorithm on the host cores: the
-CPU restatement of SSSP.cu's frontier Bellman-Ford (all host threads), of
-testBFS.cu's queue BFS (once per source for msbfs), or of testPageRank.cu's
-FP64 PageRank, on the same synthetic graph built on the host; for wpr and
-batch, which have no reference counterpart, the oracle's FP64 weighted
-PageRank and BFS + PPR-32 per instance on the same inputs.  Each step's
-sample is bounded by --ref-seconds.
+--impl reference times the reference's algorithm on the host cores:
+* sssp: the CPU restatement of SSSP.cu's frontier Bellman-Ford on all host
+  threads (the reference has no CPU SSSP), value = E_reached / t as for the
+  GPU arm (edges scanned, which include re-relaxations, reported beside it);
+* bfs: the reference's own testBFS binary (oracle/_ref, built unmodified from
+  the reference sources) on a written edge-list file up to scale 22; above
+  that (the text file passes 3 GB) the restatement of testBFS.cu:64-79;
+* pagerank: the reference's own testPageRank binary with -max 50 (its loop
+  timer; the file parse is excluded);
+* msbfs: the testBFS restatement once per source;
+* wpr, batch (no reference counterpart): the oracle's FP64 weighted PageRank
+  and BFS + PPR-32 per instance on the same inputs.
+Each step's sample is bounded by --ref-seconds (the reference binaries run as
+many whole solves as fit in about two minutes).
 """
 import argparse
+import copy
 import json
 import os
+import re
+import shutil
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -54,13 +73,20 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="bound of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default workload: skip the msbfs/pagerank/wpr/batch extra keys")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle comparison")
     ap.add_argument("--ref-seconds", type=float, default=8.0,
                     help="--impl reference: bound of one step's CPU sample")
     a = ap.parse_args()
     if a.scale is None:
-        a.scale = {"pagerank": 22, "wpr": 20, "batch": 0}.get(a.workload, 24)
+        a.scale = default_scale(a.workload)
     a.warmup = max(a.warmup, 3) if a.impl == "ours" else a.warmup
     return a
+
+
+def default_scale(w):
+    return {"pagerank": 22, "wpr": 20, "batch": 0}.get(w, 24)
 
 
 def metric_name(w, scale):
@@ -109,8 +135,7 @@ def peaks():
 
 # Committed ncu launch-list summaries (profiles/*.md) of each default workload:
 # their `traffic_bytes` line is the DRAM read + write of one solve as the
-# profiler measured it (sum over the solve's launches; ncu flushes the caches
-# before each launch, so this is a cold-cache upper bound of the warm run).
+# profiler measured it (see each file for how it was taken and scaled).
 PROFILE_OF = {("sssp", 24): "sssp_rmat24.md", ("bfs", 24): "bfs_rmat24.md",
               ("pagerank", 22): "pagerank_rmat22.md", ("msbfs", 24): "msbfs_rmat24.md",
               ("wpr", 20): "wpr_rmat20.md", ("batch", 0): "batch_er512.md"}
@@ -125,8 +150,7 @@ def profile_traffic(workload, scale, seed, key="traffic_bytes"):
         return None, None
     for line in open(path):
         if line.startswith(key + ":"):
-            return int(float(line.split(":", 1)[1].split()[0])), (
-                f"profiles/{name} ({key}: ncu launch list, cold cache per launch)")
+            return int(float(line.split(":", 1)[1].split()[0])), f"profiles/{name} ({key})"
     return None, None
 
 
@@ -151,6 +175,7 @@ class ClockSampler:
         except Exception:
             self.proc = None
         self.t0 = time.time()
+        time.sleep(0.3)   # let the sampler start before the timed region
 
     def stop(self):
         if self.proc is None:
@@ -182,15 +207,102 @@ class ClockSampler:
                 "power_w_max": max(pw) if pw else None}
 
 
-# ----------------------------------------------------------------- ours --
-def run_ours(a, rank, world, local_rank):
+# ------------------------------------------------------------- helpers --
+def timed(stream, fn, steps):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def max_over_ranks(x, world):
     import torch
     import torch.distributed as dist
-    torch.cuda.set_device(local_rank)
+    t = torch.tensor([x], device="cuda")
     if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local_rank))
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def common_line(a, world, metric_unit, value, ms, dtype, data, config, roofline, cpu, e2e,
+                launches, clk, extra):
+    line = {"metric": metric_name(a.workload, a.scale), "value": round(value, 3),
+            "unit": metric_unit, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": dtype, "data": data, "config": config,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clk}
+    line.update(extra)
+    return line
+
+
+def rel_err(got, ref):
+    got = np.asarray(got, np.float64)
+    return float(np.max(np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300))) if len(ref) else 0.0
+
+
+# ------------------------------------------------------------- parity --
+def parity_exact(got, ref, vs):
+    got = np.asarray(got).view(np.uint32)
+    ref = np.asarray(ref).view(np.uint32)
+    mism = int(np.count_nonzero(got != ref))
+    return {"checked": True, "vs": vs, "compared": int(len(ref)), "mismatches": mism,
+            "pass": mism == 0}
+
+
+def parity_float(err, tol, vs, extra=None):
+    d = {"checked": True, "vs": vs, "max_rel_err": err, "tolerance": tol, "pass": err < tol}
+    if extra:
+        d.update(extra)
+    return d
+
+
+def cold_e2e(ob, stream, rp, cl, w, src, method, reps=2):
+    """A caller that arrives with a host CSR: olv_graph_create (upload, reverse
+    graph built on the device), then the first solve into a pinned host
+    buffer, then olv_graph_destroy -- all inside the wall-clock region."""
+    import torch
+    rp_p = torch.from_numpy(rp.view(np.int32)).pin_memory()
+    cl_p = torch.from_numpy(cl.view(np.int32)).pin_memory()
+    w_p = None if w is None else torch.from_numpy(w.view(np.int32)).pin_memory()
+    host = torch.empty(len(rp) - 1, dtype=torch.int32, pin_memory=True)
+    best = None
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        # int32 tensors carry the uint32 bits; integer weights become OLV_W_U32
+        g = ob.Graph.from_csr(rp_p, cl_p) if w is None else ob.Graph.from_csr(rp_p, cl_p, w_p)
+        g.set_stream(stream)
+        getattr(g, method)(src, out=host)
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3
+        st = g.last_stats
+        g.close()
+        best = ms if best is None else min(best, ms)
+    h2d = rp.nbytes + cl.nbytes + (0 if w is None else w.nbytes)
+    return {"value": round(st.edges_traversed / (best * 1e-3) / 1e9, 3), "unit": "GTEPS",
+            "ms": round(best, 2), "h2d_bytes": int(h2d), "d2h_bytes": int(4 * (len(rp) - 1)),
+            "note": "host CSR in pinned memory -> olv_graph_create (upload + reverse graph on "
+                    "the device) -> first solve (per-graph structures built) -> pinned host "
+                    "result -> olv_graph_destroy; wall clock, best of %d" % reps}
+
+
+# ------------------------------------------------- traversal workloads --
+def traversal_line(a, rank, world, local_rank, extra_keys=True):
+    """SSSP / BFS / msBFS / PageRank on a seeded RMAT graph built on the device."""
+    import torch
     import olive_b200 as ob
 
     stream = torch.cuda.current_stream()
@@ -223,15 +335,11 @@ def run_ours(a, rank, world, local_rank):
     for _ in range(a.warmup):
         step(out)
     torch.cuda.synchronize()
-    st = g.last_stats
-    if world > 1:
-        dist.barrier()
+    barrier(world)
     clocks = ClockSampler(local_rank)
     clocks.start()
-    time.sleep(0.3)   # let the sampler start before the timed region
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    barrier(world)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -241,15 +349,11 @@ def run_ours(a, rank, world, local_rank):
         dev_ms.append(g.last_stats.device_ms)
     e1.record(stream)
     torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    barrier(world)
     ms = e0.elapsed_time(e1) / a.steps
     clk = clocks.stop()
     st = g.last_stats
-    t_ms = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t_ms, op=dist.ReduceOp.MAX)
-    ms_max = float(t_ms.item())
+    ms_max = max_over_ranks(ms, world)
 
     if a.workload == "pagerank":
         units = E * st.iterations                    # edge visits per solve
@@ -281,6 +385,8 @@ def run_ours(a, rank, world, local_rank):
                 "kernel": f"whole {a.workload} solve (all kernels of one call, CUDA graph)",
                 "algorithmic_bytes": int(alg_bytes), "bytes_formula": bytes_formula,
                 "peak_source": peak_src, "kernel_ms": round(kern_ms, 4)}
+    if traffic:
+        roofline["traffic_over_algorithmic"] = round(traffic / alg_bytes, 3)
 
     # launches of our kernels per step (kernel nodes executed by the graph):
     # sssp: fill, init, 4 per superstep, the map back to the caller's ids
@@ -308,11 +414,7 @@ def run_ours(a, rank, world, local_rank):
     x1.record(stream)
     torch.cuda.synchronize()
     wall_ms = (time.perf_counter() - t_wall) * 1e3 / a.steps
-    e2e_ms = max(x0.elapsed_time(x1) / a.steps, wall_ms)
-    t_e = torch.tensor([e2e_ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t_e, op=dist.ReduceOp.MAX)
-    e2e_ms = float(t_e.item())
+    e2e_ms = max_over_ranks(max(x0.elapsed_time(x1) / a.steps, wall_ms), world)
     e2e = {"value": round(world * units / (e2e_ms * 1e-3) / 1e9, 3), "unit": unit,
            "h2d_bytes_per_step": 256 if a.workload == "msbfs" else 0,
            "d2h_bytes_per_step": int(out.numel() * 4),
@@ -321,6 +423,13 @@ def run_ours(a, rank, world, local_rank):
                    "source id passed by value; graph resident as after Oliver::readGraph"}
 
     extra = {}
+    check = rank == 0 and not a.no_parity
+    from oracle import oracle
+    rp = cl = w = None
+    if check or (rank == 0 and world == 1 and not a.no_cpu_baseline) or \
+            (a.workload in ("sssp", "bfs") and extra_keys):
+        rp, cl, w = g.csr()
+    ref_info = None
     if a.workload == "msbfs":
         # the same 64 sources as 64 sequential plain BFS runs
         lv = torch.empty(V, dtype=torch.int32, device="cuda")
@@ -340,9 +449,36 @@ def run_ours(a, rank, world, local_rank):
         seq_gteps = seq_edges / (seq_ms * 1e-3) / 1e9
         extra["sequential_plain"] = {"value": round(seq_gteps, 3), "unit": "GTEPS",
                                      "ms_for_64": round(seq_ms, 3),
-                                     "speedup_of_batched": round(value / world / seq_gteps, 2)}
+                                     "speedup_of_batched": round(value / world / seq_gteps, 2),
+                                     "target": ">= 10x"}
+        if check:
+            bad = 0
+            for s, s0 in enumerate(src):
+                g.bfs(s0, out=lv)
+                bad += int(not torch.equal(out[s], lv))
+            orows = [0, 63]
+            obad = 0
+            for s in orows:
+                ref, _ = oracle.bfs(rp, cl, src[s])
+                obad += int(np.count_nonzero(out[s].cpu().numpy() != ref))
+            extra["parity"] = {"checked": True, "vs": "64 solo GPU BFS runs (every row) and "
+                               "the oracle BFS (rows 0 and 63)", "rows_differing_from_solo": bad,
+                               "oracle_mismatches": obad, "pass": bad == 0 and obad == 0}
+    elif check and a.workload == "sssp":
+        ref, e_ref, secs, nset = oracle.dijkstra(rp, cl, w, src)
+        extra["parity"] = parity_exact(out.cpu().numpy(), ref,
+                                       "serial binary-heap Dijkstra (complete)")
+        ref_info = (e_ref, secs, nset)
+    elif check and a.workload == "bfs":
+        ref, _ = oracle.bfs(rp, cl, src)
+        extra["parity"] = parity_exact(out.cpu().numpy(), ref, "testBFS.cu:64-79 restated")
+    elif check:
+        it = st.iterations
+        ref, it_ref, _ = oracle.pagerank(rp, cl, 0.85, it, 0.0)
+        extra["parity"] = parity_float(rel_err(out.cpu().numpy(), ref), 1e-6,
+                                       f"FP64 oracle after the same {it} iterations")
     # BFS on the same graph, reported beside the SSSP headline
-    if a.workload == "sssp":
+    if a.workload == "sssp" and extra_keys:
         lv = torch.empty(V, dtype=torch.int32, device="cuda")
         for _ in range(3):
             g.bfs(src, out=lv)
@@ -356,38 +492,45 @@ def run_ours(a, rank, world, local_rank):
         extra["bfs"] = {"metric": metric_name("bfs", a.scale), "value": round(
             bs.edges_traversed / (bms * 1e-3) / 1e9, 2), "unit": "GTEPS", "ms": round(bms, 4),
             "levels": bs.iterations, "pull_levels": bs.pull_steps,
-            "roofline_frac": round(bbytes / (bms * 1e-3) / 1e9 / peak, 4)}
+            "roofline_frac": round(bbytes / (bms * 1e-3) / 1e9 / peak, 4),
+            "roofline_note": "8 B per edge of the reached set (a TEPS normalisation: the pull "
+                             "levels stop at the first visited parent and read fewer edges)"}
+        btraffic, _ = profile_traffic("bfs", a.scale, a.seed)
+        if btraffic:
+            extra["bfs"]["dram_frac"] = round(btraffic / (bms * 1e-3) / 1e9 / peak, 4)
+            extra["bfs"]["dram_note"] = "profiled DRAM bytes of one solve / solve time / peak"
+        if check:
+            ref, _ = oracle.bfs(rp, cl, src)
+            extra["bfs"]["parity"] = parity_exact(lv.cpu().numpy(), ref,
+                                                  "testBFS.cu:64-79 restated")
+    if a.workload in ("sssp", "bfs") and extra_keys and rank == 0:
+        method = "sssp" if a.workload == "sssp" else "bfs"
+        extra["e2e_cold"] = cold_e2e(ob, stream, rp, cl, w if weights else None, src, method)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cpu = cpu_baseline(a, g, src, st)
+        cpu = cpu_baseline(a, rp, cl, w, src, st, ref_info)
 
-    line = {"metric": metric_name(a.workload, a.scale), "value": round(value, 3), "unit": unit,
-            "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_max, 4),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32" if a.workload == "pagerank" else ("u32" if weights else "i32"),
-            "data": "synthetic (seeded RMAT, generated on the device)",
-            "config": workload_config(a, V, E, src, {
-                "iterations": st.iterations, "vertices_reached": st.vertices_reached,
-                "edges_traversed": st.edges_traversed, "edges_relaxed": st.edges_relaxed}),
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk}
-    line.update(extra)
+    config = workload_config(a, V, E, src, {
+        "iterations": st.iterations, "vertices_reached": st.vertices_reached,
+        "edges_traversed": st.edges_traversed, "edges_relaxed": st.edges_relaxed})
+    dtype = "f32" if a.workload == "pagerank" else ("u32" if weights else "i32")
+    line = common_line(a, world, unit, value, ms_max, dtype,
+                       "synthetic (seeded RMAT, generated on the device)", config, roofline, cpu,
+                       e2e, launches, clk, extra)
     g.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line
 
 
-def cpu_baseline(a, g, src, st):
+def cpu_baseline(a, rp, cl, w, src, st, ref_info=None):
     """The oracle (CPU restatement of the reference's algorithm) on a bounded
     sample of the same workload, one host core."""
     from oracle import oracle
-    rp, cl, w = g.csr()
     if a.workload == "sssp":
-        _, edges, secs, settled = oracle.dijkstra(rp, cl, w, src, a.cpu_seconds)
+        if ref_info is not None:    # the complete Dijkstra the parity check already timed
+            edges, secs, settled = ref_info
+        else:
+            _, edges, secs, settled = oracle.dijkstra(rp, cl, w, src, a.cpu_seconds)
         done = settled == st.vertices_reached
         return {"value": round(edges / secs / 1e9, 5), "unit": "GTEPS", "cores": 1,
                 "kind": "port",
@@ -424,60 +567,23 @@ def cpu_baseline(a, g, src, st):
                       f"redistribution), {it} iterations on the same graph, {secs:.2f} s"}
 
 
-def common_line(a, world, metric_unit, value, ms, dtype, data, config, roofline, cpu, e2e,
-                launches, clk, extra):
-    line = {"metric": metric_name(a.workload, a.scale), "value": round(value, 3),
-            "unit": metric_unit, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": dtype, "data": data, "config": config,
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clk}
-    line.update(extra)
-    return line
-
-
-def timed(stream, fn, steps):
-    import torch
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(steps):
-        fn()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    return e0.elapsed_time(e1) / steps
-
-
-def max_over_ranks(x, world):
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def run_wpr(a, rank, world, local_rank):
+# ------------------------------------------------------ weighted PageRank --
+def wpr_line(a, rank, world, local_rank):
     """Weighted PageRank forward + adjoint on RMAT-20 (lognormal FP32 weights,
     Dirichlet(1) personalisation, g ~ N(0,1)); a step is one forward and one
     backward solve of 100 sweeps each."""
     import torch
-    import torch.distributed as dist
-    torch.cuda.set_device(local_rank)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local_rank))
     import olive_b200 as ob
     stream = torch.cuda.current_stream()
     g = ob.Graph.rmat(a.scale, 16, a.seed)
     g.set_stream(stream)
     V, E = g.V, g.E
     rng = np.random.default_rng(7)
-    w = torch.from_numpy(rng.lognormal(0.0, 1.0, E).astype(np.float32)).cuda()
+    w_np = rng.lognormal(0.0, 1.0, E).astype(np.float32)
+    w = torch.from_numpy(w_np).cuda()
     pn = rng.exponential(1.0, V)
-    p = torch.from_numpy((pn / pn.sum()).astype(np.float32)).cuda()
+    p_np = (pn / pn.sum()).astype(np.float32)
+    p = torch.from_numpy(p_np).cuda()
     gv = torch.from_numpy(rng.standard_normal(V).astype(np.float32)).cuda()
     r = torch.empty(V, dtype=torch.float32, device="cuda")
     dw = torch.empty(E, dtype=torch.float32, device="cuda")
@@ -496,13 +602,10 @@ def run_wpr(a, rank, world, local_rank):
         bwd()
     clocks = ClockSampler(local_rank)
     clocks.start()
-    time.sleep(0.3)
-    if world > 1:
-        dist.barrier()
+    barrier(world)
     ms_f = max_over_ranks(timed(stream, fwd, a.steps), world)
     ms_b = max_over_ranks(timed(stream, bwd, a.steps), world)
     clk = clocks.stop()
-    fs = g.last_stats
     units = E * it
     value = world * units / (ms_f * 1e-3) / 1e9
     peak, peak_src = peaks()
@@ -533,13 +636,21 @@ def run_wpr(a, rank, world, local_rank):
            "h2d_bytes_per_step": 8 * V, "d2h_bytes_per_step": 4 * (E + 2 * V),
            "ms_per_step": round(e2e_ms, 3),
            "note": "forward + backward through olv_wpr_* with pinned host p, g, r, dw, dp"}
+    extra = {"fwd_bwd_over_fwd": round((ms_f + ms_b) / ms_f, 3),
+             "target": "forward+adjoint <= 3x forward"}
+    from oracle import oracle
+    rp = cl = None
+    if rank == 0 and (not a.no_parity or (world == 1 and not a.no_cpu_baseline)):
+        rp, cl, _ = g.csr()
+    if rank == 0 and not a.no_parity:
+        ref = oracle.wpr_forward(rp, cl, w_np.astype(np.float64), p_np.astype(np.float64), 0.85,
+                                 it)
+        extra["parity"] = parity_float(rel_err(host_r.numpy(), ref), 1e-5,
+                                       f"FP64 oracle forward, {it} sweeps (per-vertex relative)")
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        from oracle import oracle
-        rp, cl, _ = g.csr()
-        w64 = w.double().cpu().numpy()
         t = time.perf_counter()
-        rr = oracle.wpr_forward(rp, cl, w64, p.double().cpu().numpy(), 0.85, 3)
+        oracle.wpr_forward(rp, cl, w_np.astype(np.float64), p_np.astype(np.float64), 0.85, 3)
         secs = time.perf_counter() - t
         cpu = {"value": round(E * 3 / secs / 1e9, 5), "unit": "GE/s/iter", "cores": 1,
                "kind": "port", "sample": f"FP64 weighted PageRank forward (oracle), 3 sweeps, "
@@ -548,30 +659,19 @@ def run_wpr(a, rank, world, local_rank):
     config = workload_config(a, V, E, None, {
         "weights": "lognormal(0,1) FP32, numpy seed 7", "p": "Dirichlet(1)", "g": "N(0,1)",
         "alpha": 0.85, "sweeps": it, "forward_ms": round(ms_f, 3), "backward_ms": round(ms_b, 3)})
-    extra = {"fwd_bwd_over_fwd": round((ms_f + ms_b) / ms_f, 3),
-             "target": "forward+adjoint <= 3x forward"}
     line = common_line(a, world, "GE/s/iter", value, ms_f + ms_b, "f32",
                        "synthetic (seeded RMAT on the device, numpy weights)", config, roofline,
                        cpu, e2e, launches * a.steps, clk, extra)
     g.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line
 
 
-def run_batch(a, rank, world, local_rank):
+# ---------------------------------------------------------------- batch --
+def batch_line(a, rank, world, local_rank):
     """512 ER digraphs packed block-diagonally; a step is one persistent launch
     running BFS from local vertex 0 and K=32 PPR vectors (max 50 iterations,
     tol 1e-7) for every graph."""
     import torch
-    import torch.distributed as dist
-    torch.cuda.set_device(local_rank)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local_rank))
     import olive_b200 as ob
     stream = torch.cuda.current_stream()
     count, K = 512, 32
@@ -589,12 +689,9 @@ def run_batch(a, rank, world, local_rank):
 
     for _ in range(a.warmup):
         step()
-    st = g.last_stats
     clocks = ClockSampler(local_rank)
     clocks.start()
-    time.sleep(0.3)
-    if world > 1:
-        dist.barrier()
+    barrier(world)
     ms = max_over_ranks(timed(stream, step, a.steps), world)
     clk = clocks.stop()
     st = g.last_stats
@@ -609,7 +706,11 @@ def run_batch(a, rank, world, local_rank):
                 "traffic": traffic, "traffic_source": traffic_src,
                 "kernel": "k_batch (one persistent launch)", "algorithmic_bytes": int(alg),
                 "bytes_formula": "8 B/BFS edge + 4 B per PPR edge-vector visit (128 B row per "
-                                 "in-edge for K=32) + (4 + 8K) B/vertex"}
+                                 "in-edge for K=32) + (4 + 8K) B/vertex",
+                "note": "the PPR row gathers mostly hit L2 (the instances in flight fit it), so "
+                        "the algorithmic bytes exceed the DRAM traffic"}
+    if traffic:
+        roofline["dram_frac"] = round(traffic / (ms * 1e-3) / 1e9 / peak, 4)
     host_lv = torch.empty(V, dtype=torch.int32, pin_memory=True)
     host_pr = torch.empty((V, K), dtype=torch.float32, pin_memory=True)
     t0 = time.perf_counter()
@@ -619,10 +720,33 @@ def run_batch(a, rank, world, local_rank):
     e2e = {"value": round(world * visits / (e2e_ms * 1e-3) / 1e9, 3), "unit": "G visits/s",
            "h2d_bytes_per_step": int(4 * (count + 1) + seeds.nbytes),
            "d2h_bytes_per_step": int(4 * V * (1 + K)), "ms_per_step": round(e2e_ms, 3)}
+    from oracle import oracle
+    extra = {}
+    rp = cl = None
+    if rank == 0 and (not a.no_parity or (world == 1 and not a.no_cpu_baseline)):
+        rp, cl, _ = g.csr()
+    if rank == 0 and not a.no_parity:
+        hlv, hpr = host_lv.numpy(), host_pr.numpy()
+        bfs_bad = 0
+        for i in range(count):
+            b, e = int(off[i]), int(off[i + 1])
+            lrp = (rp[b:e + 1] - rp[b]).astype(np.uint32)
+            lcl = (cl[rp[b]:rp[e]] - b).astype(np.uint32)
+            ref, _ = oracle.bfs(lrp, lcl, 0)
+            bfs_bad += int(np.count_nonzero(hlv[b:e] != ref))
+        m = 64   # PPR of the first 64 instances (all 512 in tests/test_gpu_fullsize.py)
+        pref, pit = oracle.ppr_batch(rp, cl, off[:m + 1], seeds[:m], 0.85,
+                                     iters[:m].astype(np.int32), 0.0)
+        b = int(off[m])
+        diff = np.abs(hpr[:b].astype(np.float64) - pref[:b])
+        ok = bool(np.all(diff <= 2e-5 * np.abs(pref[:b]) + 2e-7))
+        extra["parity"] = {"checked": True, "vs": "oracle BFS per instance (all 512) and FP64 "
+                           f"PPR-32 after the same iterations (first {m} instances)",
+                           "bfs_mismatches": bfs_bad, "ppr_max_abs_err": float(diff.max()),
+                           "ppr_tolerance": "|d| <= 2e-5 |ref| + 2e-7",
+                           "pass": bfs_bad == 0 and ok and bool(np.all(pit == iters[:m]))}
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        from oracle import oracle
-        rp, cl, _ = g.csr()
         t = time.perf_counter()
         done, cvis = 0, 0
         for i in range(count):
@@ -646,16 +770,63 @@ def run_batch(a, rank, world, local_rank):
               "l2": "inputs larger than L2 (PPR state 2 x V x 128 B = 4.3 GB)"}
     line = common_line(a, world, "G visits/s", value, ms, "f32+i32",
                        "synthetic (seeded ER batch generated on the host)", config, roofline,
-                       cpu, e2e, a.steps, clk, {})
+                       cpu, e2e, a.steps, clk, extra)
     g.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    return line
+
+
+# ------------------------------------------------------- default extras --
+def extras(a, rank, world, local_rank):
+    """The other benchmarked configurations, each as a compact summary in the
+    default line: msBFS-64 on RMAT-24, PageRank on RMAT-22, weighted PageRank
+    forward + adjoint on RMAT-20, the ER-512 batch."""
+    out = {}
+    for w in ("msbfs", "pagerank", "wpr", "batch"):
+        b = copy.copy(a)
+        b.workload, b.scale = w, default_scale(w)
+        b.steps, b.warmup = min(a.steps, 10), 3
+        b.no_cpu_baseline = True
+        fn = {"wpr": wpr_line, "batch": batch_line}.get(w, traversal_line)
+        ln = fn(b, rank, world, local_rank) if fn is not traversal_line else \
+            traversal_line(b, rank, world, local_rank, extra_keys=False)
+        s = {"metric": ln["metric"], "value": ln["value"], "unit": ln["unit"],
+             "ms_per_step": ln["ms_per_step"], "steps": b.steps,
+             "roofline_frac": ln["roofline"]["frac"], "clocks": ln["clocks"],
+             "e2e": {k: ln["e2e"][k] for k in ("value", "unit", "ms_per_step")}}
+        for k in ("sequential_plain", "fwd_bwd_over_fwd", "target", "parity"):
+            if k in ln:
+                s[k] = ln[k]
+        if "dram_frac" in ln["roofline"]:
+            s["dram_frac"] = ln["roofline"]["dram_frac"]
+        if w == "msbfs":
+            s["target"] = ">= 10x the aggregate GTEPS of 64 sequential plain runs"
+        out[w] = s
+    return out
 
 
 # ------------------------------------------------------------ reference --
+def _ref_binary(name):
+    p = os.path.join(ROOT, "oracle", "_ref", name)
+    return p if os.path.exists(p) else None
+
+
+def _run_ref_binary(cmd, cwd, budget_s, steps):
+    """Run a reference checker binary up to `steps` times within budget_s;
+    returns the loop times (ms) its own timer printed and the last stderr."""
+    times, err, t0 = [], "", time.perf_counter()
+    for _ in range(max(steps, 1)):
+        p = subprocess.run(cmd, cwd=cwd, capture_output=True, text=True)
+        if p.returncode != 0:
+            raise RuntimeError(f"{cmd[0]} failed: {p.stderr[-500:]}")
+        err = p.stderr
+        m = re.findall(r"time=?:?\s*([0-9.]+)\s*ms", err)
+        if m:
+            times.append(float(m[-1]))
+        if time.perf_counter() - t0 > budget_s:
+            break
+    return times, err
+
+
 def run_reference(a, rank, world):
     if rank != 0:
         return
@@ -663,6 +834,7 @@ def run_reference(a, rank, world):
     threads = oracle.max_threads()
     bound = a.ref_seconds
     vals, ms = [], []
+    extra = {}
     if a.workload == "batch":
         # the same 512 ER instances and PPR seeds as the GPU arm (the oracle's
         # restatement of the batch generator), BFS from local vertex 0 plus
@@ -706,20 +878,30 @@ def run_reference(a, rank, world):
         return
     rp, cl = oracle.rmat_csr_par(a.scale, 16, a.seed, threads)
     V, E = len(rp) - 1, len(cl)
-    src = int(np.argmax(np.diff(rp.astype(np.int64))))
+    deg = np.diff(rp.astype(np.int64))
+    src = int(np.argmax(deg))
+    kind = "port"
     if a.workload == "sssp":
         w = oracle.uint_weights_par(E, 2, 1, 255, threads)
         desc = (f"CPU restatement of SSSP.cu's frontier Bellman-Ford (edgeFilter atomicMin + "
                 f"vertexFilter supersteps, oliver.h:56-113) on {threads} OpenMP threads; each "
-                f"step a full solve or stopped after {bound:.0f} s; value = edges scanned / s")
+                f"step a full solve (stopped after {max(bound, 60.0):.0f} s at most); value = "
+                f"E_reached / t as for the GPU arm (sum of out-degrees of reached vertices)")
+        scanned = []
         for i in range(a.warmup + a.steps):
-            _, edges, secs, rounds = oracle.sssp_frontier(rp, cl, w, src, threads, bound)
+            dist, edges, secs, rounds = oracle.sssp_frontier(rp, cl, w, src, threads,
+                                                             max(bound, 60.0))
             if i >= a.warmup:
-                vals.append(edges / secs / 1e9)
+                e_reached = int(deg[dist != INF].sum())
+                vals.append(e_reached / secs / 1e9)
+                scanned.append(edges / secs / 1e9)
                 ms.append(secs * 1e3)
+        extra["edges_scanned_rate"] = {"value": round(float(np.median(scanned)), 5),
+                                       "unit": "G edges scanned/s",
+                                       "note": "frontier Bellman-Ford re-relaxes edges; this "
+                                               "counts every scan"}
         unit, cores = "GTEPS", threads
     elif a.workload == "msbfs":
-        deg = np.diff(rp.astype(np.int64))
         srcs = np.random.default_rng(4).choice(np.flatnonzero(deg > 0), 64, replace=False)
         desc = ("restatement of testBFS.cu:64-79 (serial queue BFS, 1 core) run once per source; "
                 f"each step the 64 sources in turn, stopped after {bound:.0f} s")
@@ -735,9 +917,45 @@ def run_reference(a, rank, world):
                 vals.append(edges / secs / 1e9)
                 ms.append(secs * 1e3)
         unit, cores = "GTEPS", 1
+    elif a.workload in ("bfs", "pagerank") and _ref_binary(
+            "testBFS" if a.workload == "bfs" else "testPageRank") and a.scale <= 22:
+        # the reference's own serial checker, built unmodified from its sources
+        name = "testBFS" if a.workload == "bfs" else "testPageRank"
+        exe = _ref_binary(name)
+        work = tempfile.mkdtemp(prefix="olv_ref_")
+        path = os.path.join(work, "graph.txt")
+        t = time.perf_counter()
+        oracle.write_edge_list(path, rp, cl)
+        write_s = time.perf_counter() - t
+        fsize = os.path.getsize(path)
+        if a.workload == "bfs":
+            cmd = [exe, path, "-s", str(src)]
+            _, e_reached = oracle.bfs(rp, cl, src)
+            units_per_run = e_reached
+        else:
+            cmd = [exe, path, "-max", "50"]
+        times, err = _run_ref_binary(cmd, work, 120.0, a.warmup + a.steps)
+        if a.workload == "pagerank":
+            it = int(re.findall(r"iterations:\s*(\d+)", err)[-1])
+            sweeps = min(it + 1, 50)   # it breaks before counting the converged sweep
+            units_per_run = E * sweeps
+        runs = times[a.warmup:] if len(times) > a.warmup else times
+        vals = [units_per_run / (t_ * 1e-3) / 1e9 for t_ in runs]
+        ms = runs
+        kind = "reference"
+        unit, cores = ("GTEPS" if a.workload == "bfs" else "GE/s/iter"), 1
+        desc = (f"oracle/_ref/{name} (the reference's serial checker compiled unmodified from "
+                f"its sources), {' '.join(os.path.basename(c) for c in cmd[1:])}; its own loop "
+                f"timer (file parse excluded); {len(runs)} timed runs after "
+                f"{len(times) - len(runs)} warm-up; edge-list file {fsize / 1e6:.0f} MB written "
+                f"in {write_s:.1f} s" + ("" if a.workload == "bfs" else
+                                         "; no dangling redistribution (testPageRank.cu)"))
+        shutil.rmtree(work, ignore_errors=True)
     elif a.workload == "bfs":
         desc = ("restatement of testBFS.cu:64-79 (the reference's serial queue BFS; 1 core); "
-                f"each step a full traversal or stopped after {bound:.0f} s")
+                f"each step a full traversal or stopped after {bound:.0f} s; the reference "
+                f"binary is not run at this scale: its text edge list would be "
+                f"{E * 19 / 1e9:.1f} GB and take minutes to parse per run")
         for i in range(a.warmup + a.steps):
             edges, secs, _ = oracle.bfs_timed(rp, cl, src, bound)
             if i >= a.warmup:
@@ -782,9 +1000,10 @@ def run_reference(a, rank, world):
                 "weights": "lognormal(0,1) FP32, numpy seed 7", "p": "Dirichlet(1)",
                 "sweeps_per_step": 2} if a.workload == "wpr" else None),
             "cpu_baseline": {"value": round(value, 5), "unit": unit, "cores": cores,
-                             "kind": "port", "sample": desc},
+                             "kind": kind, "sample": desc},
             "e2e": {"value": round(value, 5), "unit": unit, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+    line.update(extra)
     print(json.dumps(line), flush=True)
 
 
@@ -795,12 +1014,23 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if a.impl == "reference":
         run_reference(a, rank, world)
-    elif a.workload == "wpr":
-        run_wpr(a, rank, world, local_rank)
-    elif a.workload == "batch":
-        run_batch(a, rank, world, local_rank)
-    else:
-        run_ours(a, rank, world, local_rank)
+        return
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    fn = {"wpr": wpr_line, "batch": batch_line}.get(a.workload, traversal_line)
+    line = fn(a, rank, world, local_rank)
+    if a.workload == "sssp" and not a.no_extras:
+        line.update(extras(a, rank, world, local_rank))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 if __name__ == "__main__":
