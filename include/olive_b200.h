@@ -141,9 +141,13 @@ int olv_bfs(olv_graph *g, uint32_t src, int32_t *level_out, olv_stats *st);
  * fixed file-scope device array (about 8.6 MB per GPU that loads the
  * library), so graphs are limited to 1,048,576 vertices and 16,777,216 edges
  * (larger ones return OLV_ERR_LIMIT).  Push-only traversal; the CSR is
- * validated on the device first.  All calls on a device share the scratch:
- * calls that overlap on the GPU race.  The first call on a device looks up
- * the scratch address; make it before any stream capture.  st->device_ms is 0. */
+ * validated on the device first.  The three arrays must be device memory of
+ * the current device (or managed memory); anything else is OLV_ERR_ARG.  All
+ * calls on a device share the scratch: calls that overlap on the GPU race.
+ * The first call on a device looks up the scratch address and, under lazy
+ * module loading, loads the library's device code there, which commits the
+ * fixed scratch: make that call at initialisation time, before any stream
+ * capture; later calls commit no memory.  st->device_ms is 0.               */
 int olv_bfs_noalloc(const uint32_t *rowptr, const uint32_t *col, uint32_t V, uint64_t E,
                     uint32_t src, int32_t *level_out, void *stream, olv_stats *st);
 /* SSSP distances with non-negative uint32 weights: the frontier Bellman-Ford of

@@ -17,8 +17,15 @@
 // Every call on a device shares the one scratch array, so calls whose work
 // overlaps on the GPU (different streams, or host threads) race; serialise
 // them.  The first call on each device resolves the scratch address with
-// cudaGetSymbolAddress (with that device current); make that first call before
-// any stream capture.
+// cudaGetSymbolAddress (with that device current).  Under CUDA's lazy module
+// loading that first call also loads the library's device code on the device
+// and so commits the fixed scratch there: a memory-capped caller should make
+// its first call at initialisation time (and before any stream capture), after
+// which calls commit nothing.
+//
+// Every caller pointer must be device (or managed) memory of the current
+// device: memory of another GPU would be dereferenced by kernels that run
+// here, so such a call is rejected before anything is launched.
 #include <mutex>
 
 #include "olv_advance.cuh"
@@ -106,6 +113,17 @@ __global__ void k_noalloc_check(const uint32_t *__restrict__ rowptr,
         if (col[e] >= V) atomicOr(&c->err, 8u);
 }
 
+// Device memory of device `dev`, or managed memory (reachable from any device).
+static bool on_device(const void *p, int dev) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (a.type == cudaMemoryTypeManaged) return true;
+    return a.type == cudaMemoryTypeDevice && a.device == dev;
+}
+
 static std::mutex g_noalloc_mu;
 static void *g_noalloc_addr[64];
 
@@ -143,13 +161,15 @@ extern "C" int olv_bfs_noalloc(const uint32_t *rowptr, const uint32_t *col, uint
         return OLV_ERR_LIMIT;
     }
     OLV_CHECK_ARG(src < V, "olv_bfs_noalloc: source %u out of range (V=%u)", src, V);
-    OLV_CHECK_ARG(is_device_ptr(rowptr) && is_device_ptr(level_out) && (E == 0 || is_device_ptr(col)),
-                  "olv_bfs_noalloc: rowptr, col and level_out must be device memory");
+    int dev = 0, sms = 148;
+    OLV_CUDA(cudaGetDevice(&dev));
+    OLV_CHECK_ARG(on_device(rowptr, dev) && on_device(level_out, dev) &&
+                      (E == 0 || on_device(col, dev)),
+                  "olv_bfs_noalloc: rowptr, col and level_out must be device memory of the "
+                  "current device (%d)", dev);
     NoAllocScratch *sc = nullptr;
     OLV_TRY(noalloc_scratch(&sc));
     cudaStream_t s = (cudaStream_t)stream;
-    int dev = 0, sms = 148;
-    OLV_CUDA(cudaGetDevice(&dev));
     OLV_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     TravCtl *ctl = &sc->ctl;
 
@@ -198,7 +218,7 @@ extern "C" int olv_bfs_noalloc(const uint32_t *rowptr, const uint32_t *col, uint
         OLV_CUDA(cudaMemcpyAsync(&done, &ctl->done, sizeof done, cudaMemcpyDeviceToHost, s));
         OLV_CUDA(cudaStreamSynchronize(s));
         if (done) break;
-        if (batch < 64) batch *= 2;
+        if (batch < 16) batch *= 2;   // supersteps after the last are idle launches
     }
     TravCtl h;
     OLV_CUDA(cudaMemcpyAsync(&h, ctl, sizeof h, cudaMemcpyDeviceToHost, s));

@@ -41,6 +41,34 @@ def test_noalloc_bfs_matches_olv_bfs_twice():
             np.testing.assert_array_equal(out.cpu().numpy(), want)   # levels: exact
 
 
+def test_noalloc_bfs_commits_no_memory_and_takes_a_stream():
+    """After a first call (which may load the device code), further calls leave
+    the device's free memory unchanged; a caller's own stream works."""
+    import torch
+    import olive_b200 as ob
+    L = ob.lib()
+    rp_h, cl_h = oracle.rmat_csr(14, 16, 5)
+    V, E = len(rp_h) - 1, len(cl_h)
+    rp = torch.from_numpy(rp_h.astype(np.int32)).cuda()
+    cl = torch.from_numpy(cl_h.astype(np.int32)).cuda()
+    out = torch.empty(V, dtype=torch.int32, device="cuda")
+    want, _ = oracle.bfs(rp_h, cl_h, 3)
+    assert _call(L, rp, cl, V, E, 3, out) == 0, L.olv_last_error()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    assert _call(L, rp, cl, V, E, 3, out) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    np.testing.assert_array_equal(out.cpu().numpy(), want)
+    s = torch.cuda.Stream()
+    out2 = torch.full((V,), -5, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    assert _call(L, rp, cl, V, E, 3, out2, ctypes.c_void_p(s.cuda_stream)) == 0
+    s.synchronize()
+    np.testing.assert_array_equal(out2.cpu().numpy(), want)
+
+
 def test_noalloc_bfs_reference_fixture_and_limits():
     import torch
     import olive_b200 as ob
@@ -60,3 +88,7 @@ def test_noalloc_bfs_reference_fixture_and_limits():
     bad[5] = 1 << 30
     assert _call(L, rp, bad, len(rp_h) - 1, len(cl_h), 0, out) == -1
     assert b"invalid CSR" in L.olv_last_error()
+    # host memory is not the current device's memory: rejected before any launch
+    host_out = torch.empty(len(rp_h) - 1, dtype=torch.int32).pin_memory()
+    assert _call(L, rp, cl, len(rp_h) - 1, len(cl_h), 0, host_out) == -1
+    assert b"device memory of the current device" in L.olv_last_error()
