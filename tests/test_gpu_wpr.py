@@ -63,6 +63,27 @@ def rel_inf(a, b):
     return np.max(np.abs(a - b)) / np.max(np.abs(b))
 
 
+# Gradient tolerance.  Normwise: max|d| / max|ref| and ||d||_2 / ||ref||_2 both
+# below 1e-5.  Per element: |d_e| <= 1e-5 |ref_e| + 1e-7 max|ref|.  The floor
+# (under two FP32 units of roundoff at the largest element's scale) covers the
+# entries that are differences of nearly equal terms (lambda_v - sum_x P_ux
+# lambda_x), whose FP32 error comes from the rounding of their neighbours'
+# adjoints, not from their own size; an FP32 emulation of the solver puts
+# 99.7-99.9% of the entries within 1e-5 relative with no floor at all.
+GRAD_RTOL = 1e-5
+GRAD_FLOOR = 1e-7
+
+
+def assert_grad_close(got, ref, what):
+    got = np.asarray(got, np.float64)
+    assert rel_inf(got, ref) < GRAD_RTOL, (what, rel_inf(got, ref))
+    assert np.linalg.norm(got - ref) < GRAD_RTOL * np.linalg.norm(ref), what
+    d = np.abs(got - ref)
+    tol = GRAD_RTOL * np.abs(ref) + GRAD_FLOOR * np.max(np.abs(ref))
+    bad = np.flatnonzero(d > tol)
+    assert len(bad) == 0, (what, len(bad), bad[:5], d[bad[:5]], ref[bad[:5]])
+
+
 @pytest.mark.parametrize("seed", [1, 2])
 def test_forward_backward_vs_fp64_oracle(ob, seed):
     rp, cl, w, p, g = make_problem(10, seed)
@@ -74,8 +95,8 @@ def test_forward_backward_vs_fp64_oracle(ob, seed):
         dw, dp = G.wpr_backward(g, max_it=ITERS)
         lam, dw_ref, dp_ref = oracle.wpr_backward(rp, cl, w.astype(np.float64), r_ref,
                                                   g.astype(np.float64), ALPHA, ITERS)
-        assert rel_inf(dw.astype(np.float64), dw_ref) < 1e-5
-        assert rel_inf(dp.astype(np.float64), dp_ref) < 1e-5
+        assert_grad_close(dw, dw_ref, "dw")
+        assert_grad_close(dp, dp_ref, "dp")
 
 
 def test_dense_solve_and_finite_differences(ob):
@@ -96,8 +117,8 @@ def test_dense_solve_and_finite_differences(ob):
         r = G.wpr_forward(p, w=w, alpha=ALPHA, max_it=ITERS)
         dw, dp = G.wpr_backward(g, max_it=ITERS)
     assert rel_inf(r.astype(np.float64), r_dense) < 1e-5
-    assert rel_inf(dw.astype(np.float64), dw_dense) < 1e-5
-    assert rel_inf(dp.astype(np.float64), (1 - ALPHA) * lam_dense) < 1e-5
+    assert_grad_close(dw, dw_dense, "dw vs dense solve")
+    assert_grad_close(dp, (1 - ALPHA) * lam_dense, "dp vs dense solve")
     # FP64 central differences of L(w) = g . r(w) on the largest gradients
     for e in np.argsort(-np.abs(dw_dense))[:6]:
         h = 1e-5 * w64[e]
@@ -132,8 +153,8 @@ def test_autograd_function(torch, ob):
                                    ITERS)
         _, dw_ref, dp_ref = oracle.wpr_backward(rp, cl, w.astype(np.float64), r_ref,
                                                 g.astype(np.float64), ALPHA, ITERS)
-        assert rel_inf(wt.grad.cpu().numpy().astype(np.float64), dw_ref) < 1e-5
-        assert rel_inf(pt.grad.cpu().numpy().astype(np.float64), dp_ref) < 1e-5
+        assert_grad_close(wt.grad.cpu().numpy(), dw_ref, "autograd dw")
+        assert_grad_close(pt.grad.cpu().numpy(), dp_ref, "autograd dp")
         assert abs(loss.item() - float(g.astype(np.float64) @ r_ref)) < 1e-5 * abs(loss.item()) + 1e-7
 
 
@@ -161,12 +182,12 @@ def test_deterministic_and_dangling_rows(ob):
     assert rel_inf(r1.astype(np.float64), r_ref) < 1e-5
     _, dw_ref, dp_ref = oracle.wpr_backward(rp2, cl2, w.astype(np.float64), r_ref,
                                             g.astype(np.float64), ALPHA, ITERS)
-    assert rel_inf(d1[0].astype(np.float64), dw_ref) < 1e-5
+    assert_grad_close(d1[0], dw_ref, "dw with dangling rows")
 
 
 def test_rmat18_gradient_vs_oracle(ob):
-    """A power-law graph with long rows (segments) in both directions."""
-    rp, cl, w, p, g = make_problem(16, 5)
+    """RMAT-18: a power-law graph with long rows (segments) in both directions."""
+    rp, cl, w, p, g = make_problem(18, 5)
     with ob.Graph.from_csr(rp, cl) as G:
         r = G.wpr_forward(p, w=w, max_it=ITERS)
         dw, dp = G.wpr_backward(g, max_it=ITERS)
@@ -174,5 +195,6 @@ def test_rmat18_gradient_vs_oracle(ob):
     _, dw_ref, dp_ref = oracle.wpr_backward(rp, cl, w.astype(np.float64), r_ref,
                                             g.astype(np.float64), ALPHA, ITERS)
     assert rel_inf(r.astype(np.float64), r_ref) < 1e-5
-    assert rel_inf(dw.astype(np.float64), dw_ref) < 1e-5
-    assert rel_inf(dp.astype(np.float64), dp_ref) < 1e-5
+    assert np.max(np.abs(r - r_ref) / r_ref) < 1e-5       # every rank (all positive)
+    assert_grad_close(dw, dw_ref, "dw rmat18")
+    assert_grad_close(dp, dp_ref, "dp rmat18")
