@@ -1,7 +1,7 @@
 """Build the reference's applications, unmodified, against the
 source-compatible header layer in include/olive/.
 
-    python -m olive_b200.dropin [--ref /root/reference]
+    python -m olive_b200.dropin --ref <reference tree>   (or OLIVE_REFERENCE=<tree>)
 
 BFS.cu, SSSP.cu and PageRank.cu (and testCsrGraph.cu) are symlinked from the
 reference tree into olive_b200/_apps/src/, so their quoted includes
@@ -20,7 +20,6 @@ ROOT = os.path.dirname(PKG)
 APPS = os.path.join(PKG, "_apps")
 SRC = os.path.join(APPS, "src")
 INC = os.path.join(ROOT, "include", "olive")
-DEFAULT_REF = "/root/reference"
 APP_NAMES = ["BFS", "SSSP", "PageRank", "testCsrGraph"]
 
 
@@ -33,8 +32,8 @@ def app_path(name):
 
 
 def build_apps(ref=None, names=APP_NAMES):
-    ref = ref or os.environ.get("OLIVE_REFERENCE", DEFAULT_REF)
-    if not os.path.exists(os.path.join(ref, "BFS.cu")):
+    ref = ref or os.environ.get("OLIVE_REFERENCE")
+    if not ref or not os.path.exists(os.path.join(ref, "BFS.cu")):
         return []
     os.makedirs(SRC, exist_ok=True)
     built = []

@@ -2,7 +2,7 @@
 
 Run in a container where the reference tree exists:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <reference tree>   (or OLIVE_REFERENCE=<tree>)
 
 It builds the reference's own serial checkers (oracle/Makefile -> oracle/_ref)
 and records, for every graph file in the reference's data/ directory:
@@ -83,8 +83,11 @@ def record_generated(name, rowptr, col, srcs, work, pr=True):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("OLIVE_REFERENCE"),
+                    help="the reference source tree (or set OLIVE_REFERENCE)")
     a = ap.parse_args()
+    if not a.ref:
+        ap.error("give the reference tree with --ref or OLIVE_REFERENCE")
     import subprocess
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"REF={a.ref}"],
                    check=True)
