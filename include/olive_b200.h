@@ -111,6 +111,11 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
  *   "sssp_relabel" SSSP runs on vertices renumbered by in-degree, so the
  *                 most-read distances share cache lines (1), or on the
  *                 graph's own ids (0); results are identical            (1)
+ *   "sssp_sub"    SSSP: the light phase of the first heavy bucket(s) runs in
+ *                 sub-buckets of this width (fewer repeated light
+ *                 relaxations where that bucket holds most of the graph);
+ *                 0 or >= sssp_delta: one sub-bucket per bucket          (0)
+ *   "sssp_sub_buckets"  heavy buckets (from the first) that use sssp_sub (1)
  *   "ms_alpha"    msBFS pull when active out-edges * ms_alpha > E   (20)
  *   "use_graphs"  run supersteps inside CUDA graphs (1) or a host loop (0)
  *   "levels_per_sync" host loop: supersteps enqueued per check      (4)

@@ -521,6 +521,12 @@ int olv_tune_set(olv_graph *g, const char *key, double value) {
         t.sssp_pull = value != 0;
     } else if (!strcmp(key, "sssp_relabel")) {
         t.sssp_relabel = value != 0;
+    } else if (!strcmp(key, "sssp_sub")) {
+        OLV_CHECK_ARG(value >= 0 && value < 2147483647.0, "olv_tune_set: bad sssp_sub");
+        t.sssp_sub = (uint32_t)value;
+    } else if (!strcmp(key, "sssp_sub_buckets")) {
+        OLV_CHECK_ARG(value >= 0 && value < 2147483647.0, "olv_tune_set: bad sssp_sub_buckets");
+        t.sssp_sub_buckets = (uint32_t)value;
     } else if (!strcmp(key, "ms_alpha")) {
         OLV_CHECK_ARG(value > 0, "olv_tune_set: ms_alpha must be > 0");
         t.ms_alpha = (float)value;
@@ -554,6 +560,8 @@ int olv_tune_get(const olv_graph *g, const char *key, double *value) {
     else if (!strcmp(key, "sssp_delta")) *value = t.sssp_delta;
     else if (!strcmp(key, "sssp_pull")) *value = t.sssp_pull;
     else if (!strcmp(key, "sssp_relabel")) *value = t.sssp_relabel;
+    else if (!strcmp(key, "sssp_sub")) *value = t.sssp_sub;
+    else if (!strcmp(key, "sssp_sub_buckets")) *value = t.sssp_sub_buckets;
     else if (!strcmp(key, "sssp_hub_degree")) *value = t.sssp_hub_degree;
     else if (!strcmp(key, "sssp_piece")) *value = t.sssp_piece;
     else if (!strcmp(key, "ms_alpha")) *value = t.ms_alpha;

@@ -75,6 +75,10 @@ struct TravCtl {
     uint32_t aux_done;          // SSSP: CTAs of the collect pass that finished
     uint32_t bl_size;           // SSSP: entries in the bucket list
     uint32_t bl_over;           // SSSP: the bucket list overflowed (collect densely)
+    uint32_t bucket_end;        // SSSP: upper distance edge of the current heavy bucket
+    uint32_t sub_width;         // SSSP: light-phase sub-bucket width (0: none)
+    uint32_t sub_buckets;       // SSSP: heavy buckets whose light phase is sub-bucketed
+    uint32_t heavy_index;       // SSSP: heavy buckets started so far (0 = the first)
     unsigned long long heavy_work;  // SSSP: heavy out-edges of the collected bucket
     unsigned long long settled_in;  // SSSP: in-edges of all settled vertices
     uint32_t ms_track;          // msBFS: this push level records first-touched vertices
@@ -103,6 +107,8 @@ struct Tuning {
     uint32_t sssp_hub_degree = 256;   // SSSP: rows with more edges are split into pieces
     uint32_t sssp_piece = 256;        // SSSP: edges per piece
     int sssp_relabel = 1;             // SSSP: run on vertices renumbered by in-degree
+    uint32_t sssp_sub = 0;            // SSSP: light-phase sub-bucket width (0: none)
+    uint32_t sssp_sub_buckets = 1;    // SSSP: heavy buckets whose light phase uses it
     float ms_alpha = 20.0f;       // msBFS: pull when active out-edges * ms_alpha > E
     int levels_per_sync = 4;      // host loop: supersteps enqueued per check
     int use_graphs = 1;           // run supersteps inside a CUDA graph

@@ -62,6 +62,7 @@ constexpr uint32_t kModeRelax = 0;
 constexpr uint32_t kModeSplit = 2;
 constexpr uint32_t kModeHeavy = 3;
 constexpr uint32_t kModePull = 4;
+constexpr uint32_t kModeSubSplit = 5;
 constexpr uint32_t kDefaultDelta = 64;
 
 // Arrays the collect and pull passes read besides the queues.
@@ -218,13 +219,18 @@ struct SsspOp {
 __device__ void sssp_begin(TravCtl *c);
 
 __global__ void k_sssp_init(TravCtl *c, uint32_t *dist, uint32_t *q0, uint32_t src,
-                            uint32_t delta, const uint32_t *newid) {
+                            uint32_t delta, uint32_t sub, uint32_t sub_buckets,
+                            const uint32_t *newid) {
     if (newid) src = newid[src];   // relabelled run: the source's new id
     TravCtl t = {};
     t.qsize[0] = 1;
     t.vdata = dist;
-    t.threshold = delta;
     t.delta = delta;
+    t.bucket_end = delta;
+    t.sub_width = sub < delta ? sub : 0;
+    t.sub_buckets = sub_buckets;
+    t.heavy_index = 0;
+    t.threshold = (t.sub_width && sub_buckets > 0) ? t.sub_width : delta;
     t.epoch = 1;
     t.far_min = 0xffffffffu;
     t.heavy_done = 0;
@@ -235,14 +241,40 @@ __global__ void k_sssp_init(TravCtl *c, uint32_t *dist, uint32_t *q0, uint32_t s
     sssp_begin(c);
 }
 
-// Choose the next superstep's mode (relax light edges, relax a settled
-// bucket's heavy edges, or split the far pile) and reset its counters.
+static __device__ __forceinline__ uint32_t sat_add(uint32_t a, uint32_t b) {
+    const uint64_t t = (uint64_t)a + b;
+    return t > (uint64_t)kInf ? (uint32_t)kInf : (uint32_t)t;
+}
+
+// Choose the next superstep's mode and reset its counters:
+//   relax      the near queue is not empty: relax its light edges;
+//   sub-split  inside a heavy bucket [bucket_lo, bucket_end) whose light
+//              phase runs in sub-buckets of sub_width: when the near queue of
+//              one sub-bucket drains, every vertex under the threshold is
+//              final (light edges of later vertices land at or above it, heavy
+//              edges past bucket_end), so the far pile is split at the next
+//              sub-bucket's end; the bucket list and the pending heavy step
+//              carry over;
+//   heavy      the heavy bucket is settled: collect it and relax its heavy
+//              edges (or pull them);
+//   split      start the next heavy bucket at max(threshold, far minimum).
 __device__ void sssp_begin(TravCtl *c) {
     if (c->done) return;
     if (c->qsize[c->cur] > 0) {
         c->mode = kModeRelax;
         c->qsize[c->cur ^ 1] = 0;
         c->npieces = 0;
+        return;
+    }
+    if (!c->heavy_done && c->threshold < c->bucket_end && c->far_size[c->far_cur] > 0 &&
+        c->far_min < c->bucket_end) {
+        c->mode = kModeSubSplit;
+        c->split_lo = c->threshold;   // far entries below it were settled already
+        const uint32_t lo = c->threshold > c->far_min ? c->threshold : c->far_min;
+        const uint32_t t = sat_add(lo, c->sub_width);
+        c->threshold = t < c->bucket_end ? t : c->bucket_end;
+        c->far_size[c->far_cur ^ 1] = 0;
+        c->far_min = 0xffffffffu;
         return;
     }
     if (!c->heavy_done) {   // bucket settled: collect it and relax its heavy edges
@@ -258,13 +290,16 @@ __device__ void sssp_begin(TravCtl *c) {
         c->done = 1;
         return;
     }
-    // next bucket starts at max(threshold, smallest far distance)
+    // next heavy bucket starts at max(threshold, smallest far distance)
     c->mode = kModeSplit;
     c->split_lo = c->threshold;   // far entries below it were settled already
     c->bucket_lo = c->threshold;
-    uint32_t lo = c->threshold > c->far_min ? c->threshold : c->far_min;
-    uint64_t t = (uint64_t)lo + c->delta;
-    c->threshold = t > (uint64_t)kInf ? (uint32_t)kInf : (uint32_t)t;
+    const uint32_t lo = c->threshold > c->far_min ? c->threshold : c->far_min;
+    c->heavy_index++;
+    c->bucket_end = sat_add(lo, c->delta);
+    const bool sub = c->sub_width && c->heavy_index < c->sub_buckets;
+    const uint32_t t = sat_add(lo, sub ? c->sub_width : c->delta);
+    c->threshold = t < c->bucket_end ? t : c->bucket_end;
     c->far_size[c->far_cur ^ 1] = 0;
     c->far_min = 0xffffffffu;
 }
@@ -602,6 +637,9 @@ __global__ void k_sssp_end(TravCtl *c, cudaGraphConditionalHandle h, int use_con
         } else if (c->mode == kModePull) {
             c->pull_pending = 0;
             c->heavy_done = 1;
+        } else if (c->mode == kModeSubSplit) {
+            c->far_cur ^= 1;   // the bucket list and the pending heavy step carry over
+            c->epoch++;
         } else {
             c->bl_size = 0;   // a new bucket: its list starts empty
             c->bl_over = 0;
@@ -638,7 +676,8 @@ k_sssp_aux(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0, u
             dst[i] = qin[i];
         return;
     }
-    if (mode != kModeHeavy && mode != kModeSplit && mode != kModePull) return;
+    if (mode != kModeHeavy && mode != kModeSplit && mode != kModePull && mode != kModeSubSplit)
+        return;
     __shared__ uint32_t s_a[kBlock / 32][kWarpStage], s_b[kBlock / 32][kWarpStage];
     __shared__ uint32_t s_an[kBlock / 32], s_alim[kBlock / 32];
     __shared__ uint32_t s_bn[kBlock / 32], s_blim[kBlock / 32];
@@ -921,7 +960,8 @@ int run_sssp_device(olv_graph *g, uint32_t src, uint32_t *dist_dev) {
     uint32_t *dist = R.dist ? R.dist : dist_dev;   // renumbered run: internal distances
     OLV_CUDA(cudaMemsetAsync(g->ws.mark.p, 0, kMarks * mark_words(g->V) * 4, s));
     k_fill_i32<<<g->num_sms * 8, kBlock, 0, s>>>((int32_t *)dist, g->V, kInf);
-    k_sssp_init<<<1, 1, 0, s>>>(ctl, dist, g->ws.q0.as<uint32_t>(), src, sssp_delta(g), R.newid);
+    k_sssp_init<<<1, 1, 0, s>>>(ctl, dist, g->ws.q0.as<uint32_t>(), src, sssp_delta(g),
+                                g->tune.sssp_sub, g->tune.sssp_sub_buckets, R.newid);
     OLV_CUDA(cudaGetLastError());
     auto finish = [&]() -> int {
         if (R.dist) {

@@ -182,6 +182,22 @@ def test_sssp_hub_pieces_vs_dijkstra(ob, hub, piece):
             np.testing.assert_array_equal(g.sssp(s), oracle.dijkstra(rp, cl, w, s)[0])
 
 
+@pytest.mark.parametrize("sub,nsub", [(0, 1), (4, 1), (8, 2), (16, 1), (1, 3), (500, 1)])
+def test_sssp_sub_buckets_vs_dijkstra(ob, sub, nsub):
+    """The first heavy buckets' light phase in sub-buckets of every width
+    (0 and widths >= delta: none) gives Dijkstra's distances, with the pull
+    heavy step or the push."""
+    with ob.Graph.rmat(15, 16, 8, weights=True, wseed=12) as g:
+        g.tune(sssp_sub=sub, sssp_sub_buckets=nsub)
+        rp, cl, w = g.csr()
+        hub, _ = g.max_degree_vertex()
+        for s in (hub, int(np.flatnonzero(np.diff(rp.astype(np.int64)) > 0)[9])):
+            ref = oracle.dijkstra(rp, cl, w, s)[0]
+            np.testing.assert_array_equal(g.sssp(s), ref)
+        g.tune(sssp_pull=0)
+        np.testing.assert_array_equal(g.sssp(hub), oracle.dijkstra(rp, cl, w, hub)[0])
+
+
 def test_sssp_relabel_on_off_same_handle(ob):
     """Renumbered (default) and own-id runs on one handle, toggled back and
     forth, into host, device and unaligned device outputs."""

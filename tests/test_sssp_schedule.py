@@ -48,9 +48,12 @@ def _lower(dist, v, nd):
     return v, nd
 
 
-def schedule(rp, col, w, src, delta, pull_mode, list_collect):
+def schedule(rp, col, w, src, delta, pull_mode, list_collect, sub=0, nsub=1):
     """pull_mode: 'never', 'always' or 'rule' (the kernel's choice:
-    E - settled in-edges + V/2 < heavy out-edges of the bucket)."""
+    E - settled in-edges + V/2 < heavy out-edges of the bucket).  sub > 0:
+    the light phase of the first nsub heavy buckets runs in sub-buckets of
+    width sub (the far pile is split at each sub-bucket's end; the heavy step
+    follows the last one)."""
     rp = rp.astype(np.int64)
     col = col.astype(np.int64)
     w = w.astype(np.int64)
@@ -69,16 +72,30 @@ def schedule(rp, col, w, src, delta, pull_mode, list_collect):
     dist[src] = 0
     far = np.zeros(V, bool)
     q = np.array([src])
-    lo, hi = 0, delta
+    sw = sub if 0 < sub < delta else delta
+    hb = 0
+    lo, bend = 0, delta
+    hi = min(sw if nsub > 0 else delta, bend)
     settled_in, pulls = 0, 0
     while True:
         blist = []
-        while len(q):                       # relax supersteps: light edges
-            blist.append(q)
-            u, e = _expand(rp, deg, light, q)
-            v, nd = _lower(dist, col[e], np.minimum(dist[u] + w[e], INF))
-            far[v[nd >= hi]] = True
-            q = v[nd < hi]
+        while True:
+            while len(q):                       # relax supersteps: light edges
+                blist.append(q)
+                u, e = _expand(rp, deg, light, q)
+                v, nd = _lower(dist, col[e], np.minimum(dist[u] + w[e], INF))
+                far[v[nd >= hi]] = True
+                q = v[nd < hi]
+            fv = np.flatnonzero(far)
+            fv = fv[dist[fv] >= hi]
+            if hi < bend and len(fv) and dist[fv].min() < bend:   # next sub-bucket
+                hi = min(max(hi, int(dist[fv].min())) + sw, bend)
+                far[:] = False
+                far[fv] = True
+                q = fv[dist[fv] < hi]
+                far[q] = False
+                continue
+            break
         in_bucket = np.flatnonzero((dist >= lo) & (dist < hi))
         if list_collect:
             listed = np.unique(np.concatenate(blist)) if blist else np.empty(0, np.int64)
@@ -110,7 +127,9 @@ def schedule(rp, col, w, src, delta, pull_mode, list_collect):
         if len(fv) == 0:
             return dist, pulls
         lo = max(hi, int(dist[fv].min()))
-        hi = lo + delta
+        hb += 1
+        bend = lo + delta
+        hi = min(lo + (sw if hb < nsub else delta), bend)
         q = fv[dist[fv] < hi]
         far[q] = False
 
@@ -173,3 +192,17 @@ def test_schedule_on_renumbered_graph(scale, seed):
         ref = oracle.dijkstra(rp, col, w, src)[0].astype(np.int64)
         dnew, _ = schedule(nrp, ncol, nw, int(newid[src]), 64, "rule", list_collect=True)
         np.testing.assert_array_equal(dnew[newid], ref)   # mapped back: out[v] = dnew[newid[v]]
+
+
+@pytest.mark.parametrize("sub,nsub", [(8, 1), (4, 2), (16, 1), (1, 3)])
+@pytest.mark.parametrize("pull_mode", ["never", "rule"])
+def test_schedule_with_sub_buckets(sub, nsub, pull_mode):
+    """The first heavy buckets' light phase in sub-buckets: same distances,
+    and the bucket list still covers each heavy bucket."""
+    for scale, seed in ((11, 1), (12, 5)):
+        rp, col = oracle.rmat_csr(scale, 16, seed)
+        w = oracle.uint_weights(len(col), seed + 10)
+        hub = int(np.argmax(np.diff(rp.astype(np.int64))))
+        ref = oracle.dijkstra(rp, col, w, hub)[0].astype(np.int64)
+        dist, _ = schedule(rp, col, w, hub, 64, pull_mode, list_collect=True, sub=sub, nsub=nsub)
+        np.testing.assert_array_equal(dist, ref)
