@@ -33,6 +33,7 @@ struct BfsPushOp {
     using SV = uint32_t;
     static constexpr int kMinBlocks = 1;   // CTAs per SM the advance must fit
     static constexpr bool kHasFar = false;
+    static constexpr bool kPacked = false;
     const uint32_t *rowptr;
     int32_t *level;
     int next;

@@ -60,6 +60,7 @@ struct NoAllocBfsOp {
     using SV = uint32_t;
     static constexpr int kMinBlocks = 1;   // CTAs per SM the advance must fit
     static constexpr bool kHasFar = false;
+    static constexpr bool kPacked = false;
     const uint32_t *rowptr;
     uint32_t V;
     int32_t *level;

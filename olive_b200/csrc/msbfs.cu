@@ -76,6 +76,7 @@ struct MsPushOp {
     using SV = unsigned long long;
     static constexpr int kMinBlocks = 1;   // CTAs per SM the advance must fit
     static constexpr bool kHasFar = false;
+    static constexpr bool kPacked = false;
     MsCur cm;
     const unsigned long long *cur;
     const unsigned long long *visit;

@@ -20,6 +20,10 @@
 //                                                   used); act[j] becomes 0: nothing,
 //                                                   1: push v to the output queue,
 //                                                   2: push to the secondary (far) queue
+//   kPacked, Pre prepare_packed(SV sv, uint32_t val, uint32_t v)
+//                                                   ops that set kPacked read (column,
+//                                                   value) pairs from AdvanceArgs::cw
+//                                                   and get the value here instead
 //   bool on_input(uint32_t u)                       once per input queue entry;
 //                                                   false: skip its edges now
 //   void on_push(bool pushed, uint32_t v)           after each warp-wide push
@@ -194,45 +198,78 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *t
 constexpr int kItems = OLV_ITEMS;   // edges per thread kept in flight
 
 struct AdvanceArgs {
-    const uint32_t *rbeg;       // row u's edges are [rbeg[u], rend[u]) (CSR: rowptr, rowptr+1)
-    const uint32_t *rend;
-    const uint32_t *col;
-    TravCtl *ctl;
-    uint32_t *q0, *q1;          // queue buffers; ctl->cur selects the input
-    uint32_t *far0, *far1;      // secondary queue buffers; ctl->far_cur selects
-    uint2 *pieces;              // (row, piece index) of split hub rows
-    uint32_t hub_degree;
-    uint32_t piece;
-    uint32_t want_mode;         // kernel runs only when ctl->mode == want_mode ...
-    const uint32_t *rbeg2;      // ... or, with these row ranges, when it is want_mode2
-    const uint32_t *rend2;
-    uint32_t want_mode2;        // 0xffffffff: no second mode
+    const uint32_t *rbeg = nullptr;   // row u's edges are [rbeg[u], rend[u]) (CSR: rowptr, rowptr+1)
+    const uint32_t *rend = nullptr;
+    const uint2 *rng = nullptr;       // or, when set, [rng[u].x, rng[u].y) (one 8-byte load)
+    const uint32_t *col = nullptr;
+    const uint2 *cw = nullptr;        // Op::kPacked: (column, edge value) per edge
+    TravCtl *ctl = nullptr;
+    uint32_t *q0 = nullptr, *q1 = nullptr;       // queue buffers; ctl->cur selects the input
+    uint32_t *far0 = nullptr, *far1 = nullptr;   // secondary queues; ctl->far_cur selects
+    uint2 *pieces = nullptr;          // (row, piece index) of split hub rows
+    uint32_t hub_degree = 0;
+    uint32_t piece = 0;
+    uint32_t want_mode = 0;           // kernel runs only when ctl->mode == want_mode ...
+    const uint32_t *rbeg2 = nullptr;  // ... or, with these row ranges, when it is want_mode2
+    const uint32_t *rend2 = nullptr;
+    const uint2 *rng2 = nullptr;
+    uint32_t want_mode2 = 0xffffffffu;   // 0xffffffff: no second mode
+};
+
+// Row ranges of the current mode.
+struct RowRanges {
+    const uint32_t *beg, *end;
+    const uint2 *rng;
+    __device__ __forceinline__ uint2 of(uint32_t u) const {
+        if (rng) return __ldg(&rng[u]);
+        return make_uint2(__ldg(&beg[u]), __ldg(&end[u]));
+    }
 };
 
 // Row ranges for the current mode, or false when the kernel has nothing to do.
 __device__ __forceinline__ bool advance_ranges(const AdvanceArgs &a, const TravCtl *c,
-                                               const uint32_t *&rbeg, const uint32_t *&rend) {
+                                               RowRanges &r) {
     if (c->done) return false;
     const uint32_t m = c->mode;
     if (m == a.want_mode) {
-        rbeg = a.rbeg;
-        rend = a.rend;
+        r = RowRanges{a.rbeg, a.rend, a.rng};
         return true;
     }
     if (m == a.want_mode2) {
-        rbeg = a.rbeg2;
-        rend = a.rend2;
+        r = RowRanges{a.rbeg2, a.rend2, a.rng2};
         return true;
     }
     return false;
+}
+
+// Column (and, for packed ops, the edge value) of edge e, streamed once.
+template <class Op>
+__device__ __forceinline__ uint32_t load_edge(const AdvanceArgs &a, uint32_t e, uint32_t &val) {
+    if constexpr (Op::kPacked) {
+        const uint2 x = __ldcs(&a.cw[e]);   // evict first
+        val = x.y;
+        return x.x;
+    } else {
+        val = 0;
+        return __ldcs(&a.col[e]);
+    }
+}
+
+template <class Op>
+__device__ __forceinline__ typename Op::Pre prepare_edge(Op &op, typename Op::SV sv, uint32_t e,
+                                                         uint32_t v, uint32_t val) {
+    if constexpr (Op::kPacked)
+        return op.prepare_packed(sv, val, v);
+    else
+        return op.prepare(sv, e, v);
 }
 
 // Per-superstep chunk expansion over the input queue.
 template <class Op>
 __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_chunks(AdvanceArgs a, Op op) {
     TravCtl *c = a.ctl;
-    const uint32_t *rbeg, *rend;
-    if (!advance_ranges(a, c, rbeg, rend)) return;
+    RowRanges rr;
+    if (!advance_ranges(a, c, rr)) return;
     op.begin(c);
     const uint32_t cur = c->cur;
     const uint32_t n = c->qsize[cur];
@@ -265,8 +302,9 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_chunks(Advan
         if (i < n) {
             const uint32_t u = qin[i];
             if (op.on_input(u)) {
-                beg = __ldg(&rbeg[u]);
-                deg = __ldg(&rend[u]) - beg;
+                const uint2 r = rr.of(u);
+                beg = r.x;
+                deg = r.y - r.x;
             }
             if (deg > a.hub_degree) {
                 const uint32_t np = (deg + a.piece - 1) / a.piece;
@@ -305,13 +343,14 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_chunks(Advan
                     sv[j] = s_val[lo];
                 }
             }
+            uint32_t ev[kItems];
 #pragma unroll
             for (int j = 0; j < kItems; j++)
-                if (act[j]) v[j] = __ldcs(&a.col[e[j]]);   // streamed once: evict first
+                if (act[j]) v[j] = load_edge<Op>(a, e[j], ev[j]);
             typename Op::Pre pre[kItems];
 #pragma unroll
             for (int j = 0; j < kItems; j++)
-                if (act[j]) pre[j] = op.prepare(sv[j], e[j], v[j]);
+                if (act[j]) pre[j] = prepare_edge(op, sv[j], e[j], v[j], ev[j]);
             op.template apply_n<kItems>(pre, v, act);
             stage_push_n<kItems>(act, v, 1, s_q, &s_qn, &s_qlim, kStage, qout, qout_size);
             if (Op::kHasFar)
@@ -330,8 +369,8 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_chunks(Advan
 template <class Op>
 __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_pieces(AdvanceArgs a, Op op) {
     TravCtl *c = a.ctl;
-    const uint32_t *rbeg, *rend;
-    if (!advance_ranges(a, c, rbeg, rend)) return;
+    RowRanges rr;
+    if (!advance_ranges(a, c, rr)) return;
     const uint32_t np = c->npieces;
     if (np == 0) return;
     op.begin(c);
@@ -358,23 +397,24 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_pieces(Advan
     for (uint32_t p = warp; p < np; p += nwarps) {
         const uint2 pc = a.pieces[p];
         const uint32_t u = pc.x;
-        const uint32_t rb = __ldg(&rbeg[u]), re = __ldg(&rend[u]);
+        const uint2 r = rr.of(u);
+        const uint32_t rb = r.x, re = r.y;
         const uint32_t b = rb + pc.y * a.piece;
         const uint32_t e_end = min(re, b + a.piece);
         const typename Op::SV sv = op.src_value(u);
         for (uint32_t base = b; base < e_end; base += 32 * kItems) {
-            uint32_t e[kItems], v[kItems];
+            uint32_t e[kItems], v[kItems], ev[kItems];
             int act[kItems];
 #pragma unroll
             for (int j = 0; j < kItems; j++) {
                 e[j] = base + j * 32 + lane;
                 act[j] = e[j] < e_end;
-                v[j] = act[j] ? __ldcs(&a.col[e[j]]) : 0;   // streamed once: evict first
+                v[j] = act[j] ? load_edge<Op>(a, e[j], ev[j]) : 0;
             }
             typename Op::Pre pre[kItems];
 #pragma unroll
             for (int j = 0; j < kItems; j++)
-                if (act[j]) pre[j] = op.prepare(sv, e[j], v[j]);
+                if (act[j]) pre[j] = prepare_edge(op, sv, e[j], v[j], ev[j]);
             op.template apply_n<kItems>(pre, v, act);
             // flush before a round could overflow the warp's buffers (the
             // counts were last written by lane 0's shared atomics)

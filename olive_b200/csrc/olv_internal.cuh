@@ -120,7 +120,10 @@ struct Workspace {
     DevBuf order, cand, cand2;      // BFS pull: in-degree-sorted vertices, candidate lists
     DevBuf pull_first;              // BFS pull: each vertex's first in-edge in pull order
     DevBuf pull_idx;                // BFS pull: in-edges sorted by source out-degree (desc)
-    DevBuf sssp_col, sssp_w, rowmid; // SSSP: rows split light (w <= delta) | heavy
+    // SSSP: rows split light (w <= delta) | heavy, as (column, weight) pairs;
+    // rowmid[u] the split point; per vertex its light and heavy ranges as
+    // uint2 (one load each); the in-edges as (source, weight) pairs
+    DevBuf sssp_cw, rowmid, sssp_lr, sssp_hr, sssp_crw;
     DevBuf blist;                   // SSSP: inputs of the current bucket's relax supersteps
     DevBuf hdin;                    // SSSP: per vertex (heavy out-degree, in-degree)
     // SSSP: vertices renumbered by in-degree (descending): new -> old and
@@ -128,6 +131,7 @@ struct Workspace {
     // the distances in the new ids
     DevBuf sr_perm, sr_newid, sr_rowptr, sr_col, sr_w, sr_colptr, sr_rowidx, sr_cw, sr_dist;
     int sr_built = 0;
+    uint32_t sr_vnz = 0;            // SSSP renumbered: vertices with in-degree > 0 (a prefix)
     int sssp_part_relabel = -1;     // SSSP: the partition above was built relabelled (1) or not
     uint32_t sssp_delta_built = 0;
     uint32_t n_heavy = 0, n_light = 0;
@@ -135,7 +139,8 @@ struct Workspace {
         level.release(); q0.release(); q1.release(); pieces.release(); ctl.release();
         fbits.release(); order.release(); cand.release(); cand2.release(); pull_idx.release();
         pull_first.release();
-        sssp_col.release(); sssp_w.release(); rowmid.release(); blist.release(); hdin.release();
+        sssp_cw.release(); rowmid.release(); sssp_lr.release(); sssp_hr.release();
+        sssp_crw.release(); blist.release(); hdin.release();
         sssp_delta_built = 0;
         sr_perm.release(); sr_newid.release(); sr_rowptr.release(); sr_col.release();
         sr_w.release(); sr_colptr.release(); sr_rowidx.release(); sr_cw.release();

@@ -67,8 +67,9 @@ constexpr uint32_t kDefaultDelta = 64;
 
 // Arrays the collect and pull passes read besides the queues.
 struct SsspAux {
-    const uint32_t *colptr, *rowidx;   // CSC: in-edges and their sources
-    const uint32_t *cw;                // CSC weights
+    const uint32_t *colptr;            // CSC row offsets
+    const uint2 *crw;                  // CSC: (source, weight) per in-edge
+    uint32_t vpull;                    // vertices [vpull, V) have no in-edges
     const uint2 *hdin;                 // per vertex: (heavy out-degree, in-degree)
     uint32_t *blist;                   // bucket list: the bucket's relax inputs, in order
     uint32_t *cmark;                   // bitmap: vertices collected so far this run
@@ -77,12 +78,15 @@ struct SsspAux {
     int pull;                          // pull supersteps allowed
 };
 
-// Stable partition of every row into light (w <= delta) then heavy edges; one
-// warp per row, two passes (count, then write in order).
+// Stable partition of every row into light (w <= delta) then heavy edges,
+// written as (column, weight) pairs; one warp per row, two passes (count,
+// then write in order).  Per vertex: rowmid (the split point) and its light
+// and heavy ranges as uint2, so the advance reads a row's range with one load.
 __global__ void k_partition_rows(const uint32_t *__restrict__ rowptr,
                                  const uint32_t *__restrict__ col, const uint32_t *__restrict__ w,
-                                 uint32_t V, uint32_t delta, uint32_t *__restrict__ pcol,
-                                 uint32_t *__restrict__ pw, uint32_t *__restrict__ rowmid) {
+                                 uint32_t V, uint32_t delta, uint2 *__restrict__ pcw,
+                                 uint32_t *__restrict__ rowmid, uint2 *__restrict__ lr,
+                                 uint2 *__restrict__ hr) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -102,18 +106,27 @@ __global__ void k_partition_rows(const uint32_t *__restrict__ rowptr,
             const bool light = ok && wi <= delta;
             const unsigned ml = __ballot_sync(0xffffffffu, light);
             const unsigned mh = __ballot_sync(0xffffffffu, ok && !light);
-            if (light) {
-                pcol[lo + __popc(ml & lt)] = ci;
-                pw[lo + __popc(ml & lt)] = wi;
-            } else if (ok) {
-                pcol[hi + __popc(mh & lt)] = ci;
-                pw[hi + __popc(mh & lt)] = wi;
-            }
+            if (light)
+                pcw[lo + __popc(ml & lt)] = make_uint2(ci, wi);
+            else if (ok)
+                pcw[hi + __popc(mh & lt)] = make_uint2(ci, wi);
             lo += __popc(ml);
             hi += __popc(mh);
         }
-        if (lane == 0) rowmid[u] = b + nl;
+        if (lane == 0) {
+            rowmid[u] = b + nl;
+            lr[u] = make_uint2(b, b + nl);
+            hr[u] = make_uint2(b + nl, e);
+        }
     }
+}
+
+// In-edges as (source, weight) pairs for the pull superstep.
+__global__ void k_pack_pairs(const uint32_t *__restrict__ a, const uint32_t *__restrict__ b,
+                             unsigned long long n, uint2 *__restrict__ out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = make_uint2(a[i], b[i]);
 }
 
 #ifndef OLV_SSSP_MINB
@@ -123,7 +136,7 @@ struct SsspOp {
     static constexpr int kMinBlocks = OLV_SSSP_MINB;   // CTAs per SM the advance must fit
     using SV = uint32_t;
     static constexpr bool kHasFar = true;
-    const uint32_t *w;
+    static constexpr bool kPacked = true;   // (column, weight) pairs: one 8-byte load per edge
     // Dedupe bitmaps, 2 MB each at 16M vertices, so they stay in L2.  Near:
     // superstep t sets bits in nmark<t & 1> for the vertices it queues; those
     // vertices are superstep t+1's input queue, which clears them again
@@ -154,8 +167,8 @@ struct SsspOp {
         uint32_t nd, cur;
     };
     __device__ __forceinline__ uint32_t src_value(uint32_t u) const { return __ldcg(&dist[u]); }
-    __device__ __forceinline__ Pre prepare(uint32_t du, uint32_t e, uint32_t v) const {
-        uint32_t nd = du + __ldcs(&w[e]);   // streamed once: evict first
+    __device__ __forceinline__ Pre prepare_packed(uint32_t du, uint32_t w, uint32_t v) const {
+        uint32_t nd = du + w;
         if (nd < du || nd > (uint32_t)kInf) nd = (uint32_t)kInf;   // saturate
         return Pre{nd, __ldcg(&dist[v])};
     }
@@ -467,7 +480,8 @@ __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1
     const uint32_t lane = lane_id();
     uint32_t fmin = 0xffffffffu;
     unsigned long long scanned = 0;
-    for (uint64_t base = (uint64_t)blockIdx.x * kPullChunk; base < V;
+    // vertices past vpull have no in-edges (the renumbered ids put them last)
+    for (uint64_t base = (uint64_t)blockIdx.x * kPullChunk; base < x.vpull;
          base += (uint64_t)gridDim.x * kPullChunk) {
         const uint64_t v0 = base + 4 * (uint64_t)threadIdx.x;
         uint32_t d[4] = {0u, 0u, 0u, 0u}, b[4] = {0u, 0u, 0u, 0u}, e[4] = {0u, 0u, 0u, 0u};
@@ -528,8 +542,9 @@ __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1
                         if (s_off[lo + step] <= k) lo += step;
                     own[j] = lo;
                     const uint32_t i = s_beg[lo] + (k - s_off[lo]);
-                    u[j] = x.rowidx[i];
-                    w[j] = x.cw[i];
+                    const uint2 t = x.crw[i];
+                    u[j] = t.x;
+                    w[j] = t.y;
                 }
             }
 #pragma unroll
@@ -791,6 +806,9 @@ static int sssp_relabel(olv_graph *g) {
         perm[i] = v;
         newid[v] = i;
     }
+    uint32_t vnz = 0;   // in-degree > 0: a prefix of the new numbering
+    for (uint32_t v = 0; v < V; v++) vnz += cp[v + 1] != cp[v];
+    ws.sr_vnz = vnz;
     nrp[0] = 0;
     ncp[0] = 0;
     for (uint32_t i = 0; i < V; i++) {
@@ -853,15 +871,21 @@ static int sssp_partition(olv_graph *g) {
     if (ws.sssp_delta_built == delta && ws.sssp_part_relabel == relabel && ws.rowmid.p)
         return OLV_OK;
     const SsspCsr R = sssp_csr(g);
-    OLV_TRY(ws.sssp_col.ensure(g->E * 4 + 16));
-    OLV_TRY(ws.sssp_w.ensure(g->E * 4 + 16));
+    OLV_TRY(ws.sssp_cw.ensure(g->E * 8 + 16));
     OLV_TRY(ws.rowmid.ensure((size_t)g->V * 4 + 16));
+    OLV_TRY(ws.sssp_lr.ensure((size_t)g->V * 8 + 16));
+    OLV_TRY(ws.sssp_hr.ensure((size_t)g->V * 8 + 16));
     OLV_TRY(ws.hdin.ensure((size_t)g->V * 8 + 16));
     k_partition_rows<<<g->num_sms * 16, kBlock, 0, g->stream>>>(
-        R.rowptr, R.col, R.w, g->V, delta, ws.sssp_col.as<uint32_t>(), ws.sssp_w.as<uint32_t>(),
-        ws.rowmid.as<uint32_t>());
+        R.rowptr, R.col, R.w, g->V, delta, ws.sssp_cw.as<uint2>(), ws.rowmid.as<uint32_t>(),
+        ws.sssp_lr.as<uint2>(), ws.sssp_hr.as<uint2>());
     k_heavy_in_degrees<<<g->num_sms * 8, kBlock, 0, g->stream>>>(
         R.rowptr, ws.rowmid.as<uint32_t>(), R.colptr, g->V, ws.hdin.as<uint2>());
+    if (R.cw && R.rowidx) {   // in-edges as (source, weight) pairs for the pull
+        OLV_TRY(ws.sssp_crw.ensure(g->E * 8 + 16));
+        k_pack_pairs<<<g->num_sms * 8, kBlock, 0, g->stream>>>(R.rowidx, R.cw, g->E,
+                                                              ws.sssp_crw.as<uint2>());
+    }
     OLV_CUDA(cudaGetLastError());
     ws.sssp_delta_built = delta;
     ws.sssp_part_relabel = relabel;
@@ -874,10 +898,9 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     Workspace &ws = g->ws;
     TravCtl *ctl = ws.ctl.as<TravCtl>();
     const SsspCsr R = sssp_csr(g);
-    AdvanceArgs a;   // light edges: [rowptr[u], rowmid[u])
-    a.rbeg = R.rowptr;
-    a.rend = ws.rowmid.as<uint32_t>();
-    a.col = ws.sssp_col.as<uint32_t>();
+    AdvanceArgs a;   // light edges: [rowptr[u], rowmid[u]) = sssp_lr[u]
+    a.rng = ws.sssp_lr.as<uint2>();
+    a.cw = ws.sssp_cw.as<uint2>();
     a.ctl = ctl;
     a.q0 = ws.q0.as<uint32_t>();
     a.q1 = ws.q1.as<uint32_t>();
@@ -887,11 +910,7 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     a.hub_degree = g->tune.sssp_hub_degree;
     a.piece = g->tune.sssp_piece;
     a.want_mode = kModeRelax;
-    AdvanceArgs ah = a;   // heavy edges: [rowmid[u], rowptr[u+1])
-    ah.rbeg = ws.rowmid.as<uint32_t>();
-    ah.rend = R.rowptr + 1;
     SsspOp op = {};
-    op.w = ws.sssp_w.as<uint32_t>();
     const size_t words = mark_words(g->V);
     uint32_t *mk = ws.mark.as<uint32_t>();
     op.nmark0 = mk;
@@ -908,19 +927,18 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     int nb = 0;   // the relax kernel's own residency (it holds more registers than BFS's)
     OLV_TRY(resident_blocks(g, (const void *)k_advance_chunks<SsspOp>, &nb));
     uint32_t V = g->V;
-    a.rbeg2 = ah.rbeg;
-    a.rend2 = ah.rend;
+    a.rng2 = ws.sssp_hr.as<uint2>();   // heavy edges: [rowmid[u], rowptr[u+1])
     a.want_mode2 = kModeHeavy;
     SsspAux x;
     x.colptr = R.colptr;
-    x.rowidx = R.rowidx;
-    x.cw = R.cw;
+    x.crw = ws.sssp_crw.as<uint2>();
+    x.vpull = R.newid ? ws.sr_vnz : V;
     x.E = g->E;
     x.hdin = ws.hdin.as<uint2>();
     x.blist = ws.blist.as<uint32_t>();
     x.cmark = mk + 4 * words;
     x.bl_cap = V;
-    x.pull = g->tune.sssp_pull && x.cw != nullptr;
+    x.pull = g->tune.sssp_pull && x.crw != nullptr;
     void *a_aux[] = {&V, &ctl, &q0, &q1, &far0, &far1, &fm, &x};
     OLV_TRY(sink((const void *)k_sssp_aux, dim3(nb), dim3(kBlock), a_aux));
     void *a_adv[] = {&a, &op};
