@@ -4,34 +4,53 @@
  * sm_100a in the application's translation unit.
  *
  * They replace the reference's five kernels (oliverKernel.h:45-221):
- *   k_expand / k_expand_pieces   edgeFilter + edgeMap (oliverKernel.h:45-83,
- *        148-178).  Load-balanced: a CTA takes 256 sources (queue entries or
- *        flagged vertices), scans their out-degrees in shared memory and all
- *        256 threads walk the chunk's edges, so column reads are contiguous
- *        runs; rows longer than kHub edges are cut into kPiece-edge pieces that
- *        a second kernel spreads over every warp.  The reference gave each
- *        source a fixed group of 1..32 threads (hubs serialised).
- *   k_vertex_filter   flags -> queue with cond/update (oliverKernel.h:85-141);
- *        grid-stride, one atomic per warp (ballot/popc compaction).  cond
- *        receives the vertex's accumulator -- the reference passed the vertex
- *        id (oliverKernel.h:112,135), which SSSP.cu's cond cannot use.
- *   k_vertex_map_dense / k_vertex_map_sparse   (oliverKernel.h:184-221),
- *        grid-stride.
- * Empty edge types (Dump_Edge) take no storage: the functor receives a local
- * default-constructed value.
+ *   edgeFilter / edgeMap (oliverKernel.h:45-83, 148-178) run on the engine's
+ *     shared templates (include/olive_b200/olv_advance.cuh), the same ones the
+ *     C ABI's BFS and SSSP instantiate:
+ *       push  olv::k_advance_chunks / k_advance_pieces with PushOp: a CTA scans
+ *             256 sources' out-degrees and all threads walk the chunk's edges
+ *             (rows over kHub edges go to warp pieces); each destination's
+ *             bit is set once (a plain load first, the atomic only when it is
+ *             clear) and the newly flagged vertex is listed, so the next
+ *             vertexFilter reads only the touched vertices;
+ *       pull  olv::k_pull_chunks / k_pull_pieces with PullOp over the reverse
+ *             graph: each row reduces its in-edges from source-subset members
+ *             into a shared-memory slot (the functor's own reduce), then one
+ *             store; chosen on the device when the frontier's out-edges pass
+ *             E / pull_div (or always / never, OLIVE_DIRECTION).  A functor
+ *             may opt into a narrower pull: `pullCandidate(const V &)` skips
+ *             rows, `static constexpr bool pullFirstHit` stops a row at its
+ *             first contribution (valid when any one contribution is enough,
+ *             as for BFS levels).
+ *   k_vertex_filter  flags -> queue with cond/update (oliverKernel.h:85-141):
+ *     over the listed members (or the bitmap when no list is known); ballot
+ *     compaction, one atomic per warp; writes the queue, its bitmap and the
+ *     sum of the kept vertices' out-degrees.  cond receives the vertex's
+ *     accumulator -- the reference passed the vertex id (oliverKernel.h:112,
+ *     135), which SSSP.cu's cond cannot use.
+ *   k_vertex_map  (oliverKernel.h:184-221), over queue, list or bitmap.
+ * Every kernel is grid-stride (the reference's 65,535-block cap skipped
+ * vertices past 2^24, utils.h:68).  Empty edge types (Dump_Edge) take no
+ * storage: the functor receives a local default-constructed value.
  */
 #ifndef OLIVE_OLIVER_KERNEL_H
 #define OLIVE_OLIVER_KERNEL_H
 
 #include <type_traits>
 
+#include "../olive_b200/olv_advance.cuh"
 #include "common.h"
+#include "vertexSubset.h"
 
 namespace olive_detail {
 
-constexpr int kT = 256;          // threads per CTA
-constexpr uint32_t kHub = 4096;  // rows longer than this are split into pieces
-constexpr uint32_t kPiece = 2048;
+constexpr int kT = 256;            // threads per CTA (olv::kBlock)
+constexpr uint32_t kHub = 1024;    // push: rows with more out-edges go to pieces
+constexpr uint32_t kPiece = 1024;
+constexpr uint32_t kPullHub = 4096;   // pull: rows with more in-edges go to pieces
+constexpr uint32_t kPullPiece = 2048;
+constexpr uint32_t kModePush = 0;
+constexpr uint32_t kModePull = 1;
 
 __device__ __forceinline__ uint32_t lane() { return threadIdx.x & 31; }
 
@@ -44,160 +63,256 @@ __device__ __forceinline__ E &edge_ref(E *vals, EdgeId e, E &dummy) {
     }
 }
 
-__device__ __forceinline__ void warp_append(bool p, VertexId v, VertexId *q, VertexId *qsize) {
-    const unsigned m = __ballot_sync(0xffffffffu, p);
-    if (!m) return;
-    const uint32_t leader = __ffs(m) - 1;
-    uint32_t base = 0;
-    if (lane() == leader) base = atomicAdd(qsize, (uint32_t)__popc(m));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (p) q[base + __popc(m & ((1u << lane()) - 1u))] = v;
+__device__ __forceinline__ bool bit_of(const Word *bits, VertexId v) {
+    return (bits[v >> 6] >> (v & 63)) & 1;
 }
 
-__device__ __forceinline__ uint32_t cta_exclusive_scan(uint32_t x, uint32_t *total,
-                                                       uint32_t *s_warp) {
-    const uint32_t ln = lane(), wid = threadIdx.x >> 5;
-    uint32_t incl = x;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (ln >= (uint32_t)o) incl += t;
-    }
-    if (ln == 31) s_warp[wid] = incl;
-    __syncthreads();
-    if (wid == 0) {
-        constexpr int NW = kT / 32;
-        uint32_t t = ln < NW ? s_warp[ln] : 0, ti = t;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, ti, o);
-            if (ln >= (uint32_t)o) ti += y;
-        }
-        if (ln < NW) s_warp[ln] = ti - t;
-        if (ln == NW - 1) s_warp[32] = ti;
-    }
-    __syncthreads();
-    const uint32_t r = s_warp[wid] + incl - x;
-    *total = s_warp[32];
-    __syncthreads();
-    return r;
+// Set v's bit; true when this call set it.  A plain load first: most
+// destinations reached again in a superstep are already flagged.
+__device__ __forceinline__ bool set_bit(Word *bits, VertexId v) {
+    const Word m = (Word)1 << (v & 63);
+    if (__ldcg(&bits[v >> 6]) & m) return false;
+    const unsigned long long old =
+        atomicOr(reinterpret_cast<unsigned long long *>(&bits[v >> 6]), (unsigned long long)m);
+    return !(old & m);
 }
 
-struct ExpandArgs {
-    const VertexId *queue;      // FromQueue: sources
-    const VertexId *qsize;
-    const uint8_t *srcflags;    // !FromQueue: flag per vertex
-    VertexId n;                 // vertex count
-    const EdgeId *rowptr;
-    const VertexId *col;
-    uint8_t *dstflags;          // MarkDst: flags of the destinations
-    uint2 *pieces;
-    uint32_t *npieces;
+// ------------------------------------------------- functor opt-in traits --
+template <class F, class V, class = void>
+struct has_pull_candidate : std::false_type {};
+template <class F, class V>
+struct has_pull_candidate<
+    F, V, std::void_t<decltype(std::declval<F &>().pullCandidate(std::declval<const V &>()))>>
+    : std::true_type {};
+
+template <class F, class = void>
+struct pull_first_hit : std::false_type {};
+template <class F>
+struct pull_first_hit<F, std::void_t<decltype(F::pullFirstHit)>>
+    : std::integral_constant<bool, F::pullFirstHit> {};
+
+// ------------------------------------------------------------------ push --
+// Op for olv::k_advance_chunks / k_advance_pieces: gather + reduce per edge,
+// flag and list each destination once.
+template <class V, class A, class E, class F, bool MarkDst>
+struct PushOp {
+    static constexpr int kMinBlocks = 2;
+    static constexpr bool kHasFar = false;
+    static constexpr bool kPacked = false;
+    using SV = uint32_t;   // the source id: gather reads its value and degree
+    struct Pre {
+        A x;
+    };
+    F f;
+    const VertexId *outdeg;
+    V *vvals;
+    A *acc;
+    E *evals;
+    Word *dbits;   // destination flags (MarkDst) or the engine's written-accumulator flags
+    __device__ __forceinline__ void begin(olv::TravCtl *) {}
+    __device__ __forceinline__ SV src_value(uint32_t u) const { return u; }
+    __device__ __forceinline__ bool on_input(uint32_t) const { return true; }
+    __device__ __forceinline__ Pre prepare(uint32_t u, uint32_t e, uint32_t) {
+        E dummy{};
+        E &ev = edge_ref(evals, e, dummy);
+        return Pre{f.gather(vvals[u], outdeg[u], ev)};
+    }
+    template <int N>
+    __device__ __forceinline__ void apply_n(const Pre (&p)[N], const uint32_t (&v)[N],
+                                            int (&act)[N]) {
+#pragma unroll
+        for (int j = 0; j < N; j++)
+            if (act[j]) f.reduce(acc[v[j]], p[j].x);
+#pragma unroll
+        for (int j = 0; j < N; j++) act[j] = act[j] && set_bit(dbits, v[j]) ? 1 : 0;
+    }
+    __device__ __forceinline__ void on_push(bool, uint32_t) {}
+    __device__ __forceinline__ void flush(unsigned long long) {}
 };
 
-template <typename V, typename A, typename E, typename F, bool MarkDst>
-__device__ __forceinline__ void visit_edge(const ExpandArgs &a, F &f, const V &sv, EdgeId outdeg,
-                                           EdgeId e, V *vvals, A *acc, E *evals) {
-    E dummy{};
-    E &ev = edge_ref(evals, e, dummy);
-    const VertexId v = a.col[e];
-    A x = f.gather(sv, outdeg, ev);
-    f.reduce(acc[v], x);
-    if (MarkDst) a.dstflags[v] = 1;
+// ------------------------------------------------------------------ pull --
+template <class V, class A, class E, class F>
+struct PullOp {
+    static constexpr int kMinBlocks = 2;
+    static constexpr bool kFirstHit = pull_first_hit<F>::value;
+    using Acc = A;
+    F f;
+    const VertexId *outdeg;
+    const EdgeId *eid;      // CSR position of each in-edge (edge values)
+    const Word *sbits;      // source subset
+    V *vvals;
+    A *acc;
+    E *evals;
+    Word *dbits;
+    __device__ __forceinline__ bool row_wanted(uint32_t r) {
+        if constexpr (has_pull_candidate<F, V>::value)
+            return f.pullCandidate(vvals[r]);
+        else
+            return true;
+    }
+    __device__ __forceinline__ A acc_load(uint32_t r) const { return acc[r]; }
+    __device__ __forceinline__ bool contributes(uint32_t u, uint32_t e, A &x) {
+        if (!bit_of(sbits, u)) return false;
+        E dummy{};
+        E &ev = edge_ref(evals, eid[e], dummy);
+        x = f.gather(vvals[u], outdeg[u], ev);
+        return true;
+    }
+    __device__ __forceinline__ void reduce_slot(A &slot, const A &x) { f.reduce(slot, x); }
+    __device__ __forceinline__ void reduce_row(uint32_t r, const A &x) { f.reduce(acc[r], x); }
+    __device__ __forceinline__ void store(uint32_t r, const A &slot) { acc[r] = slot; }
+    __device__ __forceinline__ bool mark(uint32_t r) { return set_bit(dbits, r); }
+};
+
+// --------------------------------------------------------- edge pass glue --
+// Before a pass: the source count and the push/pull choice go into the
+// control block (no host round trip).  policy: 0 push, 1 pull, 2 by size.
+__global__ void k_edge_setup(olv::TravCtl *c, const SubsetMeta *src, int policy,
+                             unsigned long long pull_edges) {
+    olv::TravCtl t = {};
+    t.qsize[0] = src->qsize;
+    const unsigned long long m = src->outEdges;
+    bool pull = policy == 1 || (policy == 2 && m != kUnknownEdges && m >= pull_edges);
+    t.mode = pull ? kModePull : kModePush;
+    *c = t;
 }
 
-template <typename V, typename A, typename E, typename F, bool FromQueue, bool MarkDst>
+// After a pass: the destination's list length, its metadata, and the list
+// of written accumulators for the next reset.
+__global__ void k_edge_finish(const olv::TravCtl *c, SubsetMeta *dst, const VertexId *list,
+                              VertexId *accList, SubsetMeta *accMeta) {
+    const VertexId n = c->qsize[1];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (dst) {
+            dst->qsize = n;
+            dst->listValid = 1;
+            dst->outEdges = kUnknownEdges;
+        }
+        accMeta->qsize = n;
+        accMeta->listValid = 1;
+    }
+    if (accList != list)
+        for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+             i += (size_t)gridDim.x * blockDim.x)
+            accList[i] = list[i];
+}
+
+// Accumulators back to the default: the ones the last pass wrote when they
+// are listed, all of them otherwise (the reference refilled all V on the host
+// and copied them every superstep, oliver.h:66,127).
+template <typename A>
+__global__ void k_acc_reset(A *acc, VertexId n, A x, const VertexId *list, SubsetMeta *m) {
+    const size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    if (m->listValid) {
+        const VertexId k = m->qsize;
+        for (size_t i = tid; i < k; i += stride) acc[list[i]] = x;
+    } else {
+        for (size_t v = tid; v < n; v += stride) acc[v] = x;
+    }
+}
+
+__global__ void k_meta_set(SubsetMeta *m, VertexId qsize, uint32_t listValid) {
+    m->qsize = qsize;
+    m->listValid = listValid;
+}
+
+// Members of a flag subset without a list, written as a list (the bitmap in
+// order), with the sum of their out-degrees.
+__global__ void k_bits_to_list(const Word *bits, VertexId n, const VertexId *outdeg,
+                               VertexId *list, SubsetMeta *m) {
+    unsigned long long deg = 0;
+    for (size_t base = blockIdx.x * (size_t)blockDim.x; base < n;
+         base += (size_t)gridDim.x * blockDim.x) {
+        const size_t v = base + threadIdx.x;
+        const bool in = v < n && bit_of(bits, (VertexId)v);
+        if (in) deg += outdeg[v];
+        olv::warp_push(in, (uint32_t)v, list, &m->qsize);
+    }
+    olv::warp_add64(deg, &m->outEdges);
+}
+
+__global__ void k_meta_zero_for_list(SubsetMeta *m) {
+    m->qsize = 0;
+    m->outEdges = 0;
+}
+
+__global__ void k_meta_list_done(SubsetMeta *m) { m->listValid = 1; }
+
+// vertexFilter: members of src with cond(value, acc) are updated and queued.
+template <typename V, typename A, typename F>
 __global__ void __launch_bounds__(kT)
-k_expand(ExpandArgs a, V *vvals, A *acc, E *evals, F f) {
-    __shared__ uint32_t s_beg[kT], s_off[kT], s_src[kT];
-    __shared__ uint32_t s_warp[33];
-    const uint64_t n = FromQueue ? *a.qsize : a.n;
-    for (uint64_t chunk = blockIdx.x; chunk * kT < n; chunk += gridDim.x) {
-        const uint64_t i = chunk * kT + threadIdx.x;
-        uint32_t beg = 0, deg = 0, u = 0;
-        if (i < n) {
-            u = FromQueue ? a.queue[i] : (VertexId)i;
-            if (FromQueue || a.srcflags[u]) {
-                beg = a.rowptr[u];
-                deg = a.rowptr[u + 1] - beg;
-                if (deg > kHub) {
-                    const uint32_t np = (deg + kPiece - 1) / kPiece;
-                    const uint32_t b = atomicAdd(a.npieces, np);
-                    for (uint32_t p = 0; p < np; p++) a.pieces[b + p] = make_uint2(u, p);
-                    deg = 0;
+k_vertex_filter(const Word *sbits, const VertexId *slist, const SubsetMeta *smeta, VertexId n,
+                const VertexId *outdeg, V *vvals, A *acc, VertexId *queue, Word *qbits,
+                SubsetMeta *qmeta, F f) {
+    const bool listed = smeta->listValid;
+    const size_t count = listed ? smeta->qsize : n;
+    unsigned long long deg = 0;
+    for (size_t base = blockIdx.x * (size_t)kT; base < count; base += (size_t)gridDim.x * kT) {
+        const size_t i = base + threadIdx.x;
+        bool keep = false;
+        VertexId v = 0;
+        if (i < count) {
+            v = listed ? slist[i] : (VertexId)i;
+            if (listed || bit_of(sbits, v)) {
+                A a = acc[v];
+                if (f.cond(vvals[v], a)) {
+                    f.update(vvals[v], a);
+                    keep = true;
+                    deg += outdeg[v];
+                    atomicOr(reinterpret_cast<unsigned long long *>(&qbits[v >> 6]),
+                             (unsigned long long)((Word)1 << (v & 63)));
                 }
             }
         }
-        uint32_t total;
-        const uint32_t off = cta_exclusive_scan(deg, &total, s_warp);
-        s_beg[threadIdx.x] = beg;
-        s_off[threadIdx.x] = off;
-        s_src[threadIdx.x] = u;
-        __syncthreads();
-        for (uint32_t k = threadIdx.x; k < total; k += kT) {
-            uint32_t lo = 0;
-#pragma unroll
-            for (uint32_t step = kT / 2; step > 0; step >>= 1)
-                if (s_off[lo + step] <= k) lo += step;
-            const VertexId src = s_src[lo];
-            const EdgeId e = s_beg[lo] + (k - s_off[lo]);
-            const EdgeId outdeg = a.rowptr[src + 1] - a.rowptr[src];
-            const V sv = vvals[src];
-            visit_edge<V, A, E, F, MarkDst>(a, f, sv, outdeg, e, vvals, acc, evals);
-        }
-        __syncthreads();
+        olv::warp_push(keep, v, queue, &qmeta->qsize);
     }
+    olv::warp_add64(deg, &qmeta->outEdges);
 }
 
-template <typename V, typename A, typename E, typename F, bool MarkDst>
-__global__ void __launch_bounds__(kT)
-k_expand_pieces(ExpandArgs a, V *vvals, A *acc, E *evals, F f) {
-    const uint32_t np = *a.npieces;
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t p = warp; p < np; p += nwarps) {
-        const uint2 pc = a.pieces[p];
-        const VertexId u = pc.x;
-        const EdgeId rb = a.rowptr[u], re = a.rowptr[u + 1];
-        const EdgeId b = rb + pc.y * kPiece;
-        const EdgeId end = min(re, b + kPiece);
-        const V sv = vvals[u];
-        for (EdgeId e = b + lane(); e < end; e += 32)
-            visit_edge<V, A, E, F, MarkDst>(a, f, sv, re - rb, e, vvals, acc, evals);
-    }
-}
-
+// vertexMap over a queue, a listed flag subset or the bitmap.
 template <typename V, typename A, typename F>
-__global__ void __launch_bounds__(kT)
-k_vertex_filter(const uint8_t *flags, VertexId n, V *vvals, A *acc, VertexId *queue,
-                VertexId *qsize, F f) {
-    for (uint64_t base = (uint64_t)blockIdx.x * kT; base < n; base += (uint64_t)gridDim.x * kT) {
-        const uint64_t v = base + threadIdx.x;
-        bool keep = false;
-        if (v < n && flags[v] && f.cond(vvals[v], acc[v])) {
-            f.update(vvals[v], acc[v]);
-            keep = true;
-        }
-        warp_append(keep, (VertexId)v, queue, qsize);
+__global__ void k_vertex_map(const Word *bits, const VertexId *list, const SubsetMeta *m,
+                             bool dense, VertexId n, V *vvals, A *acc, F f) {
+    const bool listed = dense || m->listValid;
+    const size_t count = listed ? m->qsize : n;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const VertexId v = listed ? list[i] : (VertexId)i;
+        if (listed || bit_of(bits, v)) f(vvals[v], acc[v]);
     }
 }
 
-template <typename V, typename A, typename F>
-__global__ void k_vertex_map_dense(const VertexId *queue, const VertexId *qsize, V *vvals, A *acc,
-                                   F f) {
-    const uint64_t n = *qsize;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        const VertexId v = queue[i];
-        f(vvals[v], acc[v]);
-    }
+// ------------------------------------------------------ graph preparation --
+__global__ void k_out_degrees(const EdgeId *rowptr, VertexId n, VertexId *outdeg) {
+    for (size_t v = blockIdx.x * (size_t)blockDim.x + threadIdx.x; v < n;
+         v += (size_t)gridDim.x * blockDim.x)
+        outdeg[v] = rowptr[v + 1] - rowptr[v];
 }
 
-template <typename V, typename A, typename F>
-__global__ void k_vertex_map_sparse(const uint8_t *flags, VertexId n, V *vvals, A *acc, F f) {
-    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
-         v += (uint64_t)gridDim.x * blockDim.x)
-        if (flags[v]) f(vvals[v], acc[v]);
+__global__ void k_row_of_edge(const EdgeId *rowptr, VertexId n, VertexId *src) {
+    const size_t w = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+    const size_t nw = ((size_t)gridDim.x * blockDim.x) >> 5;
+    for (size_t v = w; v < n; v += nw)
+        for (EdgeId e = rowptr[v] + lane(); e < rowptr[v + 1]; e += 32) src[e] = (VertexId)v;
+}
+
+__global__ void k_iota(EdgeId *a, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        a[i] = (EdgeId)i;
+}
+
+__global__ void k_in_degrees(const VertexId *col, size_t E, VertexId *indeg) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < E;
+         i += (size_t)gridDim.x * blockDim.x)
+        atomicAdd(&indeg[col[i]], 1u);
+}
+
+__global__ void k_gather_u32(const VertexId *in, const EdgeId *idx, size_t n, VertexId *out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        out[i] = in[idx[i]];
 }
 
 }  // namespace olive_detail

@@ -29,7 +29,7 @@
 //   void on_push(bool pushed, uint32_t v)           after each warp-wide push
 //   void flush(unsigned long long relaxed)          once per thread at the end
 #pragma once
-#include "olv_internal.cuh"
+#include "olv_travctl.cuh"
 
 namespace olv {
 
@@ -436,6 +436,155 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_pieces(Advan
     warp_stage_flush(s_q[wl], &s_qn[wl], &s_qlim[wl], qout, qout_size);
     if (Op::kHasFar) warp_stage_flush(s_f[wl], &s_fn[wl], &s_flim[wl], far, far_size);
     op.flush(0);
+}
+
+// ------------------------------------------------------------------ pull --
+// Pull over in-edge rows (the reverse graph): every row r in [0, n) that the
+// Op wants reduces the contributions of its in-edges whose source passes the
+// Op's test, and is listed once when it got at least one.  Load-balanced like
+// the push: a CTA takes kBlock consecutive rows, scans their in-degrees and
+// lets all threads walk the chunk's in-edges in order, reducing into a
+// per-row slot in shared memory; each row's owner then stores the slot and
+// lists the row.  Rows over hub_degree in-edges go to pieces of `piece` edges
+// that k_pull_pieces spreads over all warps; they reduce straight into the
+// global accumulator.  An Op supplies:
+//   using Acc                                     accumulator type
+//   static constexpr int kMinBlocks
+//   static constexpr bool kFirstHit               a row stops at its first contribution
+//   bool row_wanted(uint32_t r)
+//   Acc acc_load(uint32_t r)                      the row's current (reset) value
+//   bool contributes(uint32_t u, uint32_t e, Acc &x)   source u over in-edge e
+//   void reduce_slot(Acc &slot, const Acc &x)     into shared memory
+//   void reduce_row(uint32_t r, const Acc &x)     into the global accumulator
+//   void store(uint32_t r, const Acc &slot)
+//   bool mark(uint32_t r)                         true when r is newly marked
+struct PullArgs {
+    const uint32_t *colptr = nullptr;   // in-edges of r: [colptr[r], colptr[r+1])
+    const uint32_t *rowidx = nullptr;   // their sources
+    TravCtl *ctl = nullptr;             // runs only when ctl->mode == want_mode
+    uint32_t want_mode = 0;
+    uint32_t n = 0;                     // rows
+    uint2 *pieces = nullptr;            // (row, piece) of hub rows; count in ctl->npieces
+    uint32_t hub_degree = 0;
+    uint32_t piece = 0;
+    uint32_t *qout = nullptr;           // rows with a contribution; count in ctl->qsize[1]
+};
+
+template <class Op>
+__global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_pull_chunks(PullArgs a, Op op) {
+    TravCtl *c = a.ctl;
+    if (c->done || c->mode != a.want_mode) return;
+    using Acc = typename Op::Acc;
+    __shared__ uint32_t s_beg[kBlock], s_off[kBlock], s_warp[33];
+    __shared__ int s_hit[kBlock];
+    __shared__ __align__(16) unsigned char s_acc_raw[kBlock * sizeof(Acc)];
+    Acc *s_acc = reinterpret_cast<Acc *>(s_acc_raw);
+    uint32_t *qsize = &c->qsize[1];
+    for (uint64_t base_row = (uint64_t)blockIdx.x * kBlock; base_row < a.n;
+         base_row += (uint64_t)gridDim.x * kBlock) {
+        const uint32_t r = (uint32_t)(base_row + threadIdx.x);
+        uint32_t beg = 0, deg = 0;
+        if (r < a.n && op.row_wanted(r)) {
+            beg = __ldg(&a.colptr[r]);
+            deg = __ldg(&a.colptr[r + 1]) - beg;
+            if (deg > a.hub_degree) {
+                const uint32_t np = (deg + a.piece - 1) / a.piece;
+                const uint32_t b = atomicAdd(&c->npieces, np);
+                for (uint32_t p = 0; p < np; p++) a.pieces[b + p] = make_uint2(r, p);
+                deg = 0;
+            }
+        }
+        if (deg) s_acc[threadIdx.x] = op.acc_load(r);
+        s_hit[threadIdx.x] = 0;
+        uint32_t total;
+        const uint32_t off = block_exclusive_scan(deg, &total, s_warp);
+        s_beg[threadIdx.x] = beg;
+        s_off[threadIdx.x] = off;
+        __syncthreads();
+        for (uint32_t base = 0; base < total; base += kBlock * kItems) {
+            uint32_t lo[kItems], u[kItems], e[kItems];
+            bool act[kItems];
+#pragma unroll
+            for (int j = 0; j < kItems; j++) {
+                const uint32_t k = base + j * kBlock + threadIdx.x;
+                act[j] = k < total;
+                lo[j] = 0;
+                u[j] = 0;
+                e[j] = 0;
+                if (act[j]) {
+                    uint32_t l = 0;
+#pragma unroll
+                    for (uint32_t step = kBlock / 2; step > 0; step >>= 1)
+                        if (s_off[l + step] <= k) l += step;
+                    lo[j] = l;
+                    e[j] = s_beg[l] + (k - s_off[l]);
+                    if (Op::kFirstHit && s_hit[l]) act[j] = false;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kItems; j++)
+                if (act[j]) u[j] = __ldcs(&a.rowidx[e[j]]);   // streamed once: evict first
+#pragma unroll
+            for (int j = 0; j < kItems; j++) {
+                Acc x;
+                if (act[j] && op.contributes(u[j], e[j], x)) {
+                    op.reduce_slot(s_acc[lo[j]], x);
+                    s_hit[lo[j]] = 1;
+                }
+            }
+        }
+        __syncthreads();
+        bool newly = false;
+        if (deg && s_hit[threadIdx.x]) {
+            op.store(r, s_acc[threadIdx.x]);
+            newly = op.mark(r);
+        }
+        warp_push(newly, r, a.qout, qsize);
+        __syncthreads();   // the shared arrays are rewritten by the next chunk
+    }
+}
+
+// Hub rows of the pull: one warp per piece, contributions reduced into the
+// global accumulator.
+template <class Op>
+__global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_pull_pieces(PullArgs a, Op op) {
+    TravCtl *c = a.ctl;
+    if (c->done || c->mode != a.want_mode) return;
+    const uint32_t np = c->npieces;
+    if (np == 0) return;
+    using Acc = typename Op::Acc;
+    const uint32_t lane = lane_id();
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t p = warp; p < np; p += nwarps) {
+        const uint2 pc = a.pieces[p];
+        const uint32_t r = pc.x;
+        const uint32_t rb = __ldg(&a.colptr[r]), re = __ldg(&a.colptr[r + 1]);
+        const uint32_t b = rb + pc.y * a.piece;
+        const uint32_t e_end = min(re, b + a.piece);
+        bool hit = false;
+        for (uint32_t base = b; base < e_end; base += 32 * kItems) {
+            uint32_t u[kItems], e[kItems];
+#pragma unroll
+            for (int j = 0; j < kItems; j++) {
+                e[j] = base + j * 32 + lane;
+                u[j] = e[j] < e_end ? __ldcs(&a.rowidx[e[j]]) : 0;
+            }
+#pragma unroll
+            for (int j = 0; j < kItems; j++) {
+                Acc x;
+                if (e[j] < e_end && op.contributes(u[j], e[j], x)) {
+                    op.reduce_row(r, x);
+                    hit = true;
+                }
+            }
+            if (Op::kFirstHit && __any_sync(0xffffffffu, hit)) break;
+        }
+        const bool any = __any_sync(0xffffffffu, hit);
+        bool newly = false;
+        if (any && lane == 0) newly = op.mark(r);
+        warp_push(newly, r, a.qout, &c->qsize[1]);
+    }
 }
 
 }  // namespace olv

@@ -33,7 +33,8 @@ def nvcc():
 
 def _headers():
     return glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(
-        os.path.join(ROOT, "include", "*.h"))
+        os.path.join(ROOT, "include", "*.h")) + glob.glob(
+        os.path.join(ROOT, "include", "olive_b200", "*.cuh"))
 
 
 def _stale(obj, src, deps):

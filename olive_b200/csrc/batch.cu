@@ -25,7 +25,7 @@
 
 #include <cooperative_groups.h>
 
-#include "olv_advance.cuh"
+#include "olive_b200/olv_advance.cuh"
 #include "olv_internal.cuh"
 
 namespace cg = cooperative_groups;

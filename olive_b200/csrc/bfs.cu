@@ -23,7 +23,7 @@
 
 #include <cub/cub.cuh>
 
-#include "olv_advance.cuh"
+#include "olive_b200/olv_advance.cuh"
 #include "olv_graphexec.cuh"
 #include "olv_internal.cuh"
 

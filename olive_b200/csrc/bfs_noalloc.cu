@@ -28,7 +28,7 @@
 // here, so such a call is rejected before anything is launched.
 #include <mutex>
 
-#include "olv_advance.cuh"
+#include "olive_b200/olv_advance.cuh"
 #include "olv_internal.cuh"
 
 namespace olv {

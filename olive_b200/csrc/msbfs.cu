@@ -29,7 +29,7 @@
 
 #include <vector>
 
-#include "olv_advance.cuh"
+#include "olive_b200/olv_advance.cuh"
 #include "olv_graphexec.cuh"
 #include "olv_internal.cuh"
 

@@ -49,7 +49,7 @@
 #include <algorithm>
 #include <vector>
 
-#include "olv_advance.cuh"
+#include "olive_b200/olv_advance.cuh"
 #include "olv_graphexec.cuh"
 #include "olv_internal.cuh"
 
