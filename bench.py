@@ -66,8 +66,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["sssp", "bfs", "pagerank", "msbfs", "wpr", "batch"],
-                    default="sssp")
+    ap.add_argument("--workload", choices=["sssp", "bfs", "pagerank", "msbfs", "wpr", "batch",
+                                           "ppr"], default="sssp")
     ap.add_argument("--scale", type=int, default=None)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
@@ -86,7 +86,7 @@ def parse():
 
 
 def default_scale(w):
-    return {"pagerank": 22, "wpr": 20, "batch": 0}.get(w, 24)
+    return {"pagerank": 22, "ppr": 22, "wpr": 20, "batch": 0}.get(w, 24)
 
 
 def metric_name(w, scale):
@@ -103,6 +103,9 @@ def metric_name(w, scale):
     if w == "batch":
         return ("512 ER graphs (V in [1K,64K], 8 edges/vertex) block-diagonal: BFS + K=32 PPR "
                 "per graph in one persistent launch, edge visits per second")
+    if w == "ppr":
+        return (f"K=32 personalised PageRank GE/s/iter (edge visits carrying 32 values), "
+                f"RMAT-{scale} ef16, alpha 0.85, FP32")
     return f"PageRank GE/s/iter, RMAT-{scale} ef16, alpha 0.85, FP32, dangling redistributed"
 
 
@@ -775,18 +778,90 @@ def batch_line(a, rank, world, local_rank):
     return line
 
 
+# --------------------------------------------- K-vector personalised PR --
+def ppr_line(a, rank, world, local_rank):
+    """32 personalised PageRank vectors on RMAT-22 (seeds uniform over vertices
+    with out-degree >= 1, numpy seed 3), advanced together by olv_ppr_batch;
+    a step is one solve (<= 50 iterations, tol 1e-7)."""
+    import torch
+    import olive_b200 as ob
+    stream = torch.cuda.current_stream()
+    g = ob.Graph.rmat(a.scale, 16, a.seed)
+    g.set_stream(stream)
+    V, E = g.V, g.E
+    rp, cl, _ = g.csr()
+    deg = np.diff(rp.astype(np.int64))
+    K = 32
+    seeds = np.random.default_rng(3).choice(np.flatnonzero(deg > 0), K,
+                                            replace=False).astype(np.uint32)
+    sd = torch.from_numpy(seeds.astype(np.int32)).cuda()
+    out = torch.empty((V, K), dtype=torch.float32, device="cuda")
+
+    def step():
+        g.ppr(sd, 0.85, 50, 1e-7, out=out)
+
+    for _ in range(a.warmup):
+        step()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    barrier(world)
+    ms = max_over_ranks(timed(stream, step, a.steps), world)
+    clk = clocks.stop()
+    st = g.last_stats
+    it = st.iterations
+    units = E * it                                  # edge visits (each carries K values)
+    value = world * units / (ms * 1e-3) / 1e9
+    peak, peak_src = peaks()
+    alg = (E * (4 + 4 * K) + V * (12 * K + 8)) * it
+    kern_ms = st.device_ms
+    roofline = {"bound": "hbm", "achieved": round(alg / (kern_ms * 1e-3) / 1e9, 1),
+                "peak": peak, "unit": "GB/s",
+                "frac": round(alg / (kern_ms * 1e-3) / 1e9 / peak, 4),
+                "kernel": "olv_ppr_batch solve (pull SpMM over the reverse graph, CUDA graph)",
+                "algorithmic_bytes": int(alg),
+                "bytes_formula": "per iteration: (4 B in-edge id + 4K B contribution row) per "
+                                 "edge + (x read, x write, y write: 12K B + 8 B) per vertex",
+                "peak_source": peak_src, "kernel_ms": round(kern_ms, 4)}
+    host = torch.empty((V, K), dtype=torch.float32, pin_memory=True)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        g.ppr(seeds, 0.85, 50, 1e-7, out=host)
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / a.steps, world)
+    e2e = {"value": round(world * units / (e2e_ms * 1e-3) / 1e9, 3), "unit": "GE/s/iter",
+           "h2d_bytes_per_step": int(seeds.nbytes), "d2h_bytes_per_step": int(4 * V * K),
+           "ms_per_step": round(e2e_ms, 3)}
+    extra = {"K": K, "iterations": it}
+    if rank == 0 and not a.no_parity:
+        from oracle import oracle
+        ks = [0, 31]
+        ref, _ = oracle.ppr(rp, cl, seeds[ks], 0.85, it, 0.0)
+        got = host.numpy()[:, ks].astype(np.float64)
+        err = float(max(np.max(np.abs(got[:, j] - ref[:, j])) / np.max(ref[:, j])
+                        for j in range(len(ks))))
+        extra["parity"] = parity_float(err, 1e-6, f"FP64 oracle, vectors 0 and 31, the same "
+                                                  f"{it} iterations (normwise per vector)")
+    config = workload_config(a, V, E, None, {"K": K, "seeds": "32 distinct, out-degree >= 1",
+                                             "alpha": 0.85, "max_it": 50, "tol": 1e-7})
+    config["workload"] = f"ppr32-rmat{a.scale}"
+    line = common_line(a, world, "GE/s/iter", value, ms, "f32",
+                       "synthetic (seeded RMAT, generated on the device)", config, roofline,
+                       None, e2e, a.steps * (3 * it + 4), clk, extra)
+    g.close()
+    return line
+
+
 # ------------------------------------------------------- default extras --
 def extras(a, rank, world, local_rank):
     """The other benchmarked configurations, each as a compact summary in the
     default line: msBFS-64 on RMAT-24, PageRank on RMAT-22, weighted PageRank
     forward + adjoint on RMAT-20, the ER-512 batch."""
     out = {}
-    for w in ("msbfs", "pagerank", "wpr", "batch"):
+    for w in ("msbfs", "pagerank", "ppr", "wpr", "batch"):
         b = copy.copy(a)
         b.workload, b.scale = w, default_scale(w)
         b.steps, b.warmup = min(a.steps, 10), 3
         b.no_cpu_baseline = True
-        fn = {"wpr": wpr_line, "batch": batch_line}.get(w, traversal_line)
+        fn = {"wpr": wpr_line, "batch": batch_line, "ppr": ppr_line}.get(w, traversal_line)
         ln = fn(b, rank, world, local_rank) if fn is not traversal_line else \
             traversal_line(b, rank, world, local_rank, extra_keys=False)
         s = {"metric": ln["metric"], "value": ln["value"], "unit": ln["unit"],
@@ -962,6 +1037,20 @@ def run_reference(a, rank, world):
                 vals.append(edges / secs / 1e9)
                 ms.append(secs * 1e3)
         unit, cores = "GTEPS", 1
+    elif a.workload == "ppr":
+        K = 32
+        seeds = np.random.default_rng(3).choice(np.flatnonzero(deg > 0), K,
+                                                replace=False).astype(np.uint32)
+        desc = ("oracle FP64 personalised PageRank, the GPU arm's 32 seeds (the reference has "
+                "no PPR; 1 core); each step 2 iterations")
+        for i in range(a.warmup + a.steps):
+            t = time.perf_counter()
+            oracle.ppr(rp, cl, seeds, 0.85, 2, 0.0)
+            secs = time.perf_counter() - t
+            if i >= a.warmup:
+                vals.append(E * 2 / secs / 1e9)
+                ms.append(secs * 1e3)
+        unit, cores = "GE/s/iter", 1
     elif a.workload == "wpr":
         # the GPU arm's inputs: lognormal weights and Dirichlet(1) p, numpy seed 7
         rng = np.random.default_rng(7)
@@ -994,7 +1083,7 @@ def run_reference(a, rank, world):
             "value": round(value, 5), "unit": unit, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": round(float(np.median(ms)) if ms else 0.0, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if a.workload in ("pagerank", "wpr") else "u32",
+            "dtype": "f64" if a.workload in ("pagerank", "wpr", "ppr") else "u32",
             "data": "synthetic (seeded RMAT, generated on the host)",
             "config": workload_config(a, V, E, src, {
                 "weights": "lognormal(0,1) FP32, numpy seed 7", "p": "Dirichlet(1)",
@@ -1022,7 +1111,7 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
-    fn = {"wpr": wpr_line, "batch": batch_line}.get(a.workload, traversal_line)
+    fn = {"wpr": wpr_line, "batch": batch_line, "ppr": ppr_line}.get(a.workload, traversal_line)
     line = fn(a, rank, world, local_rank)
     if a.workload == "sssp" and not a.no_extras:
         line.update(extras(a, rank, world, local_rank))

@@ -145,9 +145,14 @@ public:
             CUDA_CHECK(cudaMalloc((void **)&edgeValues_, (E ? E : 1) * sizeof(EdgeValue)));
             CUDA_CHECK(cudaMemset(edgeValues_, 0, (E ? E : 1) * sizeof(EdgeValue)));
         }
+        // hub pieces of either direction, or the first-hit pull's list of rows
+        // with more than olv::kFirstLight in-edges (uint32 entries, at most E / 32)
         const size_t np = E / olive_detail::kPiece + E / olive_detail::kHub + 16;
         const size_t npp = E / olive_detail::kPullPiece + E / olive_detail::kPullHub + 16;
-        CUDA_CHECK(cudaMalloc((void **)&pieces_, (np > npp ? np : npp) * sizeof(uint2)));
+        const size_t nlong = (E / olv::kFirstLight + 16) / 2 + 1;
+        size_t npieces = np > npp ? np : npp;
+        if (nlong > npieces) npieces = nlong;
+        CUDA_CHECK(cudaMalloc((void **)&pieces_, npieces * sizeof(uint2)));
         CUDA_CHECK(cudaMalloc((void **)&ctl_, sizeof(olv::TravCtl)));
         CUDA_CHECK(cudaMemset(ctl_, 0, sizeof(olv::TravCtl)));
         CUDA_CHECK(cudaMalloc((void **)&mapBits_, (words() ? words() : 1) * sizeof(Word)));
@@ -258,8 +263,10 @@ private:
         using PushT = PushOp<VertexValue, AccumValue, EdgeValue, F, true>;
         using PullT = PullOp<VertexValue, AccumValue, EdgeValue, F>;
         const int policy = colptr_ ? policy_ : 0;
-        const unsigned long long pull_edges =
-            (unsigned long long)((double)edgeCount_ / pullDiv_);
+        // a first-contribution pull reads far fewer in-edges than a full one,
+        // so it pays off for smaller frontiers
+        const double div = pull_first_hit<F>::value ? pullDiv_ * kFirstHitPullFactor : pullDiv_;
+        const unsigned long long pull_edges = (unsigned long long)((double)edgeCount_ / div);
         k_edge_setup<<<1, 1>>>(ctl_, src.meta, policy, pull_edges);
         olv::AdvanceArgs a;
         a.rbeg = rowptr_;
@@ -277,6 +284,7 @@ private:
         if (!push_grid) push_grid = persistentGrid(olv::k_advance_chunks<PushT>);
         olv::k_advance_chunks<PushT><<<push_grid, kT>>>(a, po);
         olv::k_advance_pieces<PushT><<<push_grid, kT>>>(a, po);
+        constexpr bool first_hit = pull_first_hit<F>::value;
         if (policy != 0) {
             olv::PullArgs p;
             p.colptr = colptr_;
@@ -290,9 +298,15 @@ private:
             p.qout = dlist;
             PullT pl{f, outdeg_, eid_, src.bits, vertexValues_, accumulators_, edgeValues_, dbits};
             static unsigned pull_grid = 0;
-            if (!pull_grid) pull_grid = persistentGrid(olv::k_pull_chunks<PullT>);
-            olv::k_pull_chunks<PullT><<<pull_grid, kT>>>(p, pl);
-            olv::k_pull_pieces<PullT><<<pull_grid, kT>>>(p, pl);
+            if constexpr (first_hit) {   // bottom-up: each row stops at its first contribution
+                if (!pull_grid) pull_grid = persistentGrid(olv::k_pull_first_rows<PullT>);
+                olv::k_pull_first_rows<PullT><<<pull_grid, kT>>>(p, pl);
+                olv::k_pull_first_long<PullT><<<pull_grid, kT>>>(p, pl);
+            } else {
+                if (!pull_grid) pull_grid = persistentGrid(olv::k_pull_chunks<PullT>);
+                olv::k_pull_chunks<PullT><<<pull_grid, kT>>>(p, pl);
+                olv::k_pull_pieces<PullT><<<pull_grid, kT>>>(p, pl);
+            }
         }
         k_edge_finish<<<gridV(), 256>>>(ctl_, dmeta, dlist, accList_, accMeta_);
         CUDA_CHECK(cudaGetLastError());

@@ -200,6 +200,17 @@ int olv_wpr_forward(olv_graph *g, const float *w, const float *p, double alpha, 
 int olv_wpr_backward(olv_wpr_ctx *ctx, const float *g, int max_it, double tol, float *dw_out,
                      float *dp_out, olv_stats *st);
 int olv_wpr_ctx_destroy(olv_wpr_ctx *ctx);
+/* K personalised PageRank vectors on a general graph (no reference
+ * counterpart; each vector follows PageRank.cu:51-75 with the teleport to its
+ * own seed): for seed s_k, from r_k = e_{s_k},
+ *   r_k'[v] = alpha * sum_{u->v} r_k[u]/outdeg(u) + [v == s_k]((1-alpha) + alpha d_k)
+ * with d_k the vector's dangling mass (it returns to the seed).  K <= 32
+ * vectors advance together: one pull over the reverse graph per iteration
+ * gathers each in-neighbour's 128-byte row of K contributions (fixed order,
+ * compensated FP32 sums; FP64 residual).  Stops after max_it iterations or
+ * when every vector's L1 change < tol.  out is [V][K] FP32, vertex-major.  */
+int olv_ppr_batch(olv_graph *g, const uint32_t *seeds, int K, double alpha, int max_it,
+                  double tol, float *out, olv_stats *st);
 /* PageRank (PageRank.cu:89-147 / testPageRank.cu:41-115), FP32 ranks from a
  * deterministic pull over the reverse graph, FP64 residual.  Runs max_it
  * iterations or until the L1 residual < tol.                                  */

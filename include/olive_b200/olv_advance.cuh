@@ -587,4 +587,84 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_pull_pieces(PullArgs
     }
 }
 
+// First-contribution pull (Ops with kFirstHit: any single contribution is
+// enough, as for BFS levels): a bottom-up step that stops each row at its
+// first contributing in-edge.  k_pull_first_rows gives every wanted row with
+// at most kFirstLight in-edges to one thread, which reads its in-edges four at
+// a time and stops at the first source that passes; longer rows are listed in
+// a.pieces (count in ctl->npieces) for k_pull_first_long, one warp per row,
+// 32 in-edges per step with a warp vote to stop.
+constexpr uint32_t kFirstLight = 32;
+
+template <class Op>
+__global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_pull_first_rows(PullArgs a, Op op) {
+    TravCtl *c = a.ctl;
+    if (c->done || c->mode != a.want_mode) return;
+    using Acc = typename Op::Acc;
+    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < a.n;
+         base += (uint64_t)gridDim.x * kBlock) {
+        const uint32_t r = (uint32_t)(base + threadIdx.x);
+        bool newly = false, is_long = false;
+        if (r < a.n && op.row_wanted(r)) {
+            const uint32_t b = __ldg(&a.colptr[r]), e = __ldg(&a.colptr[r + 1]);
+            if (e - b > kFirstLight) {
+                is_long = true;
+            } else {
+                for (uint32_t i = b; i < e; i += 4) {
+                    uint32_t u[4];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) u[j] = i + j < e ? __ldcs(&a.rowidx[i + j]) : 0;
+                    bool hit = false;
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        Acc x;
+                        if (!hit && i + j < e && op.contributes(u[j], i + j, x)) {
+                            op.reduce_row(r, x);
+                            hit = true;
+                        }
+                    }
+                    if (hit) {
+                        newly = op.mark(r);
+                        break;
+                    }
+                }
+            }
+        }
+        warp_push(is_long, r, reinterpret_cast<uint32_t *>(a.pieces), &c->npieces);
+        warp_push(newly, r, a.qout, &c->qsize[1]);
+    }
+}
+
+template <class Op>
+__global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_pull_first_long(PullArgs a, Op op) {
+    TravCtl *c = a.ctl;
+    if (c->done || c->mode != a.want_mode) return;
+    using Acc = typename Op::Acc;
+    const uint32_t nl = c->npieces;
+    const uint32_t *rows = reinterpret_cast<const uint32_t *>(a.pieces);
+    const uint32_t lane = lane_id();
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t k = warp; k < nl; k += nwarps) {
+        const uint32_t r = rows[k];
+        const uint32_t b = __ldg(&a.colptr[r]), e = __ldg(&a.colptr[r + 1]);
+        bool found = false;
+        for (uint32_t i = b; i < e; i += 32) {
+            const uint32_t j = i + lane;
+            const uint32_t u = j < e ? __ldcs(&a.rowidx[j]) : 0;
+            Acc x;
+            const bool hit = j < e && op.contributes(u, j, x);
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (m) {
+                if (lane == (uint32_t)(__ffs(m) - 1)) op.reduce_row(r, x);
+                found = true;
+                break;
+            }
+        }
+        bool newly = false;
+        if (found && lane == 0) newly = op.mark(r);
+        warp_push(newly, r, a.qout, &c->qsize[1]);
+    }
+}
+
 }  // namespace olv

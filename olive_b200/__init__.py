@@ -83,6 +83,7 @@ _SIGS = [
     ("olv_batch_run", _I, [_VP, _VP, _I, _I, _VP, _D, _I, _D, _VP, _VP, _VP,
                            ctypes.POINTER(Stats)]),
     ("olv_pagerank", _I, [_VP, _D, _I, _D, _I, _VP, ctypes.POINTER(Stats)]),
+    ("olv_ppr_batch", _I, [_VP, _VP, _I, _D, _I, _D, _VP, ctypes.POINTER(Stats)]),
     ("olv_wpr_forward", _I, [_VP, _VP, _VP, _D, _I, _D, _VP, ctypes.POINTER(_VP),
                              ctypes.POINTER(Stats)]),
     ("olv_wpr_backward", _I, [_VP, _VP, _I, _D, _VP, _VP, ctypes.POINTER(Stats)]),
@@ -345,6 +346,19 @@ class Graph:
                                       ctypes.byref(st)), "olv_wpr_backward")
         self.last_stats = st
         return dw, dp
+
+    def ppr(self, seeds, alpha=0.85, max_it=50, tol=1e-7, out=None):
+        """K <= 32 personalised PageRank vectors (one per seed), advanced
+        together: array [V, K] FP32."""
+        if not hasattr(seeds, "data_ptr"):
+            seeds = np.ascontiguousarray(seeds, np.uint32)
+        K = len(seeds)
+        out = np.empty((self.V, K), np.float32) if out is None else out
+        st = Stats()
+        _check(lib().olv_ppr_batch(self._h, _ptr(seeds), K, alpha, max_it, tol, _ptr(out),
+                                   ctypes.byref(st)), "olv_ppr_batch")
+        self.last_stats = st
+        return out
 
     def pagerank(self, alpha=0.85, max_it=50, tol=1e-7, dangling="uniform", out=None):
         out = self._out(out, np.float32)

@@ -438,6 +438,7 @@ int olv_graph_destroy(olv_graph *g) {
     g->outdeg_f.release();
     g->ws.release();
     release_pr_state(g);
+    release_ppr_state(g);
     release_ms_state(g);
     release_wpr_state(g);
     release_batch_state(g);

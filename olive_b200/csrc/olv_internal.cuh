@@ -123,6 +123,7 @@ struct olv_graph {
     olv::WhileGraph *bfs_graph = nullptr;
     olv::WhileGraph *sssp_graph = nullptr;
     void *pr_state = nullptr;            // PageRank plan + graph (pagerank.cu)
+    void *ppr_state = nullptr;           // K-vector personalised PageRank (ppr.cu)
     void *ms_state = nullptr;            // multi-source BFS masks + graph (msbfs.cu)
     void *wpr_state = nullptr;           // weighted PageRank row plans (wpr.cu)
     void *batch_state = nullptr;         // batch buffers kept between calls (batch.cu)
@@ -132,6 +133,7 @@ namespace olv {
 // Resident CTAs of kBlock threads for `kernel` on all SMs (a persistent grid).
 int resident_blocks(const olv_graph *g, const void *kernel, int *blocks);
 void release_pr_state(olv_graph *g);
+void release_ppr_state(olv_graph *g);
 void release_ms_state(olv_graph *g);
 void release_wpr_state(olv_graph *g);
 void release_batch_state(olv_graph *g);

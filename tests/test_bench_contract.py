@@ -22,7 +22,8 @@ def _run(args, env=None):
 
 
 @pytest.mark.parametrize("workload,scale", [("sssp", 10), ("bfs", 10), ("pagerank", 10),
-                                            ("msbfs", 10), ("wpr", 10), ("batch", 0)])
+                                            ("msbfs", 10), ("wpr", 10), ("batch", 0),
+                                            ("ppr", 10)])
 def test_reference_arm_line(workload, scale):
     lines = _run(["--impl", "reference", "--workload", workload, "--scale", str(scale),
                   "--steps", "2", "--warmup", "1", "--ref-seconds", "0.5"])

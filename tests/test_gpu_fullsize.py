@@ -229,3 +229,27 @@ def test_past_2pow24_vertices_header_layer(ob, big_tree, tmp_path, name):
     assert p.returncode == 0, p.stderr[-2000:]
     got = _read_ints(str(tmp_path / f"{name}.txt"))
     np.testing.assert_array_equal(got, _tree_levels(BIG_V).astype(np.int64))
+
+
+def test_ppr32_rmat22_vs_oracle(ob):
+    """32 personalised PageRank vectors on RMAT-22 (the benchmarked size)."""
+    with ob.Graph.rmat(22, 16, 1) as g:
+        rp, cl, _ = g.csr()
+        deg = np.diff(rp.astype(np.int64))
+        seeds = np.random.default_rng(3).choice(np.flatnonzero(deg > 0), 32,
+                                                replace=False).astype(np.uint32)
+        out = g.ppr(seeds, 0.85, 50, 1e-7)
+        it = g.last_stats.iterations
+    # the oracle in four parallel slices of 8 vectors (FP64, same iterations)
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(4) as ex:
+        parts = list(ex.map(lambda k: oracle.ppr(rp, cl, seeds[k:k + 8], 0.85, it, 0.0),
+                            range(0, 32, 8)))
+    ref = np.concatenate([p[0] for p in parts], axis=1)
+    got = out.astype(np.float64)
+    for k in range(32):
+        r, gk = ref[:, k], got[:, k]
+        assert np.max(np.abs(gk - r)) <= 1e-6 * np.max(np.abs(r)), k
+        nz = r > 0
+        assert np.all(gk[~nz] == 0)
+        assert np.max(np.abs(gk[nz] - r[nz]) / r[nz]) < 1e-5, k
