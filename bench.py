@@ -302,6 +302,33 @@ def cold_e2e(ob, stream, rp, cl, w, src, method, reps=2):
                     "result -> olv_graph_destroy; wall clock, best of %d" % reps}
 
 
+def writer_line(ob, dev_vals, stream):
+    """The solve's V results written as "%d\\n" text from device memory
+    (olv_write_text: formatted on the GPU, one fwrite per 2^24 values) against
+    the reference's way (a host fprintf per vertex), both to local files,
+    which must be identical."""
+    import torch
+    from oracle import oracle
+    work = tempfile.mkdtemp(prefix="olv_writer_")
+    a, b = os.path.join(work, "gpu.txt"), os.path.join(work, "printf.txt")
+    vals = dev_vals.view(torch.int32)
+    ob.write_text(a, vals, stream)               # warm-up (allocations)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    nbytes = ob.write_text(a, vals, stream)
+    gpu_s = time.perf_counter() - t0
+    host = vals.cpu().numpy()
+    cpu_s = oracle.fprintf_i32(b, host)
+    same = open(a, "rb").read() == open(b, "rb").read()
+    shutil.rmtree(work, ignore_errors=True)
+    return {"values": int(vals.numel()), "bytes": int(nbytes), "gpu_ms": round(gpu_s * 1e3, 2),
+            "gpu_GB_per_s": round(nbytes / gpu_s / 1e9, 3),
+            "printf_loop_ms": round(cpu_s * 1e3, 2), "speedup": round(cpu_s / gpu_s, 2),
+            "identical_bytes": bool(same),
+            "note": "olv_write_text from device memory to a local file (format on the GPU, "
+                    "D2H, fwrite) vs one fprintf per value on one host core"}
+
+
 # ------------------------------------------------- traversal workloads --
 def traversal_line(a, rank, world, local_rank, extra_keys=True):
     """SSSP / BFS / msBFS / PageRank on a seeded RMAT graph built on the device."""
@@ -509,6 +536,7 @@ def traversal_line(a, rank, world, local_rank, extra_keys=True):
     if a.workload in ("sssp", "bfs") and extra_keys and rank == 0:
         method = "sssp" if a.workload == "sssp" else "bfs"
         extra["e2e_cold"] = cold_e2e(ob, stream, rp, cl, w if weights else None, src, method)
+        extra["writer"] = writer_line(ob, out, stream)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:

@@ -48,6 +48,12 @@ extern "C" {
 #define OLV_FMT_EDGE_LIST 0   /* "V E" then "src dst [weight]" lines, '#' comments  */
 #define OLV_FMT_DIMACS    1   /* METIS / DIMACS-10 adjacency lines, 1-based ids     */
 
+/* type for olv_write_text */
+#define OLV_TEXT_I32 0   /* int32, "%d\n"                     */
+#define OLV_TEXT_U32 1   /* uint32, "%u\n"                    */
+#define OLV_TEXT_F32 2   /* float, "%f\n" of its double value  */
+#define OLV_TEXT_F64 3   /* double, "%f\n"                    */
+
 /* dangling_mode for olv_pagerank */
 #define OLV_DANGLING_UNIFORM 0   /* redistribute dangling mass uniformly          */
 #define OLV_DANGLING_LEAK    1   /* drop it, as PageRank.cu:63-75 / testPageRank */
@@ -84,7 +90,9 @@ int olv_graph_create_rmat(int scale, int edge_factor, uint64_t seed, int weight_
 /* Load a graph file, parsed on the device (replaces CsrGraph::fromEdgeListFile,
  * csrGraph.h:106-171, and fromDimacsFile, csrGraph.h:177-236).  Edge lists are
  * stably sorted by source (the reference assumed sorted input); an optional
- * third column becomes uint32 weights.  DIMACS stores both directions (2E). */
+ * third column becomes uint32 weights.  DIMACS stores both directions (2E).
+ * A file written by olv_graph_save (it starts with "OLVCSR1\n") is read as
+ * that binary CSR whatever the format argument.                              */
 int olv_graph_load(const char *path, int format, olv_graph **out);
 int olv_graph_destroy(olv_graph *g);
 int olv_graph_info(const olv_graph *g, uint32_t *V, uint64_t *E, int *weight_type);
@@ -216,6 +224,22 @@ int olv_ppr_batch(olv_graph *g, const uint32_t *seeds, int K, double alpha, int 
  * iterations or until the L1 residual < tol.                                  */
 int olv_pagerank(olv_graph *g, double alpha, int max_it, double tol, int dangling_mode,
                  float *rank_out, olv_stats *st);
+
+/* ---- output ----------------------------------------------------------------
+ * Write n values as text, one per line, byte for byte as the reference apps'
+ * print() loops would (printVertices, oliver.h:204-212, with "%d\n" in
+ * BFS.cu:41-43 / SSSP.cu:41-43 and "%f\n" in PageRank.cu:42-44, rounded as
+ * glibc's printf rounds), formatted on the GPU in chunks of 2^24 values.
+ * values may be host or device memory; stream is a cudaStream_t (NULL: the
+ * default stream); *bytes_out (if not NULL) gets the file size.  "%f" values
+ * of magnitude 2^107 or more return OLV_ERR_LIMIT.                           */
+int olv_write_text(const char *path, const void *values, uint64_t n, int type, void *stream,
+                   uint64_t *bytes_out);
+/* Binary CSR dump (no reference counterpart): "OLVCSR1\n", uint64 V, E, flags
+ * (bit 0: uint32 weights follow), uint32 rowptr[V+1], col[E], [weights[E]];
+ * olv_graph_load reads it (either format value) and so does the header
+ * layer's CsrGraph::fromEdgeListFile.                                         */
+int olv_graph_save(const olv_graph *g, const char *path);
 
 #ifdef __cplusplus
 }

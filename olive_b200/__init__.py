@@ -11,7 +11,7 @@ import os
 
 import numpy as np
 
-__all__ = ["Graph", "OliveError", "lib", "INF", "Stats", "write_csr_binary"]
+__all__ = ["Graph", "OliveError", "lib", "INF", "Stats", "write_csr_binary", "write_text"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libolive_b200.so")
@@ -42,6 +42,21 @@ def write_csr_binary(path, rowptr, col, values=None):
         col.tofile(f)
         if values is not None:
             np.ascontiguousarray(values, np.uint32).tofile(f)
+
+
+def write_text(path, values, stream=None):
+    """Write values (int32 -> "%d", uint32 -> "%u", float32/float64 -> "%f"),
+    one per line, formatted on the GPU (olv_write_text).  values: a numpy
+    array or a CUDA tensor.  Returns the bytes written."""
+    dt = str(values.dtype).replace("torch.", "")
+    if dt not in TEXT_TYPES:
+        raise ValueError(f"write_text: unsupported dtype {values.dtype}")
+    n = values.numel() if hasattr(values, "numel") else values.size
+    out = _U64()
+    s = getattr(stream, "cuda_stream", stream)
+    _check(lib().olv_write_text(str(path).encode(), _ptr(values), n, TEXT_TYPES[dt], s,
+                                ctypes.byref(out)), "olv_write_text")
+    return out.value
 
 
 class Stats(ctypes.Structure):
@@ -88,7 +103,11 @@ _SIGS = [
                              ctypes.POINTER(Stats)]),
     ("olv_wpr_backward", _I, [_VP, _VP, _I, _D, _VP, _VP, ctypes.POINTER(Stats)]),
     ("olv_wpr_ctx_destroy", _I, [_VP]),
+    ("olv_write_text", _I, [ctypes.c_char_p, _VP, _U64, _I, _VP, ctypes.POINTER(_U64)]),
+    ("olv_graph_save", _I, [_VP, ctypes.c_char_p]),
 ]
+
+TEXT_TYPES = {"int32": 0, "uint32": 1, "float32": 2, "float64": 3}
 
 
 def lib():
@@ -223,6 +242,10 @@ class Graph:
                                         _ptr(w) if self.weight_type else None),
                "olv_graph_copy_csr")
         return rowptr, col[:self.E], (w[:self.E] if self.weight_type else None)
+
+    def save(self, path):
+        """Binary CSR dump (olv_graph_save), read back by Graph.load."""
+        _check(lib().olv_graph_save(self._h, str(path).encode()), "olv_graph_save")
 
     def max_degree_vertex(self):
         v, d = _U32(), _U32()

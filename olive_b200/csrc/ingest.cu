@@ -392,11 +392,45 @@ static int ingest(const char *path, int dimacs, olv_graph **out, uint32_t *V_out
 
 using namespace olv;
 
+// A binary CSR file of olv_graph_save: 1 = loaded, 0 = not that format.
+static int load_binary_csr(const char *path, olv_graph **out, int *rc) {
+    FILE *f = fopen(path, "rb");
+    if (!f) return 0;
+    char magic[8];
+    uint64_t hdr[3];
+    if (fread(magic, 1, 8, f) != 8 || memcmp(magic, "OLVCSR1\n", 8) != 0) {
+        fclose(f);
+        return 0;
+    }
+    if (fread(hdr, 8, 3, f) != 3 || hdr[0] >= 0xffffffffull || hdr[1] > 0xffffffffull) {
+        fclose(f);
+        set_error("olv_graph_load: bad binary CSR header in %s", path);
+        *rc = OLV_ERR_ARG;
+        return 1;
+    }
+    const uint64_t V = hdr[0], E = hdr[1];
+    const bool wts = hdr[2] & 1;
+    std::vector<uint32_t> rp(V + 1), cl(E ? E : 1), w(wts && E ? E : 1);
+    bool ok = fread(rp.data(), 4, V + 1, f) == V + 1 && fread(cl.data(), 4, E, f) == E &&
+              (!wts || fread(w.data(), 4, E, f) == E);
+    fclose(f);
+    if (!ok) {
+        set_error("olv_graph_load: truncated binary CSR file %s", path);
+        *rc = OLV_ERR_ARG;
+        return 1;
+    }
+    *rc = olv_graph_create(rp.data(), E ? cl.data() : nullptr, wts ? w.data() : nullptr,
+                           wts ? OLV_W_U32 : OLV_W_NONE, (uint32_t)V, E, out);
+    return 1;
+}
+
 extern "C" int olv_graph_load(const char *path, int format, olv_graph **out) {
     OLV_CHECK_ARG(path && out, "olv_graph_load: null pointer");
     OLV_CHECK_ARG(format == OLV_FMT_EDGE_LIST || format == OLV_FMT_DIMACS,
                   "olv_graph_load: bad format %d", format);
     *out = nullptr;
+    int rc = OLV_OK;
+    if (load_binary_csr(path, out, &rc)) return rc;
     uint32_t V = 0;
     uint64_t E = 0;
     return ingest(path, format == OLV_FMT_DIMACS, out, &V, &E);

@@ -31,9 +31,18 @@ int cuda_fail(cudaError_t e, const char *what, const char *file, int line);
 // -------------------------------------------------------- device buffer --
 // A plain owned device allocation (no host mirror: the reference's GRD<T>,
 // grd.h:43-170, kept a host copy and synchronised it every superstep).
+// Freed when it goes out of scope; not copyable (a copy would free twice).
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    DevBuf(DevBuf &&o) noexcept : p(o.p), bytes(o.bytes) {
+        o.p = nullptr;
+        o.bytes = 0;
+    }
+    ~DevBuf() { release(); }
     int ensure(size_t n);     // grow to at least n bytes (contents not kept)
     void release();
     template <class T> T *as() const { return static_cast<T *>(p); }

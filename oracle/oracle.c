@@ -775,3 +775,18 @@ int orc_write_edge_list(const char *path, uint32_t V, const uint32_t *rowptr,
     if (fclose(f) != 0) rc = -1;
     return rc;
 }
+
+/* ------------------------------------------------------------------------ */
+/* The reference's way of writing results: one fprintf("%d\n") per vertex    */
+/* on the host (printVertices, oliver.h:204-212, through BFS_Vertex::print,  */
+/* BFS.cu:41-43).  Baseline for the GPU writer; returns seconds, < 0 when    */
+/* the file cannot be written.                                                */
+/* ------------------------------------------------------------------------ */
+double orc_fprintf_i32(const char *path, const int32_t *v, uint64_t n) {
+    double t0 = orc_now();
+    FILE *f = fopen(path, "w");
+    if (!f) return -1.0;
+    for (uint64_t i = 0; i < n; i++) fprintf(f, "%d\n", v[i]);
+    if (fclose(f) != 0) return -1.0;
+    return orc_now() - t0;
+}

@@ -77,6 +77,8 @@ def lib():
         L.orc_ppr_batch.restype = None
         L.orc_ppr_batch.argtypes = [c.c_int, u32p, u32p, u32p, c.c_int, u32p, c.c_double, c.c_int,
                                     i32p, c.c_double, f64p, i32p, c.c_int]
+        L.orc_fprintf_i32.restype = c.c_double
+        L.orc_fprintf_i32.argtypes = [c.c_char_p, i32p, c.c_uint64]
         L.orc_write_edge_list.restype = c.c_int
         L.orc_write_edge_list.argtypes = [c.c_char_p, c.c_uint32, u32p, u32p]
         L.orc_wpr_forward.restype = None
@@ -401,6 +403,13 @@ def load_edge_list_sorted(path):
     rowptr = np.cumsum(rowptr)
     return (rowptr.astype(np.uint32), np.asarray(dst, np.uint32)[order],
             np.asarray(val, np.uint32)[order])
+
+
+def fprintf_i32(path, values):
+    """Write values with one fprintf("%d\\n") each (the reference's output
+    loop); returns the seconds it took."""
+    v = np.ascontiguousarray(values, np.int32)
+    return lib().orc_fprintf_i32(str(path).encode(), _p(v, ctypes.c_int32), len(v))
 
 
 def write_edge_list(path, rowptr, col, w=None):
