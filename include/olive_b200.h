@@ -125,6 +125,10 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
  *                 0 or >= sssp_delta: one sub-bucket per bucket          (0)
  *   "sssp_sub_buckets"  heavy buckets (from the first) that use sssp_sub (1)
  *   "ms_alpha"    msBFS pull when active out-edges * ms_alpha > E   (20)
+ *   "pr_tile_u"   PageRank / weighted PageRank: entries per lane per round
+ *                 the row grouping aims at (1..32, a power of two); sets
+ *                 the lanes per row of the tile plans, rebuilt on change;
+ *                 a weighted-PR backward needs its forward run after it (8)
  *   "use_graphs"  run supersteps inside CUDA graphs (1) or a host loop (0)
  *   "levels_per_sync" host loop: supersteps enqueued per check      (4)
  *   "batch_cluster" olv_batch_run: PPR items on thread-block clusters of
@@ -132,10 +136,11 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
  *                 item (0); the float results depend on the choice       (1) */
 int olv_tune_set(olv_graph *g, const char *key, double value);
 int olv_tune_get(const olv_graph *g, const char *key, double *value);
-/* Autotuner: coordinate descent over hub_degree, alpha, beta (BFS) and, on
- * uint32-weighted graphs, sssp_delta, sssp_hub_degree and sssp_piece (SSSP),
- * each candidate timed
- * `reps` times from the highest out-degree vertex; the fastest values are
+/* Autotuner: coordinate descent over hub_degree, alpha, beta (BFS), on
+ * uint32-weighted graphs sssp_delta, sssp_hub_degree, sssp_piece and sssp_sub
+ * (SSSP), pr_tile_u (PageRank, 10 iterations) and ms_alpha (msBFS from 16
+ * sources), each candidate timed `reps` times (BFS / SSSP from the highest
+ * out-degree vertex); the fastest values are
  * applied to the handle and, if json_path is not NULL, written to a JSON table
  * keyed by GPU name and graph shape.  olv_autotune_load applies such a table
  * when its key matches the handle (*applied = 1) and leaves the handle alone
@@ -224,6 +229,34 @@ int olv_ppr_batch(olv_graph *g, const uint32_t *seeds, int K, double alpha, int 
  * iterations or until the L1 residual < tol.                                  */
 int olv_pagerank(olv_graph *g, double alpha, int max_it, double tol, int dangling_mode,
                  float *rank_out, olv_stats *st);
+
+/* ---- 1-D vertex partition (several GPUs) -----------------------------------
+ * One rank's share of a graph split by contiguous vertex ranges (no working
+ * reference counterpart: the reference's multi-GPU engine, olive.h:61-199 with
+ * partition.h:95-436 and messageBox.h:66-105, never built).  The rank owns
+ * vertices [lo, hi), lo a multiple of 64, and holds their in-edges: colptr
+ * [hi-lo+1] (from 0) and rowidx (global source ids) of rows lo..hi-1 of the
+ * reverse graph, and outdeg[hi-lo] (out-degrees in the whole graph).  The
+ * exchange between ranks is the caller's (olive_b200/parallel.py: NCCL
+ * all-gathers); the steps read replicated inputs and write the rank's slice.
+ * Their array arguments are device memory.                                    */
+typedef struct olv_part olv_part;
+int olv_part_create(uint32_t V, uint32_t lo, uint32_t hi, const uint32_t *colptr,
+                    const uint32_t *rowidx, const uint32_t *outdeg, olv_part **out);
+int olv_part_destroy(olv_part *p);
+int olv_part_set_stream(olv_part *p, void *stream);
+/* BFS level L -> L+1, bottom-up over the owned vertices with level INT_MAX:
+ * a vertex whose in-neighbour is set in frontier (V bits, 64-bit words) gets
+ * level next_level and its bit in next (the owned words, bit i = vertex
+ * lo + i; cleared first).  *found = vertices found.  Levels as testBFS.cu:64-79. */
+int olv_part_bfs_step(olv_part *p, const uint64_t *frontier, int32_t *level, int32_t next_level,
+                      uint64_t *next, uint64_t *found);
+/* PageRank iteration over the owned rows (PageRank.cu:51-75 semantics):
+ * rank[v] = base + alpha * sum_{u->v} contrib[u] (contrib = r/outdeg, all V),
+ * contrib_out[v] = rank[v]/outdeg (0 for dangling vertices); sums[0] = sum of
+ * |rank' - rank|, sums[1] = sum of the owned dangling ranks (FP64, host).    */
+int olv_part_pr_step(olv_part *p, const float *contrib, double base, double alpha, float *rank,
+                     float *contrib_out, double *sums);
 
 /* ---- output ----------------------------------------------------------------
  * Write n values as text, one per line, byte for byte as the reference apps'

@@ -105,6 +105,11 @@ _SIGS = [
     ("olv_wpr_ctx_destroy", _I, [_VP]),
     ("olv_write_text", _I, [ctypes.c_char_p, _VP, _U64, _I, _VP, ctypes.POINTER(_U64)]),
     ("olv_graph_save", _I, [_VP, ctypes.c_char_p]),
+    ("olv_part_create", _I, [_U32, _U32, _U32, _VP, _VP, _VP, ctypes.POINTER(_VP)]),
+    ("olv_part_destroy", _I, [_VP]),
+    ("olv_part_set_stream", _I, [_VP, _VP]),
+    ("olv_part_bfs_step", _I, [_VP, _VP, _VP, ctypes.c_int32, _VP, ctypes.POINTER(_U64)]),
+    ("olv_part_pr_step", _I, [_VP, _VP, _D, _D, _VP, _VP, ctypes.POINTER(_D)]),
 ]
 
 TEXT_TYPES = {"int32": 0, "uint32": 1, "float32": 2, "float64": 3}
@@ -260,6 +265,7 @@ class Graph:
         out = {}
         for k in ("hub_degree", "piece", "alpha", "beta", "sssp_delta", "sssp_pull", "sssp_relabel",
                   "sssp_sub", "sssp_sub_buckets", "sssp_hub_degree", "sssp_piece", "ms_alpha",
+                  "pr_tile_u",
                   "use_graphs", "levels_per_sync", "batch_cluster"):
             d = _D()
             _check(lib().olv_tune_get(self._h, k.encode(), ctypes.byref(d)), "olv_tune_get")

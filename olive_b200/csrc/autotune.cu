@@ -1,8 +1,13 @@
 // Autotuner (no reference counterpart; the reference fixed its launch shape
 // in util::kernelConfig, utils.h:56-72, and took the edge-group size from the
-// -g flag, BFS.cu:89).  Coordinate descent over the engine's tunables, each
-// candidate timed with CUDA events on the graph's own stream from its highest
-// out-degree vertex; the winners are applied to the handle and, optionally,
+// -g flag, BFS.cu:89).  Coordinate descent over the engine's tunables -- BFS
+// hub split and push/pull switch points, SSSP bucket width, hub split and
+// light sub-buckets, the PageRank / weighted-PageRank row grouping (entries
+// per lane, which sets the lanes per row of the tile plans), the msBFS
+// push/pull switch -- each candidate timed with CUDA events on the graph's
+// own stream (BFS/SSSP from the highest out-degree vertex, msBFS from 16
+// sources spread over the graph, PageRank 10 iterations); the winners are
+// applied to the handle and, optionally,
 // written to a JSON table keyed by GPU and graph shape, which olv_autotune_load
 // re-applies when the key matches.  Tuning changes speed only: every result
 // stays bit-exact (tests check it).
@@ -38,6 +43,20 @@ static int run_bfs(olv_graph *g, uint32_t src, void *out) {
 static int run_sssp(olv_graph *g, uint32_t src, void *out) {
     return olv_sssp(g, src, static_cast<uint32_t *>(out), nullptr);
 }
+static int run_pagerank(olv_graph *g, uint32_t, void *out) {
+    return olv_pagerank(g, 0.85, 10, 0.0, OLV_DANGLING_UNIFORM, static_cast<float *>(out), nullptr);
+}
+// msBFS from kMsTuneSources sources spread over the vertices with out-edges
+constexpr int kMsTuneSources = 16;
+struct MsTune {
+    std::vector<uint32_t> sources;
+    DevBuf out;
+};
+static int run_msbfs(olv_graph *g, uint32_t, void *arg) {
+    MsTune *m = static_cast<MsTune *>(arg);
+    return olv_msbfs(g, m->sources.data(), (int)m->sources.size(), m->out.as<int32_t>(),
+                     nullptr);
+}
 
 static std::string tune_key(olv_graph *g) {
     cudaDeviceProp prop;
@@ -63,16 +82,31 @@ extern "C" int olv_autotune(olv_graph *g, const char *json_path, int reps) {
         const char *key;
         std::vector<double> values;
         int (*fn)(olv_graph *, uint32_t, void *);
+        void *arg;   // output buffer (or the msBFS set-up)
     };
     std::vector<Cand> plan = {
-        {"hub_degree", {256, 1024, 4096}, run_bfs},
-        {"alpha", {2, 6, 14, 30, 60}, run_bfs},
-        {"beta", {6, 24, 100}, run_bfs},
+        {"hub_degree", {256, 1024, 4096}, run_bfs, out.p},
+        {"alpha", {2, 6, 14, 30, 60}, run_bfs, out.p},
+        {"beta", {6, 24, 100}, run_bfs, out.p},
     };
     if (g->weight_type == OLV_W_U32) {
-        plan.push_back({"sssp_delta", {16, 32, 64, 128, 256, 512, 1024}, run_sssp});
-        plan.push_back({"sssp_hub_degree", {128, 256, 1024}, run_sssp});
-        plan.push_back({"sssp_piece", {256, 1024}, run_sssp});
+        plan.push_back({"sssp_delta", {16, 32, 64, 128, 256, 512, 1024}, run_sssp, out.p});
+        plan.push_back({"sssp_hub_degree", {128, 256, 1024}, run_sssp, out.p});
+        plan.push_back({"sssp_piece", {256, 1024}, run_sssp, out.p});
+        plan.push_back({"sssp_sub", {0, 8, 16}, run_sssp, out.p});
+    }
+    // PageRank / weighted PageRank row grouping (entries per lane per round)
+    plan.push_back({"pr_tile_u", {4, 8, 16}, run_pagerank, out.p});
+    // multi-source BFS push -> pull switch point
+    std::vector<uint32_t> rp((size_t)g->V + 1);
+    OLV_TRY(olv_graph_copy_csr(g, rp.data(), nullptr, nullptr));
+    MsTune mst;
+    for (uint32_t v = 0, seen = 0; v < g->V && (int)mst.sources.size() < kMsTuneSources; v++)
+        if (rp[v + 1] > rp[v] && seen++ % (1 + g->V / (8 * kMsTuneSources)) == 0)
+            mst.sources.push_back(v);
+    if (!mst.sources.empty()) {
+        OLV_TRY(mst.out.ensure((size_t)g->V * 4 * mst.sources.size() + 16));
+        plan.push_back({"ms_alpha", {5, 10, 20, 40}, run_msbfs, &mst});
     }
     std::string log;
     for (auto &c : plan) {
@@ -80,7 +114,7 @@ extern "C" int olv_autotune(olv_graph *g, const char *json_path, int reps) {
         for (double v : c.values) {
             OLV_TRY(olv_tune_set(g, c.key, v));
             double ms = 0;
-            OLV_TRY(time_call(g, c.fn, src, out.p, reps, &ms));
+            OLV_TRY(time_call(g, c.fn, src, c.arg, reps, &ms));
             if (ms < best_ms) {
                 best_ms = ms;
                 best_v = v;
@@ -118,8 +152,9 @@ extern "C" int olv_autotune_load(olv_graph *g, const char *json_path, int *appli
     fclose(f);
     const std::string want = "\"key\": \"" + tune_key(g) + "\"";
     if (text.find(want) == std::string::npos) return OLV_OK;   // table is for another graph/GPU
-    const char *keys[] = {"hub_degree", "piece",      "alpha",           "beta",
-                          "sssp_delta", "sssp_piece", "sssp_hub_degree", "ms_alpha"};
+    const char *keys[] = {"hub_degree",      "piece",    "alpha",      "beta",
+                          "sssp_delta",      "sssp_piece", "sssp_hub_degree", "sssp_sub",
+                          "ms_alpha",        "pr_tile_u"};
     for (const char *k : keys) {
         const std::string pat = std::string("\"") + k + "\":";
         size_t pos = text.find(pat);

@@ -528,6 +528,15 @@ int olv_tune_set(olv_graph *g, const char *key, double value) {
     } else if (!strcmp(key, "sssp_sub_buckets")) {
         OLV_CHECK_ARG(value >= 0 && value < 2147483647.0, "olv_tune_set: bad sssp_sub_buckets");
         t.sssp_sub_buckets = (uint32_t)value;
+    } else if (!strcmp(key, "pr_tile_u")) {
+        const uint32_t u = (uint32_t)value;
+        OLV_CHECK_ARG(value >= 1 && value <= 32 && (u & (u - 1)) == 0,
+                      "olv_tune_set: pr_tile_u must be a power of two in [1, 32]");
+        if (u != t.pr_tile_u) {   // the row plans are rebuilt on their next use
+            t.pr_tile_u = u;
+            release_pr_state(g);
+            release_wpr_state(g);
+        }
     } else if (!strcmp(key, "ms_alpha")) {
         OLV_CHECK_ARG(value > 0, "olv_tune_set: ms_alpha must be > 0");
         t.ms_alpha = (float)value;
@@ -566,6 +575,7 @@ int olv_tune_get(const olv_graph *g, const char *key, double *value) {
     else if (!strcmp(key, "sssp_hub_degree")) *value = t.sssp_hub_degree;
     else if (!strcmp(key, "sssp_piece")) *value = t.sssp_piece;
     else if (!strcmp(key, "ms_alpha")) *value = t.ms_alpha;
+    else if (!strcmp(key, "pr_tile_u")) *value = t.pr_tile_u;
     else if (!strcmp(key, "use_graphs")) *value = t.use_graphs;
     else if (!strcmp(key, "batch_cluster")) *value = t.batch_cluster;
     else if (!strcmp(key, "levels_per_sync")) *value = t.levels_per_sync;

@@ -65,6 +65,8 @@ struct Tuning {
     uint32_t sssp_sub = 0;            // SSSP: light-phase sub-bucket width (0: none)
     uint32_t sssp_sub_buckets = 1;    // SSSP: heavy buckets whose light phase uses it
     float ms_alpha = 20.0f;       // msBFS: pull when active out-edges * ms_alpha > E
+    uint32_t pr_tile_u = 8;       // PageRank / weighted PR: entries per lane the row
+                                  // grouping aims at (lanes per row by row length)
     int levels_per_sync = 4;      // host loop: supersteps enqueued per check
     int use_graphs = 1;           // run supersteps inside a CUDA graph
     int batch_cluster = 1;        // batch PPR items run by thread-block clusters

@@ -126,8 +126,12 @@ struct PermOp {
 // Build the plan from a device row-offset array (n rows) and its neighbour
 // array.  The relabelling is a stable counting sort by row length
 // (descending), done on the host once per graph.
+// lanes_u: entries per lane per round the grouping aims at (rows get the
+// fewest lanes G = 1..32 with G * lanes_u >= row length); the autotuner's
+// "pr_tile_u".
 inline int build_tile_plan(const uint32_t *ptr_dev, const uint32_t *idx_dev, uint32_t n,
-                           cudaStream_t s, TilePlan &p, bool relabel = true) {
+                           cudaStream_t s, TilePlan &p, bool relabel = true,
+                           uint32_t lanes_u = kTileU) {
     std::vector<uint32_t> cp((size_t)n + 1);
     OLV_CUDA(cudaMemcpyAsync(cp.data(), ptr_dev, ((size_t)n + 1) * 4, cudaMemcpyDeviceToHost, s));
     OLV_CUDA(cudaStreamSynchronize(s));
@@ -155,7 +159,7 @@ inline int build_tile_plan(const uint32_t *ptr_dev, const uint32_t *idx_dev, uin
             continue;
         }
         uint32_t lg = 0;
-        while (lg < 5 && (1u << lg) * kTileU < d) lg++;
+        while (lg < 5 && (1u << lg) * lanes_u < d) lg++;
         tiles.push_back(make_uint2(i, lg | (kNoSeg << 8)));
         i += 32u >> lg;
     }

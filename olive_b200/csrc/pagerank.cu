@@ -196,7 +196,7 @@ struct PrPlan {
 static int build_pr_plan(olv_graph *g, PrPlan &p) {
     const uint32_t V = g->V;
     OLV_TRY(build_tile_plan(g->colptr.as<uint32_t>(), g->rowidx.as<uint32_t>(), V, g->stream,
-                            p.tp));
+                            p.tp, true, g->tune.pr_tile_u));
     OLV_TRY(p.outdeg.ensure((size_t)V * 4 + 16));
     k_outdeg_perm<<<g->num_sms * 8, kBlock, 0, g->stream>>>(
         g->rowptr.as<uint32_t>(), p.tp.perm.as<uint32_t>(), V, p.outdeg.as<uint32_t>());

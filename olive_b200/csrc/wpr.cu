@@ -219,10 +219,10 @@ static int ensure_wpr_plans(olv_graph *g) {
     int r = build_row_plan(g->rowptr.as<uint32_t>(), g->V, g->stream, p->csr);
     if (r == OLV_OK)
         r = build_tile_plan(g->colptr.as<uint32_t>(), g->rowidx.as<uint32_t>(), g->V, g->stream,
-                            p->tcsc, false);
+                            p->tcsc, false, g->tune.pr_tile_u);
     if (r == OLV_OK)
         r = build_tile_plan(g->rowptr.as<uint32_t>(), g->col.as<uint32_t>(), g->V, g->stream,
-                            p->tcsr, false);
+                            p->tcsr, false, g->tune.pr_tile_u);
     if (r == OLV_OK) r = p->wc.ensure(g->E * 4 + 16);
     if (r == OLV_OK) r = p->wr.ensure(g->E * 4 + 16);
     if (r != OLV_OK) {
@@ -379,6 +379,11 @@ extern "C" int olv_wpr_backward(olv_wpr_ctx *c, const float *gvec, int max_it, d
     OLV_CHECK_ARG(c && c->g && gvec && dw_out, "olv_wpr_backward: null pointer or no forward");
     OLV_CHECK_ARG(max_it >= 0, "olv_wpr_backward: bad max_it");
     olv_graph *g = c->g;
+    if (!wpr_plans(g)) {   // the row plans were dropped (pr_tile_u changed) since the forward
+        set_error("olv_wpr_backward: the graph's row plans changed since olv_wpr_forward; "
+                  "run the forward again");
+        return OLV_ERR_STATE;
+    }
     WprPlans &pl = *wpr_plans(g);
     const size_t V = g->V;
     const uint64_t E = g->E;

@@ -1,6 +1,11 @@
 """Run one workload a few times for a profiler.
 
-    python -m olive_b200.profile_run --workload bfs|sssp|pagerank|msbfs|wpr|batch --scale 22
+    python -m olive_b200.profile_run --workload bfs|sssp|pagerank|msbfs|wpr|batch|ppr --scale 22
+    python -m olive_b200.profile_run --workload write-graph --scale 24 --out g.bin
+
+write-graph writes the seeded RMAT graph as a binary CSR file (for the
+reference apps built on the header layer, which a profiler then runs
+directly) and prints the highest out-degree vertex.
 
 Builds the seeded RMAT graph on the device (scale, edge factor 16, seed 1;
 uint32 weights for sssp, lognormal FP32 weights for wpr), then runs the solve
@@ -24,8 +29,9 @@ import numpy as np
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", choices=["bfs", "sssp", "pagerank", "msbfs", "wpr", "batch"],
-                    default="bfs")
+    ap.add_argument("--workload", choices=["bfs", "sssp", "pagerank", "msbfs", "wpr", "batch",
+                                           "ppr", "write-graph"], default="bfs")
+    ap.add_argument("--out", default="graph.bin", help="write-graph: output path")
     ap.add_argument("--scale", type=int, default=22)
     ap.add_argument("--runs", type=int, default=2)
     ap.add_argument("--graphs", action="store_true", help="keep CUDA-graph mode")
@@ -36,6 +42,12 @@ def main():
     import torch
 
     import olive_b200 as ob
+    if a.workload == "write-graph":
+        g = ob.Graph.rmat(a.scale, 16, 1)
+        g.save(a.out)
+        print(g.max_degree_vertex()[0])
+        g.close()
+        return
     if a.workload == "batch":
         count, K = a.count, 32
         g, off = ob.Graph.er_batch(count, 1024, 65536, 8, seed=1)
@@ -87,8 +99,17 @@ def main():
         print(a.workload, g.last_stats.as_dict(), file=sys.stderr)
         g.close()
         return
+    if a.workload == "ppr":
+        rp, _, _ = g.csr()
+        deg = np.diff(rp.astype(np.int64))
+        srcs = np.random.default_rng(3).choice(np.flatnonzero(deg > 0), 32,
+                                               replace=False).astype(np.uint32)
+        out = torch.empty((g.V, 32), dtype=torch.float32, device="cuda")
+
     def solve():
-        if a.workload == "bfs":
+        if a.workload == "ppr":
+            g.ppr(srcs, 0.85, 50, 1e-7, out=out)
+        elif a.workload == "bfs":
             g.bfs(hub, out=out)
         elif a.workload == "sssp":
             g.sssp(hub, out=out)

@@ -301,6 +301,27 @@ def test_pagerank_fp32_vs_fp64_oracle(ob, scale, seed):
         assert abs(g.last_stats.residual - res[-1]) <= 1e-3 * res[-1] + 2e-7
 
 
+@pytest.mark.parametrize("tile_u", [1, 4, 16, 32])
+def test_pagerank_and_wpr_every_row_grouping(ob, tile_u):
+    """Every row grouping of the tile plans keeps PageRank within 1e-6 of the
+    FP64 oracle and weighted PageRank within 1e-5."""
+    with ob.Graph.rmat(15, 16, 11) as g:
+        g.tune(pr_tile_u=tile_u)
+        rp, cl, _ = g.csr()
+        r = g.pagerank(0.85, 25, 0.0)
+        ref, _, _ = oracle.pagerank(rp, cl, 0.85, 25, 0.0)
+        assert np.max(np.abs(r - ref) / ref) < 1e-6
+        rng = np.random.default_rng(tile_u)
+        w = rng.lognormal(0, 1, g.E).astype(np.float32)
+        p = np.full(g.V, 1.0 / g.V, np.float32)
+        rw = g.wpr_forward(p, w=w, max_it=60)
+        rref = oracle.wpr_forward(rp, cl, w.astype(np.float64), p.astype(np.float64), 0.85, 60)
+        assert np.max(np.abs(rw - rref) / rref) < 1e-5
+        g.tune(pr_tile_u=8)   # plans dropped: the backward asks for a new forward
+        with pytest.raises(ob.OliveError, match="run the forward again"):
+            g.wpr_backward(np.ones(g.V, np.float32), max_it=5)
+
+
 def test_pagerank_deterministic(ob):
     with ob.Graph.rmat(17, 16, 9) as g:
         a = g.pagerank(0.85, 30, 0.0)
@@ -384,12 +405,18 @@ def test_autotune_keeps_results_and_roundtrips(ob, tmp_path):
         best = g.autotune(path, reps=1)
         assert best["hub_degree"] in (256, 1024, 4096)
         assert best["sssp_hub_degree"] in (128, 256, 1024) and best["sssp_piece"] in (256, 1024)
+        assert best["pr_tile_u"] in (4, 8, 16) and best["ms_alpha"] in (5, 10, 20, 40)
+        assert best["sssp_sub"] in (0, 8, 16)
         np.testing.assert_array_equal(g.bfs(hub), oracle.bfs(rp, cl, hub)[0])
         np.testing.assert_array_equal(g.sssp(hub), oracle.dijkstra(rp, cl, w, hub)[0])
         txt = open(path).read()
-        assert '"key"' in txt and "sssp_delta" in txt
+        assert '"key"' in txt and "sssp_delta" in txt and "pr_tile_u" in txt and "ms_alpha" in txt
+        r = g.pagerank(0.85, 30, 0.0)
+        ref, _, _ = oracle.pagerank(rp, cl, 0.85, 30, 0.0)
+        assert np.max(np.abs(r - ref) / ref) < 1e-6
     with ob.Graph.rmat(14, 16, 3, weights=True, wseed=4) as g2:
-        g2.tune(hub_degree=4096, sssp_delta=16, sssp_hub_degree=4096, sssp_piece=4096)
+        g2.tune(hub_degree=4096, sssp_delta=16, sssp_hub_degree=4096, sssp_piece=4096,
+                pr_tile_u=32, ms_alpha=7)
         assert g2.autotune_load(path)
         assert g2.tune() == best
     with ob.Graph.rmat(13, 16, 3) as g3:       # another graph: table not applied
