@@ -11,9 +11,14 @@ atomicMin, SSSP.cu semantics) on an RMAT graph of scale 24, edge factor 16,
 highest out-degree vertex.  A step is one complete solve on the resident
 graph.  The metric is GTEPS = (sum of out-degrees of reached vertices) / time.
 The default line also carries, as extra keys, BFS on the same graph ("bfs"),
-64-source BFS on RMAT-24 ("msbfs"), PageRank on RMAT-22 ("pagerank"),
-weighted PageRank forward + adjoint on RMAT-20 ("wpr") and the 512-graph ER
-batch ("batch"), each with its own timing, roofline fraction and parity check.
+64-source BFS on RMAT-24 ("msbfs"), PageRank on RMAT-22 ("pagerank"), 32
+personalised PageRank vectors on RMAT-22 ("ppr"), weighted PageRank forward +
+adjoint on RMAT-20 ("wpr") and the 512-graph ER batch ("batch"), each with its
+own timing, roofline fraction and parity check; a caller arriving with a host
+CSR ("e2e_cold": graph upload and build + one solve + the result read back);
+the GPU text writer against the host printf loop ("writer"); and the
+reference's BFS.cu compiled unmodified against the header layer, plus the
+same loop with the pull opt-ins, on the same graph ("dropin_bfs").
 
 Parity: every line checks the GPU result of its last step against the CPU
 oracle on rank 0 ("parity" key): SSSP against a complete serial Dijkstra,
@@ -141,7 +146,8 @@ def peaks():
 # profiler measured it (see each file for how it was taken and scaled).
 PROFILE_OF = {("sssp", 24): "sssp_rmat24.md", ("bfs", 24): "bfs_rmat24.md",
               ("pagerank", 22): "pagerank_rmat22.md", ("msbfs", 24): "msbfs_rmat24.md",
-              ("wpr", 20): "wpr_rmat20.md", ("batch", 0): "batch_er512.md"}
+              ("wpr", 20): "wpr_rmat20.md", ("batch", 0): "batch_er512.md",
+              ("ppr", 22): "ppr_rmat22.md"}
 
 
 def profile_traffic(workload, scale, seed, key="traffic_bytes"):
@@ -327,6 +333,47 @@ def writer_line(ob, dev_vals, stream):
             "identical_bytes": bool(same),
             "note": "olv_write_text from device memory to a local file (format on the GPU, "
                     "D2H, fwrite) vs one fprintf per value on one host core"}
+
+
+def dropin_line(g, src, lv_dev, bfs_c_abi):
+    """The reference's BFS.cu compiled unmodified against the header layer
+    (olive_b200/_apps/BFS) and the same loop with the pull opt-ins
+    (olive_b200/_apps/BFSPullOptIn), on this graph written as a binary CSR
+    file, timed by the apps' own clock (their loop, as BFS.cu:150-151 logs
+    it), levels checked against olv_bfs."""
+    apps = os.path.join(ROOT, "olive_b200", "_apps")
+    if not os.path.exists(os.path.join(apps, "BFS")):
+        return {"unavailable": "olive_b200/_apps/BFS not built (needs the reference sources at "
+                               "build time)"}
+    work = tempfile.mkdtemp(prefix="olv_dropin_")
+    path = os.path.join(work, "g.bin")
+    g.save(path)
+    want = lv_dev.cpu().numpy().astype(np.int64)
+    e_reached = bfs_c_abi["value"] * bfs_c_abi["ms"] * 1e6
+    out = {"graph": "the SSSP line's RMAT-24 as a binary CSR file", "source": int(src),
+           "olv_bfs_ms": bfs_c_abi["ms"]}
+    for name in ("BFS", "BFSPullOptIn"):
+        best = None
+        for _ in range(2):
+            p = subprocess.run([os.path.join(apps, name), path, "-s", str(src), "-round", "100000"],
+                               cwd=work, capture_output=True, text=True, timeout=600)
+            m = re.findall(r"iterations: (\d+), time: ([0-9.]+)ms", p.stderr + p.stdout)
+            if p.returncode == 0 and m:
+                t = float(m[-1][1])
+                best = t if best is None else min(best, t)
+        import pandas as pd
+        got = pd.read_csv(os.path.join(work, "BFS.txt"), header=None, dtype=np.int64)[0].values
+        key = "unmodified" if name == "BFS" else "pull_optin"
+        out[key] = {"app": f"olive_b200/_apps/{name}", "ms": best,
+                    "gteps": round(e_reached / (best * 1e-3) / 1e9, 2) if best else None,
+                    "over_olv_bfs": round(best / bfs_c_abi["ms"], 2) if best else None,
+                    "parity": {"vs": "olv_bfs levels", "mismatches": int(np.count_nonzero(got != want))}}
+    shutil.rmtree(work, ignore_errors=True)
+    out["note"] = ("app's own loop timer (frontier.size() host reads included, file load and "
+                   "readGraph excluded); BFS.cu's functors cannot skip visited destinations, so its "
+                   "levels are top-down over every frontier edge; the opt-in variant declares "
+                   "pullCandidate / pullFirstHit")
+    return out
 
 
 # ------------------------------------------------- traversal workloads --
@@ -537,6 +584,8 @@ def traversal_line(a, rank, world, local_rank, extra_keys=True):
         method = "sssp" if a.workload == "sssp" else "bfs"
         extra["e2e_cold"] = cold_e2e(ob, stream, rp, cl, w if weights else None, src, method)
         extra["writer"] = writer_line(ob, out, stream)
+        if a.workload == "sssp":
+            extra["dropin_bfs"] = dropin_line(g, src, lv, extra["bfs"])
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -850,6 +899,8 @@ def ppr_line(a, rank, world, local_rank):
                 "bytes_formula": "per iteration: (4 B in-edge id + 4K B contribution row) per "
                                  "edge + (x read, x write, y write: 12K B + 8 B) per vertex",
                 "peak_source": peak_src, "kernel_ms": round(kern_ms, 4)}
+    traffic, traffic_src = profile_traffic("ppr", a.scale, a.seed)
+    roofline.update(traffic=traffic, traffic_source=traffic_src)
     host = torch.empty((V, K), dtype=torch.float32, pin_memory=True)
     t0 = time.perf_counter()
     for _ in range(a.steps):

@@ -27,8 +27,13 @@
  *   - cond receives the accumulator, not the vertex id (oliverKernel.h:112,135);
  *   - edge passes choose push or pull on the device: pull (over the reverse
  *     graph, built once in readGraph) when the source subset's out-edges reach
- *     E / pull_div (default 2), push otherwise; OLIVE_DIRECTION=push|pull|auto
- *     and OLIVE_PULL_DIV override.  The result is the same either way (the
+ *     E / pull_div, push otherwise.  A full pull reads every in-edge and
+ *     costs about what a push over all edges costs, so by default (pull_div
+ *     1) it runs only when the sources carry all E out-edges (edgeMap over
+ *     every vertex, as PageRank.cu does: no atomics, one store per vertex);
+ *     functors with the pullFirstHit opt-in pull from E / 16 (their rows stop
+ *     at the first contribution).  OLIVE_DIRECTION=push|pull|auto and
+ *     OLIVE_PULL_DIV override.  The result is the same either way (the
  *     reduce of every in-edge from a member), up to the order in which a
  *     non-associative reduce sees its inputs -- as in the reference, whose
  *     atomics fixed no order either;
@@ -189,9 +194,9 @@ public:
     AccumValue *deviceAccumulators() const { return accumulators_; }
 
     /** Edge-pass direction: 0 push, 1 pull, 2 by frontier size (default). */
-    void setDirection(int policy, double pull_div = 2.0) {
+    void setDirection(int policy, double pull_div = 1.0) {
         policy_ = policy;
-        pullDiv_ = pull_div > 0 ? pull_div : 2.0;
+        pullDiv_ = pull_div > 0 ? pull_div : 1.0;
         if (policy_ != 0 && edgeCount_ && !colptr_) buildReverse();
     }
 
@@ -223,7 +228,7 @@ private:
     AccumValue defaultAccum_;
     int sms_ = 148;
     int policy_ = 2;
-    double pullDiv_ = 2.0;
+    double pullDiv_ = 1.0;
     std::vector<VertexValue> hostValues_;
 
     size_t words() const { return ((size_t)vertexCount_ + 63) / 64; }

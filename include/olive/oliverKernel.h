@@ -17,13 +17,13 @@
  *             graph: each row reduces its in-edges from source-subset members
  *             into a shared-memory slot (the functor's own reduce), then one
  *             store; chosen on the device when the frontier's out-edges pass
- *             E / pull_div (or always / never, OLIVE_DIRECTION).  A functor
+ *             E / pull_div (default 1; or always / never, OLIVE_DIRECTION).  A functor
  *             may opt into a narrower pull: `pullCandidate(const V &)` skips
  *             rows, `static constexpr bool pullFirstHit` stops a row at its
  *             first contribution (valid when any one contribution is enough,
  *             as for BFS levels): the pull then runs k_pull_first_rows /
  *             k_pull_first_long (a thread or a warp per row, early exit) and
- *             is chosen from E / (pull_div * 8) frontier out-edges.
+ *             is chosen from E / (pull_div * 16) frontier out-edges.
  *   k_vertex_filter  flags -> queue with cond/update (oliverKernel.h:85-141):
  *     over the listed members (or the bitmap when no list is known); ballot
  *     compaction, one atomic per warp; writes the queue, its bitmap and the
@@ -51,7 +51,7 @@ constexpr uint32_t kHub = 1024;    // push: rows with more out-edges go to piece
 constexpr uint32_t kPiece = 1024;
 constexpr uint32_t kPullHub = 4096;   // pull: rows with more in-edges go to pieces
 constexpr uint32_t kPullPiece = 2048;
-constexpr double kFirstHitPullFactor = 8.0;   // pull at E / (pull_div * 8) for first-hit ops
+constexpr double kFirstHitPullFactor = 16.0;  // pull at E / (pull_div * 16) for first-hit ops
 constexpr uint32_t kModePush = 0;
 constexpr uint32_t kModePull = 1;
 
