@@ -156,10 +156,15 @@ struct PullOp {
     __device__ __forceinline__ A acc_load(uint32_t r) const { return acc[r]; }
     __device__ __forceinline__ bool contributes(uint32_t u, uint32_t e, A &x) {
         if (!bit_of(sbits, u)) return false;
+        x = contribution(u, e);
+        return true;
+    }
+    // split form for the first-hit kernels: membership loads first, one gather
+    __device__ __forceinline__ bool passes(uint32_t u) const { return bit_of(sbits, u); }
+    __device__ __forceinline__ A contribution(uint32_t u, uint32_t e) {
         E dummy{};
         E &ev = edge_ref(evals, eid[e], dummy);
-        x = f.gather(vvals[u], outdeg[u], ev);
-        return true;
+        return f.gather(vvals[u], outdeg[u], ev);
     }
     __device__ __forceinline__ void reduce_slot(A &slot, const A &x) { f.reduce(slot, x); }
     __device__ __forceinline__ void reduce_row(uint32_t r, const A &x) { f.reduce(acc[r], x); }

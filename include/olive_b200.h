@@ -124,6 +124,12 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
  *                 relaxations where that bucket holds most of the graph);
  *                 0 or >= sssp_delta: one sub-bucket per bucket          (0)
  *   "sssp_sub_buckets"  heavy buckets (from the first) that use sssp_sub (1)
+ *   "sssp_spt"    queued sources per thread in a relax chunk: 1, 2, 4 or 8 (1)
+ *   "sssp_fuse_end"  SSSP superstep's end step run by the last CTA of the
+ *                 relax pieces kernel instead of a launch of its own (1)
+ *   "sssp_tail_delta"  width of the SSSP buckets after the first; above
+ *                 sssp_delta those buckets relax every edge in-bucket and
+ *                 have no heavy step (0: delta, light/heavy throughout)
  *   "ms_alpha"    msBFS pull when active out-edges * ms_alpha > E   (20)
  *   "pr_tile_u"   PageRank / weighted PageRank: entries per lane per round
  *                 the row grouping aims at (1..32, a power of two); sets

@@ -28,7 +28,17 @@
 //                                                   false: skip its edges now
 //   void on_push(bool pushed, uint32_t v)           after each warp-wide push
 //   void flush(unsigned long long relaxed)          once per thread at the end
+//   kEpilogue, bool epilogue_on() / void epilogue(TravCtl *c)
+//                                                   optional: when epilogue_on(),
+//                                                   one thread of the last CTA of
+//                                                   k_advance_pieces to finish runs
+//                                                   epilogue(c) after every CTA's
+//                                                   updates are visible (the
+//                                                   superstep's control step, with
+//                                                   no launch of its own)
 #pragma once
+#include <type_traits>
+
 #include "olv_travctl.cuh"
 
 namespace olv {
@@ -214,6 +224,10 @@ struct AdvanceArgs {
     const uint32_t *rend2 = nullptr;
     const uint2 *rng2 = nullptr;
     uint32_t want_mode2 = 0xffffffffu;   // 0xffffffff: no second mode
+    const uint32_t *rbeg3 = nullptr;  // ... or, with these, when it is want_mode3
+    const uint32_t *rend3 = nullptr;
+    const uint2 *rng3 = nullptr;
+    uint32_t want_mode3 = 0xffffffffu;   // 0xffffffff: no third mode
 };
 
 // Row ranges of the current mode.
@@ -237,6 +251,10 @@ __device__ __forceinline__ bool advance_ranges(const AdvanceArgs &a, const TravC
     }
     if (m == a.want_mode2) {
         r = RowRanges{a.rbeg2, a.rend2, a.rng2};
+        return true;
+    }
+    if (m == a.want_mode3) {
+        r = RowRanges{a.rbeg3, a.rend3, a.rng3};
         return true;
     }
     return false;
@@ -264,9 +282,14 @@ __device__ __forceinline__ typename Op::Pre prepare_edge(Op &op, typename Op::SV
         return op.prepare(sv, e, v);
 }
 
-// Per-superstep chunk expansion over the input queue.
-template <class Op>
+// Per-superstep chunk expansion over the input queue.  A chunk is kBlock * S
+// queued sources (S per thread): with short rows (a few edges per source, as
+// in SSSP's light phase) a larger S spreads the scan and the barriers of a
+// chunk over more edges.
+template <class Op, uint32_t S = 1>
 __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_chunks(AdvanceArgs a, Op op) {
+    static_assert(S == 1 || S == 2 || S == 4 || S == 8, "sources per thread: 1, 2, 4 or 8");
+    constexpr uint32_t kChunk = kBlock * S;   // queued sources per chunk
     TravCtl *c = a.ctl;
     RowRanges rr;
     if (!advance_ranges(a, c, rr)) return;
@@ -280,9 +303,9 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_chunks(Advan
     uint32_t *far_size = &c->far_size[c->far_cur];
 
     using SV = typename Op::SV;
-    __shared__ uint32_t s_beg[kBlock];
-    __shared__ uint32_t s_off[kBlock];
-    __shared__ SV s_val[kBlock];
+    __shared__ uint32_t s_beg[kChunk];
+    __shared__ uint32_t s_off[kChunk];
+    __shared__ SV s_val[kChunk];
     __shared__ uint32_t s_warp[33];
     constexpr uint32_t kFarStage = Op::kHasFar ? kStage : 1;
     __shared__ uint32_t s_q[kStage], s_f[kFarStage];
@@ -295,33 +318,45 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_chunks(Advan
     }
 
     unsigned long long relaxed = 0;
-    for (uint32_t chunk = blockIdx.x; (uint64_t)chunk * kBlock < n; chunk += gridDim.x) {
-        const uint32_t i = chunk * kBlock + threadIdx.x;
-        uint32_t beg = 0, deg = 0;
-        SV sv = 0;
-        if (i < n) {
-            const uint32_t u = qin[i];
-            if (op.on_input(u)) {
-                const uint2 r = rr.of(u);
-                beg = r.x;
-                deg = r.y - r.x;
+    for (uint64_t c0 = (uint64_t)blockIdx.x * kChunk; c0 < n; c0 += (uint64_t)gridDim.x * kChunk) {
+        // thread t takes the S consecutive entries c0 + t*S .. c0 + t*S + S-1
+        uint32_t beg[S], deg[S], tdeg = 0;
+        SV sv0[S];
+#pragma unroll
+        for (uint32_t s = 0; s < S; s++) {
+            const uint64_t i = c0 + threadIdx.x * S + s;
+            beg[s] = 0;
+            deg[s] = 0;
+            sv0[s] = 0;
+            if (i < n) {
+                const uint32_t u = qin[i];
+                if (op.on_input(u)) {
+                    const uint2 r = rr.of(u);
+                    beg[s] = r.x;
+                    deg[s] = r.y - r.x;
+                }
+                if (deg[s] > a.hub_degree) {
+                    const uint32_t np = (deg[s] + a.piece - 1) / a.piece;
+                    const uint32_t b = atomicAdd(&c->npieces, np);
+                    for (uint32_t p = 0; p < np; p++) a.pieces[b + p] = make_uint2(u, p);
+                    relaxed += deg[s];
+                    deg[s] = 0;
+                } else {
+                    sv0[s] = op.src_value(u);
+                }
             }
-            if (deg > a.hub_degree) {
-                const uint32_t np = (deg + a.piece - 1) / a.piece;
-                const uint32_t b = atomicAdd(&c->npieces, np);
-                for (uint32_t p = 0; p < np; p++) a.pieces[b + p] = make_uint2(u, p);
-                relaxed += deg;
-                deg = 0;
-            } else {
-                sv = op.src_value(u);
-            }
+            relaxed += deg[s];
+            tdeg += deg[s];
         }
-        relaxed += deg;
         uint32_t total;
-        const uint32_t off = block_exclusive_scan(deg, &total, s_warp);
-        s_beg[threadIdx.x] = beg;
-        s_off[threadIdx.x] = off;
-        s_val[threadIdx.x] = sv;
+        uint32_t off = block_exclusive_scan(tdeg, &total, s_warp);
+#pragma unroll
+        for (uint32_t s = 0; s < S; s++) {
+            s_beg[threadIdx.x * S + s] = beg[s];
+            s_off[threadIdx.x * S + s] = off;
+            s_val[threadIdx.x * S + s] = sv0[s];
+            off += deg[s];
+        }
         __syncthreads();
         for (uint32_t base = 0; base < total; base += kBlock * kItems) {
             uint32_t e[kItems], v[kItems];
@@ -335,9 +370,10 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_chunks(Advan
                 sv[j] = 0;
                 v[j] = 0;
                 if (act[j]) {
+                    // the last entry whose offset is <= k owns edge slot k
                     uint32_t lo = 0;
 #pragma unroll
-                    for (uint32_t step = kBlock / 2; step > 0; step >>= 1)
+                    for (uint32_t step = kChunk / 2; step > 0; step >>= 1)
                         if (s_off[lo + step] <= k) lo += step;
                     e[j] = s_beg[lo] + (k - s_off[lo]);
                     sv[j] = s_val[lo];
@@ -365,14 +401,44 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_chunks(Advan
     op.flush(relaxed);
 }
 
+template <class Op, class = void>
+struct op_epilogue : std::false_type {};
+template <class Op>
+struct op_epilogue<Op, std::void_t<decltype(Op::kEpilogue)>>
+    : std::integral_constant<bool, Op::kEpilogue> {};
+
+template <class Op>
+__device__ __forceinline__ void advance_pieces_body(const AdvanceArgs &a, Op &op, TravCtl *c,
+                                                    const RowRanges &rr, uint32_t np);
+
 // Hub pieces: one warp per piece of up to a.piece edges.
 template <class Op>
 __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_pieces(AdvanceArgs a, Op op) {
     TravCtl *c = a.ctl;
     RowRanges rr;
-    if (!advance_ranges(a, c, rr)) return;
-    const uint32_t np = c->npieces;
-    if (np == 0) return;
+    if (advance_ranges(a, c, rr)) {
+        const uint32_t np = c->npieces;
+        if (np) advance_pieces_body(a, op, c, rr, np);
+    }
+    if constexpr (op_epilogue<Op>::value) {
+        if (!op.epilogue_on()) return;   // kernel argument: the same in every CTA
+        __shared__ uint32_t s_last;
+        __threadfence();   // this thread's updates are visible before the CTA counts itself
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_last = atomicAdd(&c->end_arrive, 1u) == gridDim.x - 1;
+            if (s_last) {
+                __threadfence();   // every other CTA's updates are visible from here
+                c->end_arrive = 0;
+                op.epilogue(c);
+            }
+        }
+    }
+}
+
+template <class Op>
+__device__ __forceinline__ void advance_pieces_body(const AdvanceArgs &a, Op &op, TravCtl *c,
+                                                    const RowRanges &rr, uint32_t np) {
     op.begin(c);
     const uint32_t cur = c->cur;
     uint32_t *__restrict__ qout = cur ? a.q0 : a.q1;
@@ -458,6 +524,10 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_pieces(Advan
 //   void reduce_row(uint32_t r, const Acc &x)     into the global accumulator
 //   void store(uint32_t r, const Acc &slot)
 //   bool mark(uint32_t r)                         true when r is newly marked
+// and, optionally, for the first-hit kernels (kFirstHit):
+//   bool passes(uint32_t u)                       source u would contribute (a plain
+//                                                 load: several are kept in flight)
+//   Acc contribution(uint32_t u, uint32_t e)      its contribution (u passes)
 struct PullArgs {
     const uint32_t *colptr = nullptr;   // in-edges of r: [colptr[r], colptr[r+1])
     const uint32_t *rowidx = nullptr;   // their sources
@@ -589,12 +659,46 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_pull_pieces(PullArgs
 
 // First-contribution pull (Ops with kFirstHit: any single contribution is
 // enough, as for BFS levels): a bottom-up step that stops each row at its
-// first contributing in-edge.  k_pull_first_rows gives every wanted row with
-// at most kFirstLight in-edges to one thread, which reads its in-edges four at
-// a time and stops at the first source that passes; longer rows are listed in
-// a.pieces (count in ctl->npieces) for k_pull_first_long, one warp per row,
-// 32 in-edges per step with a warp vote to stop.
+// first contributing in-edge (in CSC order).  k_pull_first_rows gives every
+// wanted row with at most kFirstLight in-edges to one thread, which reads its
+// in-edges four at a time and stops at the first source that passes; longer
+// rows are listed in a.pieces (count in ctl->npieces) for k_pull_first_long,
+// where a group of 8 lanes takes a row (four rows per warp) and reads 32
+// in-edges per step, four per lane.  Ops with passes() / contribution()
+// test a step's sources with all their loads in flight and gather only the
+// first passing one.
 constexpr uint32_t kFirstLight = 32;
+constexpr uint32_t kFirstGroup = 8;   // lanes per long row
+
+template <class Op, class = void>
+struct op_has_passes : std::false_type {};
+template <class Op>
+struct op_has_passes<Op, std::void_t<decltype(std::declval<Op &>().passes(0u))>>
+    : std::true_type {};
+
+// The first of n (<= 4) sources u[0..n) that contributes, in order: its index
+// (or -1) and its contribution in x.
+template <class Op>
+__device__ __forceinline__ int first_contribution(Op &op, const uint32_t (&u)[4], uint32_t e0,
+                                                  uint32_t n, typename Op::Acc &x) {
+    if constexpr (op_has_passes<Op>::value) {
+        bool p[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) p[j] = (uint32_t)j < n && op.passes(u[j]);
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if (p[j]) {
+                x = op.contribution(u[j], e0 + j);
+                return j;
+            }
+        return -1;
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+            if ((uint32_t)j < n && op.contributes(u[j], e0 + j, x)) return j;
+        return -1;
+    }
+}
 
 template <class Op>
 __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_pull_first_rows(PullArgs a, Op op) {
@@ -611,19 +715,13 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_pull_first_rows(Pull
                 is_long = true;
             } else {
                 for (uint32_t i = b; i < e; i += 4) {
+                    const uint32_t n = min(4u, e - i);
                     uint32_t u[4];
 #pragma unroll
-                    for (int j = 0; j < 4; j++) u[j] = i + j < e ? __ldcs(&a.rowidx[i + j]) : 0;
-                    bool hit = false;
-#pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        Acc x;
-                        if (!hit && i + j < e && op.contributes(u[j], i + j, x)) {
-                            op.reduce_row(r, x);
-                            hit = true;
-                        }
-                    }
-                    if (hit) {
+                    for (int j = 0; j < 4; j++) u[j] = (uint32_t)j < n ? __ldcs(&a.rowidx[i + j]) : 0;
+                    Acc x;
+                    if (first_contribution(op, u, i, n, x) >= 0) {
+                        op.reduce_row(r, x);
                         newly = op.mark(r);
                         break;
                     }
@@ -640,29 +738,58 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_pull_first_long(Pull
     TravCtl *c = a.ctl;
     if (c->done || c->mode != a.want_mode) return;
     using Acc = typename Op::Acc;
+    constexpr uint32_t kGroups = 32 / kFirstGroup;
+    constexpr uint32_t kStep = kFirstGroup * 4;   // in-edges per group step
     const uint32_t nl = c->npieces;
     const uint32_t *rows = reinterpret_cast<const uint32_t *>(a.pieces);
     const uint32_t lane = lane_id();
+    const uint32_t grp = lane / kFirstGroup, sub = lane % kFirstGroup;
+    const uint32_t gshift = grp * kFirstGroup;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t k = warp; k < nl; k += nwarps) {
-        const uint32_t r = rows[k];
-        const uint32_t b = __ldg(&a.colptr[r]), e = __ldg(&a.colptr[r + 1]);
-        bool found = false;
-        for (uint32_t i = b; i < e; i += 32) {
-            const uint32_t j = i + lane;
-            const uint32_t u = j < e ? __ldcs(&a.rowidx[j]) : 0;
-            Acc x;
-            const bool hit = j < e && op.contributes(u, j, x);
-            const unsigned m = __ballot_sync(0xffffffffu, hit);
-            if (m) {
-                if (lane == (uint32_t)(__ffs(m) - 1)) op.reduce_row(r, x);
-                found = true;
-                break;
-            }
+    for (uint32_t k0 = warp * kGroups; k0 < nl; k0 += nwarps * kGroups) {
+        const uint32_t k = k0 + grp;
+        uint32_t r = 0, i = 0, e = 0;
+        if (k < nl) {
+            r = rows[k];
+            i = __ldg(&a.colptr[r]);
+            e = __ldg(&a.colptr[r + 1]);
         }
-        bool newly = false;
-        if (found && lane == 0) newly = op.mark(r);
+        bool found = false;
+        // every lane stays in the loop until all four groups are done (warp votes)
+        while (__any_sync(0xffffffffu, !found && i < e)) {
+            const bool active = !found && i < e;
+            const uint32_t j0 = i + sub * 4;
+            const uint32_t n = active && j0 < e ? min(4u, e - j0) : 0u;
+            uint32_t u[4];
+#pragma unroll
+            for (int t = 0; t < 4; t++) u[t] = (uint32_t)t < n ? __ldcs(&a.rowidx[j0 + t]) : 0;
+            bool p[4];
+            if constexpr (op_has_passes<Op>::value) {
+#pragma unroll
+                for (int t = 0; t < 4; t++) p[t] = (uint32_t)t < n && op.passes(u[t]);
+            } else {
+                Acc y;
+#pragma unroll
+                for (int t = 0; t < 4; t++) p[t] = (uint32_t)t < n && op.contributes(u[t], j0 + t, y);
+            }
+            const bool any = p[0] || p[1] || p[2] || p[3];
+            const uint32_t gm = (__ballot_sync(0xffffffffu, any) >> gshift) & ((1u << kFirstGroup) - 1u);
+            if (active && gm) {
+                if (sub == (uint32_t)(__ffs(gm) - 1)) {   // the group's first passing lane
+                    const int t = p[0] ? 0 : p[1] ? 1 : p[2] ? 2 : 3;
+                    Acc x;
+                    if constexpr (op_has_passes<Op>::value)
+                        x = op.contribution(u[t], j0 + t);
+                    else
+                        op.contributes(u[t], j0 + t, x);
+                    op.reduce_row(r, x);
+                }
+                found = true;
+            }
+            i += kStep;
+        }
+        const bool newly = found && sub == 0 && op.mark(r);
         warp_push(newly, r, a.qout, &c->qsize[1]);
     }
 }

@@ -40,12 +40,15 @@ struct TravCtl {
     uint32_t bucket_lo;         // SSSP: lower distance edge of the current bucket
     uint32_t pull_pending;      // SSSP: the settled bucket's heavy edges go by a pull pass
     uint32_t aux_done;          // SSSP: CTAs of the collect pass that finished
+    uint32_t end_arrive;        // CTAs of a superstep's last kernel that finished (epilogue)
     uint32_t bl_size;           // SSSP: entries in the bucket list
     uint32_t bl_over;           // SSSP: the bucket list overflowed (collect densely)
     uint32_t bucket_end;        // SSSP: upper distance edge of the current heavy bucket
     uint32_t sub_width;         // SSSP: light-phase sub-bucket width (0: none)
     uint32_t sub_buckets;       // SSSP: heavy buckets whose light phase is sub-bucketed
     uint32_t heavy_index;       // SSSP: heavy buckets started so far (0 = the first)
+    uint32_t tail_width;        // SSSP: width of the buckets after the first (<= delta: delta)
+    uint32_t all_edges;         // SSSP: the current bucket relaxes every edge in-bucket
     unsigned long long heavy_work;  // SSSP: heavy out-edges of the collected bucket
     unsigned long long settled_in;  // SSSP: in-edges of all settled vertices
     uint32_t ms_track;          // msBFS: this push level records first-touched vertices

@@ -528,6 +528,15 @@ int olv_tune_set(olv_graph *g, const char *key, double value) {
     } else if (!strcmp(key, "sssp_sub_buckets")) {
         OLV_CHECK_ARG(value >= 0 && value < 2147483647.0, "olv_tune_set: bad sssp_sub_buckets");
         t.sssp_sub_buckets = (uint32_t)value;
+    } else if (!strcmp(key, "sssp_spt")) {
+        OLV_CHECK_ARG(value == 1 || value == 2 || value == 4 || value == 8,
+                      "olv_tune_set: sssp_spt must be 1, 2, 4 or 8");
+        t.sssp_spt = (uint32_t)value;
+    } else if (!strcmp(key, "sssp_tail_delta")) {
+        OLV_CHECK_ARG(value >= 0 && value < 2147483647.0, "olv_tune_set: bad sssp_tail_delta");
+        t.sssp_tail_delta = (uint32_t)value;
+    } else if (!strcmp(key, "sssp_fuse_end")) {
+        t.sssp_fuse_end = value != 0;
     } else if (!strcmp(key, "pr_tile_u")) {
         const uint32_t u = (uint32_t)value;
         OLV_CHECK_ARG(value >= 1 && value <= 32 && (u & (u - 1)) == 0,
@@ -572,6 +581,9 @@ int olv_tune_get(const olv_graph *g, const char *key, double *value) {
     else if (!strcmp(key, "sssp_relabel")) *value = t.sssp_relabel;
     else if (!strcmp(key, "sssp_sub")) *value = t.sssp_sub;
     else if (!strcmp(key, "sssp_sub_buckets")) *value = t.sssp_sub_buckets;
+    else if (!strcmp(key, "sssp_spt")) *value = t.sssp_spt;
+    else if (!strcmp(key, "sssp_fuse_end")) *value = t.sssp_fuse_end;
+    else if (!strcmp(key, "sssp_tail_delta")) *value = t.sssp_tail_delta;
     else if (!strcmp(key, "sssp_hub_degree")) *value = t.sssp_hub_degree;
     else if (!strcmp(key, "sssp_piece")) *value = t.sssp_piece;
     else if (!strcmp(key, "ms_alpha")) *value = t.ms_alpha;

@@ -64,6 +64,10 @@ struct Tuning {
     int sssp_relabel = 1;             // SSSP: run on vertices renumbered by in-degree
     uint32_t sssp_sub = 0;            // SSSP: light-phase sub-bucket width (0: none)
     uint32_t sssp_sub_buckets = 1;    // SSSP: heavy buckets whose light phase uses it
+    uint32_t sssp_spt = 1;            // SSSP: queued sources per thread in a relax chunk
+    int sssp_fuse_end = 1;            // SSSP: superstep end step in the pieces kernel's last CTA
+    uint32_t sssp_tail_delta = 0;     // SSSP: width of the buckets after the first, which
+                                      // relax every edge (<= delta: delta, light/heavy)
     float ms_alpha = 20.0f;       // msBFS: pull when active out-edges * ms_alpha > E
     uint32_t pr_tile_u = 8;       // PageRank / weighted PR: entries per lane the row
                                   // grouping aims at (lanes per row by row length)

@@ -51,8 +51,12 @@ struct PartBfsOp {
     __device__ __forceinline__ bool row_wanted(uint32_t r) const { return level[r] == kInf; }
     __device__ __forceinline__ bool contributes(uint32_t u, uint32_t, int32_t &x) const {
         x = next_level;
+        return passes(u);
+    }
+    __device__ __forceinline__ bool passes(uint32_t u) const {
         return (__ldg(&frontier[u >> 6]) >> (u & 63)) & 1;
     }
+    __device__ __forceinline__ int32_t contribution(uint32_t, uint32_t) const { return next_level; }
     __device__ __forceinline__ void reduce_row(uint32_t r, int32_t x) { level[r] = x; }
     __device__ __forceinline__ bool mark(uint32_t r) {
         const uint32_t b = r + (lo & 63);   // lo is a multiple of 64: bit r of the slice

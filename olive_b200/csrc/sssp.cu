@@ -46,6 +46,16 @@
 // relax superstep skips an input vertex that it has already queued again,
 // and a bucket is collected from the list of its relax inputs when that
 // list is short.
+//
+// Buckets after the first (sssp_tail_delta > delta).  Past the first bucket
+// the unsettled vertices are the periphery: low degree, mostly reached along
+// one path.  There a bucket of width tail_delta relaxes every edge, light and
+// heavy, in its relax supersteps and needs no heavy step, collect or bucket
+// list: the relaxations are those of the narrow buckets (each vertex's edges
+// about once; CPU replay at RMAT-22 from the hub: 1.67 M either way) in far
+// fewer supersteps (37 -> 9 at width 256).  An improvement at or above the
+// bucket's end still goes to the far pile, so the split and the result are
+// those of delta-stepping with the wider bucket.
 #include <algorithm>
 #include <vector>
 
@@ -63,6 +73,7 @@ constexpr uint32_t kModeSplit = 2;
 constexpr uint32_t kModeHeavy = 3;
 constexpr uint32_t kModePull = 4;
 constexpr uint32_t kModeSubSplit = 5;
+constexpr uint32_t kModeRelaxAll = 6;   // relax every edge (buckets after the first, when wide)
 constexpr uint32_t kDefaultDelta = 64;
 
 // Arrays the collect and pull passes read besides the queues.
@@ -132,8 +143,12 @@ __global__ void k_pack_pairs(const uint32_t *__restrict__ a, const uint32_t *__r
 #ifndef OLV_SSSP_MINB
 #define OLV_SSSP_MINB 4   // 4: <= 64 registers
 #endif
+__device__ void sssp_end_step(TravCtl *c, cudaGraphConditionalHandle h, int use_cond,
+                              uint32_t max_steps, uint32_t bl_cap);
+
 struct SsspOp {
     static constexpr int kMinBlocks = OLV_SSSP_MINB;   // CTAs per SM the advance must fit
+    static constexpr bool kEpilogue = true;   // the superstep's end step, when fused
     using SV = uint32_t;
     static constexpr bool kHasFar = true;
     static constexpr bool kPacked = true;   // (column, weight) pairs: one 8-byte load per edge
@@ -151,6 +166,15 @@ struct SsspOp {
     uint32_t threshold, fmin;
     unsigned long long *relaxed_ctr;
     uint32_t *far_min;
+    // end of the superstep run by the last CTA of the pieces kernel (instead
+    // of a k_sssp_end launch) when end_fused is set
+    cudaGraphConditionalHandle end_h;
+    int end_fused, end_use_cond;
+    uint32_t end_max_steps, end_bl_cap;
+    __device__ __forceinline__ bool epilogue_on() const { return end_fused != 0; }
+    __device__ __forceinline__ void epilogue(TravCtl *c) const {
+        sssp_end_step(c, end_h, end_use_cond, end_max_steps, end_bl_cap);
+    }
 
     __device__ __forceinline__ void begin(TravCtl *c) {
         dist = static_cast<uint32_t *>(c->vdata);
@@ -233,7 +257,7 @@ __device__ void sssp_begin(TravCtl *c);
 
 __global__ void k_sssp_init(TravCtl *c, uint32_t *dist, uint32_t *q0, uint32_t src,
                             uint32_t delta, uint32_t sub, uint32_t sub_buckets,
-                            const uint32_t *newid) {
+                            uint32_t tail_width, const uint32_t *newid) {
     if (newid) src = newid[src];   // relabelled run: the source's new id
     TravCtl t = {};
     t.qsize[0] = 1;
@@ -243,6 +267,8 @@ __global__ void k_sssp_init(TravCtl *c, uint32_t *dist, uint32_t *q0, uint32_t s
     t.sub_width = sub < delta ? sub : 0;
     t.sub_buckets = sub_buckets;
     t.heavy_index = 0;
+    t.tail_width = tail_width > delta ? tail_width : 0;
+    t.all_edges = 0;
     t.threshold = (t.sub_width && sub_buckets > 0) ? t.sub_width : delta;
     t.epoch = 1;
     t.far_min = 0xffffffffu;
@@ -274,7 +300,7 @@ static __device__ __forceinline__ uint32_t sat_add(uint32_t a, uint32_t b) {
 __device__ void sssp_begin(TravCtl *c) {
     if (c->done) return;
     if (c->qsize[c->cur] > 0) {
-        c->mode = kModeRelax;
+        c->mode = c->all_edges ? kModeRelaxAll : kModeRelax;
         c->qsize[c->cur ^ 1] = 0;
         c->npieces = 0;
         return;
@@ -309,9 +335,11 @@ __device__ void sssp_begin(TravCtl *c) {
     c->bucket_lo = c->threshold;
     const uint32_t lo = c->threshold > c->far_min ? c->threshold : c->far_min;
     c->heavy_index++;
-    c->bucket_end = sat_add(lo, c->delta);
-    const bool sub = c->sub_width && c->heavy_index < c->sub_buckets;
-    const uint32_t t = sat_add(lo, sub ? c->sub_width : c->delta);
+    c->all_edges = c->tail_width != 0;   // buckets after the first: wide, every edge
+    const uint32_t width = c->all_edges ? c->tail_width : c->delta;
+    c->bucket_end = sat_add(lo, width);
+    const bool sub = !c->all_edges && c->sub_width && c->heavy_index < c->sub_buckets;
+    const uint32_t t = sat_add(lo, sub ? c->sub_width : width);
     c->threshold = t < c->bucket_end ? t : c->bucket_end;
     c->far_size[c->far_cur ^ 1] = 0;
     c->far_min = 0xffffffffu;
@@ -632,8 +660,11 @@ __device__ void sssp_split(TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far
     if (lane_id() == 0 && m != 0xffffffffu) atomicMin(&c->far_min, m);
 }
 
-__global__ void k_sssp_end(TravCtl *c, cudaGraphConditionalHandle h, int use_cond,
-                           uint32_t max_steps, uint32_t bl_cap) {
+// End of a superstep (one thread): account for what it did, decide whether
+// the run is over, set the next superstep's mode, and tell the enclosing
+// while-conditional graph whether to run another.
+__device__ void sssp_end_step(TravCtl *c, cudaGraphConditionalHandle h, int use_cond,
+                              uint32_t max_steps, uint32_t bl_cap) {
     if (!c->done) {
         if (c->mode == kModeRelax) {
             // the aux pass appended this superstep's input to the bucket list
@@ -646,6 +677,8 @@ __global__ void k_sssp_end(TravCtl *c, cudaGraphConditionalHandle h, int use_con
                     c->bl_over = 1;
             }
             c->cur ^= 1;
+        } else if (c->mode == kModeRelaxAll) {
+            c->cur ^= 1;   // no bucket list: an all-edge bucket has no heavy step
         } else if (c->mode == kModeHeavy) {
             c->qsize[c->cur] = 0;
             c->heavy_done = c->pull_pending ? 0 : 1;   // pending: the pull superstep is next
@@ -660,7 +693,7 @@ __global__ void k_sssp_end(TravCtl *c, cudaGraphConditionalHandle h, int use_con
             c->bl_over = 0;
             c->far_cur ^= 1;
             c->epoch++;
-            c->heavy_done = 0;
+            c->heavy_done = c->all_edges ? 1 : 0;   // all-edge buckets: nothing left after relax
         }
         c->steps++;
         if (c->qsize[c->cur] == 0 && c->far_size[c->far_cur] == 0 && c->heavy_done) c->done = 1;
@@ -671,6 +704,11 @@ __global__ void k_sssp_end(TravCtl *c, cudaGraphConditionalHandle h, int use_con
         sssp_begin(c);   // mode and counters of the next superstep
     }
     if (use_cond) cudaGraphSetConditional(h, c->done ? 0u : 1u);
+}
+
+__global__ void k_sssp_end(TravCtl *c, cudaGraphConditionalHandle h, int use_cond,
+                           uint32_t max_steps, uint32_t bl_cap) {
+    sssp_end_step(c, h, use_cond, max_steps, bl_cap);
 }
 
 // The superstep's dense pass: collect the settled bucket (heavy mode), pull
@@ -924,11 +962,20 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     // a correct run needs far fewer supersteps; the bound only stops a runaway loop
     uint32_t max_steps = (uint32_t)(3ULL * g->V + 1000 > 0xfffffff0ULL ? 0xfffffff0ULL
                                                                     : 3ULL * g->V + 1000);
+    // the relax kernel for the tuned sources per thread (1, 2, 4 or 8)
+    const uint32_t spt = g->tune.sssp_spt;
+    const void *chunks = spt == 8   ? (const void *)k_advance_chunks<SsspOp, 8>
+                         : spt == 4 ? (const void *)k_advance_chunks<SsspOp, 4>
+                         : spt == 2 ? (const void *)k_advance_chunks<SsspOp, 2>
+                                    : (const void *)k_advance_chunks<SsspOp, 1>;
     int nb = 0;   // the relax kernel's own residency (it holds more registers than BFS's)
-    OLV_TRY(resident_blocks(g, (const void *)k_advance_chunks<SsspOp>, &nb));
+    OLV_TRY(resident_blocks(g, chunks, &nb));
     uint32_t V = g->V;
     a.rng2 = ws.sssp_hr.as<uint2>();   // heavy edges: [rowmid[u], rowptr[u+1])
     a.want_mode2 = kModeHeavy;
+    a.rbeg3 = R.rowptr;                // every edge: [rowptr[u], rowptr[u+1])
+    a.rend3 = R.rowptr + 1;
+    a.want_mode3 = kModeRelaxAll;
     SsspAux x;
     x.colptr = R.colptr;
     x.crw = ws.sssp_crw.as<uint2>();
@@ -941,12 +988,20 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     x.pull = g->tune.sssp_pull && x.crw != nullptr;
     void *a_aux[] = {&V, &ctl, &q0, &q1, &far0, &far1, &fm, &x};
     OLV_TRY(sink((const void *)k_sssp_aux, dim3(nb), dim3(kBlock), a_aux));
-    void *a_adv[] = {&a, &op};
-    OLV_TRY(sink((const void *)k_advance_chunks<SsspOp>, dim3(nb), dim3(kBlock), a_adv));
-    OLV_TRY(sink((const void *)k_advance_pieces<SsspOp>, dim3(nb), dim3(kBlock), a_adv));
     uint32_t bl_cap = x.bl_cap;
-    void *a_end[] = {&ctl, &h, &use_cond, &max_steps, &bl_cap};
-    OLV_TRY(sink((const void *)k_sssp_end, dim3(1), dim3(1), a_end));
+    // the end step runs in the pieces kernel's last CTA, or as its own launch
+    op.end_h = h;
+    op.end_fused = g->tune.sssp_fuse_end;
+    op.end_use_cond = use_cond;
+    op.end_max_steps = max_steps;
+    op.end_bl_cap = bl_cap;
+    void *a_adv[] = {&a, &op};
+    OLV_TRY(sink(chunks, dim3(nb), dim3(kBlock), a_adv));
+    OLV_TRY(sink((const void *)k_advance_pieces<SsspOp>, dim3(nb), dim3(kBlock), a_adv));
+    if (!op.end_fused) {
+        void *a_end[] = {&ctl, &h, &use_cond, &max_steps, &bl_cap};
+        OLV_TRY(sink((const void *)k_sssp_end, dim3(1), dim3(1), a_end));
+    }
     return OLV_OK;
 }
 
@@ -979,7 +1034,8 @@ int run_sssp_device(olv_graph *g, uint32_t src, uint32_t *dist_dev) {
     OLV_CUDA(cudaMemsetAsync(g->ws.mark.p, 0, kMarks * mark_words(g->V) * 4, s));
     k_fill_i32<<<g->num_sms * 8, kBlock, 0, s>>>((int32_t *)dist, g->V, kInf);
     k_sssp_init<<<1, 1, 0, s>>>(ctl, dist, g->ws.q0.as<uint32_t>(), src, sssp_delta(g),
-                                g->tune.sssp_sub, g->tune.sssp_sub_buckets, R.newid);
+                                g->tune.sssp_sub, g->tune.sssp_sub_buckets,
+                                g->tune.sssp_tail_delta, R.newid);
     OLV_CUDA(cudaGetLastError());
     auto finish = [&]() -> int {
         if (R.dist) {

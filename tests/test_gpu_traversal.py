@@ -182,6 +182,67 @@ def test_sssp_hub_pieces_vs_dijkstra(ob, hub, piece):
             np.testing.assert_array_equal(g.sssp(s), oracle.dijkstra(rp, cl, w, s)[0])
 
 
+@pytest.mark.parametrize("spt,fuse", [(1, 0), (1, 1), (2, 1), (4, 0), (4, 1), (8, 1)])
+def test_sssp_chunk_shape_and_fused_end_vs_dijkstra(ob, spt, fuse):
+    """Relax chunks of 256 x spt queued sources, and the superstep's end step
+    run by the pieces kernel's last CTA (fuse 1) or by its own launch: the
+    same distances, inside the CUDA graph and in the host loop."""
+    with ob.Graph.rmat(16, 16, 5, weights=True, wseed=4) as g:
+        g.tune(sssp_spt=spt, sssp_fuse_end=fuse, sssp_hub_degree=64, sssp_piece=64)
+        rp, cl, w = g.csr()
+        hub, _ = g.max_degree_vertex()
+        deg = np.diff(rp.astype(np.int64))
+        for s in (hub, int(np.flatnonzero(deg > 0)[3])):
+            ref = oracle.dijkstra(rp, cl, w, s)[0]
+            np.testing.assert_array_equal(g.sssp(s), ref)
+        g.tune(use_graphs=0)
+        np.testing.assert_array_equal(g.sssp(hub), oracle.dijkstra(rp, cl, w, hub)[0])
+        g.tune(use_graphs=1, sssp_sub=8)
+        np.testing.assert_array_equal(g.sssp(hub), oracle.dijkstra(rp, cl, w, hub)[0])
+
+
+@pytest.mark.parametrize("tail", [0, 65, 256, 1000, 1 << 30])
+def test_sssp_wide_tail_buckets_vs_dijkstra(ob, tail):
+    """Buckets after the first of width sssp_tail_delta relaxing every edge
+    (0 and widths <= delta: light/heavy throughout; 2^30: one Bellman-Ford
+    bucket after the first): Dijkstra's distances from the hub and from a
+    low-degree source, with the pull or push heavy step, sub-buckets in the
+    first bucket, in the graph and in the host loop."""
+    with ob.Graph.rmat(16, 16, 6, weights=True, wseed=8) as g:
+        g.tune(sssp_tail_delta=tail)
+        rp, cl, w = g.csr()
+        hub, _ = g.max_degree_vertex()
+        deg = np.diff(rp.astype(np.int64))
+        ref_hub = oracle.dijkstra(rp, cl, w, hub)[0]
+        for s in (hub, int(np.flatnonzero(deg == 1)[0])):
+            np.testing.assert_array_equal(g.sssp(s), oracle.dijkstra(rp, cl, w, s)[0])
+        for kw in ({"sssp_pull": 0}, {"sssp_sub": 16}, {"use_graphs": 0}, {"sssp_relabel": 0}):
+            base = g.tune()
+            g.tune(**kw)
+            np.testing.assert_array_equal(g.sssp(hub), ref_hub, err_msg=str(kw))
+            g.tune(**{k: base[k] for k in kw})
+
+
+@pytest.mark.parametrize("path", [p for p in FIXTURES if "weights" in np.load(p)], ids=_fid)
+def test_sssp_wide_tail_on_fixtures(ob, path):
+    """The weighted fixtures with narrow and wide buckets after the first."""
+    z = np.load(path)
+    rp, cl, w = z["sorted_rowptr"], z["sorted_col"], z["sorted_weights"]
+    with ob.Graph.from_csr(rp, cl, w) as g:
+        for tail in (2, 300):
+            g.tune(sssp_delta=1, sssp_tail_delta=tail)
+            for s in range(0, len(rp) - 1, 5):
+                ref, *_ = oracle.dijkstra(rp, cl, w, s)
+                np.testing.assert_array_equal(g.sssp(s), ref, err_msg=f"tail {tail} source {s}")
+
+
+def test_sssp_chunk_shape_rejects_bad_values(ob):
+    with ob.Graph.rmat(8, 4, 1, weights=True) as g:
+        for bad in (0, 3, 16):
+            with pytest.raises(ob.OliveError):
+                g.tune(sssp_spt=bad)
+
+
 @pytest.mark.parametrize("sub,nsub", [(0, 1), (4, 1), (8, 2), (16, 1), (1, 3), (500, 1)])
 def test_sssp_sub_buckets_vs_dijkstra(ob, sub, nsub):
     """The first heavy buckets' light phase in sub-buckets of every width

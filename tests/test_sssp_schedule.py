@@ -48,12 +48,13 @@ def _lower(dist, v, nd):
     return v, nd
 
 
-def schedule(rp, col, w, src, delta, pull_mode, list_collect, sub=0, nsub=1):
+def schedule(rp, col, w, src, delta, pull_mode, list_collect, sub=0, nsub=1, tail=0):
     """pull_mode: 'never', 'always' or 'rule' (the kernel's choice:
     E - settled in-edges + V/2 < heavy out-edges of the bucket).  sub > 0:
     the light phase of the first nsub heavy buckets runs in sub-buckets of
     width sub (the far pile is split at each sub-bucket's end; the heavy step
-    follows the last one)."""
+    follows the last one).  tail > delta: the buckets after the first are
+    tail wide and relax every edge in-bucket, with no heavy step."""
     rp = rp.astype(np.int64)
     col = col.astype(np.int64)
     w = w.astype(np.int64)
@@ -77,18 +78,20 @@ def schedule(rp, col, w, src, delta, pull_mode, list_collect, sub=0, nsub=1):
     lo, bend = 0, delta
     hi = min(sw if nsub > 0 else delta, bend)
     settled_in, pulls = 0, 0
+    wide = False
+    every = np.ones(E, bool)
     while True:
         blist = []
         while True:
-            while len(q):                       # relax supersteps: light edges
+            while len(q):                       # relax supersteps: light (or all) edges
                 blist.append(q)
-                u, e = _expand(rp, deg, light, q)
+                u, e = _expand(rp, deg, every if wide else light, q)
                 v, nd = _lower(dist, col[e], np.minimum(dist[u] + w[e], INF))
                 far[v[nd >= hi]] = True
                 q = v[nd < hi]
             fv = np.flatnonzero(far)
             fv = fv[dist[fv] >= hi]
-            if hi < bend and len(fv) and dist[fv].min() < bend:   # next sub-bucket
+            if not wide and hi < bend and len(fv) and dist[fv].min() < bend:   # next sub-bucket
                 hi = min(max(hi, int(dist[fv].min())) + sw, bend)
                 far[:] = False
                 far[fv] = True
@@ -97,6 +100,18 @@ def schedule(rp, col, w, src, delta, pull_mode, list_collect, sub=0, nsub=1):
                 continue
             break
         in_bucket = np.flatnonzero((dist >= lo) & (dist < hi))
+        if wide:   # every edge of the bucket was relaxed: no heavy step
+            fv = np.flatnonzero(far)
+            fv = fv[dist[fv] >= hi]
+            far[:] = False
+            far[fv] = True
+            if len(fv) == 0:
+                return dist, pulls
+            lo = max(hi, int(dist[fv].min()))
+            hi = bend = lo + tail
+            q = fv[dist[fv] < hi]
+            far[q] = False
+            continue
         if list_collect:
             listed = np.unique(np.concatenate(blist)) if blist else np.empty(0, np.int64)
             listed = listed[(dist[listed] >= lo) & (dist[listed] < hi)]
@@ -128,8 +143,12 @@ def schedule(rp, col, w, src, delta, pull_mode, list_collect, sub=0, nsub=1):
             return dist, pulls
         lo = max(hi, int(dist[fv].min()))
         hb += 1
-        bend = lo + delta
-        hi = min(lo + (sw if hb < nsub else delta), bend)
+        wide = tail > delta
+        if wide:
+            hi = bend = lo + tail
+        else:
+            bend = lo + delta
+            hi = min(lo + (sw if hb < nsub else delta), bend)
         q = fv[dist[fv] < hi]
         far[q] = False
 
@@ -206,3 +225,29 @@ def test_schedule_with_sub_buckets(sub, nsub, pull_mode):
         ref = oracle.dijkstra(rp, col, w, hub)[0].astype(np.int64)
         dist, _ = schedule(rp, col, w, hub, 64, pull_mode, list_collect=True, sub=sub, nsub=nsub)
         np.testing.assert_array_equal(dist, ref)
+
+
+@pytest.mark.parametrize("tail", [65, 128, 256, 1 << 20])
+@pytest.mark.parametrize("pull_mode", ["never", "rule"])
+def test_schedule_with_wide_tail_buckets(tail, pull_mode):
+    """Buckets after the first relaxing every edge in-bucket (width tail, no
+    heavy step): Dijkstra's distances from the hub and from a low-degree
+    vertex, and from random weights on a random graph."""
+    rp, col = oracle.rmat_csr(12, 16, 7)
+    w = oracle.uint_weights(len(col), 17)
+    deg = np.diff(rp.astype(np.int64))
+    for src in (int(np.argmax(deg)), int(np.flatnonzero(deg == 1)[0])):
+        ref = oracle.dijkstra(rp, col, w, src)[0].astype(np.int64)
+        dist, _ = schedule(rp, col, w, src, 64, pull_mode, list_collect=True, tail=tail)
+        np.testing.assert_array_equal(dist, ref)
+    rng = np.random.default_rng(5)
+    V, E = 1500, 9000
+    s = np.sort(rng.integers(0, V, E))
+    rp = np.zeros(V + 1, np.int64)
+    np.add.at(rp, s + 1, 1)
+    rp = np.cumsum(rp).astype(np.uint32)
+    col = rng.integers(0, V, E).astype(np.uint32)
+    w = rng.integers(1, 1000, E).astype(np.uint32)
+    ref = oracle.dijkstra(rp, col, w, 0)[0].astype(np.int64)
+    dist, _ = schedule(rp, col, w, 0, 32, pull_mode, list_collect=True, tail=tail)
+    np.testing.assert_array_equal(dist, ref)
