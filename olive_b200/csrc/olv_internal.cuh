@@ -68,6 +68,8 @@ struct Tuning {
     int sssp_fuse_end = 1;            // SSSP: superstep end step in the pieces kernel's last CTA
     uint32_t sssp_tail_delta = 0;     // SSSP: width of the buckets after the first, which
                                       // relax every edge (<= delta: delta, light/heavy)
+    uint32_t sssp_lpull = 0;          // SSSP: a relax superstep pulls over light in-edges when
+                                      // its sources' light out-edges * this >= light edges (0: never)
     float ms_alpha = 20.0f;       // msBFS: pull when active out-edges * ms_alpha > E
     uint32_t pr_tile_u = 8;       // PageRank / weighted PR: entries per lane the row
                                   // grouping aims at (lanes per row by row length)
@@ -83,8 +85,11 @@ struct Workspace {
     DevBuf pull_idx;                // BFS pull: in-edges sorted by source out-degree (desc)
     // SSSP: rows split light (w <= delta) | heavy, as (column, weight) pairs;
     // rowmid[u] the split point; per vertex its light and heavy ranges as
-    // uint2 (one load each); the in-edges as (source, weight) pairs
-    DevBuf sssp_cw, rowmid, sssp_lr, sssp_hr, sssp_crw;
+    // uint2 (one load each); the in-edges as (source, weight) pairs, each
+    // vertex's light in-edges first (sssp_clr: their range), and the number
+    // of light edges
+    DevBuf sssp_cw, rowmid, sssp_lr, sssp_hr, sssp_crw, sssp_clr;
+    unsigned long long sssp_n_light = 0;
     DevBuf blist;                   // SSSP: inputs of the current bucket's relax supersteps
     DevBuf hdin;                    // SSSP: per vertex (heavy out-degree, in-degree)
     // SSSP: vertices renumbered by in-degree (descending): new -> old and
@@ -101,7 +106,7 @@ struct Workspace {
         fbits.release(); order.release(); cand.release(); cand2.release(); pull_idx.release();
         pull_first.release();
         sssp_cw.release(); rowmid.release(); sssp_lr.release(); sssp_hr.release();
-        sssp_crw.release(); blist.release(); hdin.release();
+        sssp_crw.release(); sssp_clr.release(); blist.release(); hdin.release();
         sssp_delta_built = 0;
         sr_perm.release(); sr_newid.release(); sr_rowptr.release(); sr_col.release();
         sr_w.release(); sr_colptr.release(); sr_rowidx.release(); sr_cw.release();

@@ -74,6 +74,7 @@ constexpr uint32_t kModeHeavy = 3;
 constexpr uint32_t kModePull = 4;
 constexpr uint32_t kModeSubSplit = 5;
 constexpr uint32_t kModeRelaxAll = 6;   // relax every edge (buckets after the first, when wide)
+constexpr uint32_t kModePullLight = 7;  // a relax superstep run as a pull over light in-edges
 constexpr uint32_t kDefaultDelta = 64;
 
 // Arrays the collect and pull passes read besides the queues.
@@ -87,6 +88,9 @@ struct SsspAux {
     uint32_t bl_cap;                   // bucket list capacity (entries)
     unsigned long long E;
     int pull;                          // pull supersteps allowed
+    const uint2 *clr;                  // per vertex: its light in-edges [clr.x, clr.y) of crw
+    const uint2 *lrng;                 // per vertex: its light out-edges (null: m_next not kept)
+    uint32_t *nmark0, *nmark1;         // near-queue marks (as SsspOp's)
 };
 
 // Stable partition of every row into light (w <= delta) then heavy edges,
@@ -97,7 +101,8 @@ __global__ void k_partition_rows(const uint32_t *__restrict__ rowptr,
                                  const uint32_t *__restrict__ col, const uint32_t *__restrict__ w,
                                  uint32_t V, uint32_t delta, uint2 *__restrict__ pcw,
                                  uint32_t *__restrict__ rowmid, uint2 *__restrict__ lr,
-                                 uint2 *__restrict__ hr) {
+                                 uint2 *__restrict__ hr, unsigned long long *nlight) {
+    unsigned long long cnt = 0;
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -125,19 +130,13 @@ __global__ void k_partition_rows(const uint32_t *__restrict__ rowptr,
             hi += __popc(mh);
         }
         if (lane == 0) {
-            rowmid[u] = b + nl;
+            if (rowmid) rowmid[u] = b + nl;
             lr[u] = make_uint2(b, b + nl);
-            hr[u] = make_uint2(b + nl, e);
+            if (hr) hr[u] = make_uint2(b + nl, e);
+            cnt += nl;
         }
     }
-}
-
-// In-edges as (source, weight) pairs for the pull superstep.
-__global__ void k_pack_pairs(const uint32_t *__restrict__ a, const uint32_t *__restrict__ b,
-                             unsigned long long n, uint2 *__restrict__ out) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x * blockDim.x)
-        out[i] = make_uint2(a[i], b[i]);
+    if (nlight && lane == 0 && cnt) atomicAdd(nlight, cnt);
 }
 
 #ifndef OLV_SSSP_MINB
@@ -166,6 +165,11 @@ struct SsspOp {
     uint32_t threshold, fmin;
     unsigned long long *relaxed_ctr;
     uint32_t *far_min;
+    // light out-degree sum of the vertices pushed to the next near queue
+    // (lrng null: not kept), for the next superstep's push / pull choice
+    const uint2 *lrng;
+    unsigned long long mnext;
+    unsigned long long *mnext_ctr;
     // end of the superstep run by the last CTA of the pieces kernel (instead
     // of a k_sssp_end launch) when end_fused is set
     cudaGraphConditionalHandle end_h;
@@ -186,6 +190,8 @@ struct SsspOp {
         relaxed_ctr = &c->edges_relaxed;
         far_min = &c->far_min;
         fmin = 0xffffffffu;
+        mnext = 0;
+        mnext_ctr = &c->m_next;
     }
     struct Pre {
         uint32_t nd, cur;
@@ -245,11 +251,17 @@ struct SsspOp {
         atomicAnd(&nprev[u >> 5], ~bit);
         return !(__ldcg(&nbits[u >> 5]) & bit);
     }
-    __device__ __forceinline__ void on_push(bool, uint32_t) {}
+    __device__ __forceinline__ void on_push(bool pushed, uint32_t v) {
+        if (lrng && pushed) {
+            const uint2 r = __ldg(&lrng[v]);
+            mnext += r.y - r.x;
+        }
+    }
     __device__ __forceinline__ void flush(unsigned long long relaxed) {
         warp_add64(relaxed, relaxed_ctr);
         const uint32_t m = __reduce_min_sync(0xffffffffu, fmin);
         if (lane_id() == 0 && m != 0xffffffffu) atomicMin(far_min, m);
+        if (lrng) warp_add64(mnext, mnext_ctr);
     }
 };
 
@@ -257,7 +269,8 @@ __device__ void sssp_begin(TravCtl *c);
 
 __global__ void k_sssp_init(TravCtl *c, uint32_t *dist, uint32_t *q0, uint32_t src,
                             uint32_t delta, uint32_t sub, uint32_t sub_buckets,
-                            uint32_t tail_width, const uint32_t *newid) {
+                            uint32_t tail_width, uint32_t lpull_div, unsigned long long n_light,
+                            const uint32_t *newid) {
     if (newid) src = newid[src];   // relabelled run: the source's new id
     TravCtl t = {};
     t.qsize[0] = 1;
@@ -269,6 +282,8 @@ __global__ void k_sssp_init(TravCtl *c, uint32_t *dist, uint32_t *q0, uint32_t s
     t.heavy_index = 0;
     t.tail_width = tail_width > delta ? tail_width : 0;
     t.all_edges = 0;
+    t.lpull_div = lpull_div;
+    t.n_light = n_light;
     t.threshold = (t.sub_width && sub_buckets > 0) ? t.sub_width : delta;
     t.epoch = 1;
     t.far_min = 0xffffffffu;
@@ -299,8 +314,13 @@ static __device__ __forceinline__ uint32_t sat_add(uint32_t a, uint32_t b) {
 //   split      start the next heavy bucket at max(threshold, far minimum).
 __device__ void sssp_begin(TravCtl *c) {
     if (c->done) return;
+    const unsigned long long mf = c->m_next;   // light out-edges of the near queue
+    c->m_next = 0;
     if (c->qsize[c->cur] > 0) {
-        c->mode = c->all_edges ? kModeRelaxAll : kModeRelax;
+        // a large near queue relaxes its light edges by a pull over every
+        // vertex's light in-edges instead (no atomics, streamed in-edges)
+        const bool pull = c->lpull_div && c->n_light && mf * c->lpull_div >= c->n_light;
+        c->mode = c->all_edges ? kModeRelaxAll : pull ? kModePullLight : kModeRelax;
         c->qsize[c->cur ^ 1] = 0;
         c->npieces = 0;
         return;
@@ -496,14 +516,18 @@ __device__ __forceinline__ uint32_t pull_cand(uint32_t du, uint32_t w, uint32_t 
 // the scan), and fold candidates into a shared per-vertex minimum.
 constexpr int kPullItems = 4;
 constexpr uint32_t kPullChunk = 4 * kBlock;
+// Shared memory of the pull passes (one copy in the aux kernel).
+struct PullSmem {
+    uint32_t off[kPullChunk + 1], beg[kPullChunk], best[kPullChunk], warp[33];
+};
 __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1, FarMarks fm,
-                          const SsspAux &x, WarpStage sf) {
+                          const SsspAux &x, WarpStage sf, PullSmem &sm) {
     uint32_t *dist = static_cast<uint32_t *>(c->vdata);
     const uint32_t hi = c->threshold;
     uint32_t *far = c->far_cur ? far1 : far0;
     uint32_t *far_size = &c->far_size[c->far_cur];
     uint32_t *fbits = (c->epoch & 1) ? fm.m1 : fm.m0;
-    __shared__ uint32_t s_off[kPullChunk + 1], s_beg[kPullChunk], s_best[kPullChunk], s_warp[33];
+    uint32_t *s_off = sm.off, *s_beg = sm.beg, *s_best = sm.best, *s_warp = sm.warp;
     const bool vec = ((uintptr_t)dist & 15) == 0 && ((uintptr_t)x.colptr & 15) == 0;
     const uint32_t lane = lane_id();
     uint32_t fmin = 0xffffffffu;
@@ -616,7 +640,9 @@ __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1
 // dropped, entries under the new threshold become the near queue, the rest
 // move to the other far buffer under the next generation.
 __device__ void sssp_split(TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0,
-                           uint32_t *far1, FarMarks fm, WarpStage sn, WarpStage sf) {
+                           uint32_t *far1, FarMarks fm, const uint2 *lrng, WarpStage sn,
+                           WarpStage sf) {
+    unsigned long long mnext = 0;   // light out-edges of the near queue (lrng set)
     const uint32_t *dist = static_cast<const uint32_t *>(c->vdata);
     const uint32_t fc = c->far_cur;
     const uint32_t n = c->far_size[fc];
@@ -642,6 +668,10 @@ __device__ void sssp_split(TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far
             if (d >= lo) {
                 if (d < hi) {
                     act[0] = 1;
+                    if (lrng) {
+                        const uint2 r = __ldg(&lrng[v[0]]);
+                        mnext += r.y - r.x;
+                    }
                 } else {
                     act[0] = 2;
                     atomicOr(&fnext[v[0] >> 5], bit);
@@ -658,6 +688,158 @@ __device__ void sssp_split(TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far
     warp_stage_flush(sf.buf, sf.n, sf.lim, fout, fout_size);
     const uint32_t m = __reduce_min_sync(0xffffffffu, fmin);
     if (lane_id() == 0 && m != 0xffffffffu) atomicMin(&c->far_min, m);
+    if (lrng) warp_add64(mnext, &c->m_next);
+}
+
+// Light pull superstep: the relax superstep of a large near queue, run as a
+// pull.  Every vertex not settled in an earlier bucket (dist >= bucket_lo)
+// takes the minimum of dist[u] + w over its light in-edges whose source is
+// under the threshold -- a superset of the relaxations the push would make
+// from the queue (relaxing from any vertex with a valid distance is safe),
+// with no atomics on distances and the in-edges streamed.  Each vertex is
+// written by the thread that owns it; an improvement under the threshold
+// queues it for the next superstep (once: one owner), one at or above goes to
+// the far pile (once per pile generation).  The marks the previous superstep
+// set for its queue (this superstep's input) are cleared, as its push would
+// have cleared them.  Same layout as sssp_pull: 1024 vertices per CTA
+// iteration, their light in-edges balanced over the CTA.
+__device__ void sssp_pull_light(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1,
+                                uint32_t *far0, uint32_t *far1, FarMarks fm, const SsspAux &x,
+                                WarpStage sn, WarpStage sf, PullSmem &sm) {
+    uint32_t *dist = static_cast<uint32_t *>(c->vdata);
+    const uint32_t lo = c->bucket_lo, hi = c->threshold;
+    const uint32_t cur = c->cur;
+    const uint32_t *qin = cur ? q1 : q0;
+    uint32_t *qout = cur ? q0 : q1;
+    uint32_t *qout_size = &c->qsize[cur ^ 1];
+    uint32_t *far = c->far_cur ? far1 : far0;
+    uint32_t *far_size = &c->far_size[c->far_cur];
+    uint32_t *fbits = (c->epoch & 1) ? fm.m1 : fm.m0;
+    uint32_t *nprev = ((c->steps + 1) & 1) ? x.nmark0 : x.nmark1;
+    const uint32_t nin = c->qsize[cur];
+    for (uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x; i < nin;
+         i += (uint64_t)gridDim.x * kBlock) {
+        const uint32_t u = qin[i];
+        atomicAnd(&nprev[u >> 5], ~(1u << (u & 31)));
+    }
+    uint32_t *s_off = sm.off, *s_beg = sm.beg, *s_best = sm.best, *s_warp = sm.warp;
+    const bool vec = ((uintptr_t)dist & 15) == 0 && ((uintptr_t)x.clr & 15) == 0;
+    const uint32_t lane = lane_id();
+    uint32_t fmin = 0xffffffffu;
+    unsigned long long scanned = 0, mnext = 0;
+    for (uint64_t base = (uint64_t)blockIdx.x * kPullChunk; base < x.vpull;
+         base += (uint64_t)gridDim.x * kPullChunk) {
+        const uint64_t v0 = base + 4 * (uint64_t)threadIdx.x;
+        uint32_t d[4] = {0u, 0u, 0u, 0u}, b[4] = {0u, 0u, 0u, 0u}, e[4] = {0u, 0u, 0u, 0u};
+        if (vec && v0 + 4 <= V) {
+            const uint4 d4 = __ldcg(reinterpret_cast<const uint4 *>(dist + v0));
+            d[0] = d4.x;
+            d[1] = d4.y;
+            d[2] = d4.z;
+            d[3] = d4.w;
+            if (d[0] >= lo || d[1] >= lo || d[2] >= lo || d[3] >= lo) {
+                const uint4 r01 = *reinterpret_cast<const uint4 *>(x.clr + v0);
+                const uint4 r23 = *reinterpret_cast<const uint4 *>(x.clr + v0 + 2);
+                if (d[0] >= lo) { b[0] = r01.x; e[0] = r01.y; }
+                if (d[1] >= lo) { b[1] = r01.z; e[1] = r01.w; }
+                if (d[2] >= lo) { b[2] = r23.x; e[2] = r23.y; }
+                if (d[3] >= lo) { b[3] = r23.z; e[3] = r23.w; }
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (v0 + j < V) {
+                    d[j] = __ldcg(dist + v0 + j);
+                    if (d[j] >= lo) {
+                        const uint2 r = x.clr[v0 + j];
+                        b[j] = r.x;
+                        e[j] = r.y;
+                    }
+                }
+        }
+        // settled vertices and vertices past V keep an empty range
+        const uint32_t t01 = (e[0] - b[0]) + (e[1] - b[1]);
+        const uint32_t t = t01 + (e[2] - b[2]) + (e[3] - b[3]);
+        uint32_t total;
+        const uint32_t off = block_exclusive_scan(t, &total, s_warp);
+        const uint32_t r0 = 4 * threadIdx.x;
+        s_off[r0] = off;
+        s_off[r0 + 1] = off + (e[0] - b[0]);
+        s_off[r0 + 2] = off + t01;
+        s_off[r0 + 3] = off + t01 + (e[2] - b[2]);
+        if (threadIdx.x == kBlock - 1) s_off[kPullChunk] = total;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            s_beg[r0 + j] = b[j];
+            s_best[r0 + j] = d[j];
+        }
+        __syncthreads();
+        for (uint32_t k0 = threadIdx.x; k0 < total; k0 += kBlock * kPullItems) {
+            uint32_t own[kPullItems], u[kPullItems], w[kPullItems], du[kPullItems];
+#pragma unroll
+            for (int j = 0; j < kPullItems; j++) {
+                const uint32_t k = k0 + j * kBlock;
+                own[j] = kPullChunk;
+                u[j] = 0;
+                w[j] = 0;
+                if (k < total) {
+                    uint32_t l = 0;   // last vertex with s_off[vertex] <= k
+#pragma unroll
+                    for (uint32_t step = kPullChunk / 2; step > 0; step >>= 1)
+                        if (s_off[l + step] <= k) l += step;
+                    own[j] = l;
+                    const uint2 t2 = __ldcs(&x.crw[s_beg[l] + (k - s_off[l])]);
+                    u[j] = t2.x;
+                    w[j] = t2.y;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kPullItems; j++)
+                du[j] = own[j] < kPullChunk ? __ldcg(&dist[u[j]]) : 0xffffffffu;
+#pragma unroll
+            for (int j = 0; j < kPullItems; j++) {
+                if (own[j] < kPullChunk) {
+                    const uint32_t nd = pull_cand(du[j], w[j], hi);
+                    if (nd < s_best[own[j]]) atomicMin(&s_best[own[j]], nd);
+                }
+            }
+        }
+        __syncthreads();
+        scanned += t;
+        int act[4];
+        uint32_t va[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const uint32_t best = s_best[r0 + j];
+            va[j] = (uint32_t)(v0 + j);
+            act[j] = 0;
+            if (best < d[j]) {   // only vertices with light in-edges from under the threshold
+                dist[va[j]] = best;
+                if (best < hi) {
+                    act[j] = 1;
+                    if (x.lrng) {
+                        const uint2 r = __ldg(&x.lrng[va[j]]);
+                        mnext += r.y - r.x;
+                    }
+                } else {
+                    const uint32_t bit = 1u << (va[j] & 31);
+                    if (!(atomicOr(&fbits[va[j] >> 5], bit) & bit)) act[j] = 2;
+                    fmin = best < fmin ? best : fmin;
+                }
+            }
+        }
+        sn.reserve(32 * 4, qout, qout_size);
+        stage_push_n<4>(act, va, 1, sn.buf, sn.n, sn.lim, kWarpStage, qout, qout_size);
+        sf.reserve(32 * 4, far, far_size);
+        stage_push_n<4>(act, va, 2, sf.buf, sf.n, sf.lim, kWarpStage, far, far_size);
+        __syncthreads();   // s_off / s_beg / s_best are rewritten by the next chunk
+    }
+    warp_stage_flush(sn.buf, sn.n, sn.lim, qout, qout_size);
+    warp_stage_flush(sf.buf, sf.n, sf.lim, far, far_size);
+    const uint32_t m = __reduce_min_sync(0xffffffffu, fmin);
+    if (lane == 0 && m != 0xffffffffu) atomicMin(&c->far_min, m);
+    warp_add64(scanned, &c->edges_relaxed);
+    if (x.lrng) warp_add64(mnext, &c->m_next);
 }
 
 // End of a superstep (one thread): account for what it did, decide whether
@@ -666,9 +848,10 @@ __device__ void sssp_split(TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far
 __device__ void sssp_end_step(TravCtl *c, cudaGraphConditionalHandle h, int use_cond,
                               uint32_t max_steps, uint32_t bl_cap) {
     if (!c->done) {
-        if (c->mode == kModeRelax) {
+        if (c->mode == kModeRelax || c->mode == kModePullLight) {
             // the aux pass appended this superstep's input to the bucket list
             // under the same capacity test
+            if (c->mode == kModePullLight) c->pull_steps++;
             const uint32_t n = c->qsize[c->cur];
             if (!c->bl_over) {
                 if ((uint64_t)c->bl_size + n <= bl_cap)
@@ -685,6 +868,7 @@ __device__ void sssp_end_step(TravCtl *c, cudaGraphConditionalHandle h, int use_
         } else if (c->mode == kModePull) {
             c->pull_pending = 0;
             c->heavy_done = 1;
+            c->pull_steps++;
         } else if (c->mode == kModeSubSplit) {
             c->far_cur ^= 1;   // the bucket list and the pending heavy step carry over
             c->epoch++;
@@ -719,18 +903,21 @@ k_sssp_aux(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0, u
            FarMarks fm, SsspAux x) {
     if (c->done) return;
     const uint32_t mode = c->mode;
-    if (mode == kModeRelax) {   // append this superstep's input to the bucket list
+    if (mode == kModeRelax || mode == kModePullLight) {
+        // append this superstep's input to the bucket list
         const uint32_t n = c->qsize[c->cur];
-        if (c->bl_over || (uint64_t)c->bl_size + n > x.bl_cap) return;   // k_sssp_end: overflow
-        const uint32_t *qin = c->cur ? q1 : q0;
-        uint32_t *dst = x.blist + c->bl_size;
-        for (uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x; i < n;
-             i += (uint64_t)gridDim.x * kBlock)
-            dst[i] = qin[i];
+        if (!c->bl_over && (uint64_t)c->bl_size + n <= x.bl_cap) {   // else k_sssp_end: overflow
+            const uint32_t *qin = c->cur ? q1 : q0;
+            uint32_t *dst = x.blist + c->bl_size;
+            for (uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x; i < n;
+                 i += (uint64_t)gridDim.x * kBlock)
+                dst[i] = qin[i];
+        }
+        if (mode == kModeRelax) return;   // the push kernels relax the queue
+    } else if (mode != kModeHeavy && mode != kModeSplit && mode != kModePull &&
+               mode != kModeSubSplit) {
         return;
     }
-    if (mode != kModeHeavy && mode != kModeSplit && mode != kModePull && mode != kModeSubSplit)
-        return;
     __shared__ uint32_t s_a[kBlock / 32][kWarpStage], s_b[kBlock / 32][kWarpStage];
     __shared__ uint32_t s_an[kBlock / 32], s_alim[kBlock / 32];
     __shared__ uint32_t s_bn[kBlock / 32], s_blim[kBlock / 32];
@@ -739,13 +926,16 @@ k_sssp_aux(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0, u
     WarpStage sb{s_b[wl], &s_bn[wl], &s_blim[wl]};
     sa.init();
     sb.init();
+    __shared__ PullSmem sm;   // the heavy and light pulls
     if (mode == kModeHeavy) {
         sssp_collect(V, c, q0, q1, x, sa);
         if (x.pull) sssp_choose(V, c, x);
     } else if (mode == kModePull) {
-        sssp_pull(V, c, far0, far1, fm, x, sb);
+        sssp_pull(V, c, far0, far1, fm, x, sb, sm);
+    } else if (mode == kModePullLight) {
+        sssp_pull_light(V, c, q0, q1, far0, far1, fm, x, sa, sb, sm);
     } else {
-        sssp_split(c, q0, q1, far0, far1, fm, sa, sb);
+        sssp_split(c, q0, q1, far0, far1, fm, x.lrng, sa, sb);
     }
 }
 
@@ -914,17 +1104,23 @@ static int sssp_partition(olv_graph *g) {
     OLV_TRY(ws.sssp_lr.ensure((size_t)g->V * 8 + 16));
     OLV_TRY(ws.sssp_hr.ensure((size_t)g->V * 8 + 16));
     OLV_TRY(ws.hdin.ensure((size_t)g->V * 8 + 16));
+    OLV_TRY(ws.tmp.ensure(16));
+    OLV_CUDA(cudaMemsetAsync(ws.tmp.p, 0, 8, g->stream));
     k_partition_rows<<<g->num_sms * 16, kBlock, 0, g->stream>>>(
         R.rowptr, R.col, R.w, g->V, delta, ws.sssp_cw.as<uint2>(), ws.rowmid.as<uint32_t>(),
-        ws.sssp_lr.as<uint2>(), ws.sssp_hr.as<uint2>());
+        ws.sssp_lr.as<uint2>(), ws.sssp_hr.as<uint2>(), ws.tmp.as<unsigned long long>());
     k_heavy_in_degrees<<<g->num_sms * 8, kBlock, 0, g->stream>>>(
         R.rowptr, ws.rowmid.as<uint32_t>(), R.colptr, g->V, ws.hdin.as<uint2>());
-    if (R.cw && R.rowidx) {   // in-edges as (source, weight) pairs for the pull
+    if (R.cw && R.rowidx) {   // in-edges as (source, weight) pairs, light ones first
         OLV_TRY(ws.sssp_crw.ensure(g->E * 8 + 16));
-        k_pack_pairs<<<g->num_sms * 8, kBlock, 0, g->stream>>>(R.rowidx, R.cw, g->E,
-                                                              ws.sssp_crw.as<uint2>());
+        OLV_TRY(ws.sssp_clr.ensure((size_t)g->V * 8 + 16));
+        k_partition_rows<<<g->num_sms * 16, kBlock, 0, g->stream>>>(
+            R.colptr, R.rowidx, R.cw, g->V, delta, ws.sssp_crw.as<uint2>(), nullptr,
+            ws.sssp_clr.as<uint2>(), nullptr, nullptr);
     }
     OLV_CUDA(cudaGetLastError());
+    OLV_CUDA(cudaMemcpyAsync(&ws.sssp_n_light, ws.tmp.p, 8, cudaMemcpyDeviceToHost, g->stream));
+    OLV_CUDA(cudaStreamSynchronize(g->stream));
     ws.sssp_delta_built = delta;
     ws.sssp_part_relabel = relabel;
     return OLV_OK;
@@ -986,6 +1182,12 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     x.cmark = mk + 4 * words;
     x.bl_cap = V;
     x.pull = g->tune.sssp_pull && x.crw != nullptr;
+    x.clr = ws.sssp_clr.as<uint2>();
+    const bool lpull = g->tune.sssp_lpull && x.crw != nullptr && x.clr != nullptr;
+    x.lrng = lpull ? ws.sssp_lr.as<uint2>() : nullptr;   // m_next kept only for the choice
+    x.nmark0 = op.nmark0;
+    x.nmark1 = op.nmark1;
+    op.lrng = x.lrng;
     void *a_aux[] = {&V, &ctl, &q0, &q1, &far0, &far1, &fm, &x};
     OLV_TRY(sink((const void *)k_sssp_aux, dim3(nb), dim3(kBlock), a_aux));
     uint32_t bl_cap = x.bl_cap;
@@ -1035,7 +1237,9 @@ int run_sssp_device(olv_graph *g, uint32_t src, uint32_t *dist_dev) {
     k_fill_i32<<<g->num_sms * 8, kBlock, 0, s>>>((int32_t *)dist, g->V, kInf);
     k_sssp_init<<<1, 1, 0, s>>>(ctl, dist, g->ws.q0.as<uint32_t>(), src, sssp_delta(g),
                                 g->tune.sssp_sub, g->tune.sssp_sub_buckets,
-                                g->tune.sssp_tail_delta, R.newid);
+                                g->tune.sssp_tail_delta,
+                                g->ws.sssp_crw.p && g->ws.sssp_clr.p ? g->tune.sssp_lpull : 0,
+                                g->ws.sssp_n_light, R.newid);
     OLV_CUDA(cudaGetLastError());
     auto finish = [&]() -> int {
         if (R.dist) {
@@ -1101,7 +1305,7 @@ extern "C" int olv_sssp(olv_graph *g, uint32_t src, uint32_t *dist_out, olv_stat
         float ms = 0;
         OLV_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
         st->iterations = h.steps;
-        st->pull_steps = 0;
+        st->pull_steps = h.pull_steps;   // heavy-edge and light-edge pull supersteps
         st->vertices_reached = red[1];
         st->edges_traversed = red[0];
         st->edges_relaxed = h.edges_relaxed;

@@ -236,6 +236,31 @@ def test_sssp_wide_tail_on_fixtures(ob, path):
                 np.testing.assert_array_equal(g.sssp(s), ref, err_msg=f"tail {tail} source {s}")
 
 
+@pytest.mark.parametrize("lpull", [1, 3, 1000])
+@pytest.mark.parametrize("tail", [0, 512])
+def test_sssp_light_pull_vs_dijkstra(ob, lpull, tail):
+    """Relax supersteps of large near queues run as a pull over every
+    vertex's light in-edges (lpull 1000: nearly every one): Dijkstra's
+    distances, with and without the renumbering, in the graph and the host
+    loop, and the pull counted in the statistics."""
+    with ob.Graph.rmat(16, 16, 7, weights=True, wseed=3) as g:
+        g.tune(sssp_lpull=lpull, sssp_tail_delta=tail)
+        rp, cl, w = g.csr()
+        hub, _ = g.max_degree_vertex()
+        deg = np.diff(rp.astype(np.int64))
+        ref_hub = oracle.dijkstra(rp, cl, w, hub)[0]
+        np.testing.assert_array_equal(g.sssp(hub), ref_hub)
+        if lpull >= 3:
+            assert g.last_stats.pull_steps >= 2   # the heavy-edge pull and a light pull
+        s = int(np.flatnonzero(deg == 1)[0])
+        np.testing.assert_array_equal(g.sssp(s), oracle.dijkstra(rp, cl, w, s)[0])
+        for kw in ({"sssp_relabel": 0}, {"use_graphs": 0}, {"sssp_pull": 0}, {"sssp_spt": 4}):
+            base = g.tune()
+            g.tune(**kw)
+            np.testing.assert_array_equal(g.sssp(hub), ref_hub, err_msg=str(kw))
+            g.tune(**{k: base[k] for k in kw})
+
+
 def test_sssp_chunk_shape_rejects_bad_values(ob):
     with ob.Graph.rmat(8, 4, 1, weights=True) as g:
         for bad in (0, 3, 16):
