@@ -126,13 +126,13 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
  *   "sssp_sub_buckets"  heavy buckets (from the first) that use sssp_sub (1)
  *   "sssp_spt"    queued sources per thread in a relax chunk: 1, 2, 4 or 8 (1)
  *   "sssp_fuse_end"  SSSP superstep's end step run by the last CTA of the
- *                 relax pieces kernel instead of a launch of its own (1)
+ *                 relax pieces kernel instead of a launch of its own (0)
  *   "sssp_lpull"  SSSP: a relax superstep whose near queue carries at least
  *                 1/sssp_lpull of the light edges runs as a pull over every
  *                 vertex's light in-edges (0: always push)
  *   "sssp_tail_delta"  width of the SSSP buckets after the first; above
  *                 sssp_delta those buckets relax every edge in-bucket and
- *                 have no heavy step (0: delta, light/heavy throughout)
+ *                 have no heavy step (1024; 0: delta, light/heavy throughout)
  *   "ms_alpha"    msBFS pull when active out-edges * ms_alpha > E   (20)
  *   "pr_tile_u"   PageRank / weighted PageRank: entries per lane per round
  *                 the row grouping aims at (1..32, a power of two); sets
