@@ -90,6 +90,11 @@ struct Workspace {
     // of light edges
     DevBuf sssp_cw, rowmid, sssp_lr, sssp_hr, sssp_crw, sssp_clr;
     unsigned long long sssp_n_light = 0;
+    // SSSP light pull: the light in-edges as a compact CSC over the vertices
+    // that have some (lv: their ids, lcp: offsets, lcrw: (source, weight)),
+    // and the first vertex of every tile of kLTile light in-edges
+    DevBuf sssp_lv, sssp_lcp, sssp_lcrw, sssp_ltile;
+    uint32_t sssp_lm = 0, sssp_ntiles = 0;
     DevBuf blist;                   // SSSP: inputs of the current bucket's relax supersteps
     DevBuf hdin;                    // SSSP: per vertex (heavy out-degree, in-degree)
     // SSSP: vertices renumbered by in-degree (descending): new -> old and
@@ -107,6 +112,7 @@ struct Workspace {
         pull_first.release();
         sssp_cw.release(); rowmid.release(); sssp_lr.release(); sssp_hr.release();
         sssp_crw.release(); sssp_clr.release(); blist.release(); hdin.release();
+        sssp_lv.release(); sssp_lcp.release(); sssp_lcrw.release(); sssp_ltile.release();
         sssp_delta_built = 0;
         sr_perm.release(); sr_newid.release(); sr_rowptr.release(); sr_col.release();
         sr_w.release(); sr_colptr.release(); sr_rowidx.release(); sr_cw.release();

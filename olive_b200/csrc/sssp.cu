@@ -56,6 +56,8 @@
 // fewer supersteps (37 -> 9 at width 256).  An improvement at or above the
 // bucket's end still goes to the far pile, so the split and the result are
 // those of delta-stepping with the wider bucket.
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <vector>
 
@@ -88,10 +90,16 @@ struct SsspAux {
     uint32_t bl_cap;                   // bucket list capacity (entries)
     unsigned long long E;
     int pull;                          // pull supersteps allowed
-    const uint2 *clr;                  // per vertex: its light in-edges [clr.x, clr.y) of crw
     const uint2 *lrng;                 // per vertex: its light out-edges (null: m_next not kept)
     uint32_t *nmark0, *nmark1;         // near-queue marks (as SsspOp's)
+    // light pull: compact CSC of the light in-edges (see Workspace)
+    const uint32_t *lv, *lcp, *ltile;
+    const uint2 *lcrw;
+    uint32_t ntiles;
+    unsigned long long n_light;
 };
+
+constexpr uint32_t kLTile = 1024;      // light in-edges per light-pull tile
 
 // Stable partition of every row into light (w <= delta) then heavy edges,
 // written as (column, weight) pairs; one warp per row, two passes (count,
@@ -518,8 +526,9 @@ constexpr int kPullItems = 4;
 constexpr uint32_t kPullChunk = 4 * kBlock;
 // Shared memory of the pull passes (one copy in the aux kernel).
 struct PullSmem {
-    uint32_t off[kPullChunk + 1], beg[kPullChunk], best[kPullChunk], warp[33];
+    uint32_t off[kPullChunk + 2], beg[kPullChunk], best[kPullChunk + 1], warp[33];
 };
+static_assert(kLTile + 2 <= kPullChunk + 2, "a light tile's offsets fit PullSmem::off");
 __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1, FarMarks fm,
                           const SsspAux &x, WarpStage sf, PullSmem &sm) {
     uint32_t *dist = static_cast<uint32_t *>(c->vdata);
@@ -692,17 +701,19 @@ __device__ void sssp_split(TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far
 }
 
 // Light pull superstep: the relax superstep of a large near queue, run as a
-// pull.  Every vertex not settled in an earlier bucket (dist >= bucket_lo)
-// takes the minimum of dist[u] + w over its light in-edges whose source is
-// under the threshold -- a superset of the relaxations the push would make
-// from the queue (relaxing from any vertex with a valid distance is safe),
-// with no atomics on distances and the in-edges streamed.  Each vertex is
-// written by the thread that owns it; an improvement under the threshold
-// queues it for the next superstep (once: one owner), one at or above goes to
-// the far pile (once per pile generation).  The marks the previous superstep
-// set for its queue (this superstep's input) are cleared, as its push would
-// have cleared them.  Same layout as sssp_pull: 1024 vertices per CTA
-// iteration, their light in-edges balanced over the CTA.
+// pull.  Every light edge (u, v) whose source is under the threshold offers
+// dist[u] + w to v -- a superset of the relaxations the push would make from
+// the queue (relaxing from any vertex with a valid distance is safe) -- with
+// the light in-edges streamed from a compact CSC in tiles of kLTile edges
+// (balanced whatever the in-degrees: the renumbered hubs' rows span many
+// tiles).  A tile folds its edges into a per-vertex minimum in shared memory;
+// a vertex not settled in an earlier bucket (dist >= bucket_lo) whose minimum
+// beats its distance takes it by atomicMin (a vertex can span tiles), and
+// the tile that lowered it queues it for the next superstep (under the
+// threshold, once through the near mark, as a push would) or puts it on the
+// far pile (once per pile generation).  The marks the previous superstep set
+// for its queue (this superstep's input) are cleared, as its push would have
+// cleared them.
 __device__ void sssp_pull_light(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1,
                                 uint32_t *far0, uint32_t *far1, FarMarks fm, const SsspAux &x,
                                 WarpStage sn, WarpStage sf, PullSmem &sm) {
@@ -715,124 +726,89 @@ __device__ void sssp_pull_light(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *
     uint32_t *far = c->far_cur ? far1 : far0;
     uint32_t *far_size = &c->far_size[c->far_cur];
     uint32_t *fbits = (c->epoch & 1) ? fm.m1 : fm.m0;
-    uint32_t *nprev = ((c->steps + 1) & 1) ? x.nmark0 : x.nmark1;
+    const uint32_t stamp = c->steps + 1;
+    uint32_t *nbits = (stamp & 1) ? x.nmark1 : x.nmark0;
+    uint32_t *nprev = (stamp & 1) ? x.nmark0 : x.nmark1;
     const uint32_t nin = c->qsize[cur];
     for (uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x; i < nin;
          i += (uint64_t)gridDim.x * kBlock) {
         const uint32_t u = qin[i];
         atomicAnd(&nprev[u >> 5], ~(1u << (u & 31)));
     }
-    uint32_t *s_off = sm.off, *s_beg = sm.beg, *s_best = sm.best, *s_warp = sm.warp;
-    const bool vec = ((uintptr_t)dist & 15) == 0 && ((uintptr_t)x.clr & 15) == 0;
+    uint32_t *s_lcp = sm.off, *s_best = sm.best;
     const uint32_t lane = lane_id();
     uint32_t fmin = 0xffffffffu;
     unsigned long long scanned = 0, mnext = 0;
-    for (uint64_t base = (uint64_t)blockIdx.x * kPullChunk; base < x.vpull;
-         base += (uint64_t)gridDim.x * kPullChunk) {
-        const uint64_t v0 = base + 4 * (uint64_t)threadIdx.x;
-        uint32_t d[4] = {0u, 0u, 0u, 0u}, b[4] = {0u, 0u, 0u, 0u}, e[4] = {0u, 0u, 0u, 0u};
-        if (vec && v0 + 4 <= V) {
-            const uint4 d4 = __ldcg(reinterpret_cast<const uint4 *>(dist + v0));
-            d[0] = d4.x;
-            d[1] = d4.y;
-            d[2] = d4.z;
-            d[3] = d4.w;
-            if (d[0] >= lo || d[1] >= lo || d[2] >= lo || d[3] >= lo) {
-                const uint4 r01 = *reinterpret_cast<const uint4 *>(x.clr + v0);
-                const uint4 r23 = *reinterpret_cast<const uint4 *>(x.clr + v0 + 2);
-                if (d[0] >= lo) { b[0] = r01.x; e[0] = r01.y; }
-                if (d[1] >= lo) { b[1] = r01.z; e[1] = r01.w; }
-                if (d[2] >= lo) { b[2] = r23.x; e[2] = r23.y; }
-                if (d[3] >= lo) { b[3] = r23.z; e[3] = r23.w; }
-            }
-        } else {
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-                if (v0 + j < V) {
-                    d[j] = __ldcg(dist + v0 + j);
-                    if (d[j] >= lo) {
-                        const uint2 r = x.clr[v0 + j];
-                        b[j] = r.x;
-                        e[j] = r.y;
-                    }
-                }
-        }
-        // settled vertices and vertices past V keep an empty range
-        const uint32_t t01 = (e[0] - b[0]) + (e[1] - b[1]);
-        const uint32_t t = t01 + (e[2] - b[2]) + (e[3] - b[3]);
-        uint32_t total;
-        const uint32_t off = block_exclusive_scan(t, &total, s_warp);
-        const uint32_t r0 = 4 * threadIdx.x;
-        s_off[r0] = off;
-        s_off[r0 + 1] = off + (e[0] - b[0]);
-        s_off[r0 + 2] = off + t01;
-        s_off[r0 + 3] = off + t01 + (e[2] - b[2]);
-        if (threadIdx.x == kBlock - 1) s_off[kPullChunk] = total;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            s_beg[r0 + j] = b[j];
-            s_best[r0 + j] = d[j];
-        }
+    constexpr int kLItems = kLTile / kBlock;
+    for (uint32_t t = blockIdx.x; t < x.ntiles; t += gridDim.x) {
+        const uint64_t t0 = (uint64_t)t * kLTile;
+        const uint64_t t1 = t0 + kLTile < x.n_light ? t0 + kLTile : x.n_light;
+        const uint32_t k0 = x.ltile[t];
+        const uint32_t nv = x.ltile[t + 1] - k0 + 1;   // vertices the tile can touch (<= kLTile + 1)
+        for (uint32_t i = threadIdx.x; i <= nv; i += kBlock) s_lcp[i] = x.lcp[k0 + i];
+        for (uint32_t i = threadIdx.x; i < nv; i += kBlock) s_best[i] = 0xffffffffu;
         __syncthreads();
-        for (uint32_t k0 = threadIdx.x; k0 < total; k0 += kBlock * kPullItems) {
-            uint32_t own[kPullItems], u[kPullItems], w[kPullItems], du[kPullItems];
+        uint32_t own[kLItems], u[kLItems], w[kLItems], du[kLItems];
 #pragma unroll
-            for (int j = 0; j < kPullItems; j++) {
-                const uint32_t k = k0 + j * kBlock;
-                own[j] = kPullChunk;
-                u[j] = 0;
-                w[j] = 0;
-                if (k < total) {
-                    uint32_t l = 0;   // last vertex with s_off[vertex] <= k
+        for (int j = 0; j < kLItems; j++) {
+            const uint64_t e = t0 + (uint64_t)j * kBlock + threadIdx.x;
+            own[j] = nv;
+            u[j] = 0;
+            w[j] = 0;
+            if (e < t1) {
+                const uint32_t el = (uint32_t)(e - s_lcp[0]);   // offsets relative to the tile's first vertex
+                uint32_t l = 0;   // last vertex with s_lcp[l] <= e
 #pragma unroll
-                    for (uint32_t step = kPullChunk / 2; step > 0; step >>= 1)
-                        if (s_off[l + step] <= k) l += step;
-                    own[j] = l;
-                    const uint2 t2 = __ldcs(&x.crw[s_beg[l] + (k - s_off[l])]);
-                    u[j] = t2.x;
-                    w[j] = t2.y;
-                }
+                for (uint32_t step = kLTile; step > 0; step >>= 1)
+                    if (l + step < nv && s_lcp[l + step] - s_lcp[0] <= el) l += step;
+                own[j] = l;
+                const uint2 p = __ldcs(&x.lcrw[e]);
+                u[j] = p.x;
+                w[j] = p.y;
             }
+        }
 #pragma unroll
-            for (int j = 0; j < kPullItems; j++)
-                du[j] = own[j] < kPullChunk ? __ldcg(&dist[u[j]]) : 0xffffffffu;
+        for (int j = 0; j < kLItems; j++) du[j] = own[j] < nv ? __ldcg(&dist[u[j]]) : 0xffffffffu;
 #pragma unroll
-            for (int j = 0; j < kPullItems; j++) {
-                if (own[j] < kPullChunk) {
-                    const uint32_t nd = pull_cand(du[j], w[j], hi);
-                    if (nd < s_best[own[j]]) atomicMin(&s_best[own[j]], nd);
-                }
+        for (int j = 0; j < kLItems; j++) {
+            if (own[j] < nv) {
+                const uint32_t nd = pull_cand(du[j], w[j], hi);
+                if (nd < s_best[own[j]]) atomicMin(&s_best[own[j]], nd);
             }
         }
         __syncthreads();
-        scanned += t;
-        int act[4];
-        uint32_t va[4];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const uint32_t best = s_best[r0 + j];
-            va[j] = (uint32_t)(v0 + j);
-            act[j] = 0;
-            if (best < d[j]) {   // only vertices with light in-edges from under the threshold
-                dist[va[j]] = best;
-                if (best < hi) {
-                    act[j] = 1;
-                    if (x.lrng) {
-                        const uint2 r = __ldg(&x.lrng[va[j]]);
-                        mnext += r.y - r.x;
+        if (threadIdx.x == 0) scanned += t1 - t0;
+        for (uint32_t i0 = 0; i0 < nv; i0 += kBlock) {   // every lane takes part in the pushes
+            const uint32_t i = i0 + threadIdx.x;
+            int act[1] = {0};
+            uint32_t va[1] = {0};
+            const uint32_t b = i < nv ? s_best[i] : 0xffffffffu;
+            if (b != 0xffffffffu) {
+                const uint32_t v = x.lv[k0 + i];
+                const uint32_t d = __ldcg(&dist[v]);
+                if (d >= lo && b < d && b < atomicMin(&dist[v], b)) {
+                    va[0] = v;
+                    const uint32_t bit = 1u << (v & 31);
+                    if (b < hi) {
+                        if (!(atomicOr(&nbits[v >> 5], bit) & bit)) {
+                            act[0] = 1;
+                            if (x.lrng) {
+                                const uint2 r = __ldg(&x.lrng[v]);
+                                mnext += r.y - r.x;
+                            }
+                        }
+                    } else {
+                        if (!(atomicOr(&fbits[v >> 5], bit) & bit)) act[0] = 2;
+                        fmin = b < fmin ? b : fmin;
                     }
-                } else {
-                    const uint32_t bit = 1u << (va[j] & 31);
-                    if (!(atomicOr(&fbits[va[j] >> 5], bit) & bit)) act[j] = 2;
-                    fmin = best < fmin ? best : fmin;
                 }
             }
+            sn.reserve(32, qout, qout_size);
+            stage_push_n<1>(act, va, 1, sn.buf, sn.n, sn.lim, kWarpStage, qout, qout_size);
+            sf.reserve(32, far, far_size);
+            stage_push_n<1>(act, va, 2, sf.buf, sf.n, sf.lim, kWarpStage, far, far_size);
         }
-        sn.reserve(32 * 4, qout, qout_size);
-        stage_push_n<4>(act, va, 1, sn.buf, sn.n, sn.lim, kWarpStage, qout, qout_size);
-        sf.reserve(32 * 4, far, far_size);
-        stage_push_n<4>(act, va, 2, sf.buf, sf.n, sf.lim, kWarpStage, far, far_size);
-        __syncthreads();   // s_off / s_beg / s_best are rewritten by the next chunk
+        __syncthreads();   // s_lcp / s_best are rewritten by the next tile
     }
     warp_stage_flush(sn.buf, sn.n, sn.lim, qout, qout_size);
     warp_stage_flush(sf.buf, sf.n, sf.lim, far, far_size);
@@ -1091,6 +1067,110 @@ static SsspCsr sssp_csr(olv_graph *g) {
 
 // Rows split light | heavy for the current delta (built once per delta and
 // numbering).
+// Light pull data (built on the first solve with sssp_lpull set, per
+// partition): the compact CSC of the light in-edges and its tile starts.
+__global__ void k_light_deg(const uint2 *__restrict__ clr, uint32_t V, uint32_t *__restrict__ flag,
+                            uint32_t *__restrict__ deg) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+         v += (uint64_t)gridDim.x * blockDim.x) {
+        const uint2 r = clr[v];
+        deg[v] = r.y - r.x;
+        flag[v] = r.y > r.x;
+    }
+}
+
+__global__ void k_light_compact(const uint32_t *__restrict__ flag, const uint32_t *__restrict__ pos,
+                                const uint32_t *__restrict__ off, uint32_t V,
+                                uint32_t *__restrict__ lv, uint32_t *__restrict__ lcp) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
+         v += (uint64_t)gridDim.x * blockDim.x)
+        if (flag[v]) {
+            lv[pos[v]] = (uint32_t)v;
+            lcp[pos[v]] = off[v];
+        }
+}
+
+__global__ void k_light_copy(const uint2 *__restrict__ clr, const uint32_t *__restrict__ off,
+                             const uint2 *__restrict__ crw, uint32_t V, uint2 *__restrict__ lcrw) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t v = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; v < V; v += nwarps) {
+        const uint2 r = clr[v];
+        const uint32_t o = off[v];
+        for (uint32_t i = lane; i < r.y - r.x; i += 32) lcrw[o + i] = crw[r.x + i];
+    }
+}
+
+// ltile[t] = the compact vertex that holds light in-edge t * kLTile; ltile[ntiles] = m - 1.
+__global__ void k_light_tiles(const uint32_t *__restrict__ lcp, uint32_t m, uint32_t ntiles,
+                              uint32_t *__restrict__ ltile) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t <= ntiles;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        if (t == ntiles) {
+            ltile[t] = m - 1;
+            continue;
+        }
+        const uint64_t e = t * kLTile;
+        uint32_t lo = 0, hi = m;   // lcp[lo] <= e < lcp[hi] (lcp[0] = 0, lcp[m] = light edges)
+        while (hi - lo > 1) {
+            const uint32_t mid = lo + (hi - lo) / 2;
+            if (lcp[mid] <= e)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        ltile[t] = lo;
+    }
+}
+
+static int build_light_csc(olv_graph *g) {
+    Workspace &ws = g->ws;
+    if (ws.sssp_lcrw.p || !ws.sssp_crw.p || !ws.sssp_clr.p || ws.sssp_n_light == 0) return OLV_OK;
+    const uint32_t V = g->V;
+    cudaStream_t s = g->stream;
+    DevBuf flag, pos, deg, off, temp;
+    OLV_TRY(flag.ensure((size_t)V * 4 + 16));
+    OLV_TRY(pos.ensure((size_t)V * 4 + 16));
+    OLV_TRY(deg.ensure((size_t)V * 4 + 16));
+    OLV_TRY(off.ensure((size_t)V * 4 + 16));
+    k_light_deg<<<g->num_sms * 8, kBlock, 0, s>>>(ws.sssp_clr.as<uint2>(), V, flag.as<uint32_t>(),
+                                                  deg.as<uint32_t>());
+    size_t tb = 0;
+    OLV_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag.as<uint32_t>(), pos.as<uint32_t>(),
+                                           (int64_t)V, s));
+    OLV_TRY(temp.ensure(tb + 16));
+    OLV_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, tb, flag.as<uint32_t>(), pos.as<uint32_t>(),
+                                           (int64_t)V, s));
+    OLV_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, tb, deg.as<uint32_t>(), off.as<uint32_t>(),
+                                           (int64_t)V, s));
+    uint32_t last[2] = {0, 0};
+    OLV_CUDA(cudaMemcpyAsync(&last[0], pos.as<uint32_t>() + (V - 1), 4, cudaMemcpyDeviceToHost, s));
+    OLV_CUDA(cudaMemcpyAsync(&last[1], flag.as<uint32_t>() + (V - 1), 4, cudaMemcpyDeviceToHost, s));
+    OLV_CUDA(cudaStreamSynchronize(s));
+    const uint32_t m = last[0] + last[1];
+    const unsigned long long nl = ws.sssp_n_light;
+    const uint32_t ntiles = (uint32_t)((nl + kLTile - 1) / kLTile);
+    OLV_TRY(ws.sssp_lv.ensure((size_t)m * 4 + 16));
+    OLV_TRY(ws.sssp_lcp.ensure(((size_t)m + 1) * 4 + 16));
+    OLV_TRY(ws.sssp_lcrw.ensure(nl * 8 + 16));
+    OLV_TRY(ws.sssp_ltile.ensure(((size_t)ntiles + 1) * 4 + 16));
+    k_light_compact<<<g->num_sms * 8, kBlock, 0, s>>>(flag.as<uint32_t>(), pos.as<uint32_t>(),
+                                                      off.as<uint32_t>(), V, ws.sssp_lv.as<uint32_t>(),
+                                                      ws.sssp_lcp.as<uint32_t>());
+    const uint32_t nl32 = (uint32_t)nl;
+    OLV_CUDA(cudaMemcpyAsync(ws.sssp_lcp.as<uint32_t>() + m, &nl32, 4, cudaMemcpyHostToDevice, s));
+    k_light_copy<<<g->num_sms * 16, kBlock, 0, s>>>(ws.sssp_clr.as<uint2>(), off.as<uint32_t>(),
+                                                    ws.sssp_crw.as<uint2>(), V,
+                                                    ws.sssp_lcrw.as<uint2>());
+    k_light_tiles<<<g->num_sms * 4, kBlock, 0, s>>>(ws.sssp_lcp.as<uint32_t>(), m, ntiles,
+                                                    ws.sssp_ltile.as<uint32_t>());
+    OLV_CUDA(cudaGetLastError());
+    OLV_CUDA(cudaStreamSynchronize(s));   // the host value above and the scratch buffers
+    ws.sssp_lm = m;
+    ws.sssp_ntiles = ntiles;
+    return OLV_OK;
+}
+
 static int sssp_partition(olv_graph *g) {
     Workspace &ws = g->ws;
     const uint32_t delta = sssp_delta(g);
@@ -1099,6 +1179,10 @@ static int sssp_partition(olv_graph *g) {
     if (ws.sssp_delta_built == delta && ws.sssp_part_relabel == relabel && ws.rowmid.p)
         return OLV_OK;
     const SsspCsr R = sssp_csr(g);
+    ws.sssp_lv.release();   // the light pull's CSC follows the partition
+    ws.sssp_lcp.release();
+    ws.sssp_lcrw.release();
+    ws.sssp_ltile.release();
     OLV_TRY(ws.sssp_cw.ensure(g->E * 8 + 16));
     OLV_TRY(ws.rowmid.ensure((size_t)g->V * 4 + 16));
     OLV_TRY(ws.sssp_lr.ensure((size_t)g->V * 8 + 16));
@@ -1182,8 +1266,13 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     x.cmark = mk + 4 * words;
     x.bl_cap = V;
     x.pull = g->tune.sssp_pull && x.crw != nullptr;
-    x.clr = ws.sssp_clr.as<uint2>();
-    const bool lpull = g->tune.sssp_lpull && x.crw != nullptr && x.clr != nullptr;
+    x.lv = ws.sssp_lv.as<uint32_t>();
+    x.lcp = ws.sssp_lcp.as<uint32_t>();
+    x.ltile = ws.sssp_ltile.as<uint32_t>();
+    x.lcrw = ws.sssp_lcrw.as<uint2>();
+    x.ntiles = ws.sssp_ntiles;
+    x.n_light = ws.sssp_n_light;
+    const bool lpull = g->tune.sssp_lpull && x.lcrw != nullptr;
     x.lrng = lpull ? ws.sssp_lr.as<uint2>() : nullptr;   // m_next kept only for the choice
     x.nmark0 = op.nmark0;
     x.nmark1 = op.nmark1;
@@ -1229,6 +1318,10 @@ int sssp_workspace(olv_graph *g) {
 
 int run_sssp_device(olv_graph *g, uint32_t src, uint32_t *dist_dev) {
     OLV_TRY(sssp_partition(g));
+    if (g->tune.sssp_lpull && !g->ws.sssp_lcrw.p) {
+        OLV_TRY(build_light_csc(g));
+        if (g->sssp_graph) g->sssp_graph->destroy();   // its kernels captured the old pointers
+    }
     cudaStream_t s = g->stream;
     TravCtl *ctl = g->ws.ctl.as<TravCtl>();
     const SsspCsr R = sssp_csr(g);
@@ -1238,7 +1331,7 @@ int run_sssp_device(olv_graph *g, uint32_t src, uint32_t *dist_dev) {
     k_sssp_init<<<1, 1, 0, s>>>(ctl, dist, g->ws.q0.as<uint32_t>(), src, sssp_delta(g),
                                 g->tune.sssp_sub, g->tune.sssp_sub_buckets,
                                 g->tune.sssp_tail_delta,
-                                g->ws.sssp_crw.p && g->ws.sssp_clr.p ? g->tune.sssp_lpull : 0,
+                                g->ws.sssp_lcrw.p ? g->tune.sssp_lpull : 0,
                                 g->ws.sssp_n_light, R.newid);
     OLV_CUDA(cudaGetLastError());
     auto finish = [&]() -> int {
