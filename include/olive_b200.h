@@ -127,6 +127,8 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
  *   "sssp_spt"    queued sources per thread in a relax chunk: 1, 2, 4 or 8 (1)
  *   "sssp_fuse_end"  SSSP superstep's end step run by the last CTA of the
  *                 relax pieces kernel instead of a launch of its own (0)
+ *   "sssp_mark_check"  SSSP: read a queue-mark word before setting its bit
+ *                 with an atomic (1)
  *   "sssp_lpull"  SSSP: a relax superstep whose near queue carries at least
  *                 1/sssp_lpull of the light edges runs as a pull over every
  *                 vertex's light in-edges (0: always push)

@@ -178,6 +178,7 @@ struct SsspOp {
     const uint2 *lrng;
     unsigned long long mnext;
     unsigned long long *mnext_ctr;
+    int mark_check;   // read a mark word before setting its bit (see apply_n)
     // end of the superstep run by the last CTA of the pieces kernel (instead
     // of a k_sssp_end launch) when end_fused is set
     cudaGraphConditionalHandle end_h;
@@ -227,18 +228,24 @@ struct SsspOp {
             cand[j] = act[j] && p[j].nd < p[j].cur;
             if (cand[j]) atomicMin(&dist[v[j]], p[j].nd);
         }
+        // With mark_check the mark words are read first and the atomicOr is
+        // issued only where the bit is still clear: the words of the most
+        // relaxed (renumbered: lowest) ids are otherwise hit by every lane
+        // that improves one of their 32 vertices, and the atomics serialise.
         uint32_t old[N];
 #pragma unroll
         for (int j = 0; j < N; j++) {
             old[j] = 0;
+            if (cand[j] && mark_check)
+                old[j] = __ldcg(&(p[j].nd < threshold ? nbits : fbits)[v[j] >> 5]);
+        }
+#pragma unroll
+        for (int j = 0; j < N; j++) {
             if (cand[j]) {
                 const uint32_t bit = 1u << (v[j] & 31);
-                if (p[j].nd < threshold) {
-                    old[j] = atomicOr(&nbits[v[j] >> 5], bit);
-                } else {
-                    fmin = p[j].nd < fmin ? p[j].nd : fmin;
-                    old[j] = atomicOr(&fbits[v[j] >> 5], bit);
-                }
+                if (p[j].nd >= threshold) fmin = p[j].nd < fmin ? p[j].nd : fmin;
+                if (!(old[j] & bit))
+                    old[j] = atomicOr(&(p[j].nd < threshold ? nbits : fbits)[v[j] >> 5], bit);
             }
         }
 #pragma unroll
@@ -976,12 +983,26 @@ __global__ void k_sssp_relabel(const uint32_t *__restrict__ old_ptr,
 }
 
 // Distances back to the caller's ids: out[v] = dnew[newid[v]].
+// Distances back to the caller's ids; with red, also the sum of out-degrees
+// and the count of the reached vertices (k_reached_edges in the same pass).
 __global__ void k_sssp_unrelabel(const uint32_t *__restrict__ dnew,
                                  const uint32_t *__restrict__ newid, uint32_t V,
-                                 uint32_t *__restrict__ out) {
+                                 uint32_t *__restrict__ out, const uint32_t *__restrict__ rowptr,
+                                 unsigned long long *red /*[2] or null*/) {
+    unsigned long long e = 0, n = 0;
     for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
-         v += (uint64_t)gridDim.x * blockDim.x)
-        out[v] = __ldg(&dnew[newid[v]]);
+         v += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t d = __ldg(&dnew[newid[v]]);
+        out[v] = d;
+        if (red && d != (uint32_t)kInf) {
+            e += rowptr[v + 1] - rowptr[v];
+            n++;
+        }
+    }
+    if (red) {
+        warp_add64(e, &red[0]);
+        warp_add64(n, &red[1]);
+    }
 }
 
 // Renumber the vertices by in-degree, highest first (a stable counting sort
@@ -1188,11 +1209,12 @@ static int sssp_partition(olv_graph *g) {
     OLV_TRY(ws.sssp_lr.ensure((size_t)g->V * 8 + 16));
     OLV_TRY(ws.sssp_hr.ensure((size_t)g->V * 8 + 16));
     OLV_TRY(ws.hdin.ensure((size_t)g->V * 8 + 16));
-    OLV_TRY(ws.tmp.ensure(16));
-    OLV_CUDA(cudaMemsetAsync(ws.tmp.p, 0, 8, g->stream));
+    DevBuf nlight;   // light edge count
+    OLV_TRY(nlight.ensure(16));
+    OLV_CUDA(cudaMemsetAsync(nlight.p, 0, 8, g->stream));
     k_partition_rows<<<g->num_sms * 16, kBlock, 0, g->stream>>>(
         R.rowptr, R.col, R.w, g->V, delta, ws.sssp_cw.as<uint2>(), ws.rowmid.as<uint32_t>(),
-        ws.sssp_lr.as<uint2>(), ws.sssp_hr.as<uint2>(), ws.tmp.as<unsigned long long>());
+        ws.sssp_lr.as<uint2>(), ws.sssp_hr.as<uint2>(), nlight.as<unsigned long long>());
     k_heavy_in_degrees<<<g->num_sms * 8, kBlock, 0, g->stream>>>(
         R.rowptr, ws.rowmid.as<uint32_t>(), R.colptr, g->V, ws.hdin.as<uint2>());
     if (R.cw && R.rowidx) {   // in-edges as (source, weight) pairs, light ones first
@@ -1203,7 +1225,7 @@ static int sssp_partition(olv_graph *g) {
             ws.sssp_clr.as<uint2>(), nullptr, nullptr);
     }
     OLV_CUDA(cudaGetLastError());
-    OLV_CUDA(cudaMemcpyAsync(&ws.sssp_n_light, ws.tmp.p, 8, cudaMemcpyDeviceToHost, g->stream));
+    OLV_CUDA(cudaMemcpyAsync(&ws.sssp_n_light, nlight.p, 8, cudaMemcpyDeviceToHost, g->stream));
     OLV_CUDA(cudaStreamSynchronize(g->stream));
     ws.sssp_delta_built = delta;
     ws.sssp_part_relabel = relabel;
@@ -1277,6 +1299,7 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     x.nmark0 = op.nmark0;
     x.nmark1 = op.nmark1;
     op.lrng = x.lrng;
+    op.mark_check = g->tune.sssp_mark_check;
     void *a_aux[] = {&V, &ctl, &q0, &q1, &far0, &far1, &fm, &x};
     OLV_TRY(sink((const void *)k_sssp_aux, dim3(nb), dim3(kBlock), a_aux));
     uint32_t bl_cap = x.bl_cap;
@@ -1316,7 +1339,11 @@ int sssp_workspace(olv_graph *g) {
     return OLV_OK;
 }
 
-int run_sssp_device(olv_graph *g, uint32_t src, uint32_t *dist_dev) {
+// red (device, [2], zeroed; or null): reached out-edges and vertices, summed
+// by the final pass when the run is renumbered; *red_done says whether it was.
+int run_sssp_device(olv_graph *g, uint32_t src, uint32_t *dist_dev, unsigned long long *red,
+                    bool *red_done) {
+    *red_done = false;
     OLV_TRY(sssp_partition(g));
     if (g->tune.sssp_lpull && !g->ws.sssp_lcrw.p) {
         OLV_TRY(build_light_csc(g));
@@ -1336,8 +1363,10 @@ int run_sssp_device(olv_graph *g, uint32_t src, uint32_t *dist_dev) {
     OLV_CUDA(cudaGetLastError());
     auto finish = [&]() -> int {
         if (R.dist) {
-            k_sssp_unrelabel<<<g->num_sms * 8, kBlock, 0, s>>>(R.dist, R.newid, g->V, dist_dev);
+            k_sssp_unrelabel<<<g->num_sms * 8, kBlock, 0, s>>>(R.dist, R.newid, g->V, dist_dev,
+                                                              g->rowptr.as<uint32_t>(), red);
             OLV_CUDA(cudaGetLastError());
+            *red_done = red != nullptr;
         }
         return OLV_OK;
     };
@@ -1374,17 +1403,23 @@ extern "C" int olv_sssp(olv_graph *g, uint32_t src, uint32_t *dist_out, olv_stat
     if (!dev_out) OLV_TRY(g->ws.level.ensure((size_t)g->V * 4 + 16));
     uint32_t *dist = dev_out ? dist_out : g->ws.level.as<uint32_t>();
     cudaStream_t s = g->stream;
+    unsigned long long *red_dev = nullptr;
+    if (st) {
+        OLV_TRY(g->ws.tmp.ensure(16));
+        OLV_CUDA(cudaMemsetAsync(g->ws.tmp.p, 0, 16, s));
+        red_dev = g->ws.tmp.as<unsigned long long>();
+    }
+    bool red_done = false;
     OLV_CUDA(cudaEventRecord(g->ev0, s));
-    OLV_TRY(run_sssp_device(g, src, dist));
+    OLV_TRY(run_sssp_device(g, src, dist, red_dev, &red_done));
     OLV_CUDA(cudaEventRecord(g->ev1, s));
     OLV_CUDA(cudaMemcpyAsync(g->host_ctl, g->ws.ctl.p, sizeof(TravCtl), cudaMemcpyDeviceToHost, s));
     unsigned long long red[2] = {0, 0};
     if (st) {
-        OLV_TRY(g->ws.tmp.ensure(16));
-        OLV_CUDA(cudaMemsetAsync(g->ws.tmp.p, 0, 16, s));
-        k_reached_edges<<<g->num_sms * 4, kBlock, 0, s>>>(g->rowptr.as<uint32_t>(), dist, g->V,
-                                                         g->ws.tmp.as<unsigned long long>());
-        OLV_CUDA(cudaMemcpyAsync(red, g->ws.tmp.p, 16, cudaMemcpyDeviceToHost, s));
+        if (!red_done)
+            k_reached_edges<<<g->num_sms * 4, kBlock, 0, s>>>(g->rowptr.as<uint32_t>(), dist, g->V,
+                                                             red_dev);
+        OLV_CUDA(cudaMemcpyAsync(red, red_dev, 16, cudaMemcpyDeviceToHost, s));
     }
     if (!dev_out)
         OLV_CUDA(cudaMemcpyAsync(dist_out, dist, (size_t)g->V * 4, cudaMemcpyDeviceToHost, s));
