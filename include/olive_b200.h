@@ -112,7 +112,8 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
  *                 supersteps (smaller pieces even out the CTAs' work) (256)
  *   "alpha"       BFS push->pull when m_f * alpha > m_unvisited     (14)
  *   "beta"        BFS pull->push when n_f * beta < V                (24)
- *   "sssp_delta"  SSSP bucket width, 0 = default                    (0)
+ *   "sssp_delta"  SSSP width of the first bucket (and of every bucket when
+ *                 sssp_tail_delta <= it), 0 = default, 24                (0)
  *   "sssp_pull"   SSSP: a settled bucket's heavy edges may be relaxed by
  *                 a pull over the in-edges of the unsettled vertices when
  *                 that reads fewer edges (1) or always by push (0)       (1)
@@ -127,8 +128,6 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
  *   "sssp_spt"    queued sources per thread in a relax chunk: 1, 2, 4 or 8 (1)
  *   "sssp_fuse_end"  SSSP superstep's end step run by the last CTA of the
  *                 relax pieces kernel instead of a launch of its own (0)
- *   "sssp_mark_check"  SSSP: read a queue-mark word before setting its bit
- *                 with an atomic (1)
  *   "sssp_lpull"  SSSP: a relax superstep whose near queue carries at least
  *                 1/sssp_lpull of the light edges runs as a pull over every
  *                 vertex's light in-edges (0: always push)
@@ -148,8 +147,8 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
 int olv_tune_set(olv_graph *g, const char *key, double value);
 int olv_tune_get(const olv_graph *g, const char *key, double *value);
 /* Autotuner: coordinate descent over hub_degree, alpha, beta (BFS), on
- * uint32-weighted graphs sssp_delta, sssp_hub_degree, sssp_piece and sssp_sub
- * (SSSP), pr_tile_u (PageRank, 10 iterations) and ms_alpha (msBFS from 16
+ * uint32-weighted graphs sssp_delta, sssp_tail_delta, sssp_hub_degree,
+ * sssp_piece and sssp_sub (SSSP), pr_tile_u (PageRank, 10 iterations) and ms_alpha (msBFS from 16
  * sources), each candidate timed `reps` times (BFS / SSSP from the highest
  * out-degree vertex); the fastest values are
  * applied to the handle and, if json_path is not NULL, written to a JSON table

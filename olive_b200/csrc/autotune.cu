@@ -90,7 +90,8 @@ extern "C" int olv_autotune(olv_graph *g, const char *json_path, int reps) {
         {"beta", {6, 24, 100}, run_bfs, out.p},
     };
     if (g->weight_type == OLV_W_U32) {
-        plan.push_back({"sssp_delta", {16, 32, 64, 128, 256, 512, 1024}, run_sssp, out.p});
+        plan.push_back({"sssp_delta", {8, 16, 24, 32, 64, 128, 256}, run_sssp, out.p});
+        plan.push_back({"sssp_tail_delta", {0, 256, 1024, 4096}, run_sssp, out.p});
         plan.push_back({"sssp_hub_degree", {128, 256, 1024}, run_sssp, out.p});
         plan.push_back({"sssp_piece", {256, 1024}, run_sssp, out.p});
         plan.push_back({"sssp_sub", {0, 8, 16}, run_sssp, out.p});
@@ -152,9 +153,9 @@ extern "C" int olv_autotune_load(olv_graph *g, const char *json_path, int *appli
     fclose(f);
     const std::string want = "\"key\": \"" + tune_key(g) + "\"";
     if (text.find(want) == std::string::npos) return OLV_OK;   // table is for another graph/GPU
-    const char *keys[] = {"hub_degree",      "piece",    "alpha",      "beta",
+    const char *keys[] = {"hub_degree",      "piece",      "alpha",           "beta",
                           "sssp_delta",      "sssp_piece", "sssp_hub_degree", "sssp_sub",
-                          "ms_alpha",        "pr_tile_u"};
+                          "sssp_tail_delta", "ms_alpha",   "pr_tile_u"};
     for (const char *k : keys) {
         const std::string pat = std::string("\"") + k + "\":";
         size_t pos = text.find(pat);

@@ -535,8 +535,6 @@ int olv_tune_set(olv_graph *g, const char *key, double value) {
     } else if (!strcmp(key, "sssp_tail_delta")) {
         OLV_CHECK_ARG(value >= 0 && value < 2147483647.0, "olv_tune_set: bad sssp_tail_delta");
         t.sssp_tail_delta = (uint32_t)value;
-    } else if (!strcmp(key, "sssp_mark_check")) {
-        t.sssp_mark_check = value != 0;
     } else if (!strcmp(key, "sssp_lpull")) {
         OLV_CHECK_ARG(value >= 0 && value <= 1e6, "olv_tune_set: bad sssp_lpull");
         t.sssp_lpull = (uint32_t)value;
@@ -590,7 +588,6 @@ int olv_tune_get(const olv_graph *g, const char *key, double *value) {
     else if (!strcmp(key, "sssp_fuse_end")) *value = t.sssp_fuse_end;
     else if (!strcmp(key, "sssp_tail_delta")) *value = t.sssp_tail_delta;
     else if (!strcmp(key, "sssp_lpull")) *value = t.sssp_lpull;
-    else if (!strcmp(key, "sssp_mark_check")) *value = t.sssp_mark_check;
     else if (!strcmp(key, "sssp_hub_degree")) *value = t.sssp_hub_degree;
     else if (!strcmp(key, "sssp_piece")) *value = t.sssp_piece;
     else if (!strcmp(key, "ms_alpha")) *value = t.ms_alpha;

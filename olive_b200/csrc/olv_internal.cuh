@@ -68,7 +68,6 @@ struct Tuning {
     int sssp_fuse_end = 0;            // SSSP: superstep end step in the pieces kernel's last CTA
     uint32_t sssp_tail_delta = 1024;  // SSSP: width of the buckets after the first, which
                                       // relax every edge (<= delta: delta, light/heavy)
-    int sssp_mark_check = 1;          // SSSP: read a queue-mark word before its atomicOr
     uint32_t sssp_lpull = 0;          // SSSP: a relax superstep pulls over light in-edges when
                                       // its sources' light out-edges * this >= light edges (0: never)
     float ms_alpha = 20.0f;       // msBFS: pull when active out-edges * ms_alpha > E

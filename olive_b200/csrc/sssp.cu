@@ -77,7 +77,11 @@ constexpr uint32_t kModePull = 4;
 constexpr uint32_t kModeSubSplit = 5;
 constexpr uint32_t kModeRelaxAll = 6;   // relax every edge (buckets after the first, when wide)
 constexpr uint32_t kModePullLight = 7;  // a relax superstep run as a pull over light in-edges
-constexpr uint32_t kDefaultDelta = 64;
+// Default width of the first bucket.  With wide buckets after the first
+// (sssp_tail_delta), a narrow first bucket is best on RMAT-24 from the hub
+// (24: 1.90 ms; 16: 1.97; 32: 2.02; 48: 2.33; 64: 2.64): fewer light edges
+// relaxed again inside it, the rest left to the pull and the wide buckets.
+constexpr uint32_t kDefaultDelta = 24;
 
 // Arrays the collect and pull passes read besides the queues.
 struct SsspAux {
@@ -178,7 +182,6 @@ struct SsspOp {
     const uint2 *lrng;
     unsigned long long mnext;
     unsigned long long *mnext_ctr;
-    int mark_check;   // read a mark word before setting its bit (see apply_n)
     // end of the superstep run by the last CTA of the pieces kernel (instead
     // of a k_sssp_end launch) when end_fused is set
     cudaGraphConditionalHandle end_h;
@@ -228,24 +231,18 @@ struct SsspOp {
             cand[j] = act[j] && p[j].nd < p[j].cur;
             if (cand[j]) atomicMin(&dist[v[j]], p[j].nd);
         }
-        // With mark_check the mark words are read first and the atomicOr is
-        // issued only where the bit is still clear: the words of the most
-        // relaxed (renumbered: lowest) ids are otherwise hit by every lane
-        // that improves one of their 32 vertices, and the atomics serialise.
         uint32_t old[N];
 #pragma unroll
         for (int j = 0; j < N; j++) {
             old[j] = 0;
-            if (cand[j] && mark_check)
-                old[j] = __ldcg(&(p[j].nd < threshold ? nbits : fbits)[v[j] >> 5]);
-        }
-#pragma unroll
-        for (int j = 0; j < N; j++) {
             if (cand[j]) {
                 const uint32_t bit = 1u << (v[j] & 31);
-                if (p[j].nd >= threshold) fmin = p[j].nd < fmin ? p[j].nd : fmin;
-                if (!(old[j] & bit))
-                    old[j] = atomicOr(&(p[j].nd < threshold ? nbits : fbits)[v[j] >> 5], bit);
+                if (p[j].nd < threshold) {
+                    old[j] = atomicOr(&nbits[v[j] >> 5], bit);
+                } else {
+                    fmin = p[j].nd < fmin ? p[j].nd : fmin;
+                    old[j] = atomicOr(&fbits[v[j] >> 5], bit);
+                }
             }
         }
 #pragma unroll
@@ -1299,7 +1296,6 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     x.nmark0 = op.nmark0;
     x.nmark1 = op.nmark1;
     op.lrng = x.lrng;
-    op.mark_check = g->tune.sssp_mark_check;
     void *a_aux[] = {&V, &ctl, &q0, &q1, &far0, &far1, &fm, &x};
     OLV_TRY(sink((const void *)k_sssp_aux, dim3(nb), dim3(kBlock), a_aux));
     uint32_t bl_cap = x.bl_cap;

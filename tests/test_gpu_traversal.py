@@ -250,8 +250,8 @@ def test_sssp_light_pull_vs_dijkstra(ob, lpull, tail):
         deg = np.diff(rp.astype(np.int64))
         ref_hub = oracle.dijkstra(rp, cl, w, hub)[0]
         np.testing.assert_array_equal(g.sssp(hub), ref_hub)
-        if lpull >= 3:
-            assert g.last_stats.pull_steps >= 2   # the heavy-edge pull and a light pull
+        if lpull == 1000:
+            assert g.last_stats.pull_steps >= 2   # the heavy-edge pull and light pulls
         s = int(np.flatnonzero(deg == 1)[0])
         np.testing.assert_array_equal(g.sssp(s), oracle.dijkstra(rp, cl, w, s)[0])
         for kw in ({"sssp_relabel": 0}, {"use_graphs": 0}, {"sssp_pull": 0}, {"sssp_spt": 4}):
@@ -492,7 +492,8 @@ def test_autotune_keeps_results_and_roundtrips(ob, tmp_path):
         assert best["hub_degree"] in (256, 1024, 4096)
         assert best["sssp_hub_degree"] in (128, 256, 1024) and best["sssp_piece"] in (256, 1024)
         assert best["pr_tile_u"] in (4, 8, 16) and best["ms_alpha"] in (5, 10, 20, 40)
-        assert best["sssp_sub"] in (0, 8, 16)
+        assert best["sssp_sub"] in (0, 8, 16) and best["sssp_tail_delta"] in (0, 256, 1024, 4096)
+        assert best["sssp_delta"] in (8, 16, 24, 32, 64, 128, 256)
         np.testing.assert_array_equal(g.bfs(hub), oracle.bfs(rp, cl, hub)[0])
         np.testing.assert_array_equal(g.sssp(hub), oracle.dijkstra(rp, cl, w, hub)[0])
         txt = open(path).read()
@@ -502,7 +503,7 @@ def test_autotune_keeps_results_and_roundtrips(ob, tmp_path):
         assert np.max(np.abs(r - ref) / ref) < 1e-6
     with ob.Graph.rmat(14, 16, 3, weights=True, wseed=4) as g2:
         g2.tune(hub_degree=4096, sssp_delta=16, sssp_hub_degree=4096, sssp_piece=4096,
-                pr_tile_u=32, ms_alpha=7)
+                sssp_tail_delta=7, pr_tile_u=32, ms_alpha=7)
         assert g2.autotune_load(path)
         assert g2.tune() == best
     with ob.Graph.rmat(13, 16, 3) as g3:       # another graph: table not applied
