@@ -49,8 +49,6 @@ struct TravCtl {
     uint32_t heavy_index;       // SSSP: heavy buckets started so far (0 = the first)
     uint32_t tail_width;        // SSSP: width of the buckets after the first (<= delta: delta)
     uint32_t all_edges;         // SSSP: the current bucket relaxes every edge in-bucket
-    uint32_t lpull_div;         // SSSP: light pull when m_next * lpull_div >= n_light (0: never)
-    unsigned long long n_light; // SSSP: light edges of the graph
     unsigned long long heavy_work;  // SSSP: heavy out-edges of the collected bucket
     unsigned long long settled_in;  // SSSP: in-edges of all settled vertices
     uint32_t ms_track;          // msBFS: this push level records first-touched vertices
@@ -61,7 +59,6 @@ struct TravCtl {
     void *vdata;                // per-vertex result array of the run (level / dist)
     unsigned long long m_f;         // out-edges of the input frontier
     unsigned long long m_next;      // out-edges of vertices discovered this superstep
-                                    // (SSSP: light out-edges of the next near queue)
     unsigned long long m_unvisited; // out-edges of vertices not yet reached
     unsigned long long edges_traversed;
     unsigned long long edges_relaxed;

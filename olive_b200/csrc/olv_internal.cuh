@@ -65,11 +65,11 @@ struct Tuning {
     uint32_t sssp_sub = 0;            // SSSP: light-phase sub-bucket width (0: none)
     uint32_t sssp_sub_buckets = 1;    // SSSP: heavy buckets whose light phase uses it
     uint32_t sssp_spt = 1;            // SSSP: queued sources per thread in a relax chunk
+    int sssp_owner = 0;               // SSSP: relax chunks find an edge's source in an owner
+                                      // table (1) or by binary search (0)
     int sssp_fuse_end = 0;            // SSSP: superstep end step in the pieces kernel's last CTA
     uint32_t sssp_tail_delta = 1024;  // SSSP: width of the buckets after the first, which
                                       // relax every edge (<= delta: delta, light/heavy)
-    uint32_t sssp_lpull = 0;          // SSSP: a relax superstep pulls over light in-edges when
-                                      // its sources' light out-edges * this >= light edges (0: never)
     float ms_alpha = 20.0f;       // msBFS: pull when active out-edges * ms_alpha > E
     uint32_t pr_tile_u = 8;       // PageRank / weighted PR: entries per lane the row
                                   // grouping aims at (lanes per row by row length)
@@ -85,16 +85,8 @@ struct Workspace {
     DevBuf pull_idx;                // BFS pull: in-edges sorted by source out-degree (desc)
     // SSSP: rows split light (w <= delta) | heavy, as (column, weight) pairs;
     // rowmid[u] the split point; per vertex its light and heavy ranges as
-    // uint2 (one load each); the in-edges as (source, weight) pairs, each
-    // vertex's light in-edges first (sssp_clr: their range), and the number
-    // of light edges
-    DevBuf sssp_cw, rowmid, sssp_lr, sssp_hr, sssp_crw, sssp_clr;
-    unsigned long long sssp_n_light = 0;
-    // SSSP light pull: the light in-edges as a compact CSC over the vertices
-    // that have some (lv: their ids, lcp: offsets, lcrw: (source, weight)),
-    // and the first vertex of every tile of kLTile light in-edges
-    DevBuf sssp_lv, sssp_lcp, sssp_lcrw, sssp_ltile;
-    uint32_t sssp_lm = 0, sssp_ntiles = 0;
+    // uint2 (one load each); the in-edges as (source, weight) pairs
+    DevBuf sssp_cw, rowmid, sssp_lr, sssp_hr, sssp_crw;
     DevBuf blist;                   // SSSP: inputs of the current bucket's relax supersteps
     DevBuf hdin;                    // SSSP: per vertex (heavy out-degree, in-degree)
     // SSSP: vertices renumbered by in-degree (descending): new -> old and
@@ -111,8 +103,7 @@ struct Workspace {
         fbits.release(); order.release(); cand.release(); cand2.release(); pull_idx.release();
         pull_first.release();
         sssp_cw.release(); rowmid.release(); sssp_lr.release(); sssp_hr.release();
-        sssp_crw.release(); sssp_clr.release(); blist.release(); hdin.release();
-        sssp_lv.release(); sssp_lcp.release(); sssp_lcrw.release(); sssp_ltile.release();
+        sssp_crw.release(); blist.release(); hdin.release();
         sssp_delta_built = 0;
         sr_perm.release(); sr_newid.release(); sr_rowptr.release(); sr_col.release();
         sr_w.release(); sr_colptr.release(); sr_rowidx.release(); sr_cw.release();

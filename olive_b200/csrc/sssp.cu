@@ -56,8 +56,6 @@
 // fewer supersteps (37 -> 9 at width 256).  An improvement at or above the
 // bucket's end still goes to the far pile, so the split and the result are
 // those of delta-stepping with the wider bucket.
-#include <cub/cub.cuh>
-
 #include <algorithm>
 #include <vector>
 
@@ -76,7 +74,6 @@ constexpr uint32_t kModeHeavy = 3;
 constexpr uint32_t kModePull = 4;
 constexpr uint32_t kModeSubSplit = 5;
 constexpr uint32_t kModeRelaxAll = 6;   // relax every edge (buckets after the first, when wide)
-constexpr uint32_t kModePullLight = 7;  // a relax superstep run as a pull over light in-edges
 // Default width of the first bucket.  With wide buckets after the first
 // (sssp_tail_delta), a narrow first bucket is best on RMAT-24 from the hub
 // (24: 1.90 ms; 16: 1.97; 32: 2.02; 48: 2.33; 64: 2.64): fewer light edges
@@ -94,16 +91,7 @@ struct SsspAux {
     uint32_t bl_cap;                   // bucket list capacity (entries)
     unsigned long long E;
     int pull;                          // pull supersteps allowed
-    const uint2 *lrng;                 // per vertex: its light out-edges (null: m_next not kept)
-    uint32_t *nmark0, *nmark1;         // near-queue marks (as SsspOp's)
-    // light pull: compact CSC of the light in-edges (see Workspace)
-    const uint32_t *lv, *lcp, *ltile;
-    const uint2 *lcrw;
-    uint32_t ntiles;
-    unsigned long long n_light;
 };
-
-constexpr uint32_t kLTile = 1024;      // light in-edges per light-pull tile
 
 // Stable partition of every row into light (w <= delta) then heavy edges,
 // written as (column, weight) pairs; one warp per row, two passes (count,
@@ -113,8 +101,7 @@ __global__ void k_partition_rows(const uint32_t *__restrict__ rowptr,
                                  const uint32_t *__restrict__ col, const uint32_t *__restrict__ w,
                                  uint32_t V, uint32_t delta, uint2 *__restrict__ pcw,
                                  uint32_t *__restrict__ rowmid, uint2 *__restrict__ lr,
-                                 uint2 *__restrict__ hr, unsigned long long *nlight) {
-    unsigned long long cnt = 0;
+                                 uint2 *__restrict__ hr) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -142,13 +129,19 @@ __global__ void k_partition_rows(const uint32_t *__restrict__ rowptr,
             hi += __popc(mh);
         }
         if (lane == 0) {
-            if (rowmid) rowmid[u] = b + nl;
+            rowmid[u] = b + nl;
             lr[u] = make_uint2(b, b + nl);
-            if (hr) hr[u] = make_uint2(b + nl, e);
-            cnt += nl;
+            hr[u] = make_uint2(b + nl, e);
         }
     }
-    if (nlight && lane == 0 && cnt) atomicAdd(nlight, cnt);
+}
+
+// In-edges as (source, weight) pairs for the pull superstep.
+__global__ void k_pack_pairs(const uint32_t *__restrict__ a, const uint32_t *__restrict__ b,
+                             unsigned long long n, uint2 *__restrict__ out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = make_uint2(a[i], b[i]);
 }
 
 #ifndef OLV_SSSP_MINB
@@ -177,11 +170,6 @@ struct SsspOp {
     uint32_t threshold, fmin;
     unsigned long long *relaxed_ctr;
     uint32_t *far_min;
-    // light out-degree sum of the vertices pushed to the next near queue
-    // (lrng null: not kept), for the next superstep's push / pull choice
-    const uint2 *lrng;
-    unsigned long long mnext;
-    unsigned long long *mnext_ctr;
     // end of the superstep run by the last CTA of the pieces kernel (instead
     // of a k_sssp_end launch) when end_fused is set
     cudaGraphConditionalHandle end_h;
@@ -202,8 +190,6 @@ struct SsspOp {
         relaxed_ctr = &c->edges_relaxed;
         far_min = &c->far_min;
         fmin = 0xffffffffu;
-        mnext = 0;
-        mnext_ctr = &c->m_next;
     }
     struct Pre {
         uint32_t nd, cur;
@@ -263,17 +249,11 @@ struct SsspOp {
         atomicAnd(&nprev[u >> 5], ~bit);
         return !(__ldcg(&nbits[u >> 5]) & bit);
     }
-    __device__ __forceinline__ void on_push(bool pushed, uint32_t v) {
-        if (lrng && pushed) {
-            const uint2 r = __ldg(&lrng[v]);
-            mnext += r.y - r.x;
-        }
-    }
+    __device__ __forceinline__ void on_push(bool, uint32_t) {}
     __device__ __forceinline__ void flush(unsigned long long relaxed) {
         warp_add64(relaxed, relaxed_ctr);
         const uint32_t m = __reduce_min_sync(0xffffffffu, fmin);
         if (lane_id() == 0 && m != 0xffffffffu) atomicMin(far_min, m);
-        if (lrng) warp_add64(mnext, mnext_ctr);
     }
 };
 
@@ -281,8 +261,7 @@ __device__ void sssp_begin(TravCtl *c);
 
 __global__ void k_sssp_init(TravCtl *c, uint32_t *dist, uint32_t *q0, uint32_t src,
                             uint32_t delta, uint32_t sub, uint32_t sub_buckets,
-                            uint32_t tail_width, uint32_t lpull_div, unsigned long long n_light,
-                            const uint32_t *newid) {
+                            uint32_t tail_width, const uint32_t *newid) {
     if (newid) src = newid[src];   // relabelled run: the source's new id
     TravCtl t = {};
     t.qsize[0] = 1;
@@ -294,8 +273,6 @@ __global__ void k_sssp_init(TravCtl *c, uint32_t *dist, uint32_t *q0, uint32_t s
     t.heavy_index = 0;
     t.tail_width = tail_width > delta ? tail_width : 0;
     t.all_edges = 0;
-    t.lpull_div = lpull_div;
-    t.n_light = n_light;
     t.threshold = (t.sub_width && sub_buckets > 0) ? t.sub_width : delta;
     t.epoch = 1;
     t.far_min = 0xffffffffu;
@@ -326,13 +303,8 @@ static __device__ __forceinline__ uint32_t sat_add(uint32_t a, uint32_t b) {
 //   split      start the next heavy bucket at max(threshold, far minimum).
 __device__ void sssp_begin(TravCtl *c) {
     if (c->done) return;
-    const unsigned long long mf = c->m_next;   // light out-edges of the near queue
-    c->m_next = 0;
     if (c->qsize[c->cur] > 0) {
-        // a large near queue relaxes its light edges by a pull over every
-        // vertex's light in-edges instead (no atomics, streamed in-edges)
-        const bool pull = c->lpull_div && c->n_light && mf * c->lpull_div >= c->n_light;
-        c->mode = c->all_edges ? kModeRelaxAll : pull ? kModePullLight : kModeRelax;
+        c->mode = c->all_edges ? kModeRelaxAll : kModeRelax;
         c->qsize[c->cur ^ 1] = 0;
         c->npieces = 0;
         return;
@@ -528,19 +500,14 @@ __device__ __forceinline__ uint32_t pull_cand(uint32_t du, uint32_t w, uint32_t 
 // the scan), and fold candidates into a shared per-vertex minimum.
 constexpr int kPullItems = 4;
 constexpr uint32_t kPullChunk = 4 * kBlock;
-// Shared memory of the pull passes (one copy in the aux kernel).
-struct PullSmem {
-    uint32_t off[kPullChunk + 2], beg[kPullChunk], best[kPullChunk + 1], warp[33];
-};
-static_assert(kLTile + 2 <= kPullChunk + 2, "a light tile's offsets fit PullSmem::off");
 __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1, FarMarks fm,
-                          const SsspAux &x, WarpStage sf, PullSmem &sm) {
+                          const SsspAux &x, WarpStage sf) {
     uint32_t *dist = static_cast<uint32_t *>(c->vdata);
     const uint32_t hi = c->threshold;
     uint32_t *far = c->far_cur ? far1 : far0;
     uint32_t *far_size = &c->far_size[c->far_cur];
     uint32_t *fbits = (c->epoch & 1) ? fm.m1 : fm.m0;
-    uint32_t *s_off = sm.off, *s_beg = sm.beg, *s_best = sm.best, *s_warp = sm.warp;
+    __shared__ uint32_t s_off[kPullChunk + 1], s_beg[kPullChunk], s_best[kPullChunk], s_warp[33];
     const bool vec = ((uintptr_t)dist & 15) == 0 && ((uintptr_t)x.colptr & 15) == 0;
     const uint32_t lane = lane_id();
     uint32_t fmin = 0xffffffffu;
@@ -653,9 +620,7 @@ __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1
 // dropped, entries under the new threshold become the near queue, the rest
 // move to the other far buffer under the next generation.
 __device__ void sssp_split(TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0,
-                           uint32_t *far1, FarMarks fm, const uint2 *lrng, WarpStage sn,
-                           WarpStage sf) {
-    unsigned long long mnext = 0;   // light out-edges of the near queue (lrng set)
+                           uint32_t *far1, FarMarks fm, WarpStage sn, WarpStage sf) {
     const uint32_t *dist = static_cast<const uint32_t *>(c->vdata);
     const uint32_t fc = c->far_cur;
     const uint32_t n = c->far_size[fc];
@@ -681,10 +646,6 @@ __device__ void sssp_split(TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far
             if (d >= lo) {
                 if (d < hi) {
                     act[0] = 1;
-                    if (lrng) {
-                        const uint2 r = __ldg(&lrng[v[0]]);
-                        mnext += r.y - r.x;
-                    }
                 } else {
                     act[0] = 2;
                     atomicOr(&fnext[v[0] >> 5], bit);
@@ -701,125 +662,6 @@ __device__ void sssp_split(TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far
     warp_stage_flush(sf.buf, sf.n, sf.lim, fout, fout_size);
     const uint32_t m = __reduce_min_sync(0xffffffffu, fmin);
     if (lane_id() == 0 && m != 0xffffffffu) atomicMin(&c->far_min, m);
-    if (lrng) warp_add64(mnext, &c->m_next);
-}
-
-// Light pull superstep: the relax superstep of a large near queue, run as a
-// pull.  Every light edge (u, v) whose source is under the threshold offers
-// dist[u] + w to v -- a superset of the relaxations the push would make from
-// the queue (relaxing from any vertex with a valid distance is safe) -- with
-// the light in-edges streamed from a compact CSC in tiles of kLTile edges
-// (balanced whatever the in-degrees: the renumbered hubs' rows span many
-// tiles).  A tile folds its edges into a per-vertex minimum in shared memory;
-// a vertex not settled in an earlier bucket (dist >= bucket_lo) whose minimum
-// beats its distance takes it by atomicMin (a vertex can span tiles), and
-// the tile that lowered it queues it for the next superstep (under the
-// threshold, once through the near mark, as a push would) or puts it on the
-// far pile (once per pile generation).  The marks the previous superstep set
-// for its queue (this superstep's input) are cleared, as its push would have
-// cleared them.
-__device__ void sssp_pull_light(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1,
-                                uint32_t *far0, uint32_t *far1, FarMarks fm, const SsspAux &x,
-                                WarpStage sn, WarpStage sf, PullSmem &sm) {
-    uint32_t *dist = static_cast<uint32_t *>(c->vdata);
-    const uint32_t lo = c->bucket_lo, hi = c->threshold;
-    const uint32_t cur = c->cur;
-    const uint32_t *qin = cur ? q1 : q0;
-    uint32_t *qout = cur ? q0 : q1;
-    uint32_t *qout_size = &c->qsize[cur ^ 1];
-    uint32_t *far = c->far_cur ? far1 : far0;
-    uint32_t *far_size = &c->far_size[c->far_cur];
-    uint32_t *fbits = (c->epoch & 1) ? fm.m1 : fm.m0;
-    const uint32_t stamp = c->steps + 1;
-    uint32_t *nbits = (stamp & 1) ? x.nmark1 : x.nmark0;
-    uint32_t *nprev = (stamp & 1) ? x.nmark0 : x.nmark1;
-    const uint32_t nin = c->qsize[cur];
-    for (uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x; i < nin;
-         i += (uint64_t)gridDim.x * kBlock) {
-        const uint32_t u = qin[i];
-        atomicAnd(&nprev[u >> 5], ~(1u << (u & 31)));
-    }
-    uint32_t *s_lcp = sm.off, *s_best = sm.best;
-    const uint32_t lane = lane_id();
-    uint32_t fmin = 0xffffffffu;
-    unsigned long long scanned = 0, mnext = 0;
-    constexpr int kLItems = kLTile / kBlock;
-    for (uint32_t t = blockIdx.x; t < x.ntiles; t += gridDim.x) {
-        const uint64_t t0 = (uint64_t)t * kLTile;
-        const uint64_t t1 = t0 + kLTile < x.n_light ? t0 + kLTile : x.n_light;
-        const uint32_t k0 = x.ltile[t];
-        const uint32_t nv = x.ltile[t + 1] - k0 + 1;   // vertices the tile can touch (<= kLTile + 1)
-        for (uint32_t i = threadIdx.x; i <= nv; i += kBlock) s_lcp[i] = x.lcp[k0 + i];
-        for (uint32_t i = threadIdx.x; i < nv; i += kBlock) s_best[i] = 0xffffffffu;
-        __syncthreads();
-        uint32_t own[kLItems], u[kLItems], w[kLItems], du[kLItems];
-#pragma unroll
-        for (int j = 0; j < kLItems; j++) {
-            const uint64_t e = t0 + (uint64_t)j * kBlock + threadIdx.x;
-            own[j] = nv;
-            u[j] = 0;
-            w[j] = 0;
-            if (e < t1) {
-                const uint32_t el = (uint32_t)(e - s_lcp[0]);   // offsets relative to the tile's first vertex
-                uint32_t l = 0;   // last vertex with s_lcp[l] <= e
-#pragma unroll
-                for (uint32_t step = kLTile; step > 0; step >>= 1)
-                    if (l + step < nv && s_lcp[l + step] - s_lcp[0] <= el) l += step;
-                own[j] = l;
-                const uint2 p = __ldcs(&x.lcrw[e]);
-                u[j] = p.x;
-                w[j] = p.y;
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < kLItems; j++) du[j] = own[j] < nv ? __ldcg(&dist[u[j]]) : 0xffffffffu;
-#pragma unroll
-        for (int j = 0; j < kLItems; j++) {
-            if (own[j] < nv) {
-                const uint32_t nd = pull_cand(du[j], w[j], hi);
-                if (nd < s_best[own[j]]) atomicMin(&s_best[own[j]], nd);
-            }
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) scanned += t1 - t0;
-        for (uint32_t i0 = 0; i0 < nv; i0 += kBlock) {   // every lane takes part in the pushes
-            const uint32_t i = i0 + threadIdx.x;
-            int act[1] = {0};
-            uint32_t va[1] = {0};
-            const uint32_t b = i < nv ? s_best[i] : 0xffffffffu;
-            if (b != 0xffffffffu) {
-                const uint32_t v = x.lv[k0 + i];
-                const uint32_t d = __ldcg(&dist[v]);
-                if (d >= lo && b < d && b < atomicMin(&dist[v], b)) {
-                    va[0] = v;
-                    const uint32_t bit = 1u << (v & 31);
-                    if (b < hi) {
-                        if (!(atomicOr(&nbits[v >> 5], bit) & bit)) {
-                            act[0] = 1;
-                            if (x.lrng) {
-                                const uint2 r = __ldg(&x.lrng[v]);
-                                mnext += r.y - r.x;
-                            }
-                        }
-                    } else {
-                        if (!(atomicOr(&fbits[v >> 5], bit) & bit)) act[0] = 2;
-                        fmin = b < fmin ? b : fmin;
-                    }
-                }
-            }
-            sn.reserve(32, qout, qout_size);
-            stage_push_n<1>(act, va, 1, sn.buf, sn.n, sn.lim, kWarpStage, qout, qout_size);
-            sf.reserve(32, far, far_size);
-            stage_push_n<1>(act, va, 2, sf.buf, sf.n, sf.lim, kWarpStage, far, far_size);
-        }
-        __syncthreads();   // s_lcp / s_best are rewritten by the next tile
-    }
-    warp_stage_flush(sn.buf, sn.n, sn.lim, qout, qout_size);
-    warp_stage_flush(sf.buf, sf.n, sf.lim, far, far_size);
-    const uint32_t m = __reduce_min_sync(0xffffffffu, fmin);
-    if (lane == 0 && m != 0xffffffffu) atomicMin(&c->far_min, m);
-    warp_add64(scanned, &c->edges_relaxed);
-    if (x.lrng) warp_add64(mnext, &c->m_next);
 }
 
 // End of a superstep (one thread): account for what it did, decide whether
@@ -828,10 +670,9 @@ __device__ void sssp_pull_light(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *
 __device__ void sssp_end_step(TravCtl *c, cudaGraphConditionalHandle h, int use_cond,
                               uint32_t max_steps, uint32_t bl_cap) {
     if (!c->done) {
-        if (c->mode == kModeRelax || c->mode == kModePullLight) {
+        if (c->mode == kModeRelax) {
             // the aux pass appended this superstep's input to the bucket list
             // under the same capacity test
-            if (c->mode == kModePullLight) c->pull_steps++;
             const uint32_t n = c->qsize[c->cur];
             if (!c->bl_over) {
                 if ((uint64_t)c->bl_size + n <= bl_cap)
@@ -848,7 +689,6 @@ __device__ void sssp_end_step(TravCtl *c, cudaGraphConditionalHandle h, int use_
         } else if (c->mode == kModePull) {
             c->pull_pending = 0;
             c->heavy_done = 1;
-            c->pull_steps++;
         } else if (c->mode == kModeSubSplit) {
             c->far_cur ^= 1;   // the bucket list and the pending heavy step carry over
             c->epoch++;
@@ -883,21 +723,18 @@ k_sssp_aux(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0, u
            FarMarks fm, SsspAux x) {
     if (c->done) return;
     const uint32_t mode = c->mode;
-    if (mode == kModeRelax || mode == kModePullLight) {
-        // append this superstep's input to the bucket list
+    if (mode == kModeRelax) {   // append this superstep's input to the bucket list
         const uint32_t n = c->qsize[c->cur];
-        if (!c->bl_over && (uint64_t)c->bl_size + n <= x.bl_cap) {   // else k_sssp_end: overflow
-            const uint32_t *qin = c->cur ? q1 : q0;
-            uint32_t *dst = x.blist + c->bl_size;
-            for (uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x; i < n;
-                 i += (uint64_t)gridDim.x * kBlock)
-                dst[i] = qin[i];
-        }
-        if (mode == kModeRelax) return;   // the push kernels relax the queue
-    } else if (mode != kModeHeavy && mode != kModeSplit && mode != kModePull &&
-               mode != kModeSubSplit) {
+        if (c->bl_over || (uint64_t)c->bl_size + n > x.bl_cap) return;   // k_sssp_end: overflow
+        const uint32_t *qin = c->cur ? q1 : q0;
+        uint32_t *dst = x.blist + c->bl_size;
+        for (uint64_t i = (uint64_t)blockIdx.x * kBlock + threadIdx.x; i < n;
+             i += (uint64_t)gridDim.x * kBlock)
+            dst[i] = qin[i];
         return;
     }
+    if (mode != kModeHeavy && mode != kModeSplit && mode != kModePull && mode != kModeSubSplit)
+        return;
     __shared__ uint32_t s_a[kBlock / 32][kWarpStage], s_b[kBlock / 32][kWarpStage];
     __shared__ uint32_t s_an[kBlock / 32], s_alim[kBlock / 32];
     __shared__ uint32_t s_bn[kBlock / 32], s_blim[kBlock / 32];
@@ -906,16 +743,13 @@ k_sssp_aux(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0, u
     WarpStage sb{s_b[wl], &s_bn[wl], &s_blim[wl]};
     sa.init();
     sb.init();
-    __shared__ PullSmem sm;   // the heavy and light pulls
     if (mode == kModeHeavy) {
         sssp_collect(V, c, q0, q1, x, sa);
         if (x.pull) sssp_choose(V, c, x);
     } else if (mode == kModePull) {
-        sssp_pull(V, c, far0, far1, fm, x, sb, sm);
-    } else if (mode == kModePullLight) {
-        sssp_pull_light(V, c, q0, q1, far0, far1, fm, x, sa, sb, sm);
+        sssp_pull(V, c, far0, far1, fm, x, sb);
     } else {
-        sssp_split(c, q0, q1, far0, far1, fm, x.lrng, sa, sb);
+        sssp_split(c, q0, q1, far0, far1, fm, sa, sb);
     }
 }
 
@@ -1085,110 +919,6 @@ static SsspCsr sssp_csr(olv_graph *g) {
 
 // Rows split light | heavy for the current delta (built once per delta and
 // numbering).
-// Light pull data (built on the first solve with sssp_lpull set, per
-// partition): the compact CSC of the light in-edges and its tile starts.
-__global__ void k_light_deg(const uint2 *__restrict__ clr, uint32_t V, uint32_t *__restrict__ flag,
-                            uint32_t *__restrict__ deg) {
-    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
-         v += (uint64_t)gridDim.x * blockDim.x) {
-        const uint2 r = clr[v];
-        deg[v] = r.y - r.x;
-        flag[v] = r.y > r.x;
-    }
-}
-
-__global__ void k_light_compact(const uint32_t *__restrict__ flag, const uint32_t *__restrict__ pos,
-                                const uint32_t *__restrict__ off, uint32_t V,
-                                uint32_t *__restrict__ lv, uint32_t *__restrict__ lcp) {
-    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
-         v += (uint64_t)gridDim.x * blockDim.x)
-        if (flag[v]) {
-            lv[pos[v]] = (uint32_t)v;
-            lcp[pos[v]] = off[v];
-        }
-}
-
-__global__ void k_light_copy(const uint2 *__restrict__ clr, const uint32_t *__restrict__ off,
-                             const uint2 *__restrict__ crw, uint32_t V, uint2 *__restrict__ lcrw) {
-    const uint32_t lane = threadIdx.x & 31;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t v = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; v < V; v += nwarps) {
-        const uint2 r = clr[v];
-        const uint32_t o = off[v];
-        for (uint32_t i = lane; i < r.y - r.x; i += 32) lcrw[o + i] = crw[r.x + i];
-    }
-}
-
-// ltile[t] = the compact vertex that holds light in-edge t * kLTile; ltile[ntiles] = m - 1.
-__global__ void k_light_tiles(const uint32_t *__restrict__ lcp, uint32_t m, uint32_t ntiles,
-                              uint32_t *__restrict__ ltile) {
-    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t <= ntiles;
-         t += (uint64_t)gridDim.x * blockDim.x) {
-        if (t == ntiles) {
-            ltile[t] = m - 1;
-            continue;
-        }
-        const uint64_t e = t * kLTile;
-        uint32_t lo = 0, hi = m;   // lcp[lo] <= e < lcp[hi] (lcp[0] = 0, lcp[m] = light edges)
-        while (hi - lo > 1) {
-            const uint32_t mid = lo + (hi - lo) / 2;
-            if (lcp[mid] <= e)
-                lo = mid;
-            else
-                hi = mid;
-        }
-        ltile[t] = lo;
-    }
-}
-
-static int build_light_csc(olv_graph *g) {
-    Workspace &ws = g->ws;
-    if (ws.sssp_lcrw.p || !ws.sssp_crw.p || !ws.sssp_clr.p || ws.sssp_n_light == 0) return OLV_OK;
-    const uint32_t V = g->V;
-    cudaStream_t s = g->stream;
-    DevBuf flag, pos, deg, off, temp;
-    OLV_TRY(flag.ensure((size_t)V * 4 + 16));
-    OLV_TRY(pos.ensure((size_t)V * 4 + 16));
-    OLV_TRY(deg.ensure((size_t)V * 4 + 16));
-    OLV_TRY(off.ensure((size_t)V * 4 + 16));
-    k_light_deg<<<g->num_sms * 8, kBlock, 0, s>>>(ws.sssp_clr.as<uint2>(), V, flag.as<uint32_t>(),
-                                                  deg.as<uint32_t>());
-    size_t tb = 0;
-    OLV_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag.as<uint32_t>(), pos.as<uint32_t>(),
-                                           (int64_t)V, s));
-    OLV_TRY(temp.ensure(tb + 16));
-    OLV_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, tb, flag.as<uint32_t>(), pos.as<uint32_t>(),
-                                           (int64_t)V, s));
-    OLV_CUDA(cub::DeviceScan::ExclusiveSum(temp.p, tb, deg.as<uint32_t>(), off.as<uint32_t>(),
-                                           (int64_t)V, s));
-    uint32_t last[2] = {0, 0};
-    OLV_CUDA(cudaMemcpyAsync(&last[0], pos.as<uint32_t>() + (V - 1), 4, cudaMemcpyDeviceToHost, s));
-    OLV_CUDA(cudaMemcpyAsync(&last[1], flag.as<uint32_t>() + (V - 1), 4, cudaMemcpyDeviceToHost, s));
-    OLV_CUDA(cudaStreamSynchronize(s));
-    const uint32_t m = last[0] + last[1];
-    const unsigned long long nl = ws.sssp_n_light;
-    const uint32_t ntiles = (uint32_t)((nl + kLTile - 1) / kLTile);
-    OLV_TRY(ws.sssp_lv.ensure((size_t)m * 4 + 16));
-    OLV_TRY(ws.sssp_lcp.ensure(((size_t)m + 1) * 4 + 16));
-    OLV_TRY(ws.sssp_lcrw.ensure(nl * 8 + 16));
-    OLV_TRY(ws.sssp_ltile.ensure(((size_t)ntiles + 1) * 4 + 16));
-    k_light_compact<<<g->num_sms * 8, kBlock, 0, s>>>(flag.as<uint32_t>(), pos.as<uint32_t>(),
-                                                      off.as<uint32_t>(), V, ws.sssp_lv.as<uint32_t>(),
-                                                      ws.sssp_lcp.as<uint32_t>());
-    const uint32_t nl32 = (uint32_t)nl;
-    OLV_CUDA(cudaMemcpyAsync(ws.sssp_lcp.as<uint32_t>() + m, &nl32, 4, cudaMemcpyHostToDevice, s));
-    k_light_copy<<<g->num_sms * 16, kBlock, 0, s>>>(ws.sssp_clr.as<uint2>(), off.as<uint32_t>(),
-                                                    ws.sssp_crw.as<uint2>(), V,
-                                                    ws.sssp_lcrw.as<uint2>());
-    k_light_tiles<<<g->num_sms * 4, kBlock, 0, s>>>(ws.sssp_lcp.as<uint32_t>(), m, ntiles,
-                                                    ws.sssp_ltile.as<uint32_t>());
-    OLV_CUDA(cudaGetLastError());
-    OLV_CUDA(cudaStreamSynchronize(s));   // the host value above and the scratch buffers
-    ws.sssp_lm = m;
-    ws.sssp_ntiles = ntiles;
-    return OLV_OK;
-}
-
 static int sssp_partition(olv_graph *g) {
     Workspace &ws = g->ws;
     const uint32_t delta = sssp_delta(g);
@@ -1197,33 +927,22 @@ static int sssp_partition(olv_graph *g) {
     if (ws.sssp_delta_built == delta && ws.sssp_part_relabel == relabel && ws.rowmid.p)
         return OLV_OK;
     const SsspCsr R = sssp_csr(g);
-    ws.sssp_lv.release();   // the light pull's CSC follows the partition
-    ws.sssp_lcp.release();
-    ws.sssp_lcrw.release();
-    ws.sssp_ltile.release();
     OLV_TRY(ws.sssp_cw.ensure(g->E * 8 + 16));
     OLV_TRY(ws.rowmid.ensure((size_t)g->V * 4 + 16));
     OLV_TRY(ws.sssp_lr.ensure((size_t)g->V * 8 + 16));
     OLV_TRY(ws.sssp_hr.ensure((size_t)g->V * 8 + 16));
     OLV_TRY(ws.hdin.ensure((size_t)g->V * 8 + 16));
-    DevBuf nlight;   // light edge count
-    OLV_TRY(nlight.ensure(16));
-    OLV_CUDA(cudaMemsetAsync(nlight.p, 0, 8, g->stream));
     k_partition_rows<<<g->num_sms * 16, kBlock, 0, g->stream>>>(
         R.rowptr, R.col, R.w, g->V, delta, ws.sssp_cw.as<uint2>(), ws.rowmid.as<uint32_t>(),
-        ws.sssp_lr.as<uint2>(), ws.sssp_hr.as<uint2>(), nlight.as<unsigned long long>());
+        ws.sssp_lr.as<uint2>(), ws.sssp_hr.as<uint2>());
     k_heavy_in_degrees<<<g->num_sms * 8, kBlock, 0, g->stream>>>(
         R.rowptr, ws.rowmid.as<uint32_t>(), R.colptr, g->V, ws.hdin.as<uint2>());
-    if (R.cw && R.rowidx) {   // in-edges as (source, weight) pairs, light ones first
+    if (R.cw && R.rowidx) {   // in-edges as (source, weight) pairs for the pull
         OLV_TRY(ws.sssp_crw.ensure(g->E * 8 + 16));
-        OLV_TRY(ws.sssp_clr.ensure((size_t)g->V * 8 + 16));
-        k_partition_rows<<<g->num_sms * 16, kBlock, 0, g->stream>>>(
-            R.colptr, R.rowidx, R.cw, g->V, delta, ws.sssp_crw.as<uint2>(), nullptr,
-            ws.sssp_clr.as<uint2>(), nullptr, nullptr);
+        k_pack_pairs<<<g->num_sms * 8, kBlock, 0, g->stream>>>(R.rowidx, R.cw, g->E,
+                                                              ws.sssp_crw.as<uint2>());
     }
     OLV_CUDA(cudaGetLastError());
-    OLV_CUDA(cudaMemcpyAsync(&ws.sssp_n_light, nlight.p, 8, cudaMemcpyDeviceToHost, g->stream));
-    OLV_CUDA(cudaStreamSynchronize(g->stream));
     ws.sssp_delta_built = delta;
     ws.sssp_part_relabel = relabel;
     return OLV_OK;
@@ -1263,10 +982,15 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
                                                                     : 3ULL * g->V + 1000);
     // the relax kernel for the tuned sources per thread (1, 2, 4 or 8)
     const uint32_t spt = g->tune.sssp_spt;
-    const void *chunks = spt == 8   ? (const void *)k_advance_chunks<SsspOp, 8>
-                         : spt == 4 ? (const void *)k_advance_chunks<SsspOp, 4>
-                         : spt == 2 ? (const void *)k_advance_chunks<SsspOp, 2>
-                                    : (const void *)k_advance_chunks<SsspOp, 1>;
+    const bool own = g->tune.sssp_owner != 0;   // owner table instead of the binary search
+    const void *chunks =
+        spt == 8   ? (const void *)k_advance_chunks<SsspOp, 8>   // no room for the table
+        : spt == 4 ? (own ? (const void *)k_advance_chunks<SsspOp, 4, true>
+                          : (const void *)k_advance_chunks<SsspOp, 4>)
+        : spt == 2 ? (own ? (const void *)k_advance_chunks<SsspOp, 2, true>
+                          : (const void *)k_advance_chunks<SsspOp, 2>)
+                   : (own ? (const void *)k_advance_chunks<SsspOp, 1, true>
+                          : (const void *)k_advance_chunks<SsspOp, 1>);
     int nb = 0;   // the relax kernel's own residency (it holds more registers than BFS's)
     OLV_TRY(resident_blocks(g, chunks, &nb));
     uint32_t V = g->V;
@@ -1285,17 +1009,6 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     x.cmark = mk + 4 * words;
     x.bl_cap = V;
     x.pull = g->tune.sssp_pull && x.crw != nullptr;
-    x.lv = ws.sssp_lv.as<uint32_t>();
-    x.lcp = ws.sssp_lcp.as<uint32_t>();
-    x.ltile = ws.sssp_ltile.as<uint32_t>();
-    x.lcrw = ws.sssp_lcrw.as<uint2>();
-    x.ntiles = ws.sssp_ntiles;
-    x.n_light = ws.sssp_n_light;
-    const bool lpull = g->tune.sssp_lpull && x.lcrw != nullptr;
-    x.lrng = lpull ? ws.sssp_lr.as<uint2>() : nullptr;   // m_next kept only for the choice
-    x.nmark0 = op.nmark0;
-    x.nmark1 = op.nmark1;
-    op.lrng = x.lrng;
     void *a_aux[] = {&V, &ctl, &q0, &q1, &far0, &far1, &fm, &x};
     OLV_TRY(sink((const void *)k_sssp_aux, dim3(nb), dim3(kBlock), a_aux));
     uint32_t bl_cap = x.bl_cap;
@@ -1341,10 +1054,6 @@ int run_sssp_device(olv_graph *g, uint32_t src, uint32_t *dist_dev, unsigned lon
                     bool *red_done) {
     *red_done = false;
     OLV_TRY(sssp_partition(g));
-    if (g->tune.sssp_lpull && !g->ws.sssp_lcrw.p) {
-        OLV_TRY(build_light_csc(g));
-        if (g->sssp_graph) g->sssp_graph->destroy();   // its kernels captured the old pointers
-    }
     cudaStream_t s = g->stream;
     TravCtl *ctl = g->ws.ctl.as<TravCtl>();
     const SsspCsr R = sssp_csr(g);
@@ -1353,9 +1062,7 @@ int run_sssp_device(olv_graph *g, uint32_t src, uint32_t *dist_dev, unsigned lon
     k_fill_i32<<<g->num_sms * 8, kBlock, 0, s>>>((int32_t *)dist, g->V, kInf);
     k_sssp_init<<<1, 1, 0, s>>>(ctl, dist, g->ws.q0.as<uint32_t>(), src, sssp_delta(g),
                                 g->tune.sssp_sub, g->tune.sssp_sub_buckets,
-                                g->tune.sssp_tail_delta,
-                                g->ws.sssp_lcrw.p ? g->tune.sssp_lpull : 0,
-                                g->ws.sssp_n_light, R.newid);
+                                g->tune.sssp_tail_delta, R.newid);
     OLV_CUDA(cudaGetLastError());
     auto finish = [&]() -> int {
         if (R.dist) {
@@ -1429,7 +1136,7 @@ extern "C" int olv_sssp(olv_graph *g, uint32_t src, uint32_t *dist_out, olv_stat
         float ms = 0;
         OLV_CUDA(cudaEventElapsedTime(&ms, g->ev0, g->ev1));
         st->iterations = h.steps;
-        st->pull_steps = h.pull_steps;   // heavy-edge and light-edge pull supersteps
+        st->pull_steps = 0;
         st->vertices_reached = red[1];
         st->edges_traversed = red[0];
         st->edges_relaxed = h.edges_relaxed;

@@ -182,13 +182,16 @@ def test_sssp_hub_pieces_vs_dijkstra(ob, hub, piece):
             np.testing.assert_array_equal(g.sssp(s), oracle.dijkstra(rp, cl, w, s)[0])
 
 
-@pytest.mark.parametrize("spt,fuse", [(1, 0), (1, 1), (2, 1), (4, 0), (4, 1), (8, 1)])
-def test_sssp_chunk_shape_and_fused_end_vs_dijkstra(ob, spt, fuse):
-    """Relax chunks of 256 x spt queued sources, and the superstep's end step
-    run by the pieces kernel's last CTA (fuse 1) or by its own launch: the
-    same distances, inside the CUDA graph and in the host loop."""
+@pytest.mark.parametrize("spt,fuse,owner", [(1, 0, 0), (1, 1, 0), (2, 1, 0), (4, 0, 0), (4, 1, 0),
+                                              (8, 1, 0), (1, 0, 1), (2, 0, 1), (4, 1, 1)])
+def test_sssp_chunk_shape_and_fused_end_vs_dijkstra(ob, spt, fuse, owner):
+    """Relax chunks of 256 x spt queued sources, edges' sources found by
+    binary search or in the owner table (owner 1), and the superstep's end
+    step run by the pieces kernel's last CTA (fuse 1) or by its own launch:
+    the same distances, inside the CUDA graph and in the host loop."""
     with ob.Graph.rmat(16, 16, 5, weights=True, wseed=4) as g:
-        g.tune(sssp_spt=spt, sssp_fuse_end=fuse, sssp_hub_degree=64, sssp_piece=64)
+        g.tune(sssp_spt=spt, sssp_fuse_end=fuse, sssp_owner=owner, sssp_hub_degree=64,
+               sssp_piece=64)
         rp, cl, w = g.csr()
         hub, _ = g.max_degree_vertex()
         deg = np.diff(rp.astype(np.int64))
@@ -234,31 +237,6 @@ def test_sssp_wide_tail_on_fixtures(ob, path):
             for s in range(0, len(rp) - 1, 5):
                 ref, *_ = oracle.dijkstra(rp, cl, w, s)
                 np.testing.assert_array_equal(g.sssp(s), ref, err_msg=f"tail {tail} source {s}")
-
-
-@pytest.mark.parametrize("lpull", [1, 3, 1000])
-@pytest.mark.parametrize("tail", [0, 512])
-def test_sssp_light_pull_vs_dijkstra(ob, lpull, tail):
-    """Relax supersteps of large near queues run as a pull over every
-    vertex's light in-edges (lpull 1000: nearly every one): Dijkstra's
-    distances, with and without the renumbering, in the graph and the host
-    loop, and the pull counted in the statistics."""
-    with ob.Graph.rmat(16, 16, 7, weights=True, wseed=3) as g:
-        g.tune(sssp_lpull=lpull, sssp_tail_delta=tail)
-        rp, cl, w = g.csr()
-        hub, _ = g.max_degree_vertex()
-        deg = np.diff(rp.astype(np.int64))
-        ref_hub = oracle.dijkstra(rp, cl, w, hub)[0]
-        np.testing.assert_array_equal(g.sssp(hub), ref_hub)
-        if lpull == 1000:
-            assert g.last_stats.pull_steps >= 2   # the heavy-edge pull and light pulls
-        s = int(np.flatnonzero(deg == 1)[0])
-        np.testing.assert_array_equal(g.sssp(s), oracle.dijkstra(rp, cl, w, s)[0])
-        for kw in ({"sssp_relabel": 0}, {"use_graphs": 0}, {"sssp_pull": 0}, {"sssp_spt": 4}):
-            base = g.tune()
-            g.tune(**kw)
-            np.testing.assert_array_equal(g.sssp(hub), ref_hub, err_msg=str(kw))
-            g.tune(**{k: base[k] for k in kw})
 
 
 def test_sssp_chunk_shape_rejects_bad_values(ob):

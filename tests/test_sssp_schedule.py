@@ -48,16 +48,13 @@ def _lower(dist, v, nd):
     return v, nd
 
 
-def schedule(rp, col, w, src, delta, pull_mode, list_collect, sub=0, nsub=1, tail=0, lpull=0):
+def schedule(rp, col, w, src, delta, pull_mode, list_collect, sub=0, nsub=1, tail=0):
     """pull_mode: 'never', 'always' or 'rule' (the kernel's choice:
     E - settled in-edges + V/2 < heavy out-edges of the bucket).  sub > 0:
     the light phase of the first nsub heavy buckets runs in sub-buckets of
     width sub (the far pile is split at each sub-bucket's end; the heavy step
     follows the last one).  tail > delta: the buckets after the first are
-    tail wide and relax every edge in-bucket, with no heavy step.  lpull > 0:
-    a relax superstep whose queue carries at least 1/lpull of the light edges
-    is a pull (every vertex at or above the bucket's low edge takes the
-    minimum over its light in-edges from sources under the threshold)."""
+    tail wide and relax every edge in-bucket, with no heavy step."""
     rp = rp.astype(np.int64)
     col = col.astype(np.int64)
     w = w.astype(np.int64)
@@ -83,25 +80,11 @@ def schedule(rp, col, w, src, delta, pull_mode, list_collect, sub=0, nsub=1, tai
     settled_in, pulls = 0, 0
     wide = False
     every = np.ones(E, bool)
-    n_light = int(light.sum())
-    ldeg = np.bincount(row[light], minlength=V)
-    clight = light[order]                      # in-edges (CSC order) that are light
-    lpulls = 0
     while True:
         blist = []
         while True:
             while len(q):                       # relax supersteps: light (or all) edges
                 blist.append(q)
-                if not wide and lpull and n_light and int(ldeg[q].sum()) * lpull >= n_light:
-                    lpulls += 1                 # the light pull
-                    ok = clight & (dist[csrc] < hi)
-                    vv = col[order][ok]
-                    nd = np.minimum(dist[csrc][ok] + cw[ok], INF)
-                    cand = dist[vv] >= lo
-                    v, nd = _lower(dist, vv[cand], nd[cand])
-                    far[v[nd >= hi]] = True
-                    q = v[nd < hi]
-                    continue
                 u, e = _expand(rp, deg, every if wide else light, q)
                 v, nd = _lower(dist, col[e], np.minimum(dist[u] + w[e], INF))
                 far[v[nd >= hi]] = True
@@ -123,7 +106,7 @@ def schedule(rp, col, w, src, delta, pull_mode, list_collect, sub=0, nsub=1, tai
             far[:] = False
             far[fv] = True
             if len(fv) == 0:
-                return dist, pulls + lpulls
+                return dist, pulls
             lo = max(hi, int(dist[fv].min()))
             hi = bend = lo + tail
             q = fv[dist[fv] < hi]
@@ -157,7 +140,7 @@ def schedule(rp, col, w, src, delta, pull_mode, list_collect, sub=0, nsub=1, tai
         far[:] = False
         far[fv] = True
         if len(fv) == 0:
-            return dist, pulls + lpulls
+            return dist, pulls
         lo = max(hi, int(dist[fv].min()))
         hb += 1
         wide = tail > delta
@@ -268,22 +251,3 @@ def test_schedule_with_wide_tail_buckets(tail, pull_mode):
     ref = oracle.dijkstra(rp, col, w, 0)[0].astype(np.int64)
     dist, _ = schedule(rp, col, w, 0, 32, pull_mode, list_collect=True, tail=tail)
     np.testing.assert_array_equal(dist, ref)
-
-
-@pytest.mark.parametrize("lpull", [1, 3, 1000])
-@pytest.mark.parametrize("tail", [0, 512])
-def test_schedule_with_light_pull(lpull, tail):
-    """Relax supersteps of large queues run as a pull over light in-edges
-    (every one when lpull is large): Dijkstra's distances, the pull taken at
-    least once from the hub, and the bucket list still covers every bucket."""
-    rp, col = oracle.rmat_csr(12, 16, 9)
-    w = oracle.uint_weights(len(col), 19)
-    deg = np.diff(rp.astype(np.int64))
-    hub = int(np.argmax(deg))
-    for src in (hub, int(np.flatnonzero(deg == 1)[0])):
-        ref = oracle.dijkstra(rp, col, w, src)[0].astype(np.int64)
-        dist, pulls = schedule(rp, col, w, src, 64, "rule", list_collect=True, tail=tail,
-                               lpull=lpull)
-        np.testing.assert_array_equal(dist, ref)
-        if src == hub and lpull >= 3:
-            assert pulls >= 2      # the heavy pull and at least one light pull
