@@ -95,6 +95,7 @@ struct Workspace {
     DevBuf sr_perm, sr_newid, sr_rowptr, sr_col, sr_w, sr_colptr, sr_rowidx, sr_cw, sr_dist;
     int sr_built = 0;
     uint32_t sr_vnz = 0;            // SSSP renumbered: vertices with in-degree > 0 (a prefix)
+    uint32_t sr_vlong = 0;          // SSSP renumbered: vertices with in-degree > 32 (a prefix)
     int sssp_part_relabel = -1;     // SSSP: the partition above was built relabelled (1) or not
     uint32_t sssp_delta_built = 0;
     uint32_t n_heavy = 0, n_light = 0;

@@ -85,6 +85,8 @@ struct SsspAux {
     const uint32_t *colptr;            // CSC row offsets
     const uint2 *crw;                  // CSC: (source, weight) per in-edge
     uint32_t vpull;                    // vertices [vpull, V) have no in-edges
+    uint32_t vsplit;                   // the pull takes [vsplit, vpull) a thread per vertex
+                                       // (renumbered: at most kPullShort in-edges each)
     const uint2 *hdin;                 // per vertex: (heavy out-degree, in-degree)
     uint32_t *blist;                   // bucket list: the bucket's relax inputs, in order
     uint32_t *cmark;                   // bitmap: vertices collected so far this run
@@ -500,6 +502,7 @@ __device__ __forceinline__ uint32_t pull_cand(uint32_t du, uint32_t w, uint32_t 
 // the scan), and fold candidates into a shared per-vertex minimum.
 constexpr int kPullItems = 4;
 constexpr uint32_t kPullChunk = 4 * kBlock;
+constexpr uint32_t kPullShort = 32;   // renumbered rows past this in-degree go by chunks
 __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1, FarMarks fm,
                           const SsspAux &x, WarpStage sf) {
     uint32_t *dist = static_cast<uint32_t *>(c->vdata);
@@ -512,8 +515,9 @@ __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1
     const uint32_t lane = lane_id();
     uint32_t fmin = 0xffffffffu;
     unsigned long long scanned = 0;
-    // vertices past vpull have no in-edges (the renumbered ids put them last)
-    for (uint64_t base = (uint64_t)blockIdx.x * kPullChunk; base < x.vpull;
+    // vertices past vpull have no in-edges (the renumbered ids put them
+    // last); [vsplit, vpull) go a thread per vertex below
+    for (uint64_t base = (uint64_t)blockIdx.x * kPullChunk; base < x.vsplit;
          base += (uint64_t)gridDim.x * kPullChunk) {
         const uint64_t v0 = base + 4 * (uint64_t)threadIdx.x;
         uint32_t d[4] = {0u, 0u, 0u, 0u}, b[4] = {0u, 0u, 0u, 0u}, e[4] = {0u, 0u, 0u, 0u};
@@ -609,6 +613,66 @@ __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1
         sf.reserve(32 * 4, far, far_size);
         stage_push_n<4>(act, va, 2, sf.buf, sf.n, sf.lim, kWarpStage, far, far_size);
         __syncthreads();   // s_off / s_beg / s_best are rewritten by the next chunk
+    }
+    // Short rows (renumbered suffix, at most kPullShort in-edges each): a
+    // thread takes four consecutive vertices and scans the in-edges of the
+    // unsettled ones itself, four in flight; no shared memory or barriers.
+    for (uint64_t base = (uint64_t)blockIdx.x * kBlock * 4 + x.vsplit; base < x.vpull;
+         base += (uint64_t)gridDim.x * kBlock * 4) {
+        const uint64_t v0 = base + 4 * (uint64_t)threadIdx.x;
+        uint32_t d[4] = {0u, 0u, 0u, 0u}, b[4] = {0u, 0u, 0u, 0u}, e[4] = {0u, 0u, 0u, 0u};
+        if (vec && v0 + 4 <= V) {
+            const uint4 d4 = __ldcg(reinterpret_cast<const uint4 *>(dist + v0));
+            d[0] = d4.x;
+            d[1] = d4.y;
+            d[2] = d4.z;
+            d[3] = d4.w;
+            if (d[0] >= hi || d[1] >= hi || d[2] >= hi || d[3] >= hi) {
+                const uint4 c4 = *reinterpret_cast<const uint4 *>(x.colptr + v0);
+                const uint32_t c5 = x.colptr[v0 + 4];
+                if (d[0] >= hi) { b[0] = c4.x; e[0] = c4.y; }
+                if (d[1] >= hi) { b[1] = c4.y; e[1] = c4.z; }
+                if (d[2] >= hi) { b[2] = c4.z; e[2] = c4.w; }
+                if (d[3] >= hi) { b[3] = c4.w; e[3] = c5; }
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (v0 + j < V) {
+                    d[j] = __ldcg(dist + v0 + j);
+                    if (d[j] >= hi) {
+                        b[j] = x.colptr[v0 + j];
+                        e[j] = x.colptr[v0 + j + 1];
+                    }
+                }
+        }
+        int act[4];
+        uint32_t va[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            va[j] = (uint32_t)(v0 + j);
+            act[j] = 0;
+            uint32_t best = d[j];
+            scanned += e[j] - b[j];
+            for (uint32_t i = b[j]; i < e[j]; i += 4) {
+                uint2 t[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) t[k] = i + k < e[j] ? x.crw[i + k] : make_uint2(0u, 0u);
+                uint32_t du[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) du[k] = i + k < e[j] ? __ldcg(&dist[t[k].x]) : 0xffffffffu;
+#pragma unroll
+                for (int k = 0; k < 4; k++) best = min(best, pull_cand(du[k], t[k].y, hi));
+            }
+            if (best < d[j]) {   // only vertices at or above the threshold with in-edges
+                dist[va[j]] = best;
+                const uint32_t bit = 1u << (va[j] & 31);
+                if (!(atomicOr(&fbits[va[j] >> 5], bit) & bit)) act[j] = 2;
+                fmin = best < fmin ? best : fmin;
+            }
+        }
+        sf.reserve(32 * 4, far, far_size);
+        stage_push_n<4>(act, va, 2, sf.buf, sf.n, sf.lim, kWarpStage, far, far_size);
     }
     warp_stage_flush(sf.buf, sf.n, sf.lim, far, far_size);
     const uint32_t m = __reduce_min_sync(0xffffffffu, fmin);
@@ -816,18 +880,45 @@ __global__ void k_sssp_relabel(const uint32_t *__restrict__ old_ptr,
 // Distances back to the caller's ids: out[v] = dnew[newid[v]].
 // Distances back to the caller's ids; with red, also the sum of out-degrees
 // and the count of the reached vertices (k_reached_edges in the same pass).
+// Four vertices per thread, their four gathers in flight (the gather of the
+// renumbered distances is the pass's latency).
 __global__ void k_sssp_unrelabel(const uint32_t *__restrict__ dnew,
                                  const uint32_t *__restrict__ newid, uint32_t V,
                                  uint32_t *__restrict__ out, const uint32_t *__restrict__ rowptr,
                                  unsigned long long *red /*[2] or null*/) {
     unsigned long long e = 0, n = 0;
-    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < V;
-         v += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t d = __ldg(&dnew[newid[v]]);
-        out[v] = d;
-        if (red && d != (uint32_t)kInf) {
-            e += rowptr[v + 1] - rowptr[v];
-            n++;
+    const bool vec = (((uintptr_t)newid | (uintptr_t)out | (uintptr_t)rowptr) & 15) == 0;
+    for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; 4 * q < V;
+         q += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t v0 = 4 * q;
+        uint32_t d[4];
+        if (vec && v0 + 4 <= V) {
+            const uint4 k4 = *reinterpret_cast<const uint4 *>(newid + v0);
+            d[0] = __ldg(&dnew[k4.x]);
+            d[1] = __ldg(&dnew[k4.y]);
+            d[2] = __ldg(&dnew[k4.z]);
+            d[3] = __ldg(&dnew[k4.w]);
+            *reinterpret_cast<uint4 *>(out + v0) = make_uint4(d[0], d[1], d[2], d[3]);
+            if (red) {
+                const uint4 r4 = *reinterpret_cast<const uint4 *>(rowptr + v0);
+                const uint32_t r5 = rowptr[v0 + 4];
+                const uint32_t dg[4] = {r4.y - r4.x, r4.z - r4.y, r4.w - r4.z, r5 - r4.w};
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    if (d[j] != (uint32_t)kInf) {
+                        e += dg[j];
+                        n++;
+                    }
+            }
+        } else {
+            for (uint64_t v = v0; v < V && v < v0 + 4; v++) {
+                const uint32_t dv = __ldg(&dnew[newid[v]]);
+                out[v] = dv;
+                if (red && dv != (uint32_t)kInf) {
+                    e += rowptr[v + 1] - rowptr[v];
+                    n++;
+                }
+            }
         }
     }
     if (red) {
@@ -862,9 +953,13 @@ static int sssp_relabel(olv_graph *g) {
         perm[i] = v;
         newid[v] = i;
     }
-    uint32_t vnz = 0;   // in-degree > 0: a prefix of the new numbering
-    for (uint32_t v = 0; v < V; v++) vnz += cp[v + 1] != cp[v];
+    uint32_t vnz = 0, vlong = 0;   // in-degree > 0 and > kPullShort: prefixes of the new numbering
+    for (uint32_t v = 0; v < V; v++) {
+        vnz += cp[v + 1] != cp[v];
+        vlong += cp[v + 1] - cp[v] > kPullShort;
+    }
     ws.sr_vnz = vnz;
+    ws.sr_vlong = vlong;
     nrp[0] = 0;
     ncp[0] = 0;
     for (uint32_t i = 0; i < V; i++) {
@@ -1003,6 +1098,11 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     x.colptr = R.colptr;
     x.crw = ws.sssp_crw.as<uint2>();
     x.vpull = R.newid ? ws.sr_vnz : V;
+    // renumbered: rows past the long-in-degree prefix (rounded up to whole
+    // chunks) are short and go a thread per vertex; otherwise all by chunks
+    x.vsplit = R.newid ? (uint32_t)std::min<uint64_t>(
+                             ((uint64_t)ws.sr_vlong + kPullChunk - 1) / kPullChunk * kPullChunk, x.vpull)
+                       : x.vpull;
     x.E = g->E;
     x.hdin = ws.hdin.as<uint2>();
     x.blist = ws.blist.as<uint32_t>();
