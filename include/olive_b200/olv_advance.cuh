@@ -202,25 +202,6 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t *t
     return r;
 }
 
-// Exclusive maximum over the CTA (x >= 0); every thread must call.
-__device__ __forceinline__ uint32_t block_exclusive_max(uint32_t x, uint32_t *s_warp) {
-    const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
-    uint32_t incl = x;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= (uint32_t)o) incl = max(incl, t);
-    }
-    uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
-    if (lane == 0) excl = 0;
-    if (lane == 31) s_warp[wid] = incl;
-    __syncthreads();
-    uint32_t before = 0;
-    for (uint32_t w = 0; w < wid; w++) before = max(before, s_warp[w]);
-    __syncthreads();
-    return max(before, excl);
-}
-
 #ifndef OLV_ITEMS
 #define OLV_ITEMS 8
 #endif
@@ -305,18 +286,11 @@ __device__ __forceinline__ typename Op::Pre prepare_edge(Op &op, typename Op::SV
 // queued sources (S per thread): with short rows (a few edges per source, as
 // in SSSP's light phase) a larger S spreads the scan and the barriers of a
 // chunk over more edges.
-//
-// Each edge slot k of a round finds its source by a binary search over the
-// chunk's offsets (OT false), or, with OT, in an owner table built once per
-// round: every source marks the first slot of its edges in the round and a
-// CTA-wide maximum scan fills the slots in between (one shared load per
-// edge instead of log2(kBlock * S) dependent ones).
-template <class Op, uint32_t S = 1, bool OT = false>
+template <class Op, uint32_t S = 1>
 __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_chunks(AdvanceArgs a, Op op) {
     static_assert(S == 1 || S == 2 || S == 4 || S == 8, "sources per thread: 1, 2, 4 or 8");
     constexpr uint32_t kChunk = kBlock * S;   // queued sources per chunk
     constexpr uint32_t kRound = kBlock * kItems;   // edge slots per round
-    __shared__ uint32_t s_own[OT ? kRound : 1];
     TravCtl *c = a.ctl;
     RowRanges rr;
     if (!advance_ranges(a, c, rr)) return;
@@ -386,31 +360,6 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_chunks(Advan
         }
         __syncthreads();
         for (uint32_t base = 0; base < total; base += kRound) {
-            if constexpr (OT) {
-                __syncthreads();   // the previous round's lookups are done
-#pragma unroll
-                for (uint32_t i = threadIdx.x; i < kRound; i += kBlock) s_own[i] = 0;
-                __syncthreads();
-#pragma unroll
-                for (uint32_t s = 0; s < S; s++) {
-                    const uint32_t slot = threadIdx.x * S + s;
-                    const uint32_t lo = s_off[slot], hi = lo + deg[s];
-                    if (hi > lo && lo < base + kRound && hi > base)
-                        s_own[lo > base ? lo - base : 0] = slot;
-                }
-                __syncthreads();
-                // inclusive maximum over the round: kItems consecutive slots per thread
-                uint32_t m = 0, loc[kItems];
-#pragma unroll
-                for (int i = 0; i < kItems; i++) {
-                    m = max(m, s_own[threadIdx.x * kItems + i]);
-                    loc[i] = m;
-                }
-                const uint32_t before = block_exclusive_max(m, s_warp);
-#pragma unroll
-                for (int i = 0; i < kItems; i++) s_own[threadIdx.x * kItems + i] = max(before, loc[i]);
-                __syncthreads();
-            }
             uint32_t e[kItems], v[kItems];
             SV sv[kItems];
             int act[kItems];
@@ -424,13 +373,9 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_chunks(Advan
                 if (act[j]) {
                     // the last entry whose offset is <= k owns edge slot k
                     uint32_t lo = 0;
-                    if constexpr (OT) {
-                        lo = s_own[j * kBlock + threadIdx.x];
-                    } else {
 #pragma unroll
-                        for (uint32_t step = kChunk / 2; step > 0; step >>= 1)
-                            if (s_off[lo + step] <= k) lo += step;
-                    }
+                    for (uint32_t step = kChunk / 2; step > 0; step >>= 1)
+                        if (s_off[lo + step] <= k) lo += step;
                     e[j] = s_beg[lo] + (k - s_off[lo]);
                     sv[j] = s_val[lo];
                 }

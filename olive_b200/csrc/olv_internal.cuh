@@ -65,8 +65,6 @@ struct Tuning {
     uint32_t sssp_sub = 0;            // SSSP: light-phase sub-bucket width (0: none)
     uint32_t sssp_sub_buckets = 1;    // SSSP: heavy buckets whose light phase uses it
     uint32_t sssp_spt = 1;            // SSSP: queued sources per thread in a relax chunk
-    int sssp_owner = 0;               // SSSP: relax chunks find an edge's source in an owner
-                                      // table (1) or by binary search (0)
     int sssp_fuse_end = 0;            // SSSP: superstep end step in the pieces kernel's last CTA
     uint32_t sssp_tail_delta = 1024;  // SSSP: width of the buckets after the first, which
                                       // relax every edge (<= delta: delta, light/heavy)

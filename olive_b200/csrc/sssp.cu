@@ -1077,15 +1077,10 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
                                                                     : 3ULL * g->V + 1000);
     // the relax kernel for the tuned sources per thread (1, 2, 4 or 8)
     const uint32_t spt = g->tune.sssp_spt;
-    const bool own = g->tune.sssp_owner != 0;   // owner table instead of the binary search
-    const void *chunks =
-        spt == 8   ? (const void *)k_advance_chunks<SsspOp, 8>   // no room for the table
-        : spt == 4 ? (own ? (const void *)k_advance_chunks<SsspOp, 4, true>
-                          : (const void *)k_advance_chunks<SsspOp, 4>)
-        : spt == 2 ? (own ? (const void *)k_advance_chunks<SsspOp, 2, true>
-                          : (const void *)k_advance_chunks<SsspOp, 2>)
-                   : (own ? (const void *)k_advance_chunks<SsspOp, 1, true>
-                          : (const void *)k_advance_chunks<SsspOp, 1>);
+    const void *chunks = spt == 8   ? (const void *)k_advance_chunks<SsspOp, 8>
+                         : spt == 4 ? (const void *)k_advance_chunks<SsspOp, 4>
+                         : spt == 2 ? (const void *)k_advance_chunks<SsspOp, 2>
+                                    : (const void *)k_advance_chunks<SsspOp, 1>;
     int nb = 0;   // the relax kernel's own residency (it holds more registers than BFS's)
     OLV_TRY(resident_blocks(g, chunks, &nb));
     uint32_t V = g->V;

@@ -182,16 +182,13 @@ def test_sssp_hub_pieces_vs_dijkstra(ob, hub, piece):
             np.testing.assert_array_equal(g.sssp(s), oracle.dijkstra(rp, cl, w, s)[0])
 
 
-@pytest.mark.parametrize("spt,fuse,owner", [(1, 0, 0), (1, 1, 0), (2, 1, 0), (4, 0, 0), (4, 1, 0),
-                                              (8, 1, 0), (1, 0, 1), (2, 0, 1), (4, 1, 1)])
-def test_sssp_chunk_shape_and_fused_end_vs_dijkstra(ob, spt, fuse, owner):
-    """Relax chunks of 256 x spt queued sources, edges' sources found by
-    binary search or in the owner table (owner 1), and the superstep's end
-    step run by the pieces kernel's last CTA (fuse 1) or by its own launch:
-    the same distances, inside the CUDA graph and in the host loop."""
+@pytest.mark.parametrize("spt,fuse", [(1, 0), (1, 1), (2, 1), (4, 0), (4, 1), (8, 1)])
+def test_sssp_chunk_shape_and_fused_end_vs_dijkstra(ob, spt, fuse):
+    """Relax chunks of 256 x spt queued sources, and the superstep's end step
+    run by the pieces kernel's last CTA (fuse 1) or by its own launch: the
+    same distances, inside the CUDA graph and in the host loop."""
     with ob.Graph.rmat(16, 16, 5, weights=True, wseed=4) as g:
-        g.tune(sssp_spt=spt, sssp_fuse_end=fuse, sssp_owner=owner, sssp_hub_degree=64,
-               sssp_piece=64)
+        g.tune(sssp_spt=spt, sssp_fuse_end=fuse, sssp_hub_degree=64, sssp_piece=64)
         rp, cl, w = g.csr()
         hub, _ = g.max_degree_vertex()
         deg = np.diff(rp.astype(np.int64))
