@@ -320,31 +320,38 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_chunks(Advan
 
     unsigned long long relaxed = 0;
     for (uint64_t c0 = (uint64_t)blockIdx.x * kChunk; c0 < n; c0 += (uint64_t)gridDim.x * kChunk) {
-        // thread t takes the S consecutive entries c0 + t*S .. c0 + t*S + S-1
-        uint32_t beg[S], deg[S], tdeg = 0;
+        // thread t takes the S consecutive entries c0 + t*S .. c0 + t*S + S-1;
+        // the row range and the source value of every entry are loaded
+        // together, before on_input's test (a value read early is at worst
+        // older: an input whose value drops this superstep is queued again)
+        uint32_t beg[S], deg[S], tdeg = 0, u[S];
         SV sv0[S];
+        uint2 r[S];
 #pragma unroll
         for (uint32_t s = 0; s < S; s++) {
             const uint64_t i = c0 + threadIdx.x * S + s;
-            beg[s] = 0;
-            deg[s] = 0;
+            u[s] = i < n ? qin[i] : 0xffffffffu;
+        }
+#pragma unroll
+        for (uint32_t s = 0; s < S; s++) {
+            r[s] = make_uint2(0u, 0u);
             sv0[s] = 0;
-            if (i < n) {
-                const uint32_t u = qin[i];
-                if (op.on_input(u)) {
-                    const uint2 r = rr.of(u);
-                    beg[s] = r.x;
-                    deg[s] = r.y - r.x;
-                }
-                if (deg[s] > a.hub_degree) {
-                    const uint32_t np = (deg[s] + a.piece - 1) / a.piece;
-                    const uint32_t b = atomicAdd(&c->npieces, np);
-                    for (uint32_t p = 0; p < np; p++) a.pieces[b + p] = make_uint2(u, p);
-                    relaxed += deg[s];
-                    deg[s] = 0;
-                } else {
-                    sv0[s] = op.src_value(u);
-                }
+            if (u[s] != 0xffffffffu) {
+                r[s] = rr.of(u[s]);
+                sv0[s] = op.src_value(u[s]);
+            }
+        }
+#pragma unroll
+        for (uint32_t s = 0; s < S; s++) {
+            beg[s] = r[s].x;
+            deg[s] = r[s].y - r[s].x;
+            if (u[s] != 0xffffffffu && !op.on_input(u[s])) deg[s] = 0;
+            if (deg[s] > a.hub_degree) {
+                const uint32_t np = (deg[s] + a.piece - 1) / a.piece;
+                const uint32_t b = atomicAdd(&c->npieces, np);
+                for (uint32_t p = 0; p < np; p++) a.pieces[b + p] = make_uint2(u[s], p);
+                relaxed += deg[s];
+                deg[s] = 0;
             }
             relaxed += deg[s];
             tdeg += deg[s];
