@@ -646,29 +646,44 @@ __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1
                     }
                 }
         }
+        // the four vertices' in-edges are read in step, two per vertex per
+        // round, so eight loads (and then eight gathers) are in flight
+        uint32_t best[4], len = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            best[j] = d[j];
+            scanned += e[j] - b[j];
+            len = max(len, e[j] - b[j]);
+        }
+        for (uint32_t o = 0; o < len; o += 2) {
+            uint2 t[4][2];
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+#pragma unroll
+                for (int k = 0; k < 2; k++)
+                    t[j][k] = b[j] + o + k < e[j] ? x.crw[b[j] + o + k] : make_uint2(0u, 0u);
+            uint32_t du[4][2];
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+#pragma unroll
+                for (int k = 0; k < 2; k++)
+                    du[j][k] = b[j] + o + k < e[j] ? __ldcg(&dist[t[j][k].x]) : 0xffffffffu;
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+#pragma unroll
+                for (int k = 0; k < 2; k++) best[j] = min(best[j], pull_cand(du[j][k], t[j][k].y, hi));
+        }
         int act[4];
         uint32_t va[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             va[j] = (uint32_t)(v0 + j);
             act[j] = 0;
-            uint32_t best = d[j];
-            scanned += e[j] - b[j];
-            for (uint32_t i = b[j]; i < e[j]; i += 4) {
-                uint2 t[4];
-#pragma unroll
-                for (int k = 0; k < 4; k++) t[k] = i + k < e[j] ? x.crw[i + k] : make_uint2(0u, 0u);
-                uint32_t du[4];
-#pragma unroll
-                for (int k = 0; k < 4; k++) du[k] = i + k < e[j] ? __ldcg(&dist[t[k].x]) : 0xffffffffu;
-#pragma unroll
-                for (int k = 0; k < 4; k++) best = min(best, pull_cand(du[k], t[k].y, hi));
-            }
-            if (best < d[j]) {   // only vertices at or above the threshold with in-edges
-                dist[va[j]] = best;
+            if (best[j] < d[j]) {   // only vertices at or above the threshold with in-edges
+                dist[va[j]] = best[j];
                 const uint32_t bit = 1u << (va[j] & 31);
                 if (!(atomicOr(&fbits[va[j] >> 5], bit) & bit)) act[j] = 2;
-                fmin = best < fmin ? best : fmin;
+                fmin = best[j] < fmin ? best[j] : fmin;
             }
         }
         sf.reserve(32 * 4, far, far_size);
