@@ -402,10 +402,16 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_advance_chunks(Advan
 #pragma unroll
             for (int j = 0; j < kItems; j++) op.on_push(act[j] == 1, v[j]);
         }
-        stage_flush(s_q, &s_qn, &s_qlim, &s_base, qout, qout_size);
-        if (Op::kHasFar) stage_flush(s_f, &s_fn, &s_flim, &s_base, far, far_size);
+        // the staging buffers are emptied once half full, and at the end:
+        // most chunks then pay no flush (three barriers and an atomic each)
+        __syncthreads();
+        if (min(s_qn, s_qlim) >= kStage / 2) stage_flush(s_q, &s_qn, &s_qlim, &s_base, qout, qout_size);
+        if (Op::kHasFar && min(s_fn, s_flim) >= kStage / 2)
+            stage_flush(s_f, &s_fn, &s_flim, &s_base, far, far_size);
         __syncthreads();
     }
+    stage_flush(s_q, &s_qn, &s_qlim, &s_base, qout, qout_size);
+    if (Op::kHasFar) stage_flush(s_f, &s_fn, &s_flim, &s_base, far, far_size);
     op.flush(relaxed);
 }
 
