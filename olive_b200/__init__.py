@@ -264,7 +264,7 @@ class Graph:
             _check(lib().olv_tune_set(self._h, k.encode(), float(v)), f"olv_tune_set({k})")
         out = {}
         for k in ("hub_degree", "piece", "alpha", "beta", "sssp_delta", "sssp_pull", "sssp_relabel",
-                  "sssp_sub", "sssp_sub_buckets", "sssp_spt", "sssp_fuse_end",
+                  "sssp_sub", "sssp_sub_buckets", "sssp_spt", "sssp_pull_split", "sssp_fuse_end",
                   "sssp_hub_degree", "sssp_piece", "sssp_tail_delta", "ms_alpha",
                   "pr_tile_u", "use_graphs", "levels_per_sync", "batch_cluster"):
             d = _D()

@@ -535,6 +535,8 @@ int olv_tune_set(olv_graph *g, const char *key, double value) {
     } else if (!strcmp(key, "sssp_tail_delta")) {
         OLV_CHECK_ARG(value >= 0 && value < 2147483647.0, "olv_tune_set: bad sssp_tail_delta");
         t.sssp_tail_delta = (uint32_t)value;
+    } else if (!strcmp(key, "sssp_pull_split")) {
+        t.sssp_pull_split = value != 0;
     } else if (!strcmp(key, "sssp_fuse_end")) {
         t.sssp_fuse_end = value != 0;
     } else if (!strcmp(key, "pr_tile_u")) {
@@ -583,6 +585,7 @@ int olv_tune_get(const olv_graph *g, const char *key, double *value) {
     else if (!strcmp(key, "sssp_sub_buckets")) *value = t.sssp_sub_buckets;
     else if (!strcmp(key, "sssp_spt")) *value = t.sssp_spt;
     else if (!strcmp(key, "sssp_fuse_end")) *value = t.sssp_fuse_end;
+    else if (!strcmp(key, "sssp_pull_split")) *value = t.sssp_pull_split;
     else if (!strcmp(key, "sssp_tail_delta")) *value = t.sssp_tail_delta;
     else if (!strcmp(key, "sssp_hub_degree")) *value = t.sssp_hub_degree;
     else if (!strcmp(key, "sssp_piece")) *value = t.sssp_piece;

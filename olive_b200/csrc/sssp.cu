@@ -502,7 +502,7 @@ __device__ __forceinline__ uint32_t pull_cand(uint32_t du, uint32_t w, uint32_t 
 // the scan), and fold candidates into a shared per-vertex minimum.
 constexpr int kPullItems = 4;
 constexpr uint32_t kPullChunk = 4 * kBlock;
-constexpr uint32_t kPullShort = 32;   // renumbered rows past this in-degree go by chunks
+constexpr uint32_t kPullShort = 8;    // renumbered rows past this in-degree go by chunks
 __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1, FarMarks fm,
                           const SsspAux &x, WarpStage sf) {
     uint32_t *dist = static_cast<uint32_t *>(c->vdata);
@@ -646,8 +646,9 @@ __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1
                     }
                 }
         }
-        // the four vertices' in-edges are read in step, two per vertex per
-        // round, so eight loads (and then eight gathers) are in flight
+        // the four vertices' in-edges are read in step, four per vertex per
+        // round (at most two rounds), so sixteen loads (and then sixteen
+        // gathers) are in flight
         uint32_t best[4], len = 0;
 #pragma unroll
         for (int j = 0; j < 4; j++) {
@@ -655,23 +656,23 @@ __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1
             scanned += e[j] - b[j];
             len = max(len, e[j] - b[j]);
         }
-        for (uint32_t o = 0; o < len; o += 2) {
-            uint2 t[4][2];
+        for (uint32_t o = 0; o < len; o += 4) {
+            uint2 t[4][4];
 #pragma unroll
             for (int j = 0; j < 4; j++)
 #pragma unroll
-                for (int k = 0; k < 2; k++)
+                for (int k = 0; k < 4; k++)
                     t[j][k] = b[j] + o + k < e[j] ? x.crw[b[j] + o + k] : make_uint2(0u, 0u);
-            uint32_t du[4][2];
+            uint32_t du[4][4];
 #pragma unroll
             for (int j = 0; j < 4; j++)
 #pragma unroll
-                for (int k = 0; k < 2; k++)
+                for (int k = 0; k < 4; k++)
                     du[j][k] = b[j] + o + k < e[j] ? __ldcg(&dist[t[j][k].x]) : 0xffffffffu;
 #pragma unroll
             for (int j = 0; j < 4; j++)
 #pragma unroll
-                for (int k = 0; k < 2; k++) best[j] = min(best[j], pull_cand(du[j][k], t[j][k].y, hi));
+                for (int k = 0; k < 4; k++) best[j] = min(best[j], pull_cand(du[j][k], t[j][k].y, hi));
         }
         int act[4];
         uint32_t va[4];
@@ -1110,7 +1111,7 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     x.vpull = R.newid ? ws.sr_vnz : V;
     // renumbered: rows past the long-in-degree prefix (rounded up to whole
     // chunks) are short and go a thread per vertex; otherwise all by chunks
-    x.vsplit = R.newid ? (uint32_t)std::min<uint64_t>(
+    x.vsplit = R.newid && g->tune.sssp_pull_split ? (uint32_t)std::min<uint64_t>(
                              ((uint64_t)ws.sr_vlong + kPullChunk - 1) / kPullChunk * kPullChunk, x.vpull)
                        : x.vpull;
     x.E = g->E;
