@@ -126,9 +126,9 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
  *                 0 or >= sssp_delta: one sub-bucket per bucket          (0)
  *   "sssp_sub_buckets"  heavy buckets (from the first) that use sssp_sub (1)
  *   "sssp_spt"    queued sources per thread in a relax chunk: 1, 2, 4 or 8 (1)
- *   "sssp_pull_split"  SSSP pull: renumbered vertices with at most 8
- *                 in-edges a thread per vertex (1) or all by edge-balanced
- *                 chunks (0)                                             (1)
+ *   "sssp_pull_split"  SSSP pull: renumbered vertices with at most this
+ *                 many in-edges (4, 8, 16 or 32) a thread per vertex, the
+ *                 rest by edge-balanced chunks; 0: all by chunks         (8)
  *   "sssp_fuse_end"  SSSP superstep's end step run by the last CTA of the
  *                 relax pieces kernel instead of a launch of its own (0)
  *   "sssp_tail_delta"  width of the SSSP buckets after the first; above

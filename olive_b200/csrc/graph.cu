@@ -536,7 +536,9 @@ int olv_tune_set(olv_graph *g, const char *key, double value) {
         OLV_CHECK_ARG(value >= 0 && value < 2147483647.0, "olv_tune_set: bad sssp_tail_delta");
         t.sssp_tail_delta = (uint32_t)value;
     } else if (!strcmp(key, "sssp_pull_split")) {
-        t.sssp_pull_split = value != 0;
+        OLV_CHECK_ARG(value == 0 || value == 4 || value == 8 || value == 16 || value == 32,
+                      "olv_tune_set: sssp_pull_split must be 0, 4, 8, 16 or 32");
+        t.sssp_pull_split = (uint32_t)value;
     } else if (!strcmp(key, "sssp_fuse_end")) {
         t.sssp_fuse_end = value != 0;
     } else if (!strcmp(key, "pr_tile_u")) {

@@ -65,7 +65,8 @@ struct Tuning {
     uint32_t sssp_sub = 0;            // SSSP: light-phase sub-bucket width (0: none)
     uint32_t sssp_sub_buckets = 1;    // SSSP: heavy buckets whose light phase uses it
     uint32_t sssp_spt = 1;            // SSSP: queued sources per thread in a relax chunk
-    int sssp_pull_split = 1;          // SSSP pull: short renumbered rows a thread per vertex
+    uint32_t sssp_pull_split = 8;     // SSSP pull: renumbered rows with at most this many
+                                      // in-edges a thread per vertex (0: none; 4, 8, 16, 32)
     int sssp_fuse_end = 0;            // SSSP: superstep end step in the pieces kernel's last CTA
     uint32_t sssp_tail_delta = 1024;  // SSSP: width of the buckets after the first, which
                                       // relax every edge (<= delta: delta, light/heavy)
@@ -94,7 +95,8 @@ struct Workspace {
     DevBuf sr_perm, sr_newid, sr_rowptr, sr_col, sr_w, sr_colptr, sr_rowidx, sr_cw, sr_dist;
     int sr_built = 0;
     uint32_t sr_vnz = 0;            // SSSP renumbered: vertices with in-degree > 0 (a prefix)
-    uint32_t sr_vlong = 0;          // SSSP renumbered: vertices past the pull's short-row in-degree (a prefix)
+    uint32_t sr_vlong[4] = {0, 0, 0, 0};   // SSSP renumbered: vertices with in-degree > 4, 8,
+                                           // 16, 32 (prefixes)
     int sssp_part_relabel = -1;     // SSSP: the partition above was built relabelled (1) or not
     uint32_t sssp_delta_built = 0;
     uint32_t n_heavy = 0, n_light = 0;

@@ -86,7 +86,7 @@ struct SsspAux {
     const uint2 *crw;                  // CSC: (source, weight) per in-edge
     uint32_t vpull;                    // vertices [vpull, V) have no in-edges
     uint32_t vsplit;                   // the pull takes [vsplit, vpull) a thread per vertex
-                                       // (renumbered: at most kPullShort in-edges each)
+                                       // (renumbered: at most sssp_pull_split in-edges each)
     const uint2 *hdin;                 // per vertex: (heavy out-degree, in-degree)
     uint32_t *blist;                   // bucket list: the bucket's relax inputs, in order
     uint32_t *cmark;                   // bitmap: vertices collected so far this run
@@ -502,7 +502,6 @@ __device__ __forceinline__ uint32_t pull_cand(uint32_t du, uint32_t w, uint32_t 
 // the scan), and fold candidates into a shared per-vertex minimum.
 constexpr int kPullItems = 4;
 constexpr uint32_t kPullChunk = 4 * kBlock;
-constexpr uint32_t kPullShort = 8;    // renumbered rows past this in-degree go by chunks
 __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1, FarMarks fm,
                           const SsspAux &x, WarpStage sf) {
     uint32_t *dist = static_cast<uint32_t *>(c->vdata);
@@ -614,7 +613,7 @@ __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1
         stage_push_n<4>(act, va, 2, sf.buf, sf.n, sf.lim, kWarpStage, far, far_size);
         __syncthreads();   // s_off / s_beg / s_best are rewritten by the next chunk
     }
-    // Short rows (renumbered suffix, at most kPullShort in-edges each): a
+    // Short rows (renumbered suffix, at most sssp_pull_split in-edges each): a
     // thread takes four consecutive vertices and scans the in-edges of the
     // unsettled ones itself, four in flight; no shared memory or barriers.
     for (uint64_t base = (uint64_t)blockIdx.x * kBlock * 4 + x.vsplit; base < x.vpull;
@@ -969,13 +968,16 @@ static int sssp_relabel(olv_graph *g) {
         perm[i] = v;
         newid[v] = i;
     }
-    uint32_t vnz = 0, vlong = 0;   // in-degree > 0 and > kPullShort: prefixes of the new numbering
+    // in-degree > 0, and > 4, 8, 16, 32 (the pull's short-row bounds):
+    // prefixes of the new numbering
+    uint32_t vnz = 0, vlong[4] = {0, 0, 0, 0};
     for (uint32_t v = 0; v < V; v++) {
-        vnz += cp[v + 1] != cp[v];
-        vlong += cp[v + 1] - cp[v] > kPullShort;
+        const uint32_t din = cp[v + 1] - cp[v];
+        vnz += din != 0;
+        for (int k = 0; k < 4; k++) vlong[k] += din > (4u << k);
     }
     ws.sr_vnz = vnz;
-    ws.sr_vlong = vlong;
+    for (int k = 0; k < 4; k++) ws.sr_vlong[k] = vlong[k];
     nrp[0] = 0;
     ncp[0] = 0;
     for (uint32_t i = 0; i < V; i++) {
@@ -1111,9 +1113,12 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     x.vpull = R.newid ? ws.sr_vnz : V;
     // renumbered: rows past the long-in-degree prefix (rounded up to whole
     // chunks) are short and go a thread per vertex; otherwise all by chunks
-    x.vsplit = R.newid && g->tune.sssp_pull_split ? (uint32_t)std::min<uint64_t>(
-                             ((uint64_t)ws.sr_vlong + kPullChunk - 1) / kPullChunk * kPullChunk, x.vpull)
-                       : x.vpull;
+    const uint32_t ps = g->tune.sssp_pull_split;   // 0 or the short-row bound 4, 8, 16, 32
+    const uint32_t vlong = ws.sr_vlong[ps >= 32 ? 3 : ps >= 16 ? 2 : ps >= 8 ? 1 : 0];
+    x.vsplit = R.newid && ps ? (uint32_t)std::min<uint64_t>(
+                                   ((uint64_t)vlong + kPullChunk - 1) / kPullChunk * kPullChunk,
+                                   x.vpull)
+                             : x.vpull;
     x.E = g->E;
     x.hdin = ws.hdin.as<uint2>();
     x.blist = ws.blist.as<uint32_t>();
