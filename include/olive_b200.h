@@ -128,7 +128,7 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
  *   "sssp_spt"    queued sources per thread in a relax chunk: 1, 2, 4 or 8 (1)
  *   "sssp_pull_split"  SSSP pull: renumbered vertices with at most this
  *                 many in-edges (4, 8, 16 or 32) a thread per vertex, the
- *                 rest by edge-balanced chunks; 0: all by chunks         (8)
+ *                 rest by edge-balanced chunks; 0: all by chunks        (16)
  *   "sssp_fuse_end"  SSSP superstep's end step run by the last CTA of the
  *                 relax pieces kernel instead of a launch of its own (0)
  *   "sssp_tail_delta"  width of the SSSP buckets after the first; above

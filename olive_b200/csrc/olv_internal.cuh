@@ -65,7 +65,7 @@ struct Tuning {
     uint32_t sssp_sub = 0;            // SSSP: light-phase sub-bucket width (0: none)
     uint32_t sssp_sub_buckets = 1;    // SSSP: heavy buckets whose light phase uses it
     uint32_t sssp_spt = 1;            // SSSP: queued sources per thread in a relax chunk
-    uint32_t sssp_pull_split = 8;     // SSSP pull: renumbered rows with at most this many
+    uint32_t sssp_pull_split = 16;    // SSSP pull: renumbered rows with at most this many
                                       // in-edges a thread per vertex (0: none; 4, 8, 16, 32)
     int sssp_fuse_end = 0;            // SSSP: superstep end step in the pieces kernel's last CTA
     uint32_t sssp_tail_delta = 1024;  // SSSP: width of the buckets after the first, which
