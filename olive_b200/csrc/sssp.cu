@@ -147,7 +147,7 @@ __global__ void k_pack_pairs(const uint32_t *__restrict__ a, const uint32_t *__r
 }
 
 #ifndef OLV_SSSP_MINB
-#define OLV_SSSP_MINB 4   // 4: <= 64 registers
+#define OLV_SSSP_MINB 3   // 3 CTAs per SM: up to 80 registers, no spills (4: 64, spills; 2% slower)
 #endif
 __device__ void sssp_end_step(TravCtl *c, cudaGraphConditionalHandle h, int use_cond,
                               uint32_t max_steps, uint32_t bl_cap);
