@@ -719,82 +719,31 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_pull_first_rows(Pull
     TravCtl *c = a.ctl;
     if (c->done || c->mode != a.want_mode) return;
     using Acc = typename Op::Acc;
-    // a thread takes four consecutive rows and reads their in-edges in step,
-    // four per row per round, so up to sixteen loads (and then sixteen
-    // membership tests) are in flight; a row stops at its first
-    // contributing in-edge in CSC order
-    constexpr int R = 4;
-    for (uint64_t base = (uint64_t)blockIdx.x * kBlock * R; base < a.n;
-         base += (uint64_t)gridDim.x * kBlock * R) {
-        const uint64_t r0 = base + (uint64_t)threadIdx.x * R;
-        uint32_t rows[R], b[R], e[R];
-        int to_long[R], newly[R];
-        bool open[R];
-#pragma unroll
-        for (int j = 0; j < R; j++) {
-            rows[j] = (uint32_t)(r0 + j);
-            open[j] = r0 + j < a.n && op.row_wanted(rows[j]);
-            to_long[j] = 0;
-            newly[j] = 0;
-            b[j] = e[j] = 0;
-        }
-#pragma unroll
-        for (int j = 0; j < R; j++)
-            if (open[j]) {
-                b[j] = __ldg(&a.colptr[rows[j]]);
-                e[j] = __ldg(&a.colptr[rows[j] + 1]);
-            }
-        uint32_t len = 0;
-#pragma unroll
-        for (int j = 0; j < R; j++) {
-            if (open[j] && e[j] - b[j] > kFirstLight) {
-                to_long[j] = 1;   // a warp takes it in k_pull_first_long
-                open[j] = false;
-            }
-            if (open[j]) len = max(len, e[j] - b[j]);
-        }
-        for (uint32_t o = 0; o < len; o += 4) {
-            uint32_t u[R][4];
-            bool in[R][4];
-#pragma unroll
-            for (int j = 0; j < R; j++)
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    in[j][k] = open[j] && b[j] + o + k < e[j];
-                    u[j][k] = in[j][k] ? __ldcs(&a.rowidx[b[j] + o + k]) : 0;
-                }
-            if constexpr (op_has_passes<Op>::value) {
-                bool p[R][4];
-#pragma unroll
-                for (int j = 0; j < R; j++)
-#pragma unroll
-                    for (int k = 0; k < 4; k++) p[j][k] = in[j][k] && op.passes(u[j][k]);
-#pragma unroll
-                for (int j = 0; j < R; j++) {
-                    const int k = p[j][0] ? 0 : p[j][1] ? 1 : p[j][2] ? 2 : p[j][3] ? 3 : -1;
-                    if (k >= 0) {
-                        op.reduce_row(rows[j], op.contribution(u[j][k], b[j] + o + k));
-                        newly[j] = op.mark(rows[j]) ? 1 : 0;
-                        open[j] = false;
-                    }
-                }
+    for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < a.n;
+         base += (uint64_t)gridDim.x * kBlock) {
+        const uint32_t r = (uint32_t)(base + threadIdx.x);
+        bool newly = false, is_long = false;
+        if (r < a.n && op.row_wanted(r)) {
+            const uint32_t b = __ldg(&a.colptr[r]), e = __ldg(&a.colptr[r + 1]);
+            if (e - b > kFirstLight) {
+                is_long = true;
             } else {
+                for (uint32_t i = b; i < e; i += 4) {
+                    const uint32_t n = min(4u, e - i);
+                    uint32_t u[4];
 #pragma unroll
-                for (int j = 0; j < R; j++) {
-                    if (!open[j]) continue;
-                    const uint32_t n = min(4u, e[j] - (b[j] + o));
+                    for (int j = 0; j < 4; j++) u[j] = (uint32_t)j < n ? __ldcs(&a.rowidx[i + j]) : 0;
                     Acc x;
-                    if (first_contribution(op, u[j], b[j] + o, n, x) >= 0) {
-                        op.reduce_row(rows[j], x);
-                        newly[j] = op.mark(rows[j]) ? 1 : 0;
-                        open[j] = false;
+                    if (first_contribution(op, u, i, n, x) >= 0) {
+                        op.reduce_row(r, x);
+                        newly = op.mark(r);
+                        break;
                     }
                 }
             }
-            if (!(open[0] || open[1] || open[2] || open[3])) break;
         }
-        warp_push_n<R>(to_long, rows, 1, reinterpret_cast<uint32_t *>(a.pieces), &c->npieces);
-        warp_push_n<R>(newly, rows, 1, a.qout, &c->qsize[1]);
+        warp_push(is_long, r, reinterpret_cast<uint32_t *>(a.pieces), &c->npieces);
+        warp_push(newly, r, a.qout, &c->qsize[1]);
     }
 }
 
