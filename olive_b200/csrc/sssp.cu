@@ -90,6 +90,7 @@ struct SsspAux {
     const uint2 *hdin;                 // per vertex: (heavy out-degree, in-degree)
     uint32_t *blist;                   // bucket list: the bucket's relax inputs, in order
     uint32_t *cmark;                   // bitmap: vertices collected so far this run
+    uint32_t mark_words;               // words of one mark bitmap
     uint32_t bl_cap;                   // bucket list capacity (entries)
     unsigned long long E;
     int pull;                          // pull supersteps allowed
@@ -329,6 +330,10 @@ __device__ void sssp_begin(TravCtl *c) {
         c->npieces = 0;
         c->heavy_work = 0;
         c->aux_done = 0;
+        if (c->mode == kModePull && c->tail_width) {   // a routing pull refills the far pile
+            c->far_size[c->far_cur ^ 1] = 0;
+            c->far_min = 0xffffffffu;
+        }
         return;
     }
     if (c->far_size[c->far_cur] == 0) {
@@ -493,6 +498,28 @@ __device__ __forceinline__ uint32_t pull_cand(uint32_t du, uint32_t w, uint32_t 
     return nd;
 }
 
+// One pulled vertex v with old distance d and pull minimum best (<= d): the
+// push action (0 none, 1 near queue, 2 far pile).  Without routing an
+// improvement goes to the far pile once per generation (fbits); with it every
+// vertex at or above the threshold with a finite distance goes to the near
+// queue of the next bucket (under nend) or to the next generation (fnext).
+__device__ __forceinline__ int pull_out(uint32_t best, uint32_t d, uint32_t v, uint32_t hi,
+                                        bool route, uint32_t nend, uint32_t *dist,
+                                        uint32_t *fbits, uint32_t *fnext, uint32_t &fmin) {
+    const uint32_t bit = 1u << (v & 31);
+    if (best < d) dist[v] = best;
+    if (!route) {
+        if (best >= d) return 0;   // only vertices at or above the threshold can improve
+        fmin = best < fmin ? best : fmin;
+        return (atomicOr(&fbits[v >> 5], bit) & bit) ? 0 : 2;
+    }
+    if (d < hi || best >= (uint32_t)kInf) return 0;   // settled, or unreached
+    if (best < nend) return 1;
+    atomicOr(&fnext[v >> 5], bit);
+    fmin = best < fmin ? best : fmin;
+    return 2;
+}
+
 // Pull superstep: every vertex at or above the threshold takes the minimum
 // candidate over its in-edges; improved vertices go to the far pile (once
 // per pile generation).  Each CTA iteration covers 1024 vertices, four per
@@ -502,13 +529,28 @@ __device__ __forceinline__ uint32_t pull_cand(uint32_t du, uint32_t w, uint32_t 
 // the scan), and fold candidates into a shared per-vertex minimum.
 constexpr int kPullItems = 4;
 constexpr uint32_t kPullChunk = 4 * kBlock;
-__device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1, FarMarks fm,
-                          const SsspAux &x, WarpStage sf) {
+//
+// Routing (buckets after the first are wide and relax every edge): the pull
+// also opens the next bucket, [threshold, threshold + tail_width), itself.
+// Every vertex it visits with a finite distance goes to the near queue of
+// that bucket or, at or above its end, to the far pile's next generation
+// (marks set; the visits cover every vertex that can hold a distance, so the
+// old pile, whose marks are cleared word by word, is dropped), and no split
+// pass follows.
+__device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0,
+                          uint32_t *far1, FarMarks fm, const SsspAux &x, WarpStage sn,
+                          WarpStage sf) {
     uint32_t *dist = static_cast<uint32_t *>(c->vdata);
     const uint32_t hi = c->threshold;
-    uint32_t *far = c->far_cur ? far1 : far0;
-    uint32_t *far_size = &c->far_size[c->far_cur];
+    const bool route = c->tail_width != 0;
+    const uint32_t nend = route ? sat_add(hi, c->tail_width) : 0;   // end of the next bucket
     uint32_t *fbits = (c->epoch & 1) ? fm.m1 : fm.m0;
+    uint32_t *fnext = (c->epoch & 1) ? fm.m0 : fm.m1;
+    // routing fills the other far buffer (the next generation)
+    uint32_t *far = (c->far_cur ^ (route ? 1u : 0u)) ? far1 : far0;
+    uint32_t *far_size = &c->far_size[c->far_cur ^ (route ? 1u : 0u)];
+    uint32_t *qn = c->cur ? q1 : q0;
+    uint32_t *qn_size = &c->qsize[c->cur];
     __shared__ uint32_t s_off[kPullChunk + 1], s_beg[kPullChunk], s_best[kPullChunk], s_warp[33];
     const bool vec = ((uintptr_t)dist & 15) == 0 && ((uintptr_t)x.colptr & 15) == 0;
     const uint32_t lane = lane_id();
@@ -595,20 +637,18 @@ __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1
         }
         __syncthreads();
         scanned += t;
+        if (route && threadIdx.x < kPullChunk / 32 && base / 32 + threadIdx.x < x.mark_words)
+            fbits[base / 32 + threadIdx.x] = 0;   // the old pile's marks of this chunk
         int act[4];
         uint32_t va[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-            const uint32_t best = s_best[r0 + j];
             va[j] = (uint32_t)(v0 + j);
-            act[j] = 0;
-            if (best < d[j]) {   // only vertices at or above the threshold with in-edges
-                dist[va[j]] = best;
-                const uint32_t bit = 1u << (va[j] & 31);
-                if (!(atomicOr(&fbits[va[j] >> 5], bit) & bit)) act[j] = 2;
-                fmin = best < fmin ? best : fmin;
-            }
+            act[j] = pull_out(s_best[r0 + j], d[j], va[j], hi, route, nend, dist, fbits, fnext,
+                              fmin);
         }
+        sn.reserve(32 * 4, qn, qn_size);
+        stage_push_n<4>(act, va, 1, sn.buf, sn.n, sn.lim, kWarpStage, qn, qn_size);
         sf.reserve(32 * 4, far, far_size);
         stage_push_n<4>(act, va, 2, sf.buf, sf.n, sf.lim, kWarpStage, far, far_size);
         __syncthreads();   // s_off / s_beg / s_best are rewritten by the next chunk
@@ -673,22 +713,21 @@ __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *far0, uint32_t *far1
 #pragma unroll
                 for (int k = 0; k < 4; k++) best[j] = min(best[j], pull_cand(du[j][k], t[j][k].y, hi));
         }
+        if (route && threadIdx.x < kBlock * 4 / 32 && base / 32 + threadIdx.x < x.mark_words)
+            fbits[base / 32 + threadIdx.x] = 0;   // the old pile's marks of these vertices
         int act[4];
         uint32_t va[4];
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             va[j] = (uint32_t)(v0 + j);
-            act[j] = 0;
-            if (best[j] < d[j]) {   // only vertices at or above the threshold with in-edges
-                dist[va[j]] = best[j];
-                const uint32_t bit = 1u << (va[j] & 31);
-                if (!(atomicOr(&fbits[va[j] >> 5], bit) & bit)) act[j] = 2;
-                fmin = best[j] < fmin ? best[j] : fmin;
-            }
+            act[j] = pull_out(best[j], d[j], va[j], hi, route, nend, dist, fbits, fnext, fmin);
         }
+        sn.reserve(32 * 4, qn, qn_size);
+        stage_push_n<4>(act, va, 1, sn.buf, sn.n, sn.lim, kWarpStage, qn, qn_size);
         sf.reserve(32 * 4, far, far_size);
         stage_push_n<4>(act, va, 2, sf.buf, sf.n, sf.lim, kWarpStage, far, far_size);
     }
+    warp_stage_flush(sn.buf, sn.n, sn.lim, qn, qn_size);
     warp_stage_flush(sf.buf, sf.n, sf.lim, far, far_size);
     const uint32_t m = __reduce_min_sync(0xffffffffu, fmin);
     if (lane == 0 && m != 0xffffffffu) atomicMin(&c->far_min, m);
@@ -768,6 +807,17 @@ __device__ void sssp_end_step(TravCtl *c, cudaGraphConditionalHandle h, int use_
         } else if (c->mode == kModePull) {
             c->pull_pending = 0;
             c->heavy_done = 1;
+            c->pull_steps++;
+            if (c->tail_width) {   // the pull routed every vertex: the next bucket is open
+                c->bucket_lo = c->threshold;
+                c->heavy_index++;
+                c->all_edges = 1;
+                c->threshold = c->bucket_end = sat_add(c->threshold, c->tail_width);
+                c->far_cur ^= 1;
+                c->epoch++;
+                c->bl_size = 0;
+                c->bl_over = 0;
+            }
         } else if (c->mode == kModeSubSplit) {
             c->far_cur ^= 1;   // the bucket list and the pending heavy step carry over
             c->epoch++;
@@ -826,7 +876,7 @@ k_sssp_aux(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1, uint32_t *far0, u
         sssp_collect(V, c, q0, q1, x, sa);
         if (x.pull) sssp_choose(V, c, x);
     } else if (mode == kModePull) {
-        sssp_pull(V, c, far0, far1, fm, x, sb);
+        sssp_pull(V, c, q0, q1, far0, far1, fm, x, sa, sb);
     } else {
         sssp_split(c, q0, q1, far0, far1, fm, sa, sb);
     }
@@ -1123,6 +1173,7 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     x.hdin = ws.hdin.as<uint2>();
     x.blist = ws.blist.as<uint32_t>();
     x.cmark = mk + 4 * words;
+    x.mark_words = (uint32_t)words;
     x.bl_cap = V;
     x.pull = g->tune.sssp_pull && x.crw != nullptr;
     void *a_aux[] = {&V, &ctl, &q0, &q1, &far0, &far1, &fm, &x};

@@ -141,9 +141,11 @@ def schedule(rp, col, w, src, delta, pull_mode, list_collect, sub=0, nsub=1, tai
         far[fv] = True
         if len(fv) == 0:
             return dist, pulls
-        lo = max(hi, int(dist[fv].min()))
-        hb += 1
         wide = tail > delta
+        # a pull followed by wide buckets opens the next bucket at the
+        # threshold itself (it routes every vertex; no split pass)
+        lo = hi if (wide and pull) else max(hi, int(dist[fv].min()))
+        hb += 1
         if wide:
             hi = bend = lo + tail
         else:
