@@ -131,6 +131,9 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
  *                 rest by edge-balanced chunks; 0: all by chunks        (16)
  *   "sssp_fuse_end"  SSSP superstep's end step run by the last CTA of the
  *                 relax pieces kernel instead of a launch of its own (0)
+ *   "sssp_route"  SSSP with wide buckets after the first: the heavy pull
+ *                 routes every vertex into the first of them (no split pass;
+ *                 1) or leaves the far pile to a split (0)
  *   "sssp_tail_delta"  width of the SSSP buckets after the first; above
  *                 sssp_delta those buckets relax every edge in-bucket and
  *                 have no heavy step (1024; 0: delta, light/heavy throughout)

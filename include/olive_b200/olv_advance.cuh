@@ -681,7 +681,10 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_pull_pieces(PullArgs
 // in-edges per step, four per lane.  Ops with passes() / contribution()
 // test a step's sources with all their loads in flight and gather only the
 // first passing one.
-constexpr uint32_t kFirstLight = 32;
+#ifndef OLV_FIRST_LIGHT
+#define OLV_FIRST_LIGHT 32
+#endif
+constexpr uint32_t kFirstLight = OLV_FIRST_LIGHT;
 constexpr uint32_t kFirstGroup = 8;   // lanes per long row
 
 template <class Op, class = void>

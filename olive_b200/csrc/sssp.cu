@@ -264,7 +264,7 @@ __device__ void sssp_begin(TravCtl *c);
 
 __global__ void k_sssp_init(TravCtl *c, uint32_t *dist, uint32_t *q0, uint32_t src,
                             uint32_t delta, uint32_t sub, uint32_t sub_buckets,
-                            uint32_t tail_width, const uint32_t *newid) {
+                            uint32_t tail_width, uint32_t route, const uint32_t *newid) {
     if (newid) src = newid[src];   // relabelled run: the source's new id
     TravCtl t = {};
     t.qsize[0] = 1;
@@ -276,6 +276,7 @@ __global__ void k_sssp_init(TravCtl *c, uint32_t *dist, uint32_t *q0, uint32_t s
     t.heavy_index = 0;
     t.tail_width = tail_width > delta ? tail_width : 0;
     t.all_edges = 0;
+    t.route = t.tail_width != 0 && route;
     t.threshold = (t.sub_width && sub_buckets > 0) ? t.sub_width : delta;
     t.epoch = 1;
     t.far_min = 0xffffffffu;
@@ -330,7 +331,7 @@ __device__ void sssp_begin(TravCtl *c) {
         c->npieces = 0;
         c->heavy_work = 0;
         c->aux_done = 0;
-        if (c->mode == kModePull && c->tail_width) {   // a routing pull refills the far pile
+        if (c->mode == kModePull && c->route) {   // a routing pull refills the far pile
             c->far_size[c->far_cur ^ 1] = 0;
             c->far_min = 0xffffffffu;
         }
@@ -542,7 +543,7 @@ __device__ void sssp_pull(uint32_t V, TravCtl *c, uint32_t *q0, uint32_t *q1, ui
                           WarpStage sf) {
     uint32_t *dist = static_cast<uint32_t *>(c->vdata);
     const uint32_t hi = c->threshold;
-    const bool route = c->tail_width != 0;
+    const bool route = c->route != 0;
     const uint32_t nend = route ? sat_add(hi, c->tail_width) : 0;   // end of the next bucket
     uint32_t *fbits = (c->epoch & 1) ? fm.m1 : fm.m0;
     uint32_t *fnext = (c->epoch & 1) ? fm.m0 : fm.m1;
@@ -808,7 +809,7 @@ __device__ void sssp_end_step(TravCtl *c, cudaGraphConditionalHandle h, int use_
             c->pull_pending = 0;
             c->heavy_done = 1;
             c->pull_steps++;
-            if (c->tail_width) {   // the pull routed every vertex: the next bucket is open
+            if (c->route) {   // the pull routed every vertex: the next bucket is open
                 c->bucket_lo = c->threshold;
                 c->heavy_index++;
                 c->all_edges = 1;
@@ -1229,7 +1230,7 @@ int run_sssp_device(olv_graph *g, uint32_t src, uint32_t *dist_dev, unsigned lon
     k_fill_i32<<<g->num_sms * 8, kBlock, 0, s>>>((int32_t *)dist, g->V, kInf);
     k_sssp_init<<<1, 1, 0, s>>>(ctl, dist, g->ws.q0.as<uint32_t>(), src, sssp_delta(g),
                                 g->tune.sssp_sub, g->tune.sssp_sub_buckets,
-                                g->tune.sssp_tail_delta, R.newid);
+                                g->tune.sssp_tail_delta, g->tune.sssp_route, R.newid);
     OLV_CUDA(cudaGetLastError());
     auto finish = [&]() -> int {
         if (R.dist) {
