@@ -1178,7 +1178,9 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     x.bl_cap = V;
     x.pull = g->tune.sssp_pull && x.crw != nullptr;
     void *a_aux[] = {&V, &ctl, &q0, &q1, &far0, &far1, &fm, &x};
-    OLV_TRY(sink((const void *)k_sssp_aux, dim3(nb), dim3(kBlock), a_aux));
+    int nba = 0;   // the dense passes at their own residency (more warps than the relax kernels)
+    OLV_TRY(resident_blocks(g, (const void *)k_sssp_aux, &nba));
+    OLV_TRY(sink((const void *)k_sssp_aux, dim3(nba), dim3(kBlock), a_aux));
     uint32_t bl_cap = x.bl_cap;
     // the end step runs in the pieces kernel's last CTA, or as its own launch
     op.end_h = h;
