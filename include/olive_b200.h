@@ -134,6 +134,9 @@ int olv_graph_max_degree_vertex(const olv_graph *g, uint32_t *v, uint32_t *deg);
  *   "sssp_route"  SSSP with wide buckets after the first: the heavy pull
  *                 routes every vertex into the first of them (no split pass;
  *                 1) or leaves the far pile to a split (0)
+ *   "sssp_pull_direct"  with sssp_route: a first bucket whose relax
+ *                 inputs number V/16 or more goes to the pull without the
+ *                 collect pass that chooses push or pull (1)
  *   "sssp_tail_delta"  width of the SSSP buckets after the first; above
  *                 sssp_delta those buckets relax every edge in-bucket and
  *                 have no heavy step (1024; 0: delta, light/heavy throughout)

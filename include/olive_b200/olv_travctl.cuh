@@ -50,6 +50,8 @@ struct TravCtl {
     uint32_t tail_width;        // SSSP: width of the buckets after the first (<= delta: delta)
     uint32_t all_edges;         // SSSP: the current bucket relaxes every edge in-bucket
     uint32_t route;             // SSSP: the pull opens the first wide bucket itself
+    uint32_t direct_min;        // SSSP: a first bucket with this many relax inputs goes
+                                // straight to the pull, without the collect pass (0: never)
     unsigned long long heavy_work;  // SSSP: heavy out-edges of the collected bucket
     unsigned long long settled_in;  // SSSP: in-edges of all settled vertices
     uint32_t ms_track;          // msBFS: this push level records first-touched vertices

@@ -265,8 +265,9 @@ class Graph:
         out = {}
         for k in ("hub_degree", "piece", "alpha", "beta", "sssp_delta", "sssp_pull", "sssp_relabel",
                   "sssp_sub", "sssp_sub_buckets", "sssp_spt", "sssp_pull_split", "sssp_fuse_end",
-                  "sssp_hub_degree", "sssp_piece", "sssp_tail_delta", "sssp_route", "ms_alpha",
-                  "pr_tile_u", "use_graphs", "levels_per_sync", "batch_cluster"):
+                  "sssp_hub_degree", "sssp_piece", "sssp_tail_delta", "sssp_route",
+                  "sssp_pull_direct", "ms_alpha", "pr_tile_u", "use_graphs", "levels_per_sync",
+                  "batch_cluster"):
             d = _D()
             _check(lib().olv_tune_get(self._h, k.encode(), ctypes.byref(d)), "olv_tune_get")
             out[k] = d.value

@@ -539,6 +539,8 @@ int olv_tune_set(olv_graph *g, const char *key, double value) {
         OLV_CHECK_ARG(value == 0 || value == 4 || value == 8 || value == 16 || value == 32,
                       "olv_tune_set: sssp_pull_split must be 0, 4, 8, 16 or 32");
         t.sssp_pull_split = (uint32_t)value;
+    } else if (!strcmp(key, "sssp_pull_direct")) {
+        t.sssp_pull_direct = value != 0;
     } else if (!strcmp(key, "sssp_route")) {
         t.sssp_route = value != 0;
     } else if (!strcmp(key, "sssp_fuse_end")) {
@@ -590,6 +592,7 @@ int olv_tune_get(const olv_graph *g, const char *key, double *value) {
     else if (!strcmp(key, "sssp_spt")) *value = t.sssp_spt;
     else if (!strcmp(key, "sssp_fuse_end")) *value = t.sssp_fuse_end;
     else if (!strcmp(key, "sssp_route")) *value = t.sssp_route;
+    else if (!strcmp(key, "sssp_pull_direct")) *value = t.sssp_pull_direct;
     else if (!strcmp(key, "sssp_pull_split")) *value = t.sssp_pull_split;
     else if (!strcmp(key, "sssp_tail_delta")) *value = t.sssp_tail_delta;
     else if (!strcmp(key, "sssp_hub_degree")) *value = t.sssp_hub_degree;

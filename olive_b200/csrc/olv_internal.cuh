@@ -69,6 +69,8 @@ struct Tuning {
                                       // in-edges a thread per vertex (0: none; 4, 8, 16, 32)
     int sssp_fuse_end = 0;            // SSSP: superstep end step in the pieces kernel's last CTA
     int sssp_route = 1;               // SSSP: the pull opens the first wide bucket (no split)
+    int sssp_pull_direct = 1;         // SSSP: a first bucket with V/16 relax inputs pulls
+                                      // without the collect pass
     uint32_t sssp_tail_delta = 1024;  // SSSP: width of the buckets after the first, which
                                       // relax every edge (<= delta: delta, light/heavy)
     float ms_alpha = 20.0f;       // msBFS: pull when active out-edges * ms_alpha > E

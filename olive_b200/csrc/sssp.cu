@@ -264,7 +264,8 @@ __device__ void sssp_begin(TravCtl *c);
 
 __global__ void k_sssp_init(TravCtl *c, uint32_t *dist, uint32_t *q0, uint32_t src,
                             uint32_t delta, uint32_t sub, uint32_t sub_buckets,
-                            uint32_t tail_width, uint32_t route, const uint32_t *newid) {
+                            uint32_t tail_width, uint32_t route, uint32_t direct_min,
+                            const uint32_t *newid) {
     if (newid) src = newid[src];   // relabelled run: the source's new id
     TravCtl t = {};
     t.qsize[0] = 1;
@@ -277,6 +278,7 @@ __global__ void k_sssp_init(TravCtl *c, uint32_t *dist, uint32_t *q0, uint32_t s
     t.tail_width = tail_width > delta ? tail_width : 0;
     t.all_edges = 0;
     t.route = t.tail_width != 0 && route;
+    t.direct_min = t.route ? direct_min : 0;
     t.threshold = (t.sub_width && sub_buckets > 0) ? t.sub_width : delta;
     t.epoch = 1;
     t.far_min = 0xffffffffu;
@@ -325,6 +327,13 @@ __device__ void sssp_begin(TravCtl *c) {
         return;
     }
     if (!c->heavy_done) {   // bucket settled: collect it and relax its heavy edges
+        // a large first bucket (its relax inputs listed) goes straight to the
+        // pull: on a scale-free graph its heavy out-edges far outnumber the
+        // unsettled vertices' in-edges, and with wide buckets after it no
+        // later heavy step needs the collect's sums
+        if (!c->pull_pending && c->direct_min && c->heavy_index == 0 &&
+            (c->bl_over || c->bl_size >= c->direct_min))
+            c->pull_pending = 1;
         c->mode = c->pull_pending ? kModePull : kModeHeavy;
         c->qsize[c->cur] = 0;
         c->qsize[c->cur ^ 1] = 0;
@@ -1232,7 +1241,10 @@ int run_sssp_device(olv_graph *g, uint32_t src, uint32_t *dist_dev, unsigned lon
     k_fill_i32<<<g->num_sms * 8, kBlock, 0, s>>>((int32_t *)dist, g->V, kInf);
     k_sssp_init<<<1, 1, 0, s>>>(ctl, dist, g->ws.q0.as<uint32_t>(), src, sssp_delta(g),
                                 g->tune.sssp_sub, g->tune.sssp_sub_buckets,
-                                g->tune.sssp_tail_delta, g->tune.sssp_route, R.newid);
+                                g->tune.sssp_tail_delta, g->tune.sssp_route,
+                                g->tune.sssp_pull_direct && g->tune.sssp_pull && g->ws.sssp_crw.p
+                                    ? std::max<uint32_t>(1u, g->V / 16) : 0u,
+                                R.newid);
     OLV_CUDA(cudaGetLastError());
     auto finish = [&]() -> int {
         if (R.dist) {

@@ -217,7 +217,7 @@ def test_sssp_wide_tail_buckets_vs_dijkstra(ob, tail):
         for s in (hub, int(np.flatnonzero(deg == 1)[0])):
             np.testing.assert_array_equal(g.sssp(s), oracle.dijkstra(rp, cl, w, s)[0])
         for kw in ({"sssp_pull": 0}, {"sssp_sub": 16}, {"use_graphs": 0}, {"sssp_relabel": 0},
-                   {"sssp_route": 0}, {"sssp_pull_split": 0}):
+                   {"sssp_route": 0}, {"sssp_pull_split": 0}, {"sssp_pull_direct": 0}):
             base = g.tune()
             g.tune(**kw)
             np.testing.assert_array_equal(g.sssp(hub), ref_hub, err_msg=str(kw))
