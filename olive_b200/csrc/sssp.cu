@@ -1187,7 +1187,12 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     x.bl_cap = V;
     x.pull = g->tune.sssp_pull && x.crw != nullptr;
     void *a_aux[] = {&V, &ctl, &q0, &q1, &far0, &far1, &fm, &x};
-    int nba = 0;   // the dense passes at their own residency (more warps than the relax kernels)
+    // the dense passes at their own residency (more warps than the relax
+    // kernels): 45 KB of shared memory per CTA, so the carveout goes to shared
+    OLV_CUDA(cudaFuncSetAttribute((const void *)k_sssp_aux,
+                                  cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared));
+    int nba = 0;
     OLV_TRY(resident_blocks(g, (const void *)k_sssp_aux, &nba));
     OLV_TRY(sink((const void *)k_sssp_aux, dim3(nba), dim3(kBlock), a_aux));
     uint32_t bl_cap = x.bl_cap;
