@@ -1187,13 +1187,10 @@ static int sssp_superstep(olv_graph *g, Sink &&sink, cudaGraphConditionalHandle 
     x.bl_cap = V;
     x.pull = g->tune.sssp_pull && x.crw != nullptr;
     void *a_aux[] = {&V, &ctl, &q0, &q1, &far0, &far1, &fm, &x};
-    // the dense passes at their own residency (more warps than the relax
-    // kernels): 45 KB of shared memory per CTA, so the carveout goes to shared
-    OLV_CUDA(cudaFuncSetAttribute((const void *)k_sssp_aux,
-                                  cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  cudaSharedmemCarveoutMaxShared));
-    int nba = 0;
-    OLV_TRY(resident_blocks(g, (const void *)k_sssp_aux, &nba));
+    // the dense passes on 2 CTAs per SM: measured faster than 3 or 4 on
+    // RMAT-24 (1.68-1.69 ms against 1.79-1.81 at 4), the idle launches of the
+    // relax supersteps cost less and the pull's chunks stay as balanced
+    const int nba = 2 * g->num_sms;
     OLV_TRY(sink((const void *)k_sssp_aux, dim3(nba), dim3(kBlock), a_aux));
     uint32_t bl_cap = x.bl_cap;
     // the end step runs in the pieces kernel's last CTA, or as its own launch
