@@ -215,10 +215,6 @@ private:
     EdgeId *colptr_ = nullptr;     // reverse graph: in-edges of v in [colptr[v], colptr[v+1])
     VertexId *rowidx_ = nullptr;   // their sources
     EdgeId *eid_ = nullptr;        // their CSR positions (edge values)
-    // first-hit pulls: each row's in-edges again, busiest sources (highest
-    // out-degree) first, so the first member found is likely the first read
-    VertexId *hitidx_ = nullptr;
-    EdgeId *hiteid_ = nullptr;     // their CSR positions (non-empty edge types only)
     VertexValue *vertexValues_ = nullptr;
     AccumValue *accumulators_ = nullptr;
     EdgeValue *edgeValues_ = nullptr;
@@ -308,8 +304,6 @@ private:
             PullT pl{f, outdeg_, eid_, src.bits, vertexValues_, accumulators_, edgeValues_, dbits};
             static unsigned pull_grid = 0;
             if constexpr (first_hit) {   // bottom-up: each row stops at its first contribution
-                p.rowidx = hitidx_;
-                pl.eid = hiteid_ ? hiteid_ : eid_;
                 if (!pull_grid) pull_grid = persistentGrid(olv::k_pull_first_rows<PullT>);
                 olv::k_pull_first_rows<PullT><<<pull_grid, kT>>>(p, pl);
                 olv::k_pull_first_long<PullT><<<pull_grid, kT>>>(p, pl);
@@ -363,46 +357,6 @@ private:
         CUDA_CHECK(cudaFree(pos));
         CUDA_CHECK(cudaFree(indeg));
         CUDA_CHECK(cudaGetLastError());
-        buildHitOrder();
-    }
-
-    // The first-hit order of the reverse graph (built with it, in readGraph):
-    // a stable segmented sort of every row's in-edges by source out-degree,
-    // highest first.  Any single contribution decides such a
-    // row, so the order changes which member is found first, not the result.
-    void buildHitOrder() {
-        using namespace olive_detail;
-        if (hitidx_ || !edgeCount_) return;
-        const size_t V = vertexCount_, E = edgeCount_;
-        VertexId *keys = nullptr, *keys2 = nullptr;
-        EdgeId *pos = nullptr, *pos2 = nullptr;
-        CUDA_CHECK(cudaMalloc((void **)&hitidx_, E * sizeof(VertexId)));
-        CUDA_CHECK(cudaMalloc((void **)&keys, E * sizeof(VertexId)));
-        CUDA_CHECK(cudaMalloc((void **)&keys2, E * sizeof(VertexId)));
-        CUDA_CHECK(cudaMalloc((void **)&pos, E * sizeof(EdgeId)));
-        CUDA_CHECK(cudaMalloc((void **)&pos2, E * sizeof(EdgeId)));
-        k_hit_keys<<<sms_ * 8, 256>>>(rowidx_, outdeg_, E, keys);
-        k_iota<<<sms_ * 8, 256>>>(pos, E);
-        size_t tb = 0;
-        CUDA_CHECK(cub::DeviceSegmentedSort::StableSortPairs(
-            nullptr, tb, (const VertexId *)keys, keys2, (const EdgeId *)pos, pos2, (int)E, (int)V,
-            colptr_, colptr_ + 1));
-        void *temp = nullptr;
-        CUDA_CHECK(cudaMalloc(&temp, tb ? tb : 1));
-        CUDA_CHECK(cub::DeviceSegmentedSort::StableSortPairs(
-            temp, tb, (const VertexId *)keys, keys2, (const EdgeId *)pos, pos2, (int)E, (int)V,
-            colptr_, colptr_ + 1));
-        CUDA_CHECK(cudaFree(temp));
-        k_gather_u32<<<sms_ * 8, 256>>>(rowidx_, pos2, E, hitidx_);
-        if (!std::is_empty<EdgeValue>::value) {
-            CUDA_CHECK(cudaMalloc((void **)&hiteid_, E * sizeof(EdgeId)));
-            k_gather_u32<<<sms_ * 8, 256>>>(eid_, pos2, E, hiteid_);
-        }
-        CUDA_CHECK(cudaFree(keys));
-        CUDA_CHECK(cudaFree(keys2));
-        CUDA_CHECK(cudaFree(pos));
-        CUDA_CHECK(cudaFree(pos2));
-        CUDA_CHECK(cudaGetLastError());
     }
 
     void pullVertices() {
@@ -419,8 +373,6 @@ private:
         cudaFree(colptr_);
         cudaFree(rowidx_);
         cudaFree(eid_);
-        cudaFree(hitidx_);
-        cudaFree(hiteid_);
         cudaFree(vertexValues_);
         cudaFree(accumulators_);
         cudaFree(edgeValues_);
@@ -435,8 +387,6 @@ private:
         colptr_ = nullptr;
         rowidx_ = nullptr;
         eid_ = nullptr;
-        hitidx_ = nullptr;
-        hiteid_ = nullptr;
         vertexValues_ = nullptr;
         accumulators_ = nullptr;
         edgeValues_ = nullptr;

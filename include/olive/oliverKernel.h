@@ -317,15 +317,6 @@ __global__ void k_in_degrees(const VertexId *col, size_t E, VertexId *indeg) {
         atomicAdd(&indeg[col[i]], 1u);
 }
 
-// Sort key of in-edge i for the first-hit pulls: its source's out-degree,
-// complemented so that an ascending sort puts the busiest sources first.
-__global__ void k_hit_keys(const VertexId *rowidx, const VertexId *outdeg, size_t E,
-                           VertexId *keys) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < E;
-         i += (size_t)gridDim.x * blockDim.x)
-        keys[i] = ~outdeg[rowidx[i]];
-}
-
 __global__ void k_gather_u32(const VertexId *in, const EdgeId *idx, size_t n, VertexId *out) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x)
