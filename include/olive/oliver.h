@@ -32,7 +32,9 @@
  *     1) it runs only when the sources carry all E out-edges (edgeMap over
  *     every vertex, as PageRank.cu does: no atomics, one store per vertex);
  *     functors with the pullFirstHit opt-in pull from E / 16 (their rows stop
- *     at the first contribution).  OLIVE_DIRECTION=push|pull|auto and
+ *     at a contribution: first the in-neighbour with the most out-edges,
+ *     which readGraph finds for every vertex, 8 bytes a vertex; then the
+ *     others in CSC order).  OLIVE_DIRECTION=push|pull|auto and
  *     OLIVE_PULL_DIV override.  The result is the same either way (the
  *     reduce of every in-edge from a member), up to the order in which a
  *     non-associative reduce sees its inputs -- as in the reference, whose
@@ -151,10 +153,11 @@ public:
             CUDA_CHECK(cudaMemset(edgeValues_, 0, (E ? E : 1) * sizeof(EdgeValue)));
         }
         // hub pieces of either direction, or the first-hit pull's list of rows
-        // with more than olv::kFirstLight in-edges (uint32 entries, at most E / 32)
+        // whose probe failed (uint32 entries, rows with two or more in-edges:
+        // at most min(V, E / 2))
         const size_t np = E / olive_detail::kPiece + E / olive_detail::kHub + 16;
         const size_t npp = E / olive_detail::kPullPiece + E / olive_detail::kPullHub + 16;
-        const size_t nlong = (E / olv::kFirstLight + 16) / 2 + 1;
+        const size_t nlong = ((V < E / 2 ? V : E / 2) + 16) / 2 + 1;
         size_t npieces = np > npp ? np : npp;
         if (nlong > npieces) npieces = nlong;
         CUDA_CHECK(cudaMalloc((void **)&pieces_, npieces * sizeof(uint2)));
@@ -215,6 +218,8 @@ private:
     EdgeId *colptr_ = nullptr;     // reverse graph: in-edges of v in [colptr[v], colptr[v+1])
     VertexId *rowidx_ = nullptr;   // their sources
     EdgeId *eid_ = nullptr;        // their CSR positions (edge values)
+    VertexId *first_ = nullptr;    // first-hit pulls: each row's likeliest parent
+    EdgeId *firstpos_ = nullptr;   // and the CSC position of that in-edge
     VertexValue *vertexValues_ = nullptr;
     AccumValue *accumulators_ = nullptr;
     EdgeValue *edgeValues_ = nullptr;
@@ -304,6 +309,8 @@ private:
             PullT pl{f, outdeg_, eid_, src.bits, vertexValues_, accumulators_, edgeValues_, dbits};
             static unsigned pull_grid = 0;
             if constexpr (first_hit) {   // bottom-up: each row stops at its first contribution
+                p.first = first_;
+                p.firstpos = firstpos_;
                 if (!pull_grid) pull_grid = persistentGrid(olv::k_pull_first_rows<PullT>);
                 olv::k_pull_first_rows<PullT><<<pull_grid, kT>>>(p, pl);
                 olv::k_pull_first_long<PullT><<<pull_grid, kT>>>(p, pl);
@@ -345,6 +352,15 @@ private:
                                                    bits));
         CUDA_CHECK(cudaFree(temp));
         k_gather_u32<<<sms_ * 8, 256>>>(src, eid_, E, rowidx_);
+        // each row's likeliest parent, probed first by first-hit pulls
+        unsigned long long *best = nullptr;
+        CUDA_CHECK(cudaMalloc((void **)&best, V * sizeof(unsigned long long)));
+        CUDA_CHECK(cudaMemset(best, 0, V * sizeof(unsigned long long)));
+        k_first_parent_max<<<sms_ * 8, 256>>>(keys, rowidx_, outdeg_, E, best);
+        CUDA_CHECK(cudaMalloc((void **)&first_, V * sizeof(VertexId)));
+        CUDA_CHECK(cudaMalloc((void **)&firstpos_, V * sizeof(EdgeId)));
+        k_first_parent_set<<<gridV(), 256>>>(best, rowidx_, V, first_, firstpos_);
+        CUDA_CHECK(cudaFree(best));
         CUDA_CHECK(cudaMemset(indeg, 0, (V + 1) * sizeof(VertexId)));
         k_in_degrees<<<sms_ * 8, 256>>>(col_, E, indeg);
         tb = 0;
@@ -373,6 +389,8 @@ private:
         cudaFree(colptr_);
         cudaFree(rowidx_);
         cudaFree(eid_);
+        cudaFree(first_);
+        cudaFree(firstpos_);
         cudaFree(vertexValues_);
         cudaFree(accumulators_);
         cudaFree(edgeValues_);
@@ -387,6 +405,8 @@ private:
         colptr_ = nullptr;
         rowidx_ = nullptr;
         eid_ = nullptr;
+        first_ = nullptr;
+        firstpos_ = nullptr;
         vertexValues_ = nullptr;
         accumulators_ = nullptr;
         edgeValues_ = nullptr;

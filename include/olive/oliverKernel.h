@@ -22,12 +22,16 @@
  *             rows, `static constexpr bool pullFirstHit` stops a row at its
  *             first contribution (valid when any one contribution is enough,
  *             as for BFS levels): the pull then runs k_pull_first_rows /
- *             k_pull_first_long (a thread or a warp per row, early exit) and
- *             is chosen from E / (pull_div * 16) frontier out-edges.
+ *             k_pull_first_long (a thread per row probes the row's likeliest
+ *             parent, the in-neighbour of most out-edges found once by
+ *             readGraph; rows it fails go to 8-lane groups that scan their
+ *             in-edges; early exit) and is chosen from E / (pull_div * 16)
+ *             frontier out-edges.
  *   k_vertex_filter  flags -> queue with cond/update (oliverKernel.h:85-141):
  *     over the listed members (or the bitmap when no list is known); ballot
- *     compaction, one atomic per warp; writes the queue, its bitmap and the
- *     sum of the kept vertices' out-degrees.  cond receives the vertex's
+ *     compaction into a shared-memory stage, one queue atomic per flush;
+ *     writes the queue, its bitmap and the sum of the kept vertices'
+ *     out-degrees.  cond receives the vertex's
  *     accumulator -- the reference passed the vertex id (oliverKernel.h:112,
  *     135), which SSSP.cu's cond cannot use.
  *   k_vertex_map  (oliverKernel.h:184-221), over queue, list or bitmap.
@@ -170,6 +174,14 @@ struct PullOp {
     __device__ __forceinline__ void reduce_row(uint32_t r, const A &x) { f.reduce(acc[r], x); }
     __device__ __forceinline__ void store(uint32_t r, const A &slot) { acc[r] = slot; }
     __device__ __forceinline__ bool mark(uint32_t r) { return set_bit(dbits, r); }
+    // rows r0..r0+31 (r0 a multiple of 32) with bits in m, flagged with one
+    // atomic; the rows whose flags this call set
+    __device__ __forceinline__ uint32_t mark_warp(uint32_t r0, uint32_t m) {
+        const uint32_t sh = r0 & 63;
+        const unsigned long long old = atomicOr(
+            reinterpret_cast<unsigned long long *>(&dbits[r0 >> 6]), (unsigned long long)m << sh);
+        return m & ~(uint32_t)(old >> sh);
+    }
 };
 
 // --------------------------------------------------------- edge pass glue --
@@ -255,6 +267,16 @@ k_vertex_filter(const Word *sbits, const VertexId *slist, const SubsetMeta *smet
                 SubsetMeta *qmeta, F f) {
     const bool listed = smeta->listValid;
     const size_t count = listed ? smeta->qsize : n;
+    // the queue staged in shared memory: one counter atomic per flush
+    __shared__ uint32_t s_q[olv::kStage];
+    __shared__ uint32_t s_qn, s_qlim, s_base;
+    __shared__ unsigned long long s_deg;
+    if (threadIdx.x == 0) {
+        s_qn = 0;
+        s_qlim = olv::kStage;
+        s_deg = 0;
+    }
+    __syncthreads();
     unsigned long long deg = 0;
     for (size_t base = blockIdx.x * (size_t)kT; base < count; base += (size_t)gridDim.x * kT) {
         const size_t i = base + threadIdx.x;
@@ -268,14 +290,25 @@ k_vertex_filter(const Word *sbits, const VertexId *slist, const SubsetMeta *smet
                     f.update(vvals[v], a);
                     keep = true;
                     deg += outdeg[v];
-                    atomicOr(reinterpret_cast<unsigned long long *>(&qbits[v >> 6]),
-                             (unsigned long long)((Word)1 << (v & 63)));
                 }
             }
         }
-        olv::warp_push(keep, v, queue, &qmeta->qsize);
+        if (keep)
+            atomicOr(reinterpret_cast<unsigned long long *>(&qbits[v >> 6]),
+                     (unsigned long long)((Word)1 << (v & 63)));
+        const uint32_t vv[1] = {v};
+        const int ak[1] = {keep ? 1 : 0};
+        olv::stage_push_n<1>(ak, vv, 1, s_q, &s_qn, &s_qlim, olv::kStage, queue, &qmeta->qsize);
+        __syncthreads();
+        if (min(s_qn, s_qlim) >= olv::kStage / 2)
+            olv::stage_flush(s_q, &s_qn, &s_qlim, &s_base, queue, &qmeta->qsize);
+        __syncthreads();
     }
-    olv::warp_add64(deg, &qmeta->outEdges);
+    olv::stage_flush(s_q, &s_qn, &s_qlim, &s_base, queue, &qmeta->qsize);
+    // the out-degree sum: one global atomic per CTA
+    olv::warp_add64(deg, &s_deg);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_deg) atomicAdd(&qmeta->outEdges, s_deg);
 }
 
 // vertexMap over a queue, a listed flag subset or the bitmap.
@@ -315,6 +348,44 @@ __global__ void k_in_degrees(const VertexId *col, size_t E, VertexId *indeg) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < E;
          i += (size_t)gridDim.x * blockDim.x)
         atomicAdd(&indeg[col[i]], 1u);
+}
+
+// Each vertex's likeliest parent for first-hit pulls: the in-edge whose
+// source has the most out-edges (the earliest CSC position among equals),
+// kept as the maximum of (out-degree << 32 | ~position).  dst holds the
+// destination of each CSC position (sorted), so a warp's lanes with one
+// destination are adjacent: a segmented maximum in the warp, then one
+// atomicMax per destination run.
+__global__ void k_first_parent_max(const VertexId *dst, const VertexId *src, const VertexId *outdeg,
+                                   size_t E, unsigned long long *best) {
+    const uint32_t ln = lane();
+    for (size_t base = blockIdx.x * (size_t)blockDim.x; base < E;
+         base += (size_t)gridDim.x * blockDim.x) {
+        const size_t i = base + threadIdx.x;
+        const bool valid = i < E;
+        const VertexId v = valid ? dst[i] : 0xffffffffu;
+        unsigned long long key =
+            valid ? (unsigned long long)outdeg[src[i]] << 32 | (uint32_t)~(uint32_t)i : 0ull;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long k2 = __shfl_down_sync(0xffffffffu, key, o);
+            const VertexId v2 = __shfl_down_sync(0xffffffffu, v, o);
+            if (ln + o < 32 && v2 == v && k2 > key) key = k2;
+        }
+        const VertexId vp = __shfl_up_sync(0xffffffffu, v, 1);
+        if (valid && (ln == 0 || vp != v) && __ldcg(&best[v]) < key) atomicMax(&best[v], key);
+    }
+}
+
+__global__ void k_first_parent_set(const unsigned long long *best, const VertexId *src, size_t n,
+                                   VertexId *first, EdgeId *firstpos) {
+    for (size_t v = blockIdx.x * (size_t)blockDim.x + threadIdx.x; v < n;
+         v += (size_t)gridDim.x * blockDim.x) {
+        const unsigned long long b = best[v];
+        const EdgeId pos = (EdgeId)~(uint32_t)b;
+        first[v] = (b >> 32) ? src[pos] : olv::kNoFirst;
+        firstpos[v] = (b >> 32) ? pos : 0;
+    }
 }
 
 __global__ void k_gather_u32(const VertexId *in, const EdgeId *idx, size_t n, VertexId *out) {

@@ -552,7 +552,13 @@ struct PullArgs {
     uint32_t hub_degree = 0;
     uint32_t piece = 0;
     uint32_t *qout = nullptr;           // rows with a contribution; count in ctl->qsize[1]
+    // first-hit pulls: per row, the in-neighbour to probe before the others
+    // (kNoFirst: no in-edges) and that in-edge's position; null: no probe
+    const uint32_t *first = nullptr;
+    const uint32_t *firstpos = nullptr;
 };
+
+constexpr uint32_t kNoFirst = 0xffffffffu;
 
 template <class Op>
 __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_pull_chunks(PullArgs a, Op op) {
@@ -672,15 +678,19 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_pull_pieces(PullArgs
 }
 
 // First-contribution pull (Ops with kFirstHit: any single contribution is
-// enough, as for BFS levels): a bottom-up step that stops each row at its
-// first contributing in-edge (in CSC order).  k_pull_first_rows gives every
-// wanted row with at most kFirstLight in-edges to one thread, which reads its
-// in-edges four at a time and stops at the first source that passes; longer
-// rows are listed in a.pieces (count in ctl->npieces) for k_pull_first_long,
-// where a group of 8 lanes takes a row (four rows per warp) and reads 32
-// in-edges per step, four per lane.  Ops with passes() / contribution()
-// test a step's sources with all their loads in flight and gather only the
-// first passing one.
+// enough, as for BFS levels): a bottom-up step that stops each row at a
+// contributing in-edge.  k_pull_first_rows gives every wanted row to one
+// thread.  With a.first set, the thread probes one in-edge, the row's
+// likeliest parent (a.first[r], a.firstpos[r]: coalesced loads), and lists
+// the row for k_pull_first_long when the probe fails and the row has more
+// in-edges.  Without it, a row with at most kFirstLight in-edges reads them
+// four at a time and stops at the first source that passes (CSC order);
+// longer rows are listed.  The list lives in a.pieces (count in
+// ctl->npieces): k_pull_first_long gives each listed row a group of 8 lanes
+// that scans its in-edges from the start, 32 per step, and stops at the
+// first passing one in CSC order.  Ops with passes() / contribution() test a
+// step's sources with all their loads in flight and gather only the first
+// passing one; Ops with mark_warp() flag a warp's rows with one call.
 #ifndef OLV_FIRST_LIGHT
 #define OLV_FIRST_LIGHT 32
 #endif
@@ -717,39 +727,112 @@ __device__ __forceinline__ int first_contribution(Op &op, const uint32_t (&u)[4]
     }
 }
 
+template <class Op, class = void>
+struct op_has_mark_warp : std::false_type {};
+template <class Op>
+struct op_has_mark_warp<Op, std::void_t<decltype(std::declval<Op &>().mark_warp(0u, 0u))>>
+    : std::true_type {};
+
+// The rows of this warp's lanes that hit (r = r0 + lane, r0 a multiple of 32)
+// flagged by the Op: one mark_warp call for the warp when the Op has it, else
+// mark() per row.  True for the rows whose flag this call set.
+template <class Op>
+__device__ __forceinline__ bool mark_rows(Op &op, bool hit, uint32_t r) {
+    if constexpr (op_has_mark_warp<Op>::value) {
+        const uint32_t m = __ballot_sync(0xffffffffu, hit);
+        const uint32_t lane = lane_id();
+        uint32_t set = 0;
+        if (m && lane == 0) set = op.mark_warp(r, m);
+        set = __shfl_sync(0xffffffffu, set, 0);
+        return (set >> lane) & 1u;
+    } else {
+        return hit && op.mark(r);
+    }
+}
+
 template <class Op>
 __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_pull_first_rows(PullArgs a, Op op) {
     TravCtl *c = a.ctl;
     if (c->done || c->mode != a.want_mode) return;
     using Acc = typename Op::Acc;
+    // both lists staged in shared memory (one counter atomic per flush, not
+    // per warp and row block: every warp of the grid appends to them)
+    __shared__ uint32_t s_q[kStage], s_l[kStage];
+    __shared__ uint32_t s_qn, s_qlim, s_ln, s_llim, s_base;
+    uint32_t *lrows = reinterpret_cast<uint32_t *>(a.pieces);
+    if (threadIdx.x == 0) {
+        s_qn = 0;
+        s_qlim = kStage;
+        s_ln = 0;
+        s_llim = kStage;
+    }
+    __syncthreads();
     for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < a.n;
          base += (uint64_t)gridDim.x * kBlock) {
         const uint32_t r = (uint32_t)(base + threadIdx.x);
-        bool newly = false, is_long = false;
+        bool hit = false, is_long = false;
         if (r < a.n && op.row_wanted(r)) {
-            const uint32_t b = __ldg(&a.colptr[r]), e = __ldg(&a.colptr[r + 1]);
-            if (e - b > kFirstLight) {
-                is_long = true;
-            } else {
-                for (uint32_t i = b; i < e; i += 4) {
-                    const uint32_t n = min(4u, e - i);
-                    uint32_t u[4];
-#pragma unroll
-                    for (int j = 0; j < 4; j++) u[j] = (uint32_t)j < n ? __ldcs(&a.rowidx[i + j]) : 0;
+            if (a.first) {
+                // one probe of the row's likeliest parent (coalesced loads);
+                // a row it fails with more in-edges goes to the group kernel
+                const uint32_t u = __ldg(&a.first[r]);
+                if (u != kNoFirst) {
                     Acc x;
-                    if (first_contribution(op, u, i, n, x) >= 0) {
+                    bool p;
+                    if constexpr (op_has_passes<Op>::value) {
+                        p = op.passes(u);
+                        if (p) x = op.contribution(u, __ldg(&a.firstpos[r]));
+                    } else {
+                        p = op.contributes(u, __ldg(&a.firstpos[r]), x);
+                    }
+                    if (p) {
                         op.reduce_row(r, x);
-                        newly = op.mark(r);
-                        break;
+                        hit = true;
+                    } else {
+                        is_long = __ldg(&a.colptr[r + 1]) - __ldg(&a.colptr[r]) > 1;
+                    }
+                }
+            } else {
+                const uint32_t b = __ldg(&a.colptr[r]), e = __ldg(&a.colptr[r + 1]);
+                if (e - b > kFirstLight) {
+                    is_long = true;
+                } else {
+                    for (uint32_t i = b; i < e; i += 4) {
+                        const uint32_t n = min(4u, e - i);
+                        uint32_t u[4];
+#pragma unroll
+                        for (int j = 0; j < 4; j++)
+                            u[j] = (uint32_t)j < n ? __ldcs(&a.rowidx[i + j]) : 0;
+                        Acc x;
+                        if (first_contribution(op, u, i, n, x) >= 0) {
+                            op.reduce_row(r, x);
+                            hit = true;
+                            break;
+                        }
                     }
                 }
             }
         }
-        warp_push(is_long, r, reinterpret_cast<uint32_t *>(a.pieces), &c->npieces);
-        warp_push(newly, r, a.qout, &c->qsize[1]);
+        const bool newly = mark_rows(op, hit, r);
+        const uint32_t vr[1] = {r};
+        const int aq[1] = {newly ? 1 : 0}, al[1] = {is_long ? 1 : 0};
+        stage_push_n<1>(aq, vr, 1, s_q, &s_qn, &s_qlim, kStage, a.qout, &c->qsize[1]);
+        stage_push_n<1>(al, vr, 1, s_l, &s_ln, &s_llim, kStage, lrows, &c->npieces);
+        __syncthreads();
+        if (min(s_qn, s_qlim) >= kStage / 2)
+            stage_flush(s_q, &s_qn, &s_qlim, &s_base, a.qout, &c->qsize[1]);
+        if (min(s_ln, s_llim) >= kStage / 2)
+            stage_flush(s_l, &s_ln, &s_llim, &s_base, lrows, &c->npieces);
+        __syncthreads();
     }
+    stage_flush(s_q, &s_qn, &s_qlim, &s_base, a.qout, &c->qsize[1]);
+    stage_flush(s_l, &s_ln, &s_llim, &s_base, lrows, &c->npieces);
 }
 
+// Listed rows, a group of 8 lanes per row (four rows per warp): each step
+// reads the row's next 32 in-edges, lane s of the group taking positions
+// s, s+8, s+16, s+24 (every load instruction reads one 32-byte sector per
+// group), and the row stops at its first passing in-edge in CSC order.
 template <class Op>
 __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_pull_first_long(PullArgs a, Op op) {
     TravCtl *c = a.ctl;
@@ -761,6 +844,15 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_pull_first_long(Pull
     const uint32_t *rows = reinterpret_cast<const uint32_t *>(a.pieces);
     const uint32_t lane = lane_id();
     const uint32_t grp = lane / kFirstGroup, sub = lane % kFirstGroup;
+    // found rows staged per warp, one counter atomic per flush
+    const uint32_t wl = threadIdx.x >> 5;
+    __shared__ uint32_t s_q[kBlock / 32][kWarpStage];
+    __shared__ uint32_t s_qn[kBlock / 32], s_qlim[kBlock / 32];
+    if (lane == 0) {
+        s_qn[wl] = 0;
+        s_qlim[wl] = kWarpStage;
+    }
+    __syncwarp();
     const uint32_t gshift = grp * kFirstGroup;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -776,30 +868,47 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_pull_first_long(Pull
         // every lane stays in the loop until all four groups are done (warp votes)
         while (__any_sync(0xffffffffu, !found && i < e)) {
             const bool active = !found && i < e;
-            const uint32_t j0 = i + sub * 4;
-            const uint32_t n = active && j0 < e ? min(4u, e - j0) : 0u;
             uint32_t u[4];
-#pragma unroll
-            for (int t = 0; t < 4; t++) u[t] = (uint32_t)t < n ? __ldcs(&a.rowidx[j0 + t]) : 0;
             bool p[4];
-            if constexpr (op_has_passes<Op>::value) {
 #pragma unroll
-                for (int t = 0; t < 4; t++) p[t] = (uint32_t)t < n && op.passes(u[t]);
-            } else {
-                Acc y;
-#pragma unroll
-                for (int t = 0; t < 4; t++) p[t] = (uint32_t)t < n && op.contributes(u[t], j0 + t, y);
+            for (int t = 0; t < 4; t++) {
+                const uint32_t j = i + t * kFirstGroup + sub;
+                u[t] = active && j < e ? __ldcs(&a.rowidx[j]) : 0;
             }
-            const bool any = p[0] || p[1] || p[2] || p[3];
-            const uint32_t gm = (__ballot_sync(0xffffffffu, any) >> gshift) & ((1u << kFirstGroup) - 1u);
-            if (active && gm) {
-                if (sub == (uint32_t)(__ffs(gm) - 1)) {   // the group's first passing lane
-                    const int t = p[0] ? 0 : p[1] ? 1 : p[2] ? 2 : 3;
+#pragma unroll
+            for (int t = 0; t < 4; t++) {
+                const uint32_t j = i + t * kFirstGroup + sub;
+                if constexpr (op_has_passes<Op>::value) {
+                    p[t] = active && j < e && op.passes(u[t]);
+                } else {
+                    Acc y;
+                    p[t] = active && j < e && op.contributes(u[t], j, y);
+                }
+            }
+            // the first passing position of the step: lowest t, then lowest lane
+            int tw = -1;
+            uint32_t gw = 0;
+#pragma unroll
+            for (int t = 3; t >= 0; t--) {
+                const uint32_t gm =
+                    (__ballot_sync(0xffffffffu, p[t]) >> gshift) & ((1u << kFirstGroup) - 1u);
+                if (gm) {
+                    tw = t;
+                    gw = gm;
+                }
+            }
+            if (active && tw >= 0) {
+                if (sub == (uint32_t)(__ffs(gw) - 1)) {
+                    uint32_t uw = u[0];
+#pragma unroll
+                    for (int t = 1; t < 4; t++)
+                        if (t == tw) uw = u[t];
+                    const uint32_t j = i + (uint32_t)tw * kFirstGroup + sub;
                     Acc x;
                     if constexpr (op_has_passes<Op>::value)
-                        x = op.contribution(u[t], j0 + t);
+                        x = op.contribution(uw, j);
                     else
-                        op.contributes(u[t], j0 + t, x);
+                        op.contributes(uw, j, x);
                     op.reduce_row(r, x);
                 }
                 found = true;
@@ -807,8 +916,15 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_pull_first_long(Pull
             i += kStep;
         }
         const bool newly = found && sub == 0 && op.mark(r);
-        warp_push(newly, r, a.qout, &c->qsize[1]);
+        const uint32_t vr[1] = {r};
+        const int aq[1] = {newly ? 1 : 0};
+        __syncwarp();
+        if (s_qn[wl] + 32 > kWarpStage)
+            warp_stage_flush(s_q[wl], &s_qn[wl], &s_qlim[wl], a.qout, &c->qsize[1]);
+        stage_push_n<1>(aq, vr, 1, s_q[wl], &s_qn[wl], &s_qlim[wl], kWarpStage, a.qout,
+                        &c->qsize[1]);
     }
+    warp_stage_flush(s_q[wl], &s_qn[wl], &s_qlim[wl], a.qout, &c->qsize[1]);
 }
 
 }  // namespace olv
