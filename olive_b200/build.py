@@ -4,7 +4,7 @@
 
 Each olive_b200/csrc/*.cu is compiled by nvcc into olive_b200/_build/*.o and
 linked with the static CUDA runtime into olive_b200/libolive_b200.so, so the
-library loads on a GPU box without a matching libcudart.
+library loads on a machine without a matching libcudart.
 """
 import argparse
 import concurrent.futures as cf
